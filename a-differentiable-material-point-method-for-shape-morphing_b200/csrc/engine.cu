@@ -1,0 +1,1132 @@
+// engine.cu -- host engine and C ABI (include/dmpm.h) of the B200 MLS-MPM
+// forward + adjoint path.
+//
+// One context = one scene (point cloud, grid, target), one CUDA stream and
+// its device memory.  Layers follow the reference's CompGraph
+// (CompGraph.cpp:7-17, 246-267): layer 0 is the uploaded cloud, layer i+1 is
+// ForwardTimeStep(layer i), EndLayerMassLoss reads the last layer, and the
+// backward pass walks the layers in reverse.
+//
+// Layer storage.  With checkpoint interval k = 1 every layer's particle state
+// (24 planes) and grid (node4 per node) stays in HBM.  With k > 1 only layers
+// 0, k, 2k, ... and the last are kept; the backward pass recomputes each
+// segment's states and grids from its checkpoint into segment scratch before
+// running the segment's adjoint steps (recompute-in-between).
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <memory>
+#include <string>
+#include <type_traits>
+#include <vector>
+
+#include "dmpm.h"
+#include "kernels.cuh"
+
+using namespace dmpm;
+
+namespace {
+
+constexpr int kDefaultBlock = 256;
+constexpr int kDefaultTileCap = 1024;
+
+struct CudaError {
+    cudaError_t code;
+    std::string what;
+};
+
+#define DMPM_CK(call)                                                                        \
+    do {                                                                                     \
+        cudaError_t e_ = (call);                                                             \
+        if (e_ != cudaSuccess) throw CudaError{e_, std::string(#call) + ": " + cudaGetErrorString(e_)}; \
+    } while (0)
+
+struct ArgError {
+    std::string what;
+};
+struct StateError {
+    std::string what;
+};
+
+size_t round_up(size_t a, size_t b) { return (a + b - 1) / b * b; }
+
+// Device allocation owner.
+class Arena {
+   public:
+    ~Arena() { release(); }
+    void* alloc(size_t bytes) {
+        if (bytes == 0) return nullptr;
+        void* p = nullptr;
+        cudaError_t e = cudaMalloc(&p, round_up(bytes, 256));
+        if (e != cudaSuccess) {
+            cudaGetLastError();
+            throw CudaError{e, "cudaMalloc(" + std::to_string(bytes) + " bytes): " + cudaGetErrorString(e)};
+        }
+        ptrs_.push_back(p);
+        bytes_ += round_up(bytes, 256);
+        return p;
+    }
+    void release() {
+        for (void* p : ptrs_) cudaFree(p);
+        ptrs_.clear();
+        bytes_ = 0;
+    }
+    size_t bytes() const { return bytes_; }
+
+   private:
+    std::vector<void*> ptrs_;
+    size_t bytes_ = 0;
+};
+
+// ---------------------------------------------------------------- layout kernels
+template <class T> __global__ void k_unpack(const double* __restrict__ src, int width, int n, T* dst, size_t np) {
+    const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= (size_t)n * width) return;
+    const int p = (int)(i / width), q = (int)(i % width);
+    dst[(size_t)q * np + p] = (T)src[i];
+}
+template <class T> __global__ void k_pack(const T* __restrict__ src, size_t np, int width, int n, double* dst) {
+    const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= (size_t)n * width) return;
+    const int p = (int)(i / width), q = (int)(i % width);
+    dst[i] = (double)src[(size_t)q * np + p];
+}
+template <class T> __global__ void k_pack_acc(const double* __restrict__ src, size_t np, int n, double* dst) {
+    const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= (size_t)n * 9) return;
+    const int p = (int)(i / 9), q = (int)(i % 9);
+    dst[i] = src[(size_t)q * np + p];
+}
+// Reference MaterialPoint (118 floats): x 0, v 3, F 6, C 15, P 24, m 33, vol 34,
+// lam 35, mu 36, dFc 37 (MaterialPoint.h:18-46).
+template <class T>
+__global__ void k_unpack_ref(const float* __restrict__ pts, int n, size_t np, T* st, T* cst, T* dfc) {
+    const int p = blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= n) return;
+    const float* m = pts + (size_t)p * 118;
+    for (int q = 0; q < 24; q++) st[(size_t)q * np + p] = (T)m[q];  // x v F C share the plane order
+    cst[(size_t)KM * np + p] = (T)m[33];
+    cst[(size_t)KVOL * np + p] = (T)m[34];
+    cst[(size_t)KLAM * np + p] = (T)m[35];
+    cst[(size_t)KMU * np + p] = (T)m[36];
+    for (int q = 0; q < 9; q++) dfc[(size_t)q * np + p] = (T)m[37 + q];
+}
+template <class T>
+__global__ void k_grid_field(const node4<T>* __restrict__ g, size_t G, int field, double dt, double f0, double f1,
+                             double f2, double* out) {
+    const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= G) return;
+    const node4<T> nd = g[i];
+    if (field == DMPM_G_M) {
+        out[i] = (double)nd.w;
+    } else if (field == DMPM_G_P) {
+        out[3 * i] = nd.x; out[3 * i + 1] = nd.y; out[3 * i + 2] = nd.z;
+    } else {
+        const T f[3] = {(T)f0, (T)f1, (T)f2};
+        T v[3];
+        node_velocity(nd, (T)dt, f, v);
+        out[3 * i] = v[0]; out[3 * i + 1] = v[1]; out[3 * i + 2] = v[2];
+    }
+}
+template <class T> __global__ void k_node4_field(const node4<T>* __restrict__ g, size_t G, int comp, double* out) {
+    const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= G) return;
+    const node4<T> nd = g[i];
+    if (comp == 3) { out[3 * i] = nd.x; out[3 * i + 1] = nd.y; out[3 * i + 2] = nd.z; }
+    else out[i] = nd.w;
+}
+template <class T> __global__ void k_scalar_field(const T* __restrict__ g, size_t G, double* out) {
+    const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < G) out[i] = (double)g[i];
+}
+template <class T> __global__ void k_set_node_mass(const double* __restrict__ src, size_t G, T* dst) {
+    const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < G) dst[i] = (T)src[i];
+}
+template <class T> __global__ void k_copy_node_mass(const node4<T>* __restrict__ g, size_t G, T* dst) {
+    const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < G) dst[i] = g[i].w;
+}
+// sum of squares of 9 planes (Compute_dLdF_Norm), FP64
+template <class T> __global__ void k_sqnorm9(const T* __restrict__ a, size_t np, int n, double* out) {
+    __shared__ double s[32];
+    const int p = blockIdx.x * blockDim.x + threadIdx.x;
+    double v = 0.0;
+    if (p < n)
+        for (int q = 0; q < 9; q++) { const double t = (double)a[(size_t)q * np + p]; v += t * t; }
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    if ((threadIdx.x & 31) == 0) s[threadIdx.x >> 5] = v;
+    __syncthreads();
+    if (threadIdx.x < 32) {
+        v = threadIdx.x < (blockDim.x >> 5) ? s[threadIdx.x] : 0.0;
+        for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+        if (threadIdx.x == 0) atomicAdd(out, v);
+    }
+}
+
+}  // namespace
+
+// ====================================================================== engine
+struct EngineBase {
+    virtual ~EngineBase() {}
+};
+
+struct dmpm_ctx {
+    int device = 0;
+    int precision = DMPM_FP32_MIXED;
+    cudaStream_t stream = nullptr;
+    std::string err;
+    dmpm_params prm{};
+    int64_t launches = 0;
+    std::unique_ptr<EngineBase> eng;
+};
+
+namespace {
+
+template <class T> class Engine : public EngineBase {
+   public:
+    static constexpr bool kTiled = std::is_same<T, float>::value;
+
+    explicit Engine(dmpm_ctx* c) : ctx_(c) {}
+
+    // ---------------------------------------------------------- configuration
+    void set_grid(int dx_, int dy_, int dz_, double h, const double* mn) {
+        if (dx_ <= 0 || dy_ <= 0 || dz_ <= 0 || !(h > 0)) throw ArgError{"grid dims and dx must be positive"};
+        if ((double)dx_ * dy_ * dz_ > 2e9) throw ArgError{"grid has more than 2e9 nodes"};
+        geo_.dim[0] = dx_; geo_.dim[1] = dy_; geo_.dim[2] = dz_;
+        geo_.dx = h;
+        for (int a = 0; a < 3; a++) geo_.mn[a] = mn ? mn[a] : 0.0;
+        G_ = (size_t)dx_ * dy_ * dz_;
+        grid_set_ = true;
+        layers_.clear();
+        target_ = nullptr;
+        scene_arena_grid_.release();
+        target_ = (T*)scene_arena_grid_.alloc(G_ * sizeof(T));
+        DMPM_CK(cudaMemsetAsync(target_, 0, G_ * sizeof(T), ctx_->stream));
+        dldm_ = (T*)scene_arena_grid_.alloc(G_ * sizeof(T));
+        scratch_grid_ = (node4<T>*)scene_arena_grid_.alloc(G_ * sizeof(node4<T>));
+    }
+
+    void alloc_particles(int n) {
+        if (n <= 0) throw ArgError{"particle count must be positive"};
+        n_ = n;
+        np_ = round_up((size_t)n, 64);
+        layers_.clear();
+        scene_arena_.release();
+        cst_ = (T*)scene_arena_.alloc(NCONST * np_ * sizeof(T));
+        st0_ = (T*)scene_arena_.alloc(NSTATE * np_ * sizeof(T));
+        dfc0_ = (T*)scene_arena_.alloc(9 * np_ * sizeof(T));
+        DMPM_CK(cudaMemsetAsync(cst_, 0, NCONST * np_ * sizeof(T), ctx_->stream));
+        DMPM_CK(cudaMemsetAsync(st0_, 0, NSTATE * np_ * sizeof(T), ctx_->stream));
+        DMPM_CK(cudaMemsetAsync(dfc0_, 0, 9 * np_ * sizeof(T), ctx_->stream));
+    }
+
+    double* staging(size_t count) {
+        if (count > staging_count_) {
+            staging_arena_.release();
+            staging_ = (double*)staging_arena_.alloc(count * sizeof(double));
+            staging_count_ = count;
+        }
+        return staging_;
+    }
+
+    void upload_planes(const double* host, int width, T* dst) {
+        double* s = staging((size_t)n_ * width);
+        DMPM_CK(cudaMemcpyAsync(s, host, (size_t)n_ * width * sizeof(double), cudaMemcpyHostToDevice, ctx_->stream));
+        const size_t tot = (size_t)n_ * width;
+        k_unpack<T><<<(unsigned)((tot + 255) / 256), 256, 0, ctx_->stream>>>(s, width, n_, dst, np_);
+        launched();
+    }
+
+    void download_planes(const T* src, int width, double* host) {
+        double* s = staging((size_t)n_ * width);
+        const size_t tot = (size_t)n_ * width;
+        k_pack<T><<<(unsigned)((tot + 255) / 256), 256, 0, ctx_->stream>>>(src, np_, width, n_, s);
+        launched();
+        DMPM_CK(cudaMemcpyAsync(host, s, tot * sizeof(double), cudaMemcpyDeviceToHost, ctx_->stream));
+        DMPM_CK(cudaStreamSynchronize(ctx_->stream));
+    }
+
+    void set_particles(int n, const double* x, const double* v, const double* F, const double* C, const double* dFc,
+                       const double* m, const double* vol, const double* lam, const double* mu) {
+        if (!x || !m || !lam || !mu) throw ArgError{"x, m, lam and mu are required"};
+        alloc_particles(n);
+        upload_planes(x, 3, st0_ + (size_t)PX * np_);
+        if (v) upload_planes(v, 3, st0_ + (size_t)PV * np_);
+        if (F) {
+            upload_planes(F, 9, st0_ + (size_t)PF * np_);
+        } else {
+            std::vector<double> eye((size_t)n * 9, 0.0);
+            for (int p = 0; p < n; p++) eye[9 * p] = eye[9 * p + 4] = eye[9 * p + 8] = 1.0;
+            upload_planes(eye.data(), 9, st0_ + (size_t)PF * np_);
+        }
+        if (C) upload_planes(C, 9, st0_ + (size_t)PC * np_);
+        if (dFc) upload_planes(dFc, 9, dfc0_);
+        upload_planes(m, 1, cst_ + (size_t)KM * np_);
+        if (vol) upload_planes(vol, 1, cst_ + (size_t)KVOL * np_);
+        upload_planes(lam, 1, cst_ + (size_t)KLAM * np_);
+        upload_planes(mu, 1, cst_ + (size_t)KMU * np_);
+    }
+
+    void set_points_ref(const void* pts, int n) {
+        if (!pts) throw ArgError{"points is NULL"};
+        alloc_particles(n);
+        const size_t bytes = (size_t)n * 118 * sizeof(float);
+        double* s = staging((bytes + 7) / 8);
+        DMPM_CK(cudaMemcpyAsync(s, pts, bytes, cudaMemcpyHostToDevice, ctx_->stream));
+        k_unpack_ref<T><<<(n + 255) / 256, 256, 0, ctx_->stream>>>((const float*)s, n, np_, st0_, cst_, dfc0_);
+        launched();
+    }
+
+    void check_scene() {
+        if (!grid_set_) throw StateError{"dmpm_set_grid has not been called"};
+        if (n_ <= 0) throw StateError{"no particles uploaded"};
+    }
+
+    FwdArgs<T> fwd_args() const {
+        FwdArgs<T> a{};
+        a.n = n_;
+        a.np = np_;
+        a.geo = geo_;
+        a.dt = (T)ctx_->prm.dt;
+        a.drag = (T)ctx_->prm.drag;
+        a.s = (T)ctx_->prm.smoothing;
+        for (int c = 0; c < 3; c++) a.fext[c] = (T)ctx_->prm.f_ext[c];
+        a.cst = cst_;
+        a.tile_cap = tile_cap();
+        a.status = status_;
+        return a;
+    }
+
+    LossArgs<T> loss_args() const {
+        LossArgs<T> a{};
+        a.n = n_;
+        a.np = np_;
+        a.geo = geo_;
+        a.cst = cst_;
+        a.target = target_;
+        a.dldm = dldm_;
+        a.kind = ctx_->prm.loss_kind;
+        a.tile_cap = tile_cap();
+        a.status = status_;
+        return a;
+    }
+
+    int block() const { return ctx_->prm.block_size > 0 ? ctx_->prm.block_size : kDefaultBlock; }
+    int tile_cap() const { return ctx_->prm.tile_cap > 0 ? ctx_->prm.tile_cap : kDefaultTileCap; }
+    unsigned pgrid() const { return (unsigned)((n_ + block() - 1) / block()); }
+    unsigned ggrid() const { return (unsigned)((G_ + 255) / 256); }
+
+    void launched() {
+        ctx_->launches++;
+        cudaError_t e = cudaGetLastError();
+        if (e != cudaSuccess) throw CudaError{e, std::string("kernel launch: ") + cudaGetErrorString(e)};
+    }
+
+    void ensure_status() {
+        if (!status_) {
+            status_ = (unsigned*)misc_arena_.alloc(sizeof(unsigned) + sizeof(double) * 2);
+            loss_acc_ = (double*)((char*)status_ + 8);
+            DMPM_CK(cudaMallocHost(&host_misc_, 64));
+        }
+    }
+
+    unsigned read_status() {
+        DMPM_CK(cudaMemcpyAsync(host_misc_, status_, sizeof(unsigned), cudaMemcpyDeviceToHost, ctx_->stream));
+        DMPM_CK(cudaStreamSynchronize(ctx_->stream));
+        return *(unsigned*)host_misc_;
+    }
+
+    void compute_volumes() {
+        check_scene();
+        ensure_status();
+        LossArgs<T> a = loss_args();
+        a.st = st0_;
+        a.grid = scratch_grid_;
+        DMPM_CK(cudaMemsetAsync(scratch_grid_, 0, G_ * sizeof(node4<T>), ctx_->stream));
+        launch_mass(a);
+        k_volumes<T><<<pgrid(), block(), 0, ctx_->stream>>>(a, cst_ + (size_t)KVOL * np_);
+        launched();
+    }
+
+    void launch_mass(const LossArgs<T>& a) {
+        if (kTiled)
+            k_p2g_mass<T, true><<<pgrid(), block(), tile_cap() * sizeof(T), ctx_->stream>>>(a);
+        else
+            k_p2g_mass<T, false><<<pgrid(), block(), 0, ctx_->stream>>>(a);
+        launched();
+    }
+
+    void set_target_mass(const double* m) {
+        if (!grid_set_) throw StateError{"dmpm_set_grid has not been called"};
+        double* s = staging(G_);
+        DMPM_CK(cudaMemcpyAsync(s, m, G_ * sizeof(double), cudaMemcpyHostToDevice, ctx_->stream));
+        k_set_node_mass<T><<<ggrid(), 256, 0, ctx_->stream>>>(s, G_, target_);
+        launched();
+    }
+
+    // LoadCompGraph: target grid = ResetValues + P2G(target samples, dt = drag = 0),
+    // of which EndLayerMassLoss reads only m (MPMPolyscope.cpp:155-160).
+    void rasterize_target(int n, const double* x, double mp) {
+        if (!grid_set_) throw StateError{"dmpm_set_grid has not been called"};
+        if (n < 0 || (n > 0 && !x)) throw ArgError{"bad target samples"};
+        ensure_status();
+        DMPM_CK(cudaMemsetAsync(scratch_grid_, 0, G_ * sizeof(node4<T>), ctx_->stream));
+        if (n > 0) {
+            const size_t npt = round_up((size_t)n, 64);
+            Arena tmp;
+            T* st = (T*)tmp.alloc(3 * npt * sizeof(T));
+            T* cst = (T*)tmp.alloc(npt * sizeof(T));
+            double* s = staging((size_t)n * 3);
+            DMPM_CK(cudaMemcpyAsync(s, x, (size_t)n * 3 * sizeof(double), cudaMemcpyHostToDevice, ctx_->stream));
+            k_unpack<T><<<(unsigned)(((size_t)n * 3 + 255) / 256), 256, 0, ctx_->stream>>>(s, 3, n, st, npt);
+            launched();
+            std::vector<double> mh((size_t)n, mp);
+            double* s2 = staging((size_t)n * 3);
+            DMPM_CK(cudaMemcpyAsync(s2, mh.data(), (size_t)n * sizeof(double), cudaMemcpyHostToDevice, ctx_->stream));
+            k_unpack<T><<<(unsigned)((n + 255) / 256), 256, 0, ctx_->stream>>>(s2, 1, n, cst, npt);
+            launched();
+            LossArgs<T> a = loss_args();
+            a.n = n;
+            a.np = npt;
+            a.st = st;
+            a.cst = cst;
+            a.grid = scratch_grid_;
+            launch_mass(a);
+            k_copy_node_mass<T><<<ggrid(), 256, 0, ctx_->stream>>>(scratch_grid_, G_, target_);
+            launched();
+            DMPM_CK(cudaStreamSynchronize(ctx_->stream));
+        } else {
+            DMPM_CK(cudaMemsetAsync(target_, 0, G_ * sizeof(T), ctx_->stream));
+        }
+    }
+
+    // ---------------------------------------------------------- layers
+    bool stored(int l) const { return k_ == 1 || l % k_ == 0 || l == L_ - 1; }
+
+    void setup(int num_layers) {
+        check_scene();
+        if (num_layers < 1) throw ArgError{"num_layers must be >= 1"};
+        ensure_status();
+        const dmpm_params& P = ctx_->prm;
+        L_ = num_layers;
+        layer_arena_.release();
+        layers_.assign(L_, LayerSlots{});
+        const size_t st_bytes = NSTATE * np_ * sizeof(T);
+        const size_t gr_bytes = G_ * sizeof(node4<T>);
+        const bool per_layer = P.control_mode == DMPM_CTRL_PER_LAYER;
+        // choose the checkpoint interval
+        int k = P.checkpoint_every;
+        if (k <= 0) {
+            size_t free_b = 0, total_b = 0;
+            DMPM_CK(cudaMemGetInfo(&free_b, &total_b));
+            const double need = (double)L_ * (st_bytes + gr_bytes) +
+                                (per_layer ? 2.0 * L_ * 9 * np_ * sizeof(T) : 0.0) +
+                                (P.keep_adjoints ? (double)L_ * st_bytes : 0.0);
+            k = need < 0.8 * (double)free_b ? 1 : std::max(2, (int)std::ceil(std::sqrt((double)L_)));
+        }
+        k_ = std::min(k, std::max(1, L_ - 1));
+        if (k_ < 1) k_ = 1;
+        // particle states
+        int nstored = 0;
+        for (int l = 0; l < L_; l++) nstored += stored(l) ? 1 : 0;
+        T* sbase = (T*)layer_arena_.alloc((size_t)nstored * st_bytes);
+        for (int l = 0, s = 0; l < L_; l++)
+            if (stored(l)) layers_[l].st = sbase + (size_t)(s++) * NSTATE * np_;
+        if (k_ > 1) {
+            ring_[0] = (T*)layer_arena_.alloc(st_bytes);
+            ring_[1] = (T*)layer_arena_.alloc(st_bytes);
+            seg_st_.assign(k_ - 1, nullptr);
+            for (int i = 0; i < k_ - 1; i++) seg_st_[i] = (T*)layer_arena_.alloc(st_bytes);
+            seg_grid_.assign(k_, nullptr);
+            for (int i = 0; i < k_; i++) seg_grid_[i] = (node4<T>*)layer_arena_.alloc(gr_bytes);
+        } else {
+            node4<T>* gbase = (node4<T>*)layer_arena_.alloc((size_t)L_ * gr_bytes);
+            for (int l = 0; l < L_; l++) layers_[l].grid = gbase + (size_t)l * G_;
+        }
+        // controls
+        if (per_layer) {
+            T* dbase = (T*)layer_arena_.alloc((size_t)L_ * 9 * np_ * sizeof(T));
+            T* gbase = (T*)layer_arena_.alloc((size_t)L_ * 9 * np_ * sizeof(T));
+            for (int l = 0; l < L_; l++) {
+                layers_[l].dfc = dbase + (size_t)l * 9 * np_;
+                layers_[l].ctrl_grad = gbase + (size_t)l * 9 * np_;
+                DMPM_CK(cudaMemcpyAsync(layers_[l].dfc, dfc0_, 9 * np_ * sizeof(T), cudaMemcpyDeviceToDevice, ctx_->stream));
+            }
+            DMPM_CK(cudaMemsetAsync(gbase, 0, (size_t)L_ * 9 * np_ * sizeof(T), ctx_->stream));
+            ctrl_acc_ = nullptr;
+        } else {
+            for (int l = 0; l < L_; l++) layers_[l].dfc = dfc0_;
+            ctrl_acc_ = (double*)layer_arena_.alloc(9 * np_ * sizeof(double));
+            DMPM_CK(cudaMemsetAsync(ctrl_acc_, 0, 9 * np_ * sizeof(double), ctx_->stream));
+        }
+        // adjoints
+        if (P.keep_adjoints) {
+            T* abase = (T*)layer_arena_.alloc((size_t)L_ * st_bytes);
+            DMPM_CK(cudaMemsetAsync(abase, 0, (size_t)L_ * st_bytes, ctx_->stream));
+            for (int l = 0; l < L_; l++) layers_[l].adj = abase + (size_t)l * NSTATE * np_;
+        } else {
+            adj_pp_[0] = (T*)layer_arena_.alloc(st_bytes);
+            adj_pp_[1] = (T*)layer_arena_.alloc(st_bytes);
+        }
+        gadj_ = (node4<T>*)layer_arena_.alloc(gr_bytes);
+        if (!kTiled) {
+            gadj2_ = (node4<T>*)layer_arena_.alloc(gr_bytes);
+            gridv_ = (T*)layer_arena_.alloc(3 * G_ * sizeof(T));
+            pscratch_ = (T*)layer_arena_.alloc(9 * np_ * sizeof(T));
+        }
+        if (P.keep_intermediates) {
+            T* b1 = (T*)layer_arena_.alloc((size_t)L_ * 9 * np_ * sizeof(T));   // P
+            T* b2 = (T*)layer_arena_.alloc((size_t)L_ * 9 * np_ * sizeof(T));   // dLdP
+            T* b3 = (T*)layer_arena_.alloc((size_t)L_ * 3 * np_ * sizeof(T));   // dLdv_next
+            T* b4 = (T*)layer_arena_.alloc((size_t)L_ * 9 * np_ * sizeof(T));   // dLdC_next
+            node4<T>* g1 = (node4<T>*)layer_arena_.alloc((size_t)L_ * gr_bytes);  // grid dLdv
+            node4<T>* g2 = (node4<T>*)layer_arena_.alloc((size_t)L_ * gr_bytes);  // grid dLdp, dLdm
+            DMPM_CK(cudaMemsetAsync(b1, 0, (size_t)L_ * 9 * np_ * sizeof(T), ctx_->stream));
+            DMPM_CK(cudaMemsetAsync(b2, 0, (size_t)L_ * 9 * np_ * sizeof(T), ctx_->stream));
+            DMPM_CK(cudaMemsetAsync(b3, 0, (size_t)L_ * 3 * np_ * sizeof(T), ctx_->stream));
+            DMPM_CK(cudaMemsetAsync(b4, 0, (size_t)L_ * 9 * np_ * sizeof(T), ctx_->stream));
+            DMPM_CK(cudaMemsetAsync(g1, 0, (size_t)L_ * gr_bytes, ctx_->stream));
+            DMPM_CK(cudaMemsetAsync(g2, 0, (size_t)L_ * gr_bytes, ctx_->stream));
+            for (int l = 0; l < L_; l++) {
+                layers_[l].dbgP = b1 + (size_t)l * 9 * np_;
+                layers_[l].dbgdLdP = b2 + (size_t)l * 9 * np_;
+                layers_[l].dbgvn = b3 + (size_t)l * 3 * np_;
+                layers_[l].dbgCn = b4 + (size_t)l * 9 * np_;
+                layers_[l].dbggdv = g1 + (size_t)l * G_;
+                layers_[l].dbggdp = g2 + (size_t)l * G_;
+            }
+        }
+        // layer 0 = the uploaded cloud (SetUpCompGraph copies it into every layer;
+        // only layer 0's state is ever read before being recomputed)
+        DMPM_CK(cudaMemcpyAsync(layers_[0].st, st0_, st_bytes, cudaMemcpyDeviceToDevice, ctx_->stream));
+        for (int l = 1; l < L_; l++)
+            if (layers_[l].st) DMPM_CK(cudaMemcpyAsync(layers_[l].st, st0_, st_bytes, cudaMemcpyDeviceToDevice, ctx_->stream));
+        forward_done_ = false;
+        loss_done_ = false;
+        backward_lo_ = L_;
+        seg_lo_ = seg_hi_ = -1;
+    }
+
+    // pointer to the state of layer l if it is materialised (stored or in the current segment)
+    T* state_of(int l) {
+        if (layers_[l].st) return layers_[l].st;
+        if (k_ > 1 && l > seg_lo_ && l < seg_hi_) return seg_st_[l - seg_lo_ - 1];
+        return nullptr;
+    }
+    node4<T>* grid_of(int l) {
+        if (layers_[l].grid) return layers_[l].grid;
+        if (k_ > 1 && l >= seg_lo_ && l < seg_hi_) return seg_grid_[l - seg_lo_];
+        return nullptr;
+    }
+
+    // one ForwardTimeStep: layer l -> out (state of l+1), grid g
+    void step(int l, const T* st, T* out, node4<T>* g) {
+        FwdArgs<T> a = fwd_args();
+        a.st = st;
+        a.st_next = out;
+        a.dfc = layers_[l].dfc;
+        a.grid = g;
+        a.gridv = gridv_;
+        a.P = ctx_->prm.keep_intermediates ? layers_[l].dbgP : (kTiled ? nullptr : pscratch_);
+        DMPM_CK(cudaMemsetAsync(g, 0, G_ * sizeof(node4<T>), ctx_->stream));
+        const size_t tile_b = (size_t)tile_cap() * sizeof(node4<T>);
+        if (kTiled) {
+            k_p2g<T, true, true><<<pgrid(), block(), tile_b, ctx_->stream>>>(a);
+            launched();
+            k_g2p<T, true><<<pgrid(), block(), tile_b, ctx_->stream>>>(a);
+            launched();
+        } else {
+            k_p_op1<T><<<pgrid(), block(), 0, ctx_->stream>>>(a);
+            launched();
+            k_p2g<T, false, false><<<pgrid(), block(), 0, ctx_->stream>>>(a);
+            launched();
+            k_gop<T><<<ggrid(), 256, 0, ctx_->stream>>>(a, G_);
+            launched();
+            k_g2p<T, false><<<pgrid(), block(), 0, ctx_->stream>>>(a);
+            launched();
+        }
+    }
+
+    void reset_status() {
+        DMPM_CK(cudaMemsetAsync(status_, 0, sizeof(unsigned), ctx_->stream));
+    }
+
+    void forward(int start) {
+        if (L_ <= 0) throw StateError{"dmpm_setup has not been called"};
+        if (start < 0 || start >= L_) throw ArgError{"start_layer out of range"};
+        reset_status();
+        if (k_ == 1) {
+            for (int l = start; l + 1 < L_; l++) step(l, layers_[l].st, layers_[l + 1].st, layers_[l].grid);
+        } else {
+            const T* cur = materialize_state(start);
+            int r = 0;
+            for (int l = start; l + 1 < L_; l++) {
+                T* out = layers_[l + 1].st ? layers_[l + 1].st : ring_[r];
+                if (!layers_[l + 1].st) r ^= 1;
+                // the current state may live in ring_[r] already (ping-pong)
+                step(l, cur, out, seg_grid_[0]);
+                cur = out;
+            }
+            seg_lo_ = seg_hi_ = -1;  // segment scratch no longer matches
+        }
+        forward_done_ = true;
+        loss_done_ = false;
+        last_status_ = read_status();
+    }
+
+    // Make layer l's state available; for a non-stored layer recompute its
+    // segment (and the grids of the segment) from the checkpoint below it.
+    const T* materialize_state(int l) {
+        if (T* s = state_of(l)) return s;
+        materialize_segment(l - l % k_);
+        return state_of(l);
+    }
+
+    void materialize_segment(int c) {
+        const int e = std::min(c + k_, L_ - 1);
+        const T* cur = layers_[c].st;
+        for (int l = c; l < e; l++) {
+            T* out = (l + 1 == e) ? nullptr : seg_st_[l - c];
+            if (out) {
+                step(l, cur, out, seg_grid_[l - c]);
+                cur = out;
+            } else {
+                // last step of the segment: only its grid is needed; the output
+                // (layer e) is a stored layer already, write it to scratch ring
+                step(l, cur, ring_[0], seg_grid_[l - c]);
+            }
+        }
+        seg_lo_ = c;
+        seg_hi_ = e;
+    }
+
+    double loss() {
+        if (!forward_done_ && L_ > 1) throw StateError{"dmpm_forward has not been run"};
+        if (L_ <= 0) throw StateError{"dmpm_setup has not been called"};
+        reset_status();
+        LossArgs<T> a = loss_args();
+        a.st = layers_[L_ - 1].st;
+        node4<T>* g = (k_ == 1) ? layers_[L_ - 1].grid : scratch_grid_;
+        a.grid = g;
+        a.adj = adj_of(L_ - 1, true);
+        a.loss = loss_acc_;
+        DMPM_CK(cudaMemsetAsync(g, 0, G_ * sizeof(node4<T>), ctx_->stream));
+        DMPM_CK(cudaMemsetAsync(loss_acc_, 0, sizeof(double), ctx_->stream));
+        launch_mass(a);
+        k_node_loss<T><<<ggrid(), 256, 0, ctx_->stream>>>(a, G_);
+        launched();
+        k_loss_dldx<T><<<pgrid(), block(), 0, ctx_->stream>>>(a);
+        launched();
+        DMPM_CK(cudaMemcpyAsync((char*)host_misc_ + 8, loss_acc_, sizeof(double), cudaMemcpyDeviceToHost, ctx_->stream));
+        last_status_ = read_status();
+        loss_done_ = true;
+        backward_lo_ = L_ - 1;
+        return *(double*)((char*)host_misc_ + 8);
+    }
+
+    // adjoint buffer of layer l (ping-pong when adjoints are not kept)
+    T* adj_of(int l, bool for_write) {
+        (void)for_write;
+        if (layers_[l].adj) return layers_[l].adj;
+        return adj_pp_[l & 1];
+    }
+
+    void adjoint_step(int i) {
+        const dmpm_params& P = ctx_->prm;
+        AdjArgs<T> a{};
+        a.n = n_;
+        a.np = np_;
+        a.geo = geo_;
+        a.dt = (T)P.dt;
+        a.drag = (T)P.drag;
+        a.s = (T)P.smoothing;
+        for (int c = 0; c < 3; c++) a.fext[c] = (T)P.f_ext[c];
+        a.st = state_of(i);
+        a.st_next = state_of(i + 1);
+        a.cst = cst_;
+        a.dfc = layers_[i].dfc;
+        a.grid = grid_of(i);
+        a.adj_next = adj_of(i + 1, false);
+        a.adj = adj_of(i, true);
+        a.gadj = gadj_;
+        a.gadj2 = gadj2_;
+        a.ctrl_grad = layers_[i].ctrl_grad;
+        a.ctrl_acc = ctrl_acc_;
+        a.dbg_dLdP = P.keep_intermediates ? layers_[i].dbgdLdP : nullptr;
+        a.dbg_vnext = P.keep_intermediates ? layers_[i].dbgvn : nullptr;
+        a.dbg_Cnext = P.keep_intermediates ? layers_[i].dbgCn : nullptr;
+        a.tile_cap = tile_cap();
+        a.status = status_;
+        if (!a.st || !a.st_next || !a.grid) throw StateError{"internal: layer not materialised"};
+        DMPM_CK(cudaMemsetAsync(gadj_, 0, G_ * sizeof(node4<T>), ctx_->stream));
+        const size_t tile_b = (size_t)tile_cap() * sizeof(node4<T>);
+        const bool ex = P.adjoint_mode == DMPM_ADJ_EXACT;
+        if (kTiled) {
+            if (ex) k_adj_scatter<T, true, true><<<pgrid(), block(), tile_b, ctx_->stream>>>(a);
+            else k_adj_scatter<T, true, false><<<pgrid(), block(), tile_b, ctx_->stream>>>(a);
+            launched();
+            if (P.keep_intermediates) debug_grid_adjoint(i, a, ex);
+            if (ex) k_adj_gather<T, true, true><<<pgrid(), block(), 2 * tile_b, ctx_->stream>>>(a);
+            else k_adj_gather<T, true, false><<<pgrid(), block(), 2 * tile_b, ctx_->stream>>>(a);
+            launched();
+        } else {
+            if (ex) k_adj_scatter<T, false, true><<<pgrid(), block(), 0, ctx_->stream>>>(a);
+            else k_adj_scatter<T, false, false><<<pgrid(), block(), 0, ctx_->stream>>>(a);
+            launched();
+            if (ex) k_adj_gop<T, true><<<ggrid(), 256, 0, ctx_->stream>>>(a, G_);
+            else k_adj_gop<T, false><<<ggrid(), 256, 0, ctx_->stream>>>(a, G_);
+            launched();
+            if (P.keep_intermediates) debug_grid_adjoint(i, a, ex);
+            if (ex) k_adj_gather<T, false, true><<<pgrid(), block(), 0, ctx_->stream>>>(a);
+            else k_adj_gather<T, false, false><<<pgrid(), block(), 0, ctx_->stream>>>(a);
+            launched();
+        }
+    }
+
+    void debug_grid_adjoint(int i, AdjArgs<T>& a, bool ex) {
+        DMPM_CK(cudaMemcpyAsync(layers_[i].dbggdv, gadj_, G_ * sizeof(node4<T>), cudaMemcpyDeviceToDevice, ctx_->stream));
+        AdjArgs<T> b = a;
+        b.gadj2 = layers_[i].dbggdp;
+        if (ex) k_adj_gop<T, true><<<ggrid(), 256, 0, ctx_->stream>>>(b, G_);
+        else k_adj_gop<T, false><<<ggrid(), 256, 0, ctx_->stream>>>(b, G_);
+        launched();
+    }
+
+    void backward(int control) {
+        if (!loss_done_) throw StateError{"dmpm_loss must run before dmpm_backward"};
+        if (control < 0 || control > L_ - 1) throw ArgError{"control_layer out of range"};
+        reset_status();
+        if (ctrl_acc_) DMPM_CK(cudaMemsetAsync(ctrl_acc_, 0, 9 * np_ * sizeof(double), ctx_->stream));
+        if (k_ == 1) {
+            for (int i = L_ - 2; i >= control; i--) adjoint_step(i);
+        } else {
+            int i = L_ - 2;
+            while (i >= control) {
+                const int c = i - i % k_;
+                materialize_segment(c);
+                for (; i >= std::max(c, control); i--) adjoint_step(i);
+            }
+        }
+        backward_lo_ = control;
+        last_status_ = read_status();
+    }
+
+    // ---------------------------------------------------------- downloads
+    void get_particles(int l, int field, double* out) {
+        if (l < 0 || l >= L_) throw ArgError{"layer out of range"};
+        if (!out) throw ArgError{"out is NULL"};
+        auto need_adj = [&]() -> const T* {
+            if (layers_[l].adj) return layers_[l].adj;
+            if (l >= backward_lo_ && (l == backward_lo_ || l == L_ - 1)) return adj_of(l, false);
+            throw StateError{"adjoint of this layer is not kept (set keep_adjoints)"};
+        };
+        auto need_dbg = [&](const T* p) -> const T* {
+            if (!p) throw StateError{"intermediates are not kept (set keep_intermediates)"};
+            return p;
+        };
+        switch (field) {
+            case DMPM_F_X: download_planes(materialize_state(l) + (size_t)PX * np_, 3, out); break;
+            case DMPM_F_V: download_planes(materialize_state(l) + (size_t)PV * np_, 3, out); break;
+            case DMPM_F_F: download_planes(materialize_state(l) + (size_t)PF * np_, 9, out); break;
+            case DMPM_F_C: download_planes(materialize_state(l) + (size_t)PC * np_, 9, out); break;
+            case DMPM_F_P: {
+                if (layers_[l].dbgP && l < L_ - 1) { download_planes(layers_[l].dbgP, 9, out); break; }
+                // recompute P_op_1 of this layer on demand
+                Arena tmp;
+                T* P = (T*)tmp.alloc(9 * np_ * sizeof(T));
+                FwdArgs<T> a = fwd_args();
+                a.st = materialize_state(l);
+                a.dfc = layers_[l].dfc;
+                a.P = P;
+                k_p_op1<T><<<pgrid(), block(), 0, ctx_->stream>>>(a);
+                launched();
+                download_planes(P, 9, out);
+                break;
+            }
+            case DMPM_F_M: download_planes(cst_ + (size_t)KM * np_, 1, out); break;
+            case DMPM_F_VOL: download_planes(cst_ + (size_t)KVOL * np_, 1, out); break;
+            case DMPM_F_LAM: download_planes(cst_ + (size_t)KLAM * np_, 1, out); break;
+            case DMPM_F_MU: download_planes(cst_ + (size_t)KMU * np_, 1, out); break;
+            case DMPM_F_DFC: download_planes(layers_[l].dfc, 9, out); break;
+            case DMPM_F_DLDX: download_planes(need_adj() + (size_t)PX * np_, 3, out); break;
+            case DMPM_F_DLDV: download_planes(need_adj() + (size_t)PV * np_, 3, out); break;
+            case DMPM_F_DLDF: download_planes(need_adj() + (size_t)PF * np_, 9, out); break;
+            case DMPM_F_DLDC: download_planes(need_adj() + (size_t)PC * np_, 9, out); break;
+            case DMPM_F_DLDP: download_planes(need_dbg(layers_[l].dbgdLdP), 9, out); break;
+            case DMPM_F_DLDV_NEXT: download_planes(need_dbg(layers_[l].dbgvn), 3, out); break;
+            case DMPM_F_DLDC_NEXT: download_planes(need_dbg(layers_[l].dbgCn), 9, out); break;
+            case DMPM_F_DLDFE:
+                if (!layers_[l].ctrl_grad) throw StateError{"tied controls: use dmpm_get_control_grad"};
+                download_planes(layers_[l].ctrl_grad, 9, out);
+                break;
+            default: throw ArgError{"unknown particle field"};
+        }
+    }
+
+    void set_layer_particles(int l, int field, const double* in) {
+        if (l < 0 || l >= L_) throw ArgError{"layer out of range"};
+        if (!in) throw ArgError{"in is NULL"};
+        switch (field) {
+            case DMPM_F_DFC: upload_planes(in, 9, layers_[l].dfc); break;
+            case DMPM_F_X: case DMPM_F_V: case DMPM_F_F: case DMPM_F_C: {
+                if (!layers_[l].st) throw StateError{"layer state is not stored (checkpointing)"};
+                const int off = field == DMPM_F_X ? PX : field == DMPM_F_V ? PV : field == DMPM_F_F ? PF : PC;
+                upload_planes(in, (field == DMPM_F_X || field == DMPM_F_V) ? 3 : 9, layers_[l].st + (size_t)off * np_);
+                break;
+            }
+            default: throw ArgError{"field cannot be set per layer"};
+        }
+    }
+
+    void get_control_grad(int l, double* out) {
+        if (!out) throw ArgError{"out is NULL"};
+        if (ctrl_acc_) {
+            double* s = staging((size_t)n_ * 9);
+            k_pack_acc<T><<<(unsigned)(((size_t)n_ * 9 + 255) / 256), 256, 0, ctx_->stream>>>(ctrl_acc_, np_, n_, s);
+            launched();
+            DMPM_CK(cudaMemcpyAsync(out, s, (size_t)n_ * 9 * sizeof(double), cudaMemcpyDeviceToHost, ctx_->stream));
+            DMPM_CK(cudaStreamSynchronize(ctx_->stream));
+            return;
+        }
+        if (l < 0 || l >= L_) throw ArgError{"layer out of range"};
+        download_planes(layers_[l].ctrl_grad, 9, out);
+    }
+
+    double dldf_norm(int l) {
+        const T* a = nullptr;
+        if (l < 0 || l >= L_) throw ArgError{"layer out of range"};
+        if (layers_[l].adj) a = layers_[l].adj;
+        else if (l == backward_lo_ || l == L_ - 1) a = adj_of(l, false);
+        else throw StateError{"adjoint of this layer is not kept"};
+        DMPM_CK(cudaMemsetAsync(loss_acc_ + 1, 0, sizeof(double), ctx_->stream));
+        k_sqnorm9<T><<<pgrid(), block(), 0, ctx_->stream>>>(a + (size_t)PF * np_, np_, n_, loss_acc_ + 1);
+        launched();
+        DMPM_CK(cudaMemcpyAsync((char*)host_misc_ + 16, loss_acc_ + 1, sizeof(double), cudaMemcpyDeviceToHost, ctx_->stream));
+        DMPM_CK(cudaStreamSynchronize(ctx_->stream));
+        return std::sqrt(*(double*)((char*)host_misc_ + 16));
+    }
+
+    void get_grid(int l, int field, double* out) {
+        if (l < 0 || l >= L_) throw ArgError{"layer out of range"};
+        if (!out) throw ArgError{"out is NULL"};
+        const dmpm_params& P = ctx_->prm;
+        if (field == DMPM_G_M || field == DMPM_G_V || field == DMPM_G_P) {
+            node4<T>* g = nullptr;
+            if (l == L_ - 1) g = (k_ == 1) ? layers_[l].grid : scratch_grid_;
+            else {
+                g = grid_of(l);
+                if (!g) {
+                    materialize_segment(l - l % k_);
+                    g = grid_of(l);
+                }
+            }
+            double* s = staging(3 * G_);
+            k_grid_field<T><<<ggrid(), 256, 0, ctx_->stream>>>(g, G_, field, P.dt, P.f_ext[0], P.f_ext[1], P.f_ext[2], s);
+            launched();
+            const size_t cnt = (field == DMPM_G_M) ? G_ : 3 * G_;
+            DMPM_CK(cudaMemcpyAsync(out, s, cnt * sizeof(double), cudaMemcpyDeviceToHost, ctx_->stream));
+            DMPM_CK(cudaStreamSynchronize(ctx_->stream));
+            return;
+        }
+        if (field == DMPM_G_DLDM && l == L_ - 1) {
+            double* s = staging(G_);
+            k_scalar_field<T><<<ggrid(), 256, 0, ctx_->stream>>>(dldm_, G_, s);
+            launched();
+            DMPM_CK(cudaMemcpyAsync(out, s, G_ * sizeof(double), cudaMemcpyDeviceToHost, ctx_->stream));
+            DMPM_CK(cudaStreamSynchronize(ctx_->stream));
+            return;
+        }
+        const node4<T>* g = nullptr;
+        int comp = 3;
+        if (field == DMPM_G_DLDV) g = layers_[l].dbggdv;
+        else if (field == DMPM_G_DLDP) g = layers_[l].dbggdp;
+        else if (field == DMPM_G_DLDM) { g = layers_[l].dbggdp; comp = 4; }
+        else throw ArgError{"unknown grid field"};
+        if (!g) throw StateError{"grid adjoints are not kept (set keep_intermediates)"};
+        double* s = staging(3 * G_);
+        k_node4_field<T><<<ggrid(), 256, 0, ctx_->stream>>>(g, G_, comp, s);
+        launched();
+        DMPM_CK(cudaMemcpyAsync(out, s, (comp == 3 ? 3 : 1) * G_ * sizeof(double), cudaMemcpyDeviceToHost, ctx_->stream));
+        DMPM_CK(cudaStreamSynchronize(ctx_->stream));
+    }
+
+    void get_points_ref(int l, void* pts) {
+        if (!pts) throw ArgError{"points is NULL"};
+        float* mp = (float*)pts;
+        std::vector<double> buf((size_t)n_ * 9);
+        auto put = [&](int field, int off, int width) {
+            get_particles(l, field, buf.data());
+            for (int p = 0; p < n_; p++)
+                for (int q = 0; q < width; q++) mp[(size_t)p * 118 + off + q] = (float)buf[(size_t)p * width + q];
+        };
+        put(DMPM_F_X, 0, 3);
+        put(DMPM_F_V, 3, 3);
+        put(DMPM_F_F, 6, 9);
+        put(DMPM_F_C, 15, 9);
+        put(DMPM_F_M, 33, 1);
+        put(DMPM_F_VOL, 34, 1);
+        put(DMPM_F_LAM, 35, 1);
+        put(DMPM_F_MU, 36, 1);
+        put(DMPM_F_DFC, 37, 9);
+        if (layers_[l].adj || l == backward_lo_ || (l == L_ - 1 && loss_done_)) {
+            put(DMPM_F_DLDX, 46, 3);
+            put(DMPM_F_DLDV, 49, 3);
+            put(DMPM_F_DLDF, 52, 9);
+            put(DMPM_F_DLDC, 61, 9);
+        }
+    }
+
+    void info(int64_t* out, int count) const {
+        const int64_t v[] = {n_, geo_.dim[0], geo_.dim[1], geo_.dim[2], L_, ctx_->precision, k_,
+                             (int64_t)(scene_arena_.bytes() + scene_arena_grid_.bytes() + layer_arena_.bytes() +
+                                       staging_arena_.bytes() + misc_arena_.bytes()),
+                             ctx_->launches, (int64_t)last_status_};
+        for (int i = 0; i < count && i < (int)(sizeof(v) / sizeof(v[0])); i++) out[i] = v[i];
+    }
+
+    unsigned last_status() const { return last_status_; }
+
+    ~Engine() override {
+        if (host_misc_) cudaFreeHost(host_misc_);
+    }
+
+   private:
+    struct LayerSlots {
+        T* st = nullptr;
+        node4<T>* grid = nullptr;
+        T* dfc = nullptr;
+        T* ctrl_grad = nullptr;
+        T* adj = nullptr;
+        T* dbgP = nullptr;
+        T* dbgdLdP = nullptr;
+        T* dbgvn = nullptr;
+        T* dbgCn = nullptr;
+        node4<T>* dbggdv = nullptr;
+        node4<T>* dbggdp = nullptr;
+    };
+
+    dmpm_ctx* ctx_;
+    GridGeom geo_{};
+    size_t G_ = 0;
+    bool grid_set_ = false;
+    int n_ = 0;
+    size_t np_ = 0;
+    Arena scene_arena_, scene_arena_grid_, layer_arena_, staging_arena_, misc_arena_;
+    T* cst_ = nullptr;
+    T* st0_ = nullptr;
+    T* dfc0_ = nullptr;
+    T* target_ = nullptr;
+    T* dldm_ = nullptr;
+    node4<T>* scratch_grid_ = nullptr;
+    double* staging_ = nullptr;
+    size_t staging_count_ = 0;
+    unsigned* status_ = nullptr;
+    double* loss_acc_ = nullptr;
+    void* host_misc_ = nullptr;
+    int L_ = 0, k_ = 1;
+    std::vector<LayerSlots> layers_;
+    T* ring_[2] = {nullptr, nullptr};
+    std::vector<T*> seg_st_;
+    std::vector<node4<T>*> seg_grid_;
+    int seg_lo_ = -1, seg_hi_ = -1;
+    T* adj_pp_[2] = {nullptr, nullptr};
+    node4<T>* gadj_ = nullptr;
+    node4<T>* gadj2_ = nullptr;
+    T* gridv_ = nullptr;
+    T* pscratch_ = nullptr;
+    double* ctrl_acc_ = nullptr;
+    bool forward_done_ = false, loss_done_ = false;
+    int backward_lo_ = 0;
+    unsigned last_status_ = 0;
+};
+
+template <class Fn> int guarded(dmpm_ctx* ctx, Fn fn) {
+    if (!ctx) return DMPM_ERR_ARG;
+    try {
+        if (cudaSetDevice(ctx->device) != cudaSuccess) {
+            ctx->err = "cudaSetDevice failed";
+            return DMPM_ERR_CUDA;
+        }
+        return fn();
+    } catch (const CudaError& e) {
+        ctx->err = e.what;
+        return e.code == cudaErrorMemoryAllocation ? DMPM_ERR_OOM : DMPM_ERR_CUDA;
+    } catch (const ArgError& e) {
+        ctx->err = e.what;
+        return DMPM_ERR_ARG;
+    } catch (const StateError& e) {
+        ctx->err = e.what;
+        return DMPM_ERR_STATE;
+    } catch (const std::bad_alloc&) {
+        ctx->err = "host allocation failed";
+        return DMPM_ERR_OOM;
+    }
+}
+
+template <class Fn> int with_engine(dmpm_ctx* ctx, Fn fn) {
+    return guarded(ctx, [&]() -> int {
+        if (ctx->precision == DMPM_FP64) return fn(*static_cast<Engine<double>*>(ctx->eng.get()));
+        return fn(*static_cast<Engine<float>*>(ctx->eng.get()));
+    });
+}
+
+}  // namespace
+
+// ====================================================================== C ABI
+extern "C" {
+
+void dmpm_default_params(dmpm_params* p) {
+    if (!p) return;
+    std::memset(p, 0, sizeof(*p));
+    p->dt = 1.0 / 120.0;  // CompGraph.h:56-58 defaults
+    p->drag = 0.5;
+    p->smoothing = 0.1;
+    p->adjoint_mode = DMPM_ADJ_REFCOMPAT;
+    p->control_mode = DMPM_CTRL_PER_LAYER;
+    p->loss_kind = DMPM_LOSS_REF_LOGMASS;
+}
+
+int dmpm_create(int device, int precision, dmpm_ctx** out) {
+    if (!out) return DMPM_ERR_ARG;
+    *out = nullptr;
+    if (precision != DMPM_FP64 && precision != DMPM_FP32_MIXED) return DMPM_ERR_ARG;
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || device < 0 || device >= ndev) {
+        cudaGetLastError();
+        return DMPM_ERR_CUDA;
+    }
+    dmpm_ctx* c = new dmpm_ctx();
+    c->device = device;
+    c->precision = precision;
+    dmpm_default_params(&c->prm);
+    if (cudaSetDevice(device) != cudaSuccess || cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess) {
+        delete c;
+        return DMPM_ERR_CUDA;
+    }
+    if (precision == DMPM_FP64) c->eng.reset(new Engine<double>(c));
+    else c->eng.reset(new Engine<float>(c));
+    *out = c;
+    return DMPM_OK;
+}
+
+int dmpm_destroy(dmpm_ctx* ctx) {
+    if (!ctx) return DMPM_ERR_ARG;
+    cudaSetDevice(ctx->device);
+    cudaStreamSynchronize(ctx->stream);
+    ctx->eng.reset();
+    cudaStreamDestroy(ctx->stream);
+    delete ctx;
+    return DMPM_OK;
+}
+
+const char* dmpm_last_error(const dmpm_ctx* ctx) { return ctx ? ctx->err.c_str() : "null context"; }
+
+int dmpm_get_info(const dmpm_ctx* ctx, int64_t* info, int count) {
+    if (!ctx || !info) return DMPM_ERR_ARG;
+    if (ctx->precision == DMPM_FP64) static_cast<Engine<double>*>(ctx->eng.get())->info(info, count);
+    else static_cast<Engine<float>*>(ctx->eng.get())->info(info, count);
+    return DMPM_OK;
+}
+
+int dmpm_set_grid(dmpm_ctx* ctx, int dim_x, int dim_y, int dim_z, double dx, const double* min_point) {
+    return with_engine(ctx, [&](auto& e) { e.set_grid(dim_x, dim_y, dim_z, dx, min_point); return DMPM_OK; });
+}
+
+int dmpm_set_params(dmpm_ctx* ctx, const dmpm_params* p) {
+    if (!ctx || !p) return DMPM_ERR_ARG;
+    if (!(p->dt >= 0) || p->adjoint_mode < 0 || p->adjoint_mode > 1 || p->control_mode < 0 || p->control_mode > 1 ||
+        p->loss_kind < 0 || p->loss_kind > 1 || p->checkpoint_every < 0 || p->block_size < 0 || p->block_size > 256 ||
+        (p->block_size % 32) != 0 || p->tile_cap < 0 || p->tile_cap > 1536) {
+        ctx->err = "invalid dmpm_params";
+        return DMPM_ERR_ARG;
+    }
+    ctx->prm = *p;
+    return DMPM_OK;
+}
+
+int dmpm_set_particles(dmpm_ctx* ctx, int n, const double* x, const double* v, const double* F, const double* C,
+                       const double* dFc, const double* m, const double* vol, const double* lam, const double* mu) {
+    return with_engine(ctx, [&](auto& e) { e.set_particles(n, x, v, F, C, dFc, m, vol, lam, mu); return DMPM_OK; });
+}
+
+int dmpm_set_points_ref(dmpm_ctx* ctx, const void* points, int n) {
+    return with_engine(ctx, [&](auto& e) { e.set_points_ref(points, n); return DMPM_OK; });
+}
+
+int dmpm_compute_volumes(dmpm_ctx* ctx) {
+    return with_engine(ctx, [&](auto& e) { e.compute_volumes(); return DMPM_OK; });
+}
+
+int dmpm_set_target_mass(dmpm_ctx* ctx, const double* target_m) {
+    if (!target_m) return DMPM_ERR_ARG;
+    return with_engine(ctx, [&](auto& e) { e.set_target_mass(target_m); return DMPM_OK; });
+}
+
+int dmpm_rasterize_target(dmpm_ctx* ctx, int n, const double* x, double point_mass) {
+    return with_engine(ctx, [&](auto& e) { e.rasterize_target(n, x, point_mass); return DMPM_OK; });
+}
+
+int dmpm_setup(dmpm_ctx* ctx, int num_layers) {
+    return with_engine(ctx, [&](auto& e) { e.setup(num_layers); return DMPM_OK; });
+}
+
+int dmpm_forward(dmpm_ctx* ctx, int start_layer) {
+    return with_engine(ctx, [&](auto& e) {
+        e.forward(start_layer);
+        return (e.last_status() & ST_NONFINITE_FWD) ? DMPM_ERR_NONFINITE : DMPM_OK;
+    });
+}
+
+int dmpm_loss(dmpm_ctx* ctx, double* loss) {
+    return with_engine(ctx, [&](auto& e) {
+        const double L = e.loss();
+        if (loss) *loss = L;
+        return (e.last_status() & ST_NONFINITE_LOSS) ? DMPM_ERR_NONFINITE : DMPM_OK;
+    });
+}
+
+int dmpm_backward(dmpm_ctx* ctx, int control_layer) {
+    return with_engine(ctx, [&](auto& e) {
+        e.backward(control_layer);
+        return (e.last_status() & ST_NONFINITE_ADJ) ? DMPM_ERR_NONFINITE : DMPM_OK;
+    });
+}
+
+int dmpm_get_particles(dmpm_ctx* ctx, int layer, int field, double* out) {
+    return with_engine(ctx, [&](auto& e) { e.get_particles(layer, field, out); return DMPM_OK; });
+}
+
+int dmpm_set_layer_particles(dmpm_ctx* ctx, int layer, int field, const double* in) {
+    return with_engine(ctx, [&](auto& e) { e.set_layer_particles(layer, field, in); return DMPM_OK; });
+}
+
+int dmpm_get_grid(dmpm_ctx* ctx, int layer, int field, double* out) {
+    return with_engine(ctx, [&](auto& e) { e.get_grid(layer, field, out); return DMPM_OK; });
+}
+
+int dmpm_get_control_grad(dmpm_ctx* ctx, int layer, double* out) {
+    return with_engine(ctx, [&](auto& e) { e.get_control_grad(layer, out); return DMPM_OK; });
+}
+
+int dmpm_dldf_norm(dmpm_ctx* ctx, int layer, double* norm) {
+    if (!norm) return DMPM_ERR_ARG;
+    return with_engine(ctx, [&](auto& e) { *norm = e.dldf_norm(layer); return DMPM_OK; });
+}
+
+int dmpm_get_points_ref(dmpm_ctx* ctx, int layer, void* points) {
+    return with_engine(ctx, [&](auto& e) { e.get_points_ref(layer, points); return DMPM_OK; });
+}
+
+int dmpm_synchronize(dmpm_ctx* ctx) {
+    return guarded(ctx, [&]() { DMPM_CK(cudaStreamSynchronize(ctx->stream)); return DMPM_OK; });
+}
+
+void* dmpm_stream(dmpm_ctx* ctx) { return ctx ? (void*)ctx->stream : nullptr; }
+
+int64_t dmpm_launch_count(const dmpm_ctx* ctx) { return ctx ? ctx->launches : -1; }
+
+}  // extern "C"

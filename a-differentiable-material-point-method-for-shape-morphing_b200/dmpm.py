@@ -1,0 +1,303 @@
+"""Python binding of libdmpm.so (include/dmpm.h) over ctypes.
+
+This is plumbing for tests and the benchmark; the engine and its C ABI are
+the product.  There is no CPU fallback: importing works anywhere, but
+creating a Context raises DmpmError when the CUDA library or a GPU is missing.
+
+Matrices are numpy (N, 3, 3) arrays indexed [p, row, col]; they are converted
+to the ABI's column-major layout here.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+from typing import Optional, Sequence
+
+import numpy as np
+
+PKG_DIR = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(PKG_DIR, "libdmpm.so")
+
+# status codes / enums of include/dmpm.h
+OK, ERR_ARG, ERR_OOM, ERR_CUDA, ERR_NONFINITE, ERR_STATE = 0, 1, 2, 3, 4, 5
+FP64, FP32_MIXED = 0, 1
+ADJ_REFCOMPAT, ADJ_EXACT = 0, 1
+CTRL_PER_LAYER, CTRL_TIED = 0, 1
+LOSS_REF_LOGMASS, LOSS_L2 = 0, 1
+
+FIELDS = {"x": 0, "v": 1, "F": 2, "C": 3, "P": 4, "m": 5, "vol": 6, "lam": 7, "mu": 8, "dFc": 9, "dLdx": 10,
+          "dLdv": 11, "dLdF": 12, "dLdC": 13, "dLdP": 14, "dLdv_next": 15, "dLdC_next": 16, "dLdFe": 19}
+WIDTH = {"x": 3, "v": 3, "F": 9, "C": 9, "P": 9, "m": 1, "vol": 1, "lam": 1, "mu": 1, "dFc": 9, "dLdx": 3,
+         "dLdv": 3, "dLdF": 9, "dLdC": 9, "dLdP": 9, "dLdv_next": 3, "dLdC_next": 9, "dLdFe": 9}
+GRID_FIELDS = {"grid_m": 0, "grid_v": 1, "grid_p": 2, "grid_dLdv": 3, "grid_dLdp": 4, "grid_dLdm": 5}
+GRID_WIDTH = {"grid_m": 1, "grid_v": 3, "grid_p": 3, "grid_dLdv": 3, "grid_dLdp": 3, "grid_dLdm": 1}
+
+
+class DmpmError(RuntimeError):
+    def __init__(self, status: int, message: str):
+        super().__init__("dmpm status %d: %s" % (status, message))
+        self.status = status
+
+
+class Params(ctypes.Structure):
+    _fields_ = [("dt", ctypes.c_double), ("drag", ctypes.c_double), ("f_ext", ctypes.c_double * 3),
+                ("smoothing", ctypes.c_double), ("adjoint_mode", ctypes.c_int), ("control_mode", ctypes.c_int),
+                ("loss_kind", ctypes.c_int), ("checkpoint_every", ctypes.c_int), ("keep_adjoints", ctypes.c_int),
+                ("keep_intermediates", ctypes.c_int), ("block_size", ctypes.c_int), ("tile_cap", ctypes.c_int)]
+
+
+_P = ctypes.c_void_p
+_lib = None
+
+
+def load_library(path: str = LIB_PATH) -> ctypes.CDLL:
+    """Load libdmpm.so; raises if it has not been built (no fallback)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(path):
+        raise DmpmError(ERR_CUDA, "libdmpm.so not built at %s (run __graft_entry__.build())" % path)
+    L = ctypes.CDLL(path)
+    L.dmpm_create.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.POINTER(_P)]
+    L.dmpm_destroy.argtypes = [_P]
+    L.dmpm_last_error.argtypes = [_P]
+    L.dmpm_last_error.restype = ctypes.c_char_p
+    L.dmpm_get_info.argtypes = [_P, ctypes.POINTER(ctypes.c_int64), ctypes.c_int]
+    L.dmpm_set_grid.argtypes = [_P, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_double, _P]
+    L.dmpm_set_params.argtypes = [_P, ctypes.POINTER(Params)]
+    L.dmpm_default_params.argtypes = [ctypes.POINTER(Params)]
+    L.dmpm_default_params.restype = None
+    L.dmpm_set_particles.argtypes = [_P, ctypes.c_int] + [_P] * 9
+    L.dmpm_set_points_ref.argtypes = [_P, _P, ctypes.c_int]
+    L.dmpm_compute_volumes.argtypes = [_P]
+    L.dmpm_set_target_mass.argtypes = [_P, _P]
+    L.dmpm_rasterize_target.argtypes = [_P, ctypes.c_int, _P, ctypes.c_double]
+    L.dmpm_setup.argtypes = [_P, ctypes.c_int]
+    L.dmpm_forward.argtypes = [_P, ctypes.c_int]
+    L.dmpm_loss.argtypes = [_P, ctypes.POINTER(ctypes.c_double)]
+    L.dmpm_backward.argtypes = [_P, ctypes.c_int]
+    L.dmpm_get_particles.argtypes = [_P, ctypes.c_int, ctypes.c_int, _P]
+    L.dmpm_set_layer_particles.argtypes = [_P, ctypes.c_int, ctypes.c_int, _P]
+    L.dmpm_get_grid.argtypes = [_P, ctypes.c_int, ctypes.c_int, _P]
+    L.dmpm_get_control_grad.argtypes = [_P, ctypes.c_int, _P]
+    L.dmpm_dldf_norm.argtypes = [_P, ctypes.c_int, ctypes.POINTER(ctypes.c_double)]
+    L.dmpm_get_points_ref.argtypes = [_P, ctypes.c_int, _P]
+    L.dmpm_synchronize.argtypes = [_P]
+    L.dmpm_stream.argtypes = [_P]
+    L.dmpm_stream.restype = _P
+    L.dmpm_launch_count.argtypes = [_P]
+    L.dmpm_launch_count.restype = ctypes.c_int64
+    _lib = L
+    return L
+
+
+def _cm(M) -> np.ndarray:
+    return np.ascontiguousarray(np.asarray(M, dtype=np.float64).transpose(0, 2, 1).reshape(-1, 9))
+
+
+def _from_cm(a) -> np.ndarray:
+    return a.reshape(-1, 3, 3).transpose(0, 2, 1)
+
+
+def _ptr(a) -> Optional[int]:
+    """numpy array, torch tensor (data_ptr) or raw int -> address."""
+    if a is None:
+        return None
+    if isinstance(a, int):
+        return a
+    if hasattr(a, "data_ptr"):
+        return a.data_ptr()
+    return a.ctypes.data
+
+
+class Context:
+    """One engine context (one scene, one stream) on one GPU."""
+
+    def __init__(self, precision: str = "fp32", device: int = 0):
+        self.lib = load_library()
+        self.precision = FP64 if precision in ("fp64", FP64) else FP32_MIXED
+        h = _P()
+        st = self.lib.dmpm_create(device, self.precision, ctypes.byref(h))
+        if st != OK:
+            raise DmpmError(st, "dmpm_create(device=%d) failed (no CUDA device?)" % device)
+        self.h = h
+        self.n = 0
+        self.dims = (0, 0, 0)
+        self.num_layers = 0
+        self._keep = []
+
+    # -------------------------------------------------------------- plumbing
+    def _ck(self, st: int, what: str, allow_nonfinite: bool = False) -> int:
+        if st == OK or (allow_nonfinite and st == ERR_NONFINITE):
+            return st
+        msg = self.lib.dmpm_last_error(self.h)
+        raise DmpmError(st, "%s: %s" % (what, msg.decode() if msg else ""))
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.lib.dmpm_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def info(self) -> dict:
+        buf = (ctypes.c_int64 * 10)()
+        self.lib.dmpm_get_info(self.h, buf, 10)
+        keys = ["n", "dim_x", "dim_y", "dim_z", "layers", "precision", "checkpoint_every", "device_bytes",
+                "launches", "status"]
+        return dict(zip(keys, list(buf)))
+
+    @property
+    def launch_count(self) -> int:
+        return int(self.lib.dmpm_launch_count(self.h))
+
+    @property
+    def stream(self) -> int:
+        return int(self.lib.dmpm_stream(self.h) or 0)
+
+    def synchronize(self):
+        self._ck(self.lib.dmpm_synchronize(self.h), "synchronize")
+
+    # -------------------------------------------------------------- setup
+    def set_grid(self, dims: Sequence[int], dx: float = 1.0, min_point=(0.0, 0.0, 0.0)):
+        mn = np.ascontiguousarray(min_point, dtype=np.float64)
+        self._ck(self.lib.dmpm_set_grid(self.h, int(dims[0]), int(dims[1]), int(dims[2]), float(dx), mn.ctypes.data),
+                 "set_grid")
+        self.dims = tuple(int(d) for d in dims)
+
+    def set_params(self, dt: float, drag: float = 0.0, f_ext=(0.0, 0.0, 0.0), smoothing: float = 0.0,
+                   adjoint: str = "refcompat", control: str = "per_layer", loss: str = "ref",
+                   checkpoint_every: int = 0, keep_adjoints: bool = False, keep_intermediates: bool = False,
+                   block_size: int = 0, tile_cap: int = 0):
+        p = Params()
+        self.lib.dmpm_default_params(ctypes.byref(p))
+        p.dt, p.drag, p.smoothing = float(dt), float(drag), float(smoothing)
+        for i in range(3):
+            p.f_ext[i] = float(f_ext[i])
+        p.adjoint_mode = ADJ_EXACT if adjoint == "exact" else ADJ_REFCOMPAT
+        p.control_mode = CTRL_TIED if control == "tied" else CTRL_PER_LAYER
+        p.loss_kind = LOSS_L2 if loss == "l2" else LOSS_REF_LOGMASS
+        p.checkpoint_every = int(checkpoint_every)
+        p.keep_adjoints = int(bool(keep_adjoints))
+        p.keep_intermediates = int(bool(keep_intermediates))
+        p.block_size = int(block_size)
+        p.tile_cap = int(tile_cap)
+        self._ck(self.lib.dmpm_set_params(self.h, ctypes.byref(p)), "set_params")
+        self.params = p
+
+    def set_particles(self, x, m, lam, mu, v=None, F=None, C=None, dFc=None, vol=None):
+        n = int(np.asarray(x).shape[0])
+        arrs = {
+            "x": np.ascontiguousarray(x, dtype=np.float64),
+            "v": None if v is None else np.ascontiguousarray(v, dtype=np.float64),
+            "F": None if F is None else _cm(F),
+            "C": None if C is None else _cm(C),
+            "dFc": None if dFc is None else _cm(dFc),
+            "m": np.ascontiguousarray(m, dtype=np.float64),
+            "vol": None if vol is None else np.ascontiguousarray(vol, dtype=np.float64),
+            "lam": np.ascontiguousarray(lam, dtype=np.float64),
+            "mu": np.ascontiguousarray(mu, dtype=np.float64),
+        }
+        self._set_particles_raw(n, **arrs)
+
+    def _set_particles_raw(self, n, x, v, F, C, dFc, m, vol, lam, mu):
+        """Upload already laid-out host buffers (numpy, torch or int pointers)."""
+        st = self.lib.dmpm_set_particles(self.h, n, _ptr(x), _ptr(v), _ptr(F), _ptr(C), _ptr(dFc), _ptr(m),
+                                         _ptr(vol), _ptr(lam), _ptr(mu))
+        self._ck(st, "set_particles")
+        self.n = n
+
+    def set_points_ref(self, points: np.ndarray):
+        """points: float32 array (N, 118) in the reference MaterialPoint layout."""
+        pts = np.ascontiguousarray(points, dtype=np.float32)
+        self._ck(self.lib.dmpm_set_points_ref(self.h, pts.ctypes.data, pts.shape[0]), "set_points_ref")
+        self.n = pts.shape[0]
+
+    def compute_volumes(self):
+        self._ck(self.lib.dmpm_compute_volumes(self.h), "compute_volumes")
+
+    def set_target_mass(self, m):
+        a = np.ascontiguousarray(m, dtype=np.float64)
+        self._ck(self.lib.dmpm_set_target_mass(self.h, a.ctypes.data), "set_target_mass")
+
+    def rasterize_target(self, points, point_mass: float):
+        a = np.ascontiguousarray(points, dtype=np.float64)
+        self._ck(self.lib.dmpm_rasterize_target(self.h, a.shape[0], a.ctypes.data, float(point_mass)),
+                 "rasterize_target")
+
+    def load_scene(self, scene, with_volumes: bool = True, with_target: bool = True):
+        """Grid, particles, volumes (CalculatePointCloudVolumes) and target raster of a scenes.Scene."""
+        self.set_grid(scene.dims, scene.dx, scene.min_point)
+        self.set_particles(scene.x, scene.m, scene.lam, scene.mu, v=scene.v, F=scene.F, C=scene.C, dFc=scene.dFc,
+                           vol=scene.vol)
+        if with_volumes:
+            self.compute_volumes()
+        if with_target:
+            self.rasterize_target(scene.target_points, scene.target_mp)
+
+    # -------------------------------------------------------------- graph
+    def setup(self, num_layers: int):
+        self._ck(self.lib.dmpm_setup(self.h, int(num_layers)), "setup")
+        self.num_layers = int(num_layers)
+
+    def forward(self, start_layer: int = 0, allow_nonfinite: bool = True) -> int:
+        return self._ck(self.lib.dmpm_forward(self.h, int(start_layer)), "forward", allow_nonfinite)
+
+    def loss(self, allow_nonfinite: bool = True) -> float:
+        out = ctypes.c_double()
+        self._ck(self.lib.dmpm_loss(self.h, ctypes.byref(out)), "loss", allow_nonfinite)
+        return float(out.value)
+
+    def backward(self, control_layer: int = 0, allow_nonfinite: bool = True) -> int:
+        return self._ck(self.lib.dmpm_backward(self.h, int(control_layer)), "backward", allow_nonfinite)
+
+    # -------------------------------------------------------------- reads / writes
+    def get(self, layer: int, field: str) -> np.ndarray:
+        w = WIDTH[field]
+        out = np.empty(self.n * w, dtype=np.float64)
+        self._ck(self.lib.dmpm_get_particles(self.h, int(layer), FIELDS[field], out.ctypes.data), "get " + field)
+        if w == 9:
+            return _from_cm(out)
+        if w == 3:
+            return out.reshape(-1, 3)
+        return out
+
+    def set_layer(self, layer: int, field: str, value):
+        a = _cm(value) if WIDTH[field] == 9 else np.ascontiguousarray(value, dtype=np.float64)
+        self._ck(self.lib.dmpm_set_layer_particles(self.h, int(layer), FIELDS[field], a.ctypes.data), "set " + field)
+
+    def get_grid(self, layer: int, field: str) -> np.ndarray:
+        G = int(np.prod(self.dims))
+        w = GRID_WIDTH[field]
+        out = np.empty(G * w, dtype=np.float64)
+        self._ck(self.lib.dmpm_get_grid(self.h, int(layer), GRID_FIELDS[field], out.ctypes.data), "grid " + field)
+        return out.reshape(-1, 3) if w == 3 else out
+
+    def control_grad(self, layer: int = 0, out=None) -> np.ndarray:
+        """dL/d dFc as (N, 3, 3); `out` may be a (pinned) buffer of N*9 doubles (returned column-major)."""
+        if out is not None:
+            self._ck(self.lib.dmpm_get_control_grad(self.h, int(layer), _ptr(out)), "control_grad")
+            return out
+        a = np.empty(self.n * 9, dtype=np.float64)
+        self._ck(self.lib.dmpm_get_control_grad(self.h, int(layer), a.ctypes.data), "control_grad")
+        return _from_cm(a)
+
+    def dldf_norm(self, layer: int = 0) -> float:
+        out = ctypes.c_double()
+        self._ck(self.lib.dmpm_dldf_norm(self.h, int(layer), ctypes.byref(out)), "dldf_norm")
+        return float(out.value)
+
+    def get_points_ref(self, layer: int, points: np.ndarray) -> np.ndarray:
+        assert points.dtype == np.float32 and points.shape == (self.n, 118) and points.flags.c_contiguous
+        self._ck(self.lib.dmpm_get_points_ref(self.h, int(layer), points.ctypes.data), "get_points_ref")
+        return points

@@ -1,0 +1,176 @@
+/*
+ * dmpm.h -- C ABI of the B200 MLS-MPM forward + adjoint engine (libdmpm.so).
+ *
+ * This ABI replaces, for one caller thread, the hot-path entry points of the
+ * reference library DiffMPMLib3D (paths relative to that project):
+ *
+ *   dmpm_set_particles / dmpm_set_points_ref
+ *                          <- CompGraph::CompGraph(initial_point_cloud, grid, target)
+ *                             deep copy of the initial PointCloud          (CompGraph.h:20, CompGraph.cpp:269-278)
+ *   dmpm_set_grid          <- Grid::Grid(dim_x, dim_y, dim_z, dx, min_point) (Grid.h:11, Grid.cpp:3-28)
+ *   dmpm_set_target_mass / dmpm_rasterize_target
+ *                          <- CompGraph::target_grid, built by LoadCompGraph as a
+ *                             mass-only P2G of target samples             (CompGraph.h:52, MPMPolyscope.cpp:155-160)
+ *   dmpm_compute_volumes   <- SingleThreadMPM::CalculatePointCloudVolumes   (ForwardSimulation.h:39, .cpp:262-290)
+ *   dmpm_set_params        <- the dt / drag / f_ext / smoothing_factor members that
+ *                             OptimizeDefGradControlSequence sets          (CompGraph.h:54-58, CompGraph.cpp:296-300)
+ *   dmpm_setup             <- CompGraph::SetUpCompGraph(num_layers)         (CompGraph.h:40, CompGraph.cpp:7-17)
+ *   dmpm_forward           <- CompGraph::ComputeForwardPass(start_layer), i.e. one
+ *                             SingleThreadMPM::ForwardTimeStep per layer   (CompGraph.h:44, CompGraph.cpp:246-256,
+ *                                                                           ForwardSimulation.h:17-18, .cpp:126-157)
+ *   dmpm_loss              <- CompGraph::EndLayerMassLoss()                 (CompGraph.h:42, CompGraph.cpp:110-244)
+ *   dmpm_backward          <- CompGraph::ComputeBackwardPass(control_layer), i.e. one
+ *                             Back_Timestep per layer                       (CompGraph.h:45, CompGraph.cpp:258-267,
+ *                                                                           BackPropagation.h:7, .cpp:6-125)
+ *   dmpm_get_particles / dmpm_get_points_ref / dmpm_set_layer_particles
+ *                          <- reads and writes of CompGraph::layers[i].point_cloud->points
+ *                                                                           (CompGraph.h:50, MaterialPoint.h:8-75)
+ *   dmpm_get_grid          <- reads of CompGraph::layers[i].grid->nodes     (GridNode.h:5-24)
+ *   dmpm_get_control_grad  <- MaterialPoint::dLdF of layer i, the gradient the
+ *                             reference optimisers descend                  (PointCloud.cpp:83-99)
+ *   dmpm_dldf_norm         <- PointCloud::Compute_dLdF_Norm                 (PointCloud.cpp:24-35)
+ *
+ * Conventions
+ *   - All functions return a status (DMPM_OK = 0); dmpm_last_error() gives the
+ *     message of the last failure on a context.
+ *   - Host arrays are double, one particle after another: vectors as 3 values,
+ *     3x3 matrices as 9 values in column-major order (Eigen::Matrix3f storage,
+ *     element (i, j) at [9p + i + 3j]).  Grid arrays use the reference's node
+ *     order (i * dim_y + j) * dim_z + k, vectors as 3 values per node.
+ *   - Host buffers may be pageable or pinned; pinned buffers make copies
+ *     asynchronous with respect to the host thread.
+ *   - A context owns one CUDA stream and its device memory.  It is not
+ *     thread-safe (the reference's CompGraph is not either).
+ *   - Units: the reference is only physically consistent with dx = 1 (its
+ *     particle volume is m / sum w m_g); callers use lattice units.
+ */
+#ifndef DMPM_H
+#define DMPM_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct dmpm_ctx dmpm_ctx;
+
+/* status codes */
+#define DMPM_OK 0
+#define DMPM_ERR_ARG 1       /* invalid argument or size */
+#define DMPM_ERR_OOM 2       /* device or pinned allocation failed */
+#define DMPM_ERR_CUDA 3      /* a CUDA runtime call failed */
+#define DMPM_ERR_NONFINITE 4 /* a stage produced NaN/inf (results still written, as the reference does) */
+#define DMPM_ERR_STATE 5     /* call order: e.g. backward before loss, or a layer that is not stored */
+
+/* precision paths */
+#define DMPM_FP64 0       /* plain FP64 path: one kernel per reference stage, global atomics */
+#define DMPM_FP32_MIXED 1 /* FP32 state and grid, shared-memory tiles; FP64 polar/SVD, stress
+                             derivative, loss and control-gradient sums */
+
+/* adjoint modes */
+#define DMPM_ADJ_REFCOMPAT 0 /* reproduces Back_Timestep term by term */
+#define DMPM_ADJ_EXACT 1     /* true derivative of the forward map */
+
+/* control (dFc) modes */
+#define DMPM_CTRL_PER_LAYER 0 /* one dFc per layer, as CompGraph::layers[i] */
+#define DMPM_CTRL_TIED 1      /* one dFc shared by every layer; gradient = sum over layers */
+
+/* loss kinds */
+#define DMPM_LOSS_REF_LOGMASS 0 /* EndLayerMassLoss: log-mass L2 + min-mass penalty */
+#define DMPM_LOSS_L2 1          /* 1/2 sum (m - t)^2 */
+
+/* particle fields (dmpm_get_particles / dmpm_set_layer_particles) */
+#define DMPM_F_X 0
+#define DMPM_F_V 1
+#define DMPM_F_F 2
+#define DMPM_F_C 3
+#define DMPM_F_P 4
+#define DMPM_F_M 5
+#define DMPM_F_VOL 6
+#define DMPM_F_LAM 7
+#define DMPM_F_MU 8
+#define DMPM_F_DFC 9
+#define DMPM_F_DLDX 10
+#define DMPM_F_DLDV 11
+#define DMPM_F_DLDF 12
+#define DMPM_F_DLDC 13
+#define DMPM_F_DLDP 14
+#define DMPM_F_DLDV_NEXT 15
+#define DMPM_F_DLDC_NEXT 16
+#define DMPM_F_DLDFE 19 /* dL/d dFc of the layer (EXACT: differs from dLdF when smoothing != 0) */
+
+/* grid fields (dmpm_get_grid) */
+#define DMPM_G_M 0
+#define DMPM_G_V 1
+#define DMPM_G_P 2
+#define DMPM_G_DLDV 3
+#define DMPM_G_DLDP 4
+#define DMPM_G_DLDM 5
+
+typedef struct {
+    double dt;               /* CompGraph::dt */
+    double drag;             /* CompGraph::drag */
+    double f_ext[3];         /* CompGraph::f_ext */
+    double smoothing;        /* CompGraph::smoothing_factor */
+    int adjoint_mode;        /* DMPM_ADJ_* */
+    int control_mode;        /* DMPM_CTRL_* */
+    int loss_kind;           /* DMPM_LOSS_* */
+    int checkpoint_every;    /* 0: keep every layer if it fits in HBM, else checkpoint;
+                                1: keep every layer; k > 1: keep layers 0, k, 2k, ... and the
+                                last, recompute the others during backward */
+    int keep_adjoints;       /* keep every layer's adjoint state readable after backward */
+    int keep_intermediates;  /* keep P, dLdP, dLdv_next, dLdC_next and grid adjoints per layer */
+    int block_size;          /* threads per CTA for particle kernels; 0 = default (256) */
+    int tile_cap;            /* max nodes of a shared-memory tile; 0 = default */
+} dmpm_params;
+
+void dmpm_default_params(dmpm_params* p);
+
+int dmpm_create(int device, int precision, dmpm_ctx** out);
+int dmpm_destroy(dmpm_ctx* ctx);
+const char* dmpm_last_error(const dmpm_ctx* ctx);
+int dmpm_get_info(const dmpm_ctx* ctx, int64_t* info, int count); /* n, dims, layers, precision,
+                                                                      checkpoint_every, device bytes, ... */
+
+int dmpm_set_grid(dmpm_ctx* ctx, int dim_x, int dim_y, int dim_z, double dx, const double* min_point);
+int dmpm_set_params(dmpm_ctx* ctx, const dmpm_params* params);
+
+/* Initial point cloud (layer 0).  dFc, vol may be NULL (zeros). */
+int dmpm_set_particles(dmpm_ctx* ctx, int n, const double* x, const double* v, const double* F,
+                       const double* C, const double* dFc, const double* m, const double* vol,
+                       const double* lam, const double* mu);
+/* Initial point cloud from an array of the reference's MaterialPoint structs
+ * (118 floats = 472 bytes each, field order of MaterialPoint.h:18-46). */
+int dmpm_set_points_ref(dmpm_ctx* ctx, const void* points, int n);
+
+int dmpm_compute_volumes(dmpm_ctx* ctx);
+int dmpm_set_target_mass(dmpm_ctx* ctx, const double* target_m);
+int dmpm_rasterize_target(dmpm_ctx* ctx, int n, const double* x, double point_mass);
+
+int dmpm_setup(dmpm_ctx* ctx, int num_layers);
+int dmpm_forward(dmpm_ctx* ctx, int start_layer);
+int dmpm_loss(dmpm_ctx* ctx, double* loss);
+int dmpm_backward(dmpm_ctx* ctx, int control_layer);
+
+int dmpm_get_particles(dmpm_ctx* ctx, int layer, int field, double* out);
+int dmpm_set_layer_particles(dmpm_ctx* ctx, int layer, int field, const double* in);
+int dmpm_get_grid(dmpm_ctx* ctx, int layer, int field, double* out);
+/* dL/d dFc: per-layer controls -> that layer's gradient; tied controls -> the
+ * sum over layers (layer ignored). */
+int dmpm_get_control_grad(dmpm_ctx* ctx, int layer, double* out);
+int dmpm_dldf_norm(dmpm_ctx* ctx, int layer, double* norm);
+/* Fill the state and gradient fields of an array of reference MaterialPoints for one layer. */
+int dmpm_get_points_ref(dmpm_ctx* ctx, int layer, void* points);
+
+int dmpm_synchronize(dmpm_ctx* ctx);
+/* The context's CUDA stream (cudaStream_t) for callers that order their own work after it. */
+void* dmpm_stream(dmpm_ctx* ctx);
+/* Number of kernels this context has launched since creation. */
+int64_t dmpm_launch_count(const dmpm_ctx* ctx);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* DMPM_H */

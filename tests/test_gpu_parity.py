@@ -1,0 +1,287 @@
+"""GPU parity: the engine through its C ABI against the reference's golden
+vectors (FP64 retyped reference) and the CPU oracle.
+
+Tolerances (relative, max-abs over the field / max-abs of the reference):
+  FP64 plain path vs FP64 reference:  1e-10 forward state, loss, volumes;
+                                      1e-9 for adjoint fields (float atomics
+                                      reorder sums; the reference's own polar
+                                      stops at 1024 eps).
+  FP32 mixed path vs FP64 oracle:     positions 1e-5, deformation 1e-4,
+                                      velocities/grid 1e-3, loss 1e-4,
+                                      exact control gradient 1e-3 (norm-relative).
+"""
+import numpy as np
+import pytest
+
+import dmpm
+import scenes
+from oracle.lib import OracleGraph
+from tests.golden.make_golden import ROLLOUT_LAYERS, rollout_scene
+from tests.helpers import load_golden, normrel, relerr
+
+pytestmark = pytest.mark.gpu
+
+
+def make_ctx(sc, prec, target, **params):
+    c = dmpm.Context(prec)
+    c.set_grid(sc.dims, sc.dx, sc.min_point)
+    c.set_particles(sc.x, sc.m, sc.lam, sc.mu, v=sc.v, F=sc.F, C=sc.C, dFc=sc.dFc, vol=sc.vol)
+    c.set_target_mass(target)
+    kw = dict(dt=sc.dt, drag=sc.drag, f_ext=sc.f_ext, smoothing=sc.smoothing)
+    kw.update(params)
+    c.set_params(**kw)
+    return c
+
+
+@pytest.fixture(scope="module")
+def g64():
+    return load_golden("rollout_f64")
+
+
+@pytest.fixture(scope="module")
+def golden_scene(g64):
+    sc = rollout_scene()
+    sc.vol = np.asarray(g64["vol"], dtype=np.float64)
+    return sc
+
+
+def test_volumes_and_target_raster(gpu_ready, g64):
+    sc = rollout_scene()
+    for prec, tol in (("fp64", 1e-12), ("fp32", 1e-5)):
+        with dmpm.Context(prec) as c:
+            c.set_grid(sc.dims, sc.dx, sc.min_point)
+            c.set_particles(sc.x, sc.m, sc.lam, sc.mu, v=sc.v, F=sc.F, C=sc.C, dFc=sc.dFc)
+            c.compute_volumes()
+            c.rasterize_target(sc.target_points, sc.target_mp)
+            c.set_params(dt=sc.dt)
+            c.setup(2)
+            assert relerr(c.get(0, "vol"), g64["vol"]) < tol
+            c.forward(0)
+            c.loss()
+            # the target raster is observable through dL/dm = f(m, target)
+            assert np.all(np.isfinite(c.get_grid(1, "grid_dLdm")))
+
+
+def test_fp64_forward_matches_reference(gpu_ready, g64, golden_scene):
+    sc = golden_scene
+    with make_ctx(sc, "fp64", g64["target"], keep_intermediates=True) as c:
+        c.setup(ROLLOUT_LAYERS)
+        assert c.forward(0) == dmpm.OK
+        for lay in range(ROLLOUT_LAYERS):
+            for k in ("x", "v", "F", "C"):
+                assert relerr(c.get(lay, k), g64["%s_%d" % (k, lay)]) < 1e-10, (k, lay)
+            if lay < ROLLOUT_LAYERS - 1:
+                assert relerr(c.get(lay, "P"), g64["P_%d" % lay]) < 1e-10, lay
+                assert relerr(c.get_grid(lay, "grid_m"), g64["grid_m_%d" % lay]) < 1e-12, lay
+                assert relerr(c.get_grid(lay, "grid_p"), g64["grid_p_%d" % lay]) < 1e-10, lay
+                assert relerr(c.get_grid(lay, "grid_v"), g64["grid_v_%d" % lay]) < 1e-10, lay
+        L = c.loss()
+        assert abs(L - float(g64["loss"])) / abs(float(g64["loss"])) < 1e-10
+        last = ROLLOUT_LAYERS - 1
+        assert relerr(c.get_grid(last, "grid_m"), g64["grid_m_%d" % last]) < 1e-12
+        assert relerr(c.get_grid(last, "grid_dLdm"), g64["grid_dLdm_%d" % last]) < 1e-10
+
+
+def test_fp64_refcompat_adjoint_matches_reference(gpu_ready, g64, golden_scene):
+    sc = golden_scene
+    with make_ctx(sc, "fp64", g64["target"], keep_adjoints=True, keep_intermediates=True) as c:
+        c.setup(ROLLOUT_LAYERS)
+        c.forward(0)
+        c.loss()
+        assert c.backward(0) == dmpm.OK
+        for lay in range(ROLLOUT_LAYERS):
+            for k in ("dLdx", "dLdv", "dLdF", "dLdC"):
+                assert relerr(c.get(lay, k), g64["%s_%d" % (k, lay)]) < 1e-9, (k, lay)
+        for lay in range(ROLLOUT_LAYERS - 1):
+            for k in ("dLdP", "dLdv_next", "dLdC_next"):
+                assert relerr(c.get(lay, k), g64["%s_%d" % (k, lay)]) < 1e-9, (k, lay)
+            for k in ("grid_dLdv", "grid_dLdp", "grid_dLdm"):
+                assert relerr(c.get_grid(lay, k), g64["%s_%d" % (k, lay)]) < 1e-9, (k, lay)
+        assert abs(c.dldf_norm(0) - np.linalg.norm(g64["dLdF_0"])) / np.linalg.norm(g64["dLdF_0"]) < 1e-9
+
+
+def _oracle(sc, L, mode, prec="f64", target=None, control="per_layer"):
+    o = OracleGraph(sc, prec, target_m=target)
+    o.setup(L, sc.dt, sc.drag, sc.f_ext, sc.smoothing)
+    o.forward(0)
+    loss = o.loss()
+    o.backward(0, mode)
+    return o, loss
+
+
+@pytest.fixture(scope="module")
+def exact_case():
+    sc = scenes.small_scene(seed=5, res=16, steps=6, v_std=0.4, drag=0.2, smoothing=0.1, f_ext=(0.0, -1.0, 0.0),
+                            dt=2e-4)
+    o = OracleGraph(sc, "f64")
+    sc.vol = o.calc_volumes()
+    L = 7
+    o, loss = _oracle(sc, L, 1)
+    return sc, o, loss, L
+
+
+def test_fp64_exact_adjoint_matches_oracle(gpu_ready, exact_case):
+    sc, o, loss, L = exact_case
+    with make_ctx(sc, "fp64", o.target, adjoint="exact", keep_adjoints=True) as c:
+        c.setup(L)
+        c.forward(0)
+        assert abs(c.loss() - loss) / abs(loss) < 1e-10
+        c.backward(0)
+        for lay in range(L - 1):
+            assert relerr(c.get(lay, "dLdFe"), o.get(lay, "dLdFe")) < 1e-9, lay
+            assert relerr(c.get(lay, "dLdF"), o.get(lay, "dLdF")) < 1e-9, lay
+            assert relerr(c.get(lay, "dLdx"), o.get(lay, "dLdx")) < 1e-9, lay
+
+
+def test_fp32_mixed_matches_fp64_oracle(gpu_ready, exact_case):
+    sc, o, loss, L = exact_case
+    with make_ctx(sc, "fp32", o.target, adjoint="exact", keep_adjoints=True) as c:
+        c.setup(L)
+        c.forward(0)
+        for lay in (1, L - 1):
+            assert relerr(c.get(lay, "x"), o.get(lay, "x")) < 1e-5
+            assert relerr(c.get(lay, "F"), o.get(lay, "F")) < 1e-4
+            assert relerr(c.get(lay, "v"), o.get(lay, "v")) < 2e-3
+        assert relerr(c.get_grid(0, "grid_m"), o.get(0, "grid_m")) < 1e-5
+        assert abs(c.loss() - loss) / abs(loss) < 1e-4
+        c.backward(0)
+        assert normrel(c.get(0, "dLdFe"), o.get(0, "dLdFe")) < 1e-3
+        assert normrel(c.get(0, "dLdx"), o.get(0, "dLdx")) < 1e-3
+
+
+def test_fp32_untiled_fallback_matches_tiled(gpu_ready, exact_case):
+    """tile_cap smaller than any stencil box forces every CTA onto the global path."""
+    sc, o, loss, L = exact_case
+    res = []
+    for cap in (0, 8):
+        with make_ctx(sc, "fp32", o.target, adjoint="exact", tile_cap=cap) as c:
+            c.setup(L)
+            c.forward(0)
+            lo = c.loss()
+            c.backward(0)
+            res.append((c.get(L - 1, "x"), lo, c.get(0, "dLdFe")))
+    assert relerr(res[0][0], res[1][0]) < 1e-5
+    assert abs(res[0][1] - res[1][1]) / abs(res[1][1]) < 1e-5
+    assert normrel(res[0][2], res[1][2]) < 1e-3
+
+
+def test_tied_controls_gradient_is_sum_over_layers(gpu_ready, exact_case):
+    sc, o, loss, L = exact_case
+    with make_ctx(sc, "fp64", o.target, adjoint="exact", control="tied") as c:
+        c.setup(L)
+        c.forward(0)
+        c.loss()
+        c.backward(0)
+        g = c.control_grad()
+    want = sum(o.get(k, "dLdFe") for k in range(L - 1))
+    assert relerr(g, want) < 1e-9
+
+
+@pytest.mark.parametrize("k", [2, 3])
+def test_checkpointing_matches_store_all(gpu_ready, exact_case, k):
+    sc, o, loss, L = exact_case
+    with make_ctx(sc, "fp64", o.target, adjoint="exact", control="tied", checkpoint_every=k) as c:
+        c.setup(L)
+        assert c.info()["checkpoint_every"] == k
+        c.forward(0)
+        lo = c.loss()
+        c.backward(0)
+        g = c.control_grad()
+        x3 = c.get(3, "x")
+    assert abs(lo - loss) / abs(loss) < 1e-10
+    assert relerr(g, sum(o.get(j, "dLdFe") for j in range(L - 1))) < 1e-9
+    assert relerr(x3, o.get(3, "x")) < 1e-10
+
+
+def test_fd_gradient_on_gpu_fp64(gpu_ready):
+    """Central differences (h = 1e-5) of the GPU FP64 loss along seeded random
+    directions in tied-dFc space against the exact adjoint."""
+    sc = scenes.small_scene(seed=8, res=12, steps=5, v_std=0.3, drag=0.1, smoothing=0.05, dt=2e-4)
+    sc.vol = OracleGraph(sc, "f64").calc_volumes()
+    L = 6
+    tgt = OracleGraph(sc, "f64").target
+
+    def loss_at(dfc):
+        s2 = scenes.Scene(**{**sc.__dict__})
+        s2.dFc = dfc
+        with make_ctx(s2, "fp64", tgt, adjoint="exact", control="tied") as c:
+            c.setup(L)
+            c.forward(0)
+            return c.loss()
+
+    with make_ctx(sc, "fp64", tgt, adjoint="exact", control="tied") as c:
+        c.setup(L)
+        c.forward(0)
+        c.loss()
+        c.backward(0)
+        g = c.control_grad()
+    rng = np.random.default_rng(123)
+    h = 1e-5
+    for _ in range(4):
+        D = rng.normal(size=(sc.n, 3, 3))
+        fd = (loss_at(sc.dFc + h * D) - loss_at(sc.dFc - h * D)) / (2 * h)
+        an = float(np.sum(g * D))
+        assert abs(fd - an) <= 1e-5 * abs(fd) + 1e-14, (fd, an)
+
+
+def test_reference_layout_upload_and_download(gpu_ready, golden_scene, g64):
+    sc = golden_scene
+    pts = np.zeros((sc.n, 118), dtype=np.float32)
+    pts[:, 0:3] = sc.x
+    pts[:, 3:6] = sc.v
+    pts[:, 6:15] = sc.F.transpose(0, 2, 1).reshape(-1, 9)
+    pts[:, 15:24] = sc.C.transpose(0, 2, 1).reshape(-1, 9)
+    pts[:, 33] = sc.m
+    pts[:, 34] = sc.vol
+    pts[:, 35] = sc.lam
+    pts[:, 36] = sc.mu
+    pts[:, 37:46] = sc.dFc.transpose(0, 2, 1).reshape(-1, 9)
+    with dmpm.Context("fp64") as c:
+        c.set_grid(sc.dims, sc.dx, sc.min_point)
+        c.set_points_ref(pts)
+        c.set_target_mass(g64["target"])
+        c.set_params(dt=sc.dt, drag=sc.drag, f_ext=sc.f_ext, smoothing=sc.smoothing)
+        c.setup(3)
+        c.forward(0)
+        c.loss()
+        c.backward(0)
+        out = np.zeros_like(pts)
+        c.get_points_ref(2, out)
+        assert relerr(out[:, 0:3], c.get(2, "x")) < 1e-6
+        out0 = np.zeros_like(pts)
+        c.get_points_ref(0, out0)
+        assert relerr(out0[:, 52:61].reshape(-1, 3, 3).transpose(0, 2, 1), c.get(0, "dLdF")) < 1e-6
+        assert np.array_equal(out0[:, 33], pts[:, 33])
+
+
+def test_errors_are_reported(gpu_ready):
+    c = dmpm.Context("fp32")
+    with pytest.raises(dmpm.DmpmError) as e:
+        c.set_grid((0, 4, 4))
+    assert e.value.status == dmpm.ERR_ARG
+    c.set_grid((8, 8, 8))
+    with pytest.raises(dmpm.DmpmError) as e:
+        c.setup(3)
+    assert e.value.status == dmpm.ERR_STATE
+    sc = scenes.small_scene(seed=1, res=8, radius=0.2)
+    c.set_particles(sc.x, sc.m, sc.lam, sc.mu)
+    c.set_params(dt=1e-4)
+    c.setup(3)
+    with pytest.raises(dmpm.DmpmError) as e:
+        c.backward(0)
+    assert e.value.status == dmpm.ERR_STATE
+    c.close()
+
+
+def test_nonfinite_is_flagged_not_faulted(gpu_ready):
+    """A blown-up rollout (dt far above the explicit limit) reports
+    DMPM_ERR_NONFINITE; the context stays usable."""
+    sc = scenes.small_scene(seed=4, res=12, dt=5.0, steps=6, dfc_std=0.05)
+    sc.vol = OracleGraph(sc, "f64").calc_volumes()
+    with make_ctx(sc, "fp32", np.zeros(int(np.prod(sc.dims)))) as c:
+        c.setup(12)
+        st = c.forward(0)
+        assert st == dmpm.ERR_NONFINITE
+        c.set_params(dt=1e-4)
+        c.setup(3)
+        assert c.forward(0) == dmpm.OK
