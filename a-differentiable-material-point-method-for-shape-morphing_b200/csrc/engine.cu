@@ -33,6 +33,15 @@ namespace {
 constexpr int kDefaultBlock = 256;
 constexpr int kDefaultTileCap = 1024;
 
+// Kernel identifiers for the per-kernel device-time accounting
+// (dmpm_set_profiling / dmpm_kernel_stats).
+enum KernelId {
+    K_P_OP1 = 0, K_P2G, K_GOP, K_G2P, K_MASS, K_NODE_LOSS, K_LOSS_DLDX, K_ADJ_SCATTER, K_ADJ_GOP, K_ADJ_GATHER,
+    K_COUNT
+};
+const char* const kKernelNames[K_COUNT] = {"p_op1", "p2g", "g_op", "g2p_p_op2", "p2g_mass", "node_loss",
+                                          "loss_dldx", "adj_g2p_scatter", "adj_g_op", "adj_p2g_gather"};
+
 struct CudaError {
     cudaError_t code;
     std::string what;
@@ -196,12 +205,15 @@ template <class T> class Engine : public EngineBase {
     void set_grid(int dx_, int dy_, int dz_, double h, const double* mn) {
         if (dx_ <= 0 || dy_ <= 0 || dz_ <= 0 || !(h > 0)) throw ArgError{"grid dims and dx must be positive"};
         if ((double)dx_ * dy_ * dz_ > 2e9) throw ArgError{"grid has more than 2e9 nodes"};
+        const bool same = grid_set_ && geo_.dim[0] == dx_ && geo_.dim[1] == dy_ && geo_.dim[2] == dz_;
         geo_.dim[0] = dx_; geo_.dim[1] = dy_; geo_.dim[2] = dz_;
         geo_.dx = h;
         for (int a = 0; a < 3; a++) geo_.mn[a] = mn ? mn[a] : 0.0;
         G_ = (size_t)dx_ * dy_ * dz_;
         grid_set_ = true;
+        if (same) return;
         layers_.clear();
+        layout_ = Layout{};
         target_ = nullptr;
         scene_arena_grid_.release();
         target_ = (T*)scene_arena_grid_.alloc(G_ * sizeof(T));
@@ -212,9 +224,17 @@ template <class T> class Engine : public EngineBase {
 
     void alloc_particles(int n) {
         if (n <= 0) throw ArgError{"particle count must be positive"};
+        if (n == n_ && cst_) {
+            // same cloud size: overwrite in place and keep the layer storage
+            DMPM_CK(cudaMemsetAsync(cst_, 0, NCONST * np_ * sizeof(T), ctx_->stream));
+            DMPM_CK(cudaMemsetAsync(st0_, 0, NSTATE * np_ * sizeof(T), ctx_->stream));
+            DMPM_CK(cudaMemsetAsync(dfc0_, 0, 9 * np_ * sizeof(T), ctx_->stream));
+            return;
+        }
         n_ = n;
         np_ = round_up((size_t)n, 64);
         layers_.clear();
+        layout_ = Layout{};
         scene_arena_.release();
         cst_ = (T*)scene_arena_.alloc(NCONST * np_ * sizeof(T));
         st0_ = (T*)scene_arena_.alloc(NSTATE * np_ * sizeof(T));
@@ -326,6 +346,53 @@ template <class T> class Engine : public EngineBase {
         if (e != cudaSuccess) throw CudaError{e, std::string("kernel launch: ") + cudaGetErrorString(e)};
     }
 
+    // ---------------------------------------------------------- profiling
+    void set_profiling(bool on) {
+        harvest();
+        prof_ = on;
+        for (int k = 0; k < K_COUNT; k++) { prof_ms_[k] = 0.0; prof_cnt_[k] = 0; }
+    }
+    void pbeg(int kid) {
+        if (!prof_) return;
+        cudaEvent_t e0 = take_event(), e1 = take_event();
+        DMPM_CK(cudaEventRecord(e0, ctx_->stream));
+        pend_.push_back(Pending{kid, e0, e1});
+    }
+    void pend() {
+        if (!prof_) return;
+        DMPM_CK(cudaEventRecord(pend_.back().e1, ctx_->stream));
+    }
+    cudaEvent_t take_event() {
+        if (!event_pool_.empty()) {
+            cudaEvent_t e = event_pool_.back();
+            event_pool_.pop_back();
+            return e;
+        }
+        cudaEvent_t e;
+        DMPM_CK(cudaEventCreate(&e));
+        return e;
+    }
+    // called after the stream has been synchronised
+    void harvest() {
+        for (const Pending& q : pend_) {
+            float ms = 0.f;
+            if (cudaEventElapsedTime(&ms, q.e0, q.e1) == cudaSuccess) {
+                prof_ms_[q.kid] += ms;
+                prof_cnt_[q.kid] += 1;
+            }
+            event_pool_.push_back(q.e0);
+            event_pool_.push_back(q.e1);
+        }
+        pend_.clear();
+    }
+    void kernel_stats(int kid, double* ms, int64_t* cnt) {
+        if (kid < 0 || kid >= K_COUNT) throw ArgError{"kernel id out of range"};
+        DMPM_CK(cudaStreamSynchronize(ctx_->stream));
+        harvest();
+        if (ms) *ms = prof_ms_[kid];
+        if (cnt) *cnt = prof_cnt_[kid];
+    }
+
     void ensure_status() {
         if (!status_) {
             status_ = (unsigned*)misc_arena_.alloc(sizeof(unsigned) + sizeof(double) * 2);
@@ -337,6 +404,7 @@ template <class T> class Engine : public EngineBase {
     unsigned read_status() {
         DMPM_CK(cudaMemcpyAsync(host_misc_, status_, sizeof(unsigned), cudaMemcpyDeviceToHost, ctx_->stream));
         DMPM_CK(cudaStreamSynchronize(ctx_->stream));
+        harvest();
         return *(unsigned*)host_misc_;
     }
 
@@ -366,6 +434,16 @@ template <class T> class Engine : public EngineBase {
         DMPM_CK(cudaMemcpyAsync(s, m, G_ * sizeof(double), cudaMemcpyHostToDevice, ctx_->stream));
         k_set_node_mass<T><<<ggrid(), 256, 0, ctx_->stream>>>(s, G_, target_);
         launched();
+    }
+
+    void get_target_mass(double* out) {
+        if (!grid_set_) throw StateError{"dmpm_set_grid has not been called"};
+        if (!out) throw ArgError{"out is NULL"};
+        double* s = staging(G_);
+        k_scalar_field<T><<<ggrid(), 256, 0, ctx_->stream>>>(target_, G_, s);
+        launched();
+        DMPM_CK(cudaMemcpyAsync(out, s, G_ * sizeof(double), cudaMemcpyDeviceToHost, ctx_->stream));
+        DMPM_CK(cudaStreamSynchronize(ctx_->stream));
     }
 
     // LoadCompGraph: target grid = ResetValues + P2G(target samples, dt = drag = 0),
@@ -412,6 +490,13 @@ template <class T> class Engine : public EngineBase {
         if (num_layers < 1) throw ArgError{"num_layers must be >= 1"};
         ensure_status();
         const dmpm_params& P = ctx_->prm;
+        Layout want;
+        want.L = num_layers; want.k_req = P.checkpoint_every; want.control = P.control_mode;
+        want.keep_adj = P.keep_adjoints; want.keep_int = P.keep_intermediates; want.np = np_; want.G = G_;
+        if (want == layout_ && (int)layers_.size() == num_layers) {
+            reset_layers();
+            return;
+        }
         L_ = num_layers;
         layer_arena_.release();
         layers_.assign(L_, LayerSlots{});
@@ -454,14 +539,11 @@ template <class T> class Engine : public EngineBase {
             for (int l = 0; l < L_; l++) {
                 layers_[l].dfc = dbase + (size_t)l * 9 * np_;
                 layers_[l].ctrl_grad = gbase + (size_t)l * 9 * np_;
-                DMPM_CK(cudaMemcpyAsync(layers_[l].dfc, dfc0_, 9 * np_ * sizeof(T), cudaMemcpyDeviceToDevice, ctx_->stream));
             }
-            DMPM_CK(cudaMemsetAsync(gbase, 0, (size_t)L_ * 9 * np_ * sizeof(T), ctx_->stream));
             ctrl_acc_ = nullptr;
         } else {
             for (int l = 0; l < L_; l++) layers_[l].dfc = dfc0_;
             ctrl_acc_ = (double*)layer_arena_.alloc(9 * np_ * sizeof(double));
-            DMPM_CK(cudaMemsetAsync(ctrl_acc_, 0, 9 * np_ * sizeof(double), ctx_->stream));
         }
         // adjoints
         if (P.keep_adjoints) {
@@ -500,11 +582,25 @@ template <class T> class Engine : public EngineBase {
                 layers_[l].dbggdp = g2 + (size_t)l * G_;
             }
         }
-        // layer 0 = the uploaded cloud (SetUpCompGraph copies it into every layer;
-        // only layer 0's state is ever read before being recomputed)
+        layout_ = want;
+        reset_layers();
+    }
+
+    // SetUpCompGraph semantics on allocated storage: layer 0 = the uploaded
+    // cloud, every layer's dFc = the uploaded dFc, gradients cleared.  Layer
+    // states other than 0 are not copied: each is written by the forward pass
+    // before anything reads it.
+    void reset_layers() {
+        const size_t st_bytes = NSTATE * np_ * sizeof(T);
         DMPM_CK(cudaMemcpyAsync(layers_[0].st, st0_, st_bytes, cudaMemcpyDeviceToDevice, ctx_->stream));
-        for (int l = 1; l < L_; l++)
-            if (layers_[l].st) DMPM_CK(cudaMemcpyAsync(layers_[l].st, st0_, st_bytes, cudaMemcpyDeviceToDevice, ctx_->stream));
+        if (ctx_->prm.control_mode == DMPM_CTRL_PER_LAYER) {
+            for (int l = 0; l < L_; l++) {
+                DMPM_CK(cudaMemcpyAsync(layers_[l].dfc, dfc0_, 9 * np_ * sizeof(T), cudaMemcpyDeviceToDevice, ctx_->stream));
+                DMPM_CK(cudaMemsetAsync(layers_[l].ctrl_grad, 0, 9 * np_ * sizeof(T), ctx_->stream));
+            }
+        } else {
+            DMPM_CK(cudaMemsetAsync(ctrl_acc_, 0, 9 * np_ * sizeof(double), ctx_->stream));
+        }
         forward_done_ = false;
         loss_done_ = false;
         backward_lo_ = L_;
@@ -535,19 +631,31 @@ template <class T> class Engine : public EngineBase {
         DMPM_CK(cudaMemsetAsync(g, 0, G_ * sizeof(node4<T>), ctx_->stream));
         const size_t tile_b = (size_t)tile_cap() * sizeof(node4<T>);
         if (kTiled) {
+            pbeg(K_P2G);
             k_p2g<T, true, true><<<pgrid(), block(), tile_b, ctx_->stream>>>(a);
             launched();
+            pend();
+            pbeg(K_G2P);
             k_g2p<T, true><<<pgrid(), block(), tile_b, ctx_->stream>>>(a);
             launched();
+            pend();
         } else {
+            pbeg(K_P_OP1);
             k_p_op1<T><<<pgrid(), block(), 0, ctx_->stream>>>(a);
             launched();
+            pend();
+            pbeg(K_P2G);
             k_p2g<T, false, false><<<pgrid(), block(), 0, ctx_->stream>>>(a);
             launched();
+            pend();
+            pbeg(K_GOP);
             k_gop<T><<<ggrid(), 256, 0, ctx_->stream>>>(a, G_);
             launched();
+            pend();
+            pbeg(K_G2P);
             k_g2p<T, false><<<pgrid(), block(), 0, ctx_->stream>>>(a);
             launched();
+            pend();
         }
     }
 
@@ -616,11 +724,17 @@ template <class T> class Engine : public EngineBase {
         a.loss = loss_acc_;
         DMPM_CK(cudaMemsetAsync(g, 0, G_ * sizeof(node4<T>), ctx_->stream));
         DMPM_CK(cudaMemsetAsync(loss_acc_, 0, sizeof(double), ctx_->stream));
+        pbeg(K_MASS);
         launch_mass(a);
+        pend();
+        pbeg(K_NODE_LOSS);
         k_node_loss<T><<<ggrid(), 256, 0, ctx_->stream>>>(a, G_);
         launched();
+        pend();
+        pbeg(K_LOSS_DLDX);
         k_loss_dldx<T><<<pgrid(), block(), 0, ctx_->stream>>>(a);
         launched();
+        pend();
         DMPM_CK(cudaMemcpyAsync((char*)host_misc_ + 8, loss_acc_, sizeof(double), cudaMemcpyDeviceToHost, ctx_->stream));
         last_status_ = read_status();
         loss_done_ = true;
@@ -666,24 +780,34 @@ template <class T> class Engine : public EngineBase {
         const size_t tile_b = (size_t)tile_cap() * sizeof(node4<T>);
         const bool ex = P.adjoint_mode == DMPM_ADJ_EXACT;
         if (kTiled) {
+            pbeg(K_ADJ_SCATTER);
             if (ex) k_adj_scatter<T, true, true><<<pgrid(), block(), tile_b, ctx_->stream>>>(a);
             else k_adj_scatter<T, true, false><<<pgrid(), block(), tile_b, ctx_->stream>>>(a);
             launched();
+            pend();
             if (P.keep_intermediates) debug_grid_adjoint(i, a, ex);
+            pbeg(K_ADJ_GATHER);
             if (ex) k_adj_gather<T, true, true><<<pgrid(), block(), 2 * tile_b, ctx_->stream>>>(a);
             else k_adj_gather<T, true, false><<<pgrid(), block(), 2 * tile_b, ctx_->stream>>>(a);
             launched();
+            pend();
         } else {
+            pbeg(K_ADJ_SCATTER);
             if (ex) k_adj_scatter<T, false, true><<<pgrid(), block(), 0, ctx_->stream>>>(a);
             else k_adj_scatter<T, false, false><<<pgrid(), block(), 0, ctx_->stream>>>(a);
             launched();
+            pend();
+            pbeg(K_ADJ_GOP);
             if (ex) k_adj_gop<T, true><<<ggrid(), 256, 0, ctx_->stream>>>(a, G_);
             else k_adj_gop<T, false><<<ggrid(), 256, 0, ctx_->stream>>>(a, G_);
             launched();
+            pend();
             if (P.keep_intermediates) debug_grid_adjoint(i, a, ex);
+            pbeg(K_ADJ_GATHER);
             if (ex) k_adj_gather<T, false, true><<<pgrid(), block(), 0, ctx_->stream>>>(a);
             else k_adj_gather<T, false, false><<<pgrid(), block(), 0, ctx_->stream>>>(a);
             launched();
+            pend();
         }
     }
 
@@ -891,6 +1015,9 @@ template <class T> class Engine : public EngineBase {
     unsigned last_status() const { return last_status_; }
 
     ~Engine() override {
+        cudaStreamSynchronize(ctx_->stream);
+        harvest();
+        for (cudaEvent_t e : event_pool_) cudaEventDestroy(e);
         if (host_misc_) cudaFreeHost(host_misc_);
     }
 
@@ -942,6 +1069,25 @@ template <class T> class Engine : public EngineBase {
     bool forward_done_ = false, loss_done_ = false;
     int backward_lo_ = 0;
     unsigned last_status_ = 0;
+    // profiling
+    struct Pending {
+        int kid;
+        cudaEvent_t e0, e1;
+    };
+    bool prof_ = false;
+    std::vector<Pending> pend_;
+    std::vector<cudaEvent_t> event_pool_;
+    double prof_ms_[K_COUNT] = {};
+    int64_t prof_cnt_[K_COUNT] = {};
+    // the layout the layer storage was allocated for (setup reuses it when unchanged)
+    struct Layout {
+        int L = -1, k_req = -1, control = -1, keep_adj = -1, keep_int = -1;
+        size_t np = 0, G = 0;
+        bool operator==(const Layout& o) const {
+            return L == o.L && k_req == o.k_req && control == o.control && keep_adj == o.keep_adj &&
+                   keep_int == o.keep_int && np == o.np && G == o.G;
+        }
+    } layout_;
 };
 
 template <class Fn> int guarded(dmpm_ctx* ctx, Fn fn) {
@@ -1066,6 +1212,10 @@ int dmpm_set_target_mass(dmpm_ctx* ctx, const double* target_m) {
     return with_engine(ctx, [&](auto& e) { e.set_target_mass(target_m); return DMPM_OK; });
 }
 
+int dmpm_get_target_mass(dmpm_ctx* ctx, double* out) {
+    return with_engine(ctx, [&](auto& e) { e.get_target_mass(out); return DMPM_OK; });
+}
+
 int dmpm_rasterize_target(dmpm_ctx* ctx, int n, const double* x, double point_mass) {
     return with_engine(ctx, [&](auto& e) { e.rasterize_target(n, x, point_mass); return DMPM_OK; });
 }
@@ -1126,6 +1276,18 @@ int dmpm_synchronize(dmpm_ctx* ctx) {
 }
 
 void* dmpm_stream(dmpm_ctx* ctx) { return ctx ? (void*)ctx->stream : nullptr; }
+
+int dmpm_set_profiling(dmpm_ctx* ctx, int on) {
+    return with_engine(ctx, [&](auto& e) { e.set_profiling(on != 0); return DMPM_OK; });
+}
+
+int dmpm_kernel_stats(dmpm_ctx* ctx, int kernel_id, double* total_ms, int64_t* launches) {
+    return with_engine(ctx, [&](auto& e) { e.kernel_stats(kernel_id, total_ms, launches); return DMPM_OK; });
+}
+
+const char* dmpm_kernel_name(int kernel_id) {
+    return (kernel_id >= 0 && kernel_id < K_COUNT) ? kKernelNames[kernel_id] : nullptr;
+}
 
 int64_t dmpm_launch_count(const dmpm_ctx* ctx) { return ctx ? ctx->launches : -1; }
 

@@ -439,11 +439,11 @@ template <class T> __global__ void __launch_bounds__(256) k_node_loss(LossArgs<T
         const double cm = (double)a.grid[g].w, tm = (double)a.target[g];
         double dl;
         if (a.kind == 0) {
-            const double eps = (double)1e-4f;
+            const double eps = 1e-4;  // CompGraph.cpp:115 (FP64 semantics: the loss is evaluated in FP64)
             const double clog = log(cm + 1.0 + eps) - log(tm + 1.0 + eps);
             l = 0.5 * clog * clog;
             dl = clog / (cm + 1.0 + eps);
-            const double min_mass = (double)1e-3f;
+            const double min_mass = 1e-3;  // CompGraph.cpp:122
             if (cm < min_mass) {
                 const double diff = min_mass - cm;
                 l += 10.0 * diff * diff;

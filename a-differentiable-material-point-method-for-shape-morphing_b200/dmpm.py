@@ -30,6 +30,7 @@ FIELDS = {"x": 0, "v": 1, "F": 2, "C": 3, "P": 4, "m": 5, "vol": 6, "lam": 7, "m
 WIDTH = {"x": 3, "v": 3, "F": 9, "C": 9, "P": 9, "m": 1, "vol": 1, "lam": 1, "mu": 1, "dFc": 9, "dLdx": 3,
          "dLdv": 3, "dLdF": 9, "dLdC": 9, "dLdP": 9, "dLdv_next": 3, "dLdC_next": 9, "dLdFe": 9}
 GRID_FIELDS = {"grid_m": 0, "grid_v": 1, "grid_p": 2, "grid_dLdv": 3, "grid_dLdp": 4, "grid_dLdm": 5}
+NUM_KERNEL_IDS = 10
 GRID_WIDTH = {"grid_m": 1, "grid_v": 3, "grid_p": 3, "grid_dLdv": 3, "grid_dLdp": 3, "grid_dLdm": 1}
 
 
@@ -72,6 +73,7 @@ def load_library(path: str = LIB_PATH) -> ctypes.CDLL:
     L.dmpm_compute_volumes.argtypes = [_P]
     L.dmpm_set_target_mass.argtypes = [_P, _P]
     L.dmpm_rasterize_target.argtypes = [_P, ctypes.c_int, _P, ctypes.c_double]
+    L.dmpm_get_target_mass.argtypes = [_P, _P]
     L.dmpm_setup.argtypes = [_P, ctypes.c_int]
     L.dmpm_forward.argtypes = [_P, ctypes.c_int]
     L.dmpm_loss.argtypes = [_P, ctypes.POINTER(ctypes.c_double)]
@@ -87,6 +89,10 @@ def load_library(path: str = LIB_PATH) -> ctypes.CDLL:
     L.dmpm_stream.restype = _P
     L.dmpm_launch_count.argtypes = [_P]
     L.dmpm_launch_count.restype = ctypes.c_int64
+    L.dmpm_set_profiling.argtypes = [_P, ctypes.c_int]
+    L.dmpm_kernel_stats.argtypes = [_P, ctypes.c_int, ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_int64)]
+    L.dmpm_kernel_name.argtypes = [ctypes.c_int]
+    L.dmpm_kernel_name.restype = ctypes.c_char_p
     _lib = L
     return L
 
@@ -165,6 +171,21 @@ class Context:
     def stream(self) -> int:
         return int(self.lib.dmpm_stream(self.h) or 0)
 
+    def set_profiling(self, on: bool = True):
+        """Bracket every hot-path kernel with CUDA events on the context stream."""
+        self._ck(self.lib.dmpm_set_profiling(self.h, int(bool(on))), "set_profiling")
+
+    def kernel_stats(self) -> dict:
+        """{kernel name: (total device ms, launches)} since profiling was enabled."""
+        out = {}
+        for k in range(NUM_KERNEL_IDS):
+            ms = ctypes.c_double()
+            cnt = ctypes.c_int64()
+            self._ck(self.lib.dmpm_kernel_stats(self.h, k, ctypes.byref(ms), ctypes.byref(cnt)), "kernel_stats")
+            if cnt.value:
+                out[self.lib.dmpm_kernel_name(k).decode()] = (float(ms.value), int(cnt.value))
+        return out
+
     def synchronize(self):
         self._ck(self.lib.dmpm_synchronize(self.h), "synchronize")
 
@@ -234,6 +255,11 @@ class Context:
         a = np.ascontiguousarray(points, dtype=np.float64)
         self._ck(self.lib.dmpm_rasterize_target(self.h, a.shape[0], a.ctypes.data, float(point_mass)),
                  "rasterize_target")
+
+    def target_mass(self) -> np.ndarray:
+        out = np.empty(int(np.prod(self.dims)), dtype=np.float64)
+        self._ck(self.lib.dmpm_get_target_mass(self.h, out.ctypes.data), "get_target_mass")
+        return out
 
     def load_scene(self, scene, with_volumes: bool = True, with_target: bool = True):
         """Grid, particles, volumes (CalculatePointCloudVolumes) and target raster of a scenes.Scene."""

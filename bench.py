@@ -1,0 +1,452 @@
+#!/usr/bin/env python
+"""Benchmark: forward + adjoint particle-steps/s of the MLS-MPM morphing path.
+
+Workload (one "step" = one gradient evaluation): the ellipsoid-to-torus
+scene -- solid ellipsoid with semi-axes (0.3, 0.2, 0.15) in the unit box,
+jittered stratified sampling at 27 particles per cell (~267k particles),
+64^3 grid, fixed-corotated E = 1e4, nu = 0.3, 200 time steps, target a solid
+torus R = 0.25, r = 0.08 -- run as forward rollout + end-layer mass loss +
+full adjoint (exact mode, tied controls, FP64 gradient accumulation), every
+layer kept in HBM.  Seeded synthetic inputs stand in for the reference's
+OBJ meshes (which are not part of its tree).
+
+Our arm (default) prints one JSON line with
+  value      device-resident throughput (particle-steps/s, whole job)
+  e2e        the same through the C ABI with host buffers: pinned-host upload of
+             every particle input, forward, loss, adjoint and the read-back of
+             the control gradient inside the timed region
+  roofline   the dominant kernel's algorithmic bytes / its CUDA-event duration
+  fp64       the plain FP64 GPU path on the same workload, speedup and
+             gradient relative error of the FP32-mixed path against it
+  cpu_baseline the reference's own CPU code (oracle/_ref) on a bounded sample
+`--impl reference` times the reference's CPU implementation alone.
+Multi-GPU (torchrun): one independent instance per rank (seed = rank), no
+data-path collective; timing is the max over ranks.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+REPO = os.path.dirname(os.path.abspath(__file__))
+PKG = os.path.join(REPO, "a-differentiable-material-point-method-for-shape-morphing_b200")
+for _p in (REPO, PKG):
+    if _p not in sys.path:
+        sys.path.insert(0, _p)
+
+import scenes  # noqa: E402
+
+METRIC = "fwd+adjoint particle-steps/s, FP32-mixed vs FP64 GPU @ grad relerr≤1e-4"
+UNIT = "particle-steps/s"
+HBM_FALLBACK_GBS = 6650.0
+
+
+# ---------------------------------------------------------------- helpers
+def measured_hbm_gbs():
+    try:
+        with open(os.path.join(REPO, "MEASURED_PEAKS.json")) as f:
+            return float(json.load(f)["hbm_gbs"]), "measured"
+    except Exception:
+        return HBM_FALLBACK_GBS, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+         "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+         "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device: int):
+        self.device = device
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "--query-gpu=" + self.Q, "--format=csv,noheader,nounits",
+                                          "-lms", "200", "-i", str(self.device)], stdout=subprocess.PIPE,
+                                         stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except Exception:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if not self.proc:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        self.t.join(timeout=2)
+        sm, mx, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx.append(float(f[2]))
+            except ValueError:
+                continue
+            for nm, v in zip(names, f[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(nm)
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def dist_setup(ngpus):
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import datetime
+
+        import torch
+        import torch.distributed as dist
+
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+    return world, rank, local
+
+
+def max_over_ranks(value: float, world: int) -> float:
+    if world <= 1:
+        return value
+    import torch
+    import torch.distributed as dist
+
+    t = torch.tensor([value], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def barrier(world: int):
+    if world > 1:
+        import torch.distributed as dist
+
+        dist.barrier()
+
+
+# ---------------------------------------------------------------- workload
+def build_scene(instance: int, ppc_root: int):
+    sc = scenes.config_scene(1, instance=instance, ppc_root=ppc_root)
+    return sc
+
+
+def setup_ctx(dmpm, sc, prec, device, vol, target, dt, checkpoint_every):
+    c = dmpm.Context(prec, device)
+    c.set_grid(sc.dims, sc.dx, sc.min_point)
+    c.set_particles(sc.x, sc.m, sc.lam, sc.mu, v=sc.v, F=sc.F, C=sc.C, dFc=sc.dFc, vol=vol)
+    c.set_target_mass(target)
+    c.set_params(dt=dt, drag=sc.drag, f_ext=sc.f_ext, smoothing=sc.smoothing, adjoint="exact", control="tied",
+                 loss="ref", checkpoint_every=checkpoint_every)
+    c.setup(sc.steps + 1)
+    return c
+
+
+def gradient_step(c):
+    c.forward(0)
+    loss = c.loss()
+    c.backward(0)
+    return loss
+
+
+def finite_gradient(dmpm, c) -> bool:
+    st_f = c.forward(0)
+    loss = c.loss()
+    st_b = c.backward(0)
+    ok = st_f == dmpm.OK and st_b == dmpm.OK and math.isfinite(loss)
+    return ok and bool(np.all(np.isfinite(c.control_grad())))
+
+
+def timed_steps(torch, c, steps, fn):
+    """CUDA events on the context's stream around `steps` calls of fn."""
+    s = torch.cuda.ExternalStream(c.stream)
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    e0.record(s)
+    for _ in range(steps):
+        fn()
+    e1.record(s)
+    e1.synchronize()
+    torch.cuda.synchronize()
+    return e0.elapsed_time(e1)
+
+
+# algorithmic bytes per launch of each kernel, FP32 tiled path
+def algorithmic_bytes(kernel: str, n: int, touched: int) -> float:
+    per_particle = {
+        "p2g": 37 * 4, "g2p_p_op2": (21 + 24) * 4, "adj_g2p_scatter": 45 * 4,
+        "adj_p2g_gather": 70 * 4 + 24 * 4 + 9 * 8 * 2, "p2g_mass": 4 * 4, "loss_dldx": 4 * 4 + 24 * 4,
+    }
+    per_node = {"p2g": 16, "g2p_p_op2": 16, "adj_g2p_scatter": 16, "adj_p2g_gather": 32, "p2g_mass": 4,
+                "loss_dldx": 4}
+    return per_particle.get(kernel, 0) * n + per_node.get(kernel, 0) * touched
+
+
+def committed_traffic(kernel: str):
+    """DRAM bytes per launch recorded from an ncu capture (profiles/roofline_traffic.txt), if any."""
+    path = os.path.join(REPO, "profiles", "roofline_traffic.txt")
+    try:
+        for line in open(path):
+            k, _, v = line.partition("=")
+            if k.strip() == kernel:
+                return float(v.split()[0])
+    except Exception:
+        pass
+    return None
+
+
+# ---------------------------------------------------------------- CPU baseline
+def cpu_baseline(sc, sample_steps=1, threads=None):
+    """The reference's own CPU implementation (oracle/_ref) on a bounded sample:
+    MultiThreadMPM forward (all host threads) + EndLayerMassLoss +
+    ComputeBackwardPass (serial) over `sample_steps` time steps of the workload."""
+    from oracle import lib as olib
+
+    threads = threads or os.cpu_count() or 1
+    if olib.ref_available("f32"):
+        r = olib.RefGraph(sc, "f32", target_from_points=True)
+        vol = r.calc_volumes()
+        sc2 = scenes.Scene(**{**sc.__dict__})
+        sc2.vol = vol.astype(np.float64)
+        r = olib.RefGraph(sc2, "f32", target_from_points=True)
+        r.setup(sample_steps + 1, sc.dt, sc.drag, sc.f_ext, 0.0)
+        t_fwd = r.time_forward_multithread(sample_steps, threads)
+        t_bwd, _ = r.time_loss_backward()
+        kind = "reference"
+        desc = ("DiffMPMLib3D compiled from its sources (serial build): MultiThreadMPM::ForwardTimeStep with %d "
+                "threads + EndLayerMassLoss + ComputeBackwardPass (1 thread) over %d time step(s) of the full "
+                "%d-particle workload" % (threads, sample_steps, sc.n))
+    else:
+        g = olib.OracleGraph(sc, "f32")
+        sc2 = scenes.Scene(**{**sc.__dict__})
+        sc2.vol = g.calc_volumes().astype(np.float64)
+        g = olib.OracleGraph(sc2, "f32")
+        g.setup(sample_steps + 1, sc.dt, sc.drag, sc.f_ext, 0.0)
+        t0 = time.perf_counter()
+        g.forward(0)
+        t_fwd = time.perf_counter() - t0
+        t0 = time.perf_counter()
+        g.loss()
+        g.backward(0, 1)
+        t_bwd = time.perf_counter() - t0
+        threads = 1
+        kind = "port"
+        desc = "serial CPU restatement (oracle), %d time step(s) of the %d-particle workload" % (sample_steps, sc.n)
+    total = t_fwd + t_bwd
+    return {"value": sc.n * sample_steps / total, "unit": UNIT, "cores": threads, "kind": kind, "sample": desc,
+            "forward_s": t_fwd, "loss_backward_s": t_bwd}
+
+
+# ---------------------------------------------------------------- arms
+def run_reference(args):
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return 0
+    sc = build_scene(0, args.ppc_root)
+    if args.rollout_steps:
+        sc.steps = args.rollout_steps
+    # the configured dt (5e-4) is 3.7x the explicit CFL limit and diverges; both
+    # arms run at half the limit (throughput does not depend on dt)
+    dt_sub = sc.dt
+    sc.dt = args.dt if args.dt else 0.5 * sc.cfl_dt()
+    for _ in range(args.warmup):
+        cpu_baseline(sc, 1)
+    times = []
+    cb = None
+    for _ in range(args.steps):
+        cb = cpu_baseline(sc, 1)
+        times.append(cb["forward_s"] + cb["loss_backward_s"])
+    total = sum(times)
+    value = sc.n * args.steps / total
+    cb = dict(cb)
+    cb["value"] = value
+    line = {"impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000 * total / args.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic", "config": workload_config(sc, None if args.dt else dt_sub, 1),
+            "cpu_baseline": {k: cb[k] for k in ("value", "unit", "cores", "kind", "sample")},
+            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def workload_config(sc, dt_sub, ckpt):
+    return {"workload": "ellipsoid(0.3,0.2,0.15)->torus(R=0.25,r=0.08), 64^3 grid, %d particles (%d per cell), "
+                        "%d steps, forward + end-layer mass loss + adjoint" % (sc.n, sc.meta["ppc"], sc.steps),
+            "particles": sc.n, "grid": list(sc.dims), "layers": sc.steps + 1, "dt": sc.dt,
+            "dt_substituted_from": dt_sub, "checkpoint_every": ckpt, "loss": "reference log-mass + min-mass penalty",
+            "l2_policy": "inputs larger than L2 (per-rollout layer state > 5 GB, 126 MB L2)",
+            "parallelism": "replicas: one independent instance per GPU"}
+
+
+def run_ours(args):
+    import torch
+
+    import dmpm
+
+    world, rank, local = dist_setup(args.gpus)
+    device = local
+    torch.cuda.set_device(device)
+    sc = build_scene(rank, args.ppc_root)
+    if args.rollout_steps:
+        sc.steps = args.rollout_steps
+    dt_cfg = sc.dt
+    # volumes (CalculatePointCloudVolumes) and the target raster (mass-only P2G of the
+    # target samples, as LoadCompGraph builds it) on the FP64 path, shared by both paths
+    with dmpm.Context("fp64", device) as c64:
+        c64.load_scene(sc)
+        c64.set_params(dt=sc.dt)
+        c64.setup(1)
+        vol = c64.get(0, "vol")
+        target = c64.target_mass()
+    ckpt = args.checkpoint_every
+    # run the configured dt; fall back to half the explicit CFL limit if it blows up
+    dt_sub = None
+    if args.dt:
+        sc.dt = args.dt
+    c = setup_ctx(dmpm, sc, "fp32", device, vol, target, sc.dt, ckpt)
+    if not args.dt and not finite_gradient(dmpm, c):
+        # the configured dt is above the explicit limit and the rollout or its
+        # adjoint diverges: rerun at half the CFL limit and record the substitution
+        dt_sub = dt_cfg
+        sc.dt = 0.5 * sc.cfl_dt()
+        c.close()
+        c = setup_ctx(dmpm, sc, "fp32", device, vol, target, sc.dt, ckpt)
+        assert finite_gradient(dmpm, c), "gradient not finite at half the CFL limit"
+    units_per_step = sc.n * sc.steps  # particle-steps of one gradient evaluation
+    for _ in range(args.warmup):
+        gradient_step(c)
+    c.set_profiling(True)
+    l0 = c.launch_count
+    barrier(world)
+    sampler = ClockSampler(device)
+    sampler.start()
+    ms = timed_steps(torch, c, args.steps, lambda: gradient_step(c))
+    clocks = sampler.stop()
+    launches = c.launch_count - l0
+    kstats = c.kernel_stats()
+    c.set_profiling(False)
+    barrier(world)
+    ms_max = max_over_ranks(ms, world)
+    value = units_per_step * args.steps * world / (ms_max / 1000.0)
+    grad32 = c.control_grad()
+
+    # e2e through the C ABI with pinned host buffers
+    pin = lambda a: torch.from_numpy(np.ascontiguousarray(a, dtype=np.float64)).pin_memory()
+    cm = lambda M: np.ascontiguousarray(np.asarray(M).transpose(0, 2, 1).reshape(-1, 9))
+    hx, hv, hF, hC, hd = pin(sc.x), pin(sc.v), pin(cm(sc.F)), pin(cm(sc.C)), pin(cm(sc.dFc))
+    hm, hvol, hl, hmu = pin(sc.m), pin(vol), pin(sc.lam), pin(sc.mu)
+    hgrad = torch.empty(sc.n * 9, dtype=torch.float64).pin_memory()
+    h2d = sum(t.numel() * 8 for t in (hx, hv, hF, hC, hd, hm, hvol, hl, hmu))
+    d2h = hgrad.numel() * 8 + 8
+
+    def e2e_step():
+        c._set_particles_raw(sc.n, hx, hv, hF, hC, hd, hm, hvol, hl, hmu)
+        c.setup(sc.steps + 1)
+        gradient_step(c)
+        c.control_grad(0, out=hgrad)
+
+    e2e_step()
+    barrier(world)
+    ms_e2e = max_over_ranks(timed_steps(torch, c, args.steps, e2e_step), world)
+    e2e_value = units_per_step * args.steps * world / (ms_e2e / 1000.0)
+    touched = int(np.count_nonzero(c.get_grid(0, "grid_m")))
+    c.close()
+
+    # plain FP64 GPU path on the same workload
+    fp64 = None
+    if not args.no_fp64:
+        c64 = setup_ctx(dmpm, sc, "fp64", device, vol, target, sc.dt, ckpt)
+        gradient_step(c64)
+        n64 = max(1, min(args.steps, 2))
+        ms64 = timed_steps(torch, c64, n64, lambda: gradient_step(c64))
+        grad64 = c64.control_grad()
+        c64.close()
+        v64 = units_per_step * n64 / (ms64 / 1000.0)
+        relerr = float(np.linalg.norm(grad32 - grad64) / np.linalg.norm(grad64))
+        fp64 = {"value": v64 * world, "unit": UNIT, "ms_per_step": ms64 / n64,
+                "speedup_fp32_mixed_over_fp64": (value / world) / v64, "grad_relerr_vs_fp64": relerr,
+                "grad_relerr_bar": 1e-4, "meets_bar": relerr <= 1e-4}
+
+    # roofline of the dominant kernel (largest total device time)
+    peak, peak_kind = measured_hbm_gbs()
+    kern = {k: {"total_ms": v[0], "launches": v[1], "avg_us": 1000.0 * v[0] / v[1]} for k, v in kstats.items()}
+    top = max(kern, key=lambda k: kern[k]["total_ms"]) if kern else None
+    roof = None
+    if top:
+        alg = algorithmic_bytes(top, sc.n, touched)
+        achieved = alg / (kern[top]["avg_us"] * 1e-6) / 1e9
+        roof = {"kernel": top, "bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                "frac": achieved / peak, "peak_source": peak_kind + " (MEASURED_PEAKS.json hbm_gbs)",
+                "traffic": committed_traffic(top), "algorithmic_bytes_per_launch": alg,
+                "avg_launch_us": kern[top]["avg_us"]}
+        for k in kern:
+            b = algorithmic_bytes(k, sc.n, touched)
+            if b:
+                kern[k]["hbm_frac"] = b / (kern[k]["avg_us"] * 1e-6) / 1e9 / peak
+
+    cb = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        cb = cpu_baseline(sc, 1)
+        cb = {k: cb[k] for k in ("value", "unit", "cores", "kind", "sample")}
+
+    if rank == 0:
+        line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+                "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True,
+                "scaling": "weak", "vs_baseline": None,
+                "dtype": "f32 (f64 polar/SVD, stress derivative, loss and gradient sums)", "data": "synthetic",
+                "config": workload_config(sc, dt_sub, ckpt),
+                "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
+                "gpu_launches": launches, "roofline": roof, "cpu_baseline": cb, "clocks": clocks, "fp64": fp64,
+                "kernels": kern}
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        import torch.distributed as dist
+
+        dist.destroy_process_group()
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser(description=__doc__, formatter_class=argparse.RawDescriptionHelpFormatter)
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--ppc-root", type=int, default=3, help="particles per cell = ppc_root^3 (3 -> ~267k)")
+    ap.add_argument("--dt", type=float, default=0.0, help="override dt (default: configured, CFL fallback)")
+    ap.add_argument("--checkpoint-every", type=int, default=1)
+    ap.add_argument("--rollout-steps", type=int, default=0, help="override the 200 time steps (profiling runs)")
+    ap.add_argument("--no-fp64", action="store_true")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        args.warmup = 3
+    if args.impl == "reference":
+        return run_reference(args)
+    return run_ours(args)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -148,6 +148,7 @@ int dmpm_set_points_ref(dmpm_ctx* ctx, const void* points, int n);
 int dmpm_compute_volumes(dmpm_ctx* ctx);
 int dmpm_set_target_mass(dmpm_ctx* ctx, const double* target_m);
 int dmpm_rasterize_target(dmpm_ctx* ctx, int n, const double* x, double point_mass);
+int dmpm_get_target_mass(dmpm_ctx* ctx, double* out);
 
 int dmpm_setup(dmpm_ctx* ctx, int num_layers);
 int dmpm_forward(dmpm_ctx* ctx, int start_layer);
@@ -169,6 +170,16 @@ int dmpm_synchronize(dmpm_ctx* ctx);
 void* dmpm_stream(dmpm_ctx* ctx);
 /* Number of kernels this context has launched since creation. */
 int64_t dmpm_launch_count(const dmpm_ctx* ctx);
+
+/* Per-kernel device time.  With profiling on, every hot-path launch is
+ * bracketed by CUDA events on the context's stream; dmpm_kernel_stats returns
+ * the summed milliseconds and the launch count of one kernel since profiling
+ * was (re)enabled.  Kernel ids run from 0 to DMPM_NUM_KERNEL_IDS - 1;
+ * dmpm_kernel_name gives their names (p2g, g2p_p_op2, adj_p2g_gather, ...). */
+#define DMPM_NUM_KERNEL_IDS 10
+int dmpm_set_profiling(dmpm_ctx* ctx, int on);
+int dmpm_kernel_stats(dmpm_ctx* ctx, int kernel_id, double* total_ms, int64_t* launches);
+const char* dmpm_kernel_name(int kernel_id);
 
 #ifdef __cplusplus
 }

@@ -274,14 +274,22 @@ def test_errors_are_reported(gpu_ready):
 
 
 def test_nonfinite_is_flagged_not_faulted(gpu_ready):
-    """A blown-up rollout (dt far above the explicit limit) reports
-    DMPM_ERR_NONFINITE; the context stays usable."""
-    sc = scenes.small_scene(seed=4, res=12, dt=5.0, steps=6, dfc_std=0.05)
+    """A NaN control on one particle propagates to the grid and the cloud (as in
+    the reference); the engine reports DMPM_ERR_NONFINITE from forward and
+    backward, and the context stays usable."""
+    sc = scenes.small_scene(seed=4, res=12, steps=3)
     sc.vol = OracleGraph(sc, "f64").calc_volumes()
-    with make_ctx(sc, "fp32", np.zeros(int(np.prod(sc.dims)))) as c:
-        c.setup(12)
-        st = c.forward(0)
-        assert st == dmpm.ERR_NONFINITE
-        c.set_params(dt=1e-4)
-        c.setup(3)
-        assert c.forward(0) == dmpm.OK
+    bad = sc.dFc.copy()
+    bad[sc.n // 2, 0, 0] = np.nan
+    s2 = scenes.Scene(**{**sc.__dict__})
+    s2.dFc = bad
+    for prec in ("fp32", "fp64"):
+        with make_ctx(s2, prec, np.zeros(int(np.prod(sc.dims)))) as c:
+            c.setup(4)
+            assert c.forward(0) == dmpm.ERR_NONFINITE
+            c.loss()
+            assert c.backward(0) == dmpm.ERR_NONFINITE
+            c.set_particles(sc.x, sc.m, sc.lam, sc.mu, dFc=sc.dFc, vol=sc.vol)
+            c.setup(4)
+            assert c.forward(0) == dmpm.OK
+            assert np.all(np.isfinite(c.get(3, "x")))
