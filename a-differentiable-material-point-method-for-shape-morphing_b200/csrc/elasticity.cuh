@@ -76,7 +76,7 @@ template <class T> DMPM_HD m3<T> djfit_fd_mult(const m3<T>& F, const m3<T>& dF) 
     const T delta = T(1e-6);
     m3<T> acc = m3_zero<T>();
     m3<T> G = F;
-#pragma unroll 1
+#pragma unroll
     for (int ij = 0; ij < 9; ij++) {
         const int i = ij / 3, j = ij % 3;  // row-major sweep and contraction order, as Elasticity.cpp:126-140
         const T orig = G.a[i][j];

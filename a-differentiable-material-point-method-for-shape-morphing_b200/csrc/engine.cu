@@ -25,6 +25,7 @@
 
 #include "dmpm.h"
 #include "kernels.cuh"
+#include "kernels_warp.cuh"
 
 using namespace dmpm;
 
@@ -37,10 +38,14 @@ constexpr int kDefaultTileCap = 1024;
 // (dmpm_set_profiling / dmpm_kernel_stats).
 enum KernelId {
     K_P_OP1 = 0, K_P2G, K_GOP, K_G2P, K_MASS, K_NODE_LOSS, K_LOSS_DLDX, K_ADJ_SCATTER, K_ADJ_GOP, K_ADJ_GATHER,
-    K_COUNT
+    K_ADJ_FINALIZE, K_COUNT
 };
 const char* const kKernelNames[K_COUNT] = {"p_op1", "p2g", "g_op", "g2p_p_op2", "p2g_mass", "node_loss",
-                                          "loss_dldx", "adj_g2p_scatter", "adj_g_op", "adj_p2g_gather"};
+                                          "loss_dldx", "adj_g2p_scatter", "adj_g_op", "adj_p2g_gather",
+                                          "adj_finalize"};
+constexpr int kDefaultSortEvery = 8;
+// per-layer auxiliary planes of the FP32 path: G (9), polar R (9), polar S (6)
+constexpr int kAuxPlanes = 24;
 
 struct CudaError {
     cudaError_t code;
@@ -197,7 +202,17 @@ namespace {
 
 template <class T> class Engine : public EngineBase {
    public:
+    // FP32 path: cell-sorted warp items (kernels_warp.cuh); FP64 path: plain kernels (kernels.cuh)
     static constexpr bool kTiled = std::is_same<T, float>::value;
+    static constexpr bool kWarp = kTiled;
+    // one cell sort: the stable order and warp items used for steps
+    // [e * sort_every, (e + 1) * sort_every)
+    struct Epoch {
+        uint32_t* order = nullptr;
+        uint32_t* items = nullptr;
+        int n_items = 0;
+        bool valid = false;
+    };
 
     explicit Engine(dmpm_ctx* c) : ctx_(c) {}
 
@@ -338,6 +353,7 @@ template <class T> class Engine : public EngineBase {
     int block() const { return ctx_->prm.block_size > 0 ? ctx_->prm.block_size : kDefaultBlock; }
     int tile_cap() const { return ctx_->prm.tile_cap > 0 ? ctx_->prm.tile_cap : kDefaultTileCap; }
     unsigned pgrid() const { return (unsigned)((n_ + block() - 1) / block()); }
+    unsigned pgrid256() const { return (unsigned)((n_ + 255) / 256); }
     unsigned ggrid() const { return (unsigned)((G_ + 255) / 256); }
 
     void launched() {
@@ -493,6 +509,7 @@ template <class T> class Engine : public EngineBase {
         Layout want;
         want.L = num_layers; want.k_req = P.checkpoint_every; want.control = P.control_mode;
         want.keep_adj = P.keep_adjoints; want.keep_int = P.keep_intermediates; want.np = np_; want.G = G_;
+        want.sort_every = P.sort_every;
         if (want == layout_ && (int)layers_.size() == num_layers) {
             reset_layers();
             return;
@@ -555,10 +572,24 @@ template <class T> class Engine : public EngineBase {
             adj_pp_[1] = (T*)layer_arena_.alloc(st_bytes);
         }
         gadj_ = (node4<T>*)layer_arena_.alloc(gr_bytes);
-        if (!kTiled) {
-            gadj2_ = (node4<T>*)layer_arena_.alloc(gr_bytes);
+        gadj2_ = (node4<T>*)layer_arena_.alloc(2 * gr_bytes);
+        if (!kWarp) {
             gridv_ = (T*)layer_arena_.alloc(3 * G_ * sizeof(T));
             pscratch_ = (T*)layer_arena_.alloc(9 * np_ * sizeof(T));
+        } else {
+            // affine momentum matrix G of every stored/segment layer, adjoint scratch, sort state
+            const size_t g_bytes = kAuxPlanes * np_ * sizeof(T);
+            if (k_ == 1) {
+                T* base = (T*)layer_arena_.alloc((size_t)L_ * g_bytes);
+                for (int l = 0; l < L_; l++) layers_[l].G = base + (size_t)l * kAuxPlanes * np_;
+            } else {
+                gscratch_ = (T*)layer_arena_.alloc(g_bytes);
+                seg_G_.assign(k_, nullptr);
+                for (int i = 0; i < k_; i++) seg_G_[i] = (T*)layer_arena_.alloc(g_bytes);
+            }
+            adjn_ = (T*)layer_arena_.alloc(12 * np_ * sizeof(T));
+            gath_ = (T*)layer_arena_.alloc(18 * np_ * sizeof(T));
+            alloc_sort();
         }
         if (P.keep_intermediates) {
             T* b1 = (T*)layer_arena_.alloc((size_t)L_ * 9 * np_ * sizeof(T));   // P
@@ -601,10 +632,128 @@ template <class T> class Engine : public EngineBase {
         } else {
             DMPM_CK(cudaMemsetAsync(ctrl_acc_, 0, 9 * np_ * sizeof(double), ctx_->stream));
         }
+        for (Epoch& e : epochs_) e.valid = false;
         forward_done_ = false;
         loss_done_ = false;
         backward_lo_ = L_;
         seg_lo_ = seg_hi_ = -1;
+    }
+
+    // ---------------------------------------------------------- cell sort (FP32 path)
+    int sort_every() const { return ctx_->prm.sort_every > 0 ? ctx_->prm.sort_every : kDefaultSortEvery; }
+
+    void alloc_sort() {
+        const int nep = std::max(1, (L_ - 1 + sort_every() - 1) / sort_every());
+        epochs_.assign(nep, Epoch{});
+        for (Epoch& e : epochs_) {
+            e.order = (uint32_t*)layer_arena_.alloc((size_t)n_ * sizeof(uint32_t));
+            e.items = (uint32_t*)layer_arena_.alloc(((size_t)n_ + 1) * sizeof(uint32_t));
+        }
+        const size_t n = (size_t)n_;
+        sk_[0] = (uint32_t*)layer_arena_.alloc(n * 4);
+        sk_[1] = (uint32_t*)layer_arena_.alloc(n * 4);
+        sv_[0] = (uint32_t*)layer_arena_.alloc(n * 4);
+        sv_[1] = (uint32_t*)layer_arena_.alloc(n * 4);
+        sh_ = (uint32_t*)layer_arena_.alloc(n * 4);
+        sf_ = (uint32_t*)layer_arena_.alloc(n * 4);
+        const size_t rs_tiles = (n + RS_TILE - 1) / RS_TILE;
+        counts_ = (uint32_t*)layer_arena_.alloc(256 * rs_tiles * 4);
+        const size_t mx = std::max(n, 256 * rs_tiles);
+        tile_tot_ = (uint32_t*)layer_arena_.alloc(((mx + SCAN_TILE - 1) / SCAN_TILE + 1) * 4);
+        nitems_dev_ = (uint32_t*)layer_arena_.alloc(16);
+    }
+
+    template <class Op> void device_scan(uint32_t* data, size_t n, uint32_t* grand) {
+        const int tiles = (int)((n + SCAN_TILE - 1) / SCAN_TILE);
+        k_scan_tiles<Op><<<tiles, SCAN_THREADS, 0, ctx_->stream>>>(data, (int)n, tile_tot_);
+        launched();
+        k_scan_totals<Op><<<1, 1024, 0, ctx_->stream>>>(tile_tot_, tiles, grand);
+        launched();
+        k_scan_add<Op><<<tiles, SCAN_THREADS, 0, ctx_->stream>>>(data, (int)n, tile_tot_);
+        launched();
+    }
+
+    // Stable sort of the particles of a layer state by cell key; fills the
+    // epoch's order and warp items.  Keys stay in sk_[sorted_] for inspection.
+    void cell_sort(const T* st, Epoch& e) {
+        const int n = n_;
+        KeyArgs<T> ka{};
+        ka.n = n;
+        ka.np = np_;
+        ka.geo = geo_;
+        ka.st = st;
+        ka.keys = sk_[0];
+        ka.vals = sv_[0];
+        k_cell_keys<T><<<(n + 255) / 256, 256, 0, ctx_->stream>>>(ka);
+        launched();
+        const uint64_t max_key = (uint64_t)(geo_.dim[0] + 8) * (geo_.dim[1] + 8) * (geo_.dim[2] + 8);
+        int bits = 1;
+        while (bits < 32 && (1ull << bits) < max_key) bits++;
+        const int rs_tiles = (n + RS_TILE - 1) / RS_TILE;
+        int cur = 0;
+        for (int shift = 0; shift < bits; shift += 8) {
+            k_rs_upsweep<<<rs_tiles, RS_THREADS, 0, ctx_->stream>>>(sk_[cur], n, shift, counts_, rs_tiles);
+            launched();
+            device_scan<OpSum>(counts_, (size_t)256 * rs_tiles, nullptr);
+            k_rs_downsweep<<<rs_tiles, RS_THREADS, 0, ctx_->stream>>>(sk_[cur], sv_[cur], sk_[cur ^ 1], sv_[cur ^ 1], n,
+                                                                     shift, counts_, rs_tiles);
+            launched();
+            cur ^= 1;
+        }
+        sorted_ = cur;
+        DMPM_CK(cudaMemcpyAsync(e.order, sv_[cur], (size_t)n * 4, cudaMemcpyDeviceToDevice, ctx_->stream));
+        k_run_heads<<<(n + 255) / 256, 256, 0, ctx_->stream>>>(sk_[cur], n, sh_);
+        launched();
+        device_scan<OpMax>(sh_, (size_t)n, nullptr);
+        k_item_flags<<<(n + 255) / 256, 256, 0, ctx_->stream>>>(sk_[cur], sh_, n, sf_);
+        launched();
+        device_scan<OpSum>(sf_, (size_t)n, nitems_dev_);
+        k_item_starts<<<(n + 255) / 256, 256, 0, ctx_->stream>>>(sk_[cur], sh_, sf_, n, e.items);
+        launched();
+        k_item_sentinel<<<1, 1, 0, ctx_->stream>>>(e.items, nitems_dev_, n);
+        launched();
+        DMPM_CK(cudaMemcpyAsync((char*)host_misc_ + 24, nitems_dev_, 4, cudaMemcpyDeviceToHost, ctx_->stream));
+        DMPM_CK(cudaStreamSynchronize(ctx_->stream));
+        harvest();
+        e.n_items = (int)*(uint32_t*)((char*)host_misc_ + 24);
+        e.valid = true;
+    }
+
+    Epoch& epoch_for(int l, const T* st, bool allow_sort) {
+        Epoch& e = epochs_[std::min((int)epochs_.size() - 1, l / sort_every())];
+        if (allow_sort && (l % sort_every() == 0 || !e.valid)) cell_sort(st, e);
+        if (!e.valid) cell_sort(st, e);
+        return e;
+    }
+
+    void debug_cell_sort(int l, uint32_t* keys, uint32_t* order, uint32_t* items, int* n_items) {
+        if (!kWarp) throw StateError{"the cell sort belongs to the FP32 path"};
+        if (l < 0 || l >= L_) throw ArgError{"layer out of range"};
+        Epoch e{};
+        Arena tmp;
+        e.order = (uint32_t*)tmp.alloc((size_t)n_ * 4);
+        e.items = (uint32_t*)tmp.alloc(((size_t)n_ + 1) * 4);
+        cell_sort(materialize_state(l), e);
+        if (keys) DMPM_CK(cudaMemcpyAsync(keys, sk_[sorted_], (size_t)n_ * 4, cudaMemcpyDeviceToHost, ctx_->stream));
+        if (order) DMPM_CK(cudaMemcpyAsync(order, e.order, (size_t)n_ * 4, cudaMemcpyDeviceToHost, ctx_->stream));
+        if (items) DMPM_CK(cudaMemcpyAsync(items, e.items, ((size_t)e.n_items + 1) * 4, cudaMemcpyDeviceToHost, ctx_->stream));
+        DMPM_CK(cudaStreamSynchronize(ctx_->stream));
+        if (n_items) *n_items = e.n_items;
+    }
+
+    WArgs warp_args() const {
+        WArgs a{};
+        const dmpm_params& P = ctx_->prm;
+        a.n = n_;
+        a.np = np_;
+        a.geo = geo_;
+        a.dt = (float)P.dt;
+        a.drag = (float)P.drag;
+        a.s = (float)P.smoothing;
+        for (int c = 0; c < 3; c++) a.fext[c] = (float)P.f_ext[c];
+        a.cst = (const float*)cst_;
+        a.status = status_;
+        return a;
     }
 
     // pointer to the state of layer l if it is materialised (stored or in the current segment)
@@ -618,9 +767,49 @@ template <class T> class Engine : public EngineBase {
         if (k_ > 1 && l >= seg_lo_ && l < seg_hi_) return seg_grid_[l - seg_lo_];
         return nullptr;
     }
+    T* G_of(int l) {
+        if (layers_[l].G) return layers_[l].G;
+        if (k_ > 1 && l >= seg_lo_ && l < seg_hi_) return seg_G_[l - seg_lo_];
+        return nullptr;
+    }
 
-    // one ForwardTimeStep: layer l -> out (state of l+1), grid g
-    void step(int l, const T* st, T* out, node4<T>* g) {
+    // one ForwardTimeStep: layer l -> out (state of l+1), grid g, G of layer l into Gd
+    void step(int l, const T* st, T* out, node4<T>* g, T* Gd, bool allow_sort) {
+        if constexpr (kWarp) {
+            Epoch& ep = epoch_for(l, st, allow_sort);
+            WArgs a = warp_args();
+            a.items = WarpItems{ep.order, ep.items, ep.n_items};
+            a.st = (const float*)st;
+            a.st_next = (float*)out;
+            a.dfc = (const float*)layers_[l].dfc;
+            a.G = (float*)Gd;
+            a.grid = (node4<float>*)g;
+            a.P = ctx_->prm.keep_intermediates ? (float*)layers_[l].dbgP : nullptr;
+            DMPM_CK(cudaMemsetAsync(g, 0, G_ * sizeof(node4<T>), ctx_->stream));
+            const unsigned wg = (unsigned)((ep.n_items + 7) / 8);
+            pbeg(K_P_OP1);
+            k_stress<<<pgrid256(), 256, 0, ctx_->stream>>>(a);
+            launched();
+            pend();
+            if (wg) {
+                pbeg(K_P2G);
+                if (ctx_->prm.warp_general) k_p2g_w<true><<<wg, 256, 0, ctx_->stream>>>(a);
+                else k_p2g_w<false><<<wg, 256, 0, ctx_->stream>>>(a);
+                launched();
+                pend();
+            }
+            pbeg(K_GOP);
+            k_gop_inplace<<<ggrid(), 256, 0, ctx_->stream>>>((node4<float>*)g, G_, a.dt, a.fext[0], a.fext[1], a.fext[2]);
+            launched();
+            pend();
+            if (wg) {
+                pbeg(K_G2P);
+                k_g2p_w<<<wg, 256, 0, ctx_->stream>>>(a);
+                launched();
+                pend();
+            }
+            return;
+        }
         FwdArgs<T> a = fwd_args();
         a.st = st;
         a.st_next = out;
@@ -630,16 +819,10 @@ template <class T> class Engine : public EngineBase {
         a.P = ctx_->prm.keep_intermediates ? layers_[l].dbgP : (kTiled ? nullptr : pscratch_);
         DMPM_CK(cudaMemsetAsync(g, 0, G_ * sizeof(node4<T>), ctx_->stream));
         const size_t tile_b = (size_t)tile_cap() * sizeof(node4<T>);
-        if (kTiled) {
-            pbeg(K_P2G);
-            k_p2g<T, true, true><<<pgrid(), block(), tile_b, ctx_->stream>>>(a);
-            launched();
-            pend();
-            pbeg(K_G2P);
-            k_g2p<T, true><<<pgrid(), block(), tile_b, ctx_->stream>>>(a);
-            launched();
-            pend();
-        } else {
+        (void)tile_b;
+        (void)Gd;
+        (void)allow_sort;
+        {
             pbeg(K_P_OP1);
             k_p_op1<T><<<pgrid(), block(), 0, ctx_->stream>>>(a);
             launched();
@@ -668,7 +851,8 @@ template <class T> class Engine : public EngineBase {
         if (start < 0 || start >= L_) throw ArgError{"start_layer out of range"};
         reset_status();
         if (k_ == 1) {
-            for (int l = start; l + 1 < L_; l++) step(l, layers_[l].st, layers_[l + 1].st, layers_[l].grid);
+            for (int l = start; l + 1 < L_; l++)
+                step(l, layers_[l].st, layers_[l + 1].st, layers_[l].grid, layers_[l].G, true);
         } else {
             const T* cur = materialize_state(start);
             int r = 0;
@@ -676,7 +860,7 @@ template <class T> class Engine : public EngineBase {
                 T* out = layers_[l + 1].st ? layers_[l + 1].st : ring_[r];
                 if (!layers_[l + 1].st) r ^= 1;
                 // the current state may live in ring_[r] already (ping-pong)
-                step(l, cur, out, seg_grid_[0]);
+                step(l, cur, out, seg_grid_[0], gscratch_, true);
                 cur = out;
             }
             seg_lo_ = seg_hi_ = -1;  // segment scratch no longer matches
@@ -699,13 +883,14 @@ template <class T> class Engine : public EngineBase {
         const T* cur = layers_[c].st;
         for (int l = c; l < e; l++) {
             T* out = (l + 1 == e) ? nullptr : seg_st_[l - c];
+            T* Gd = seg_G_.empty() ? nullptr : seg_G_[l - c];
             if (out) {
-                step(l, cur, out, seg_grid_[l - c]);
+                step(l, cur, out, seg_grid_[l - c], Gd, false);
                 cur = out;
             } else {
                 // last step of the segment: only its grid is needed; the output
                 // (layer e) is a stored layer already, write it to scratch ring
-                step(l, cur, ring_[0], seg_grid_[l - c]);
+                step(l, cur, ring_[0], seg_grid_[l - c], Gd, false);
             }
         }
         seg_lo_ = c;
@@ -751,6 +936,66 @@ template <class T> class Engine : public EngineBase {
 
     void adjoint_step(int i) {
         const dmpm_params& P = ctx_->prm;
+        if constexpr (kWarp) {
+            Epoch& ep = epoch_for(i, state_of(i), false);
+            WArgs a = warp_args();
+            a.items = WarpItems{ep.order, ep.items, ep.n_items};
+            a.st = (const float*)state_of(i);
+            a.st_next = (float*)state_of(i + 1);
+            a.dfc = (const float*)layers_[i].dfc;
+            a.G = (float*)G_of(i);
+            a.grid = (node4<float>*)grid_of(i);
+            a.adj_next = (const float*)adj_of(i + 1, false);
+            a.adj = (float*)adj_of(i, true);
+            a.adjn = (float*)adjn_;
+            a.gath = (float*)gath_;
+            a.gadj = (node4<float>*)gadj_;
+            a.gadj2 = (node4<float>*)gadj2_;
+            a.ctrl_grad = (float*)layers_[i].ctrl_grad;
+            a.ctrl_acc = ctrl_acc_;
+            a.dbg_dLdP = P.keep_intermediates ? (float*)layers_[i].dbgdLdP : nullptr;
+            a.dbg_vnext = P.keep_intermediates ? (float*)layers_[i].dbgvn : nullptr;
+            a.dbg_Cnext = P.keep_intermediates ? (float*)layers_[i].dbgCn : nullptr;
+            if (!a.st || !a.st_next || !a.grid || !a.G) throw StateError{"internal: layer not materialised"};
+            DMPM_CK(cudaMemsetAsync(gadj_, 0, G_ * sizeof(node4<T>), ctx_->stream));
+            const bool ex = P.adjoint_mode == DMPM_ADJ_EXACT;
+            const unsigned wg = (unsigned)((ep.n_items + 7) / 8);
+            if (wg) {
+                pbeg(K_ADJ_SCATTER);
+                if (P.warp_general) {
+                    if (ex) k_adj_scatter_w<true, true><<<wg, 256, 0, ctx_->stream>>>(a);
+                    else k_adj_scatter_w<false, true><<<wg, 256, 0, ctx_->stream>>>(a);
+                } else {
+                    if (ex) k_adj_scatter_w<true, false><<<wg, 256, 0, ctx_->stream>>>(a);
+                    else k_adj_scatter_w<false, false><<<wg, 256, 0, ctx_->stream>>>(a);
+                }
+                launched();
+                pend();
+            }
+            pbeg(K_ADJ_GOP);
+            if (ex) k_adj_gop_w<true><<<ggrid(), 256, 0, ctx_->stream>>>(a.grid, a.gadj, a.gadj2, G_, a.dt, a.fext[0], a.fext[1], a.fext[2]);
+            else k_adj_gop_w<false><<<ggrid(), 256, 0, ctx_->stream>>>(a.grid, a.gadj, a.gadj2, G_, a.dt, a.fext[0], a.fext[1], a.fext[2]);
+            launched();
+            pend();
+            if (P.keep_intermediates) {
+                DMPM_CK(cudaMemcpyAsync(layers_[i].dbggdv, gadj_, G_ * sizeof(node4<T>), cudaMemcpyDeviceToDevice, ctx_->stream));
+                DMPM_CK(cudaMemcpy2DAsync(layers_[i].dbggdp, sizeof(node4<T>), gadj2_, 2 * sizeof(node4<T>),
+                                          sizeof(node4<T>), G_, cudaMemcpyDeviceToDevice, ctx_->stream));
+            }
+            if (wg) {
+                pbeg(K_ADJ_GATHER);
+                if (ex) k_adj_gather_w<true><<<wg, 256, 0, ctx_->stream>>>(a);
+                else k_adj_gather_w<false><<<wg, 256, 0, ctx_->stream>>>(a);
+                launched();
+                pend();
+            }
+            pbeg(K_ADJ_FINALIZE);
+            if (ex) k_adj_finalize<true><<<(n_ + 127) / 128, 128, 0, ctx_->stream>>>(a);
+            else k_adj_finalize<false><<<(n_ + 127) / 128, 128, 0, ctx_->stream>>>(a);
+            launched();
+            pend();
+            return;
+        }
         AdjArgs<T> a{};
         a.n = n_;
         a.np = np_;
@@ -777,21 +1022,8 @@ template <class T> class Engine : public EngineBase {
         a.status = status_;
         if (!a.st || !a.st_next || !a.grid) throw StateError{"internal: layer not materialised"};
         DMPM_CK(cudaMemsetAsync(gadj_, 0, G_ * sizeof(node4<T>), ctx_->stream));
-        const size_t tile_b = (size_t)tile_cap() * sizeof(node4<T>);
         const bool ex = P.adjoint_mode == DMPM_ADJ_EXACT;
-        if (kTiled) {
-            pbeg(K_ADJ_SCATTER);
-            if (ex) k_adj_scatter<T, true, true><<<pgrid(), block(), tile_b, ctx_->stream>>>(a);
-            else k_adj_scatter<T, true, false><<<pgrid(), block(), tile_b, ctx_->stream>>>(a);
-            launched();
-            pend();
-            if (P.keep_intermediates) debug_grid_adjoint(i, a, ex);
-            pbeg(K_ADJ_GATHER);
-            if (ex) k_adj_gather<T, true, true><<<pgrid(), block(), 2 * tile_b, ctx_->stream>>>(a);
-            else k_adj_gather<T, true, false><<<pgrid(), block(), 2 * tile_b, ctx_->stream>>>(a);
-            launched();
-            pend();
-        } else {
+        {
             pbeg(K_ADJ_SCATTER);
             if (ex) k_adj_scatter<T, false, true><<<pgrid(), block(), 0, ctx_->stream>>>(a);
             else k_adj_scatter<T, false, false><<<pgrid(), block(), 0, ctx_->stream>>>(a);
@@ -1023,6 +1255,7 @@ template <class T> class Engine : public EngineBase {
 
    private:
     struct LayerSlots {
+        T* G = nullptr;
         T* st = nullptr;
         node4<T>* grid = nullptr;
         T* dfc = nullptr;
@@ -1065,6 +1298,20 @@ template <class T> class Engine : public EngineBase {
     node4<T>* gadj2_ = nullptr;
     T* gridv_ = nullptr;
     T* pscratch_ = nullptr;
+    // FP32 path
+    T* gscratch_ = nullptr;
+    std::vector<T*> seg_G_;
+    T* adjn_ = nullptr;
+    T* gath_ = nullptr;
+    std::vector<Epoch> epochs_;
+    uint32_t* sk_[2] = {nullptr, nullptr};
+    uint32_t* sv_[2] = {nullptr, nullptr};
+    uint32_t* sh_ = nullptr;
+    uint32_t* sf_ = nullptr;
+    uint32_t* counts_ = nullptr;
+    uint32_t* tile_tot_ = nullptr;
+    uint32_t* nitems_dev_ = nullptr;
+    int sorted_ = 0;
     double* ctrl_acc_ = nullptr;
     bool forward_done_ = false, loss_done_ = false;
     int backward_lo_ = 0;
@@ -1081,11 +1328,11 @@ template <class T> class Engine : public EngineBase {
     int64_t prof_cnt_[K_COUNT] = {};
     // the layout the layer storage was allocated for (setup reuses it when unchanged)
     struct Layout {
-        int L = -1, k_req = -1, control = -1, keep_adj = -1, keep_int = -1;
+        int L = -1, k_req = -1, control = -1, keep_adj = -1, keep_int = -1, sort_every = -1;
         size_t np = 0, G = 0;
         bool operator==(const Layout& o) const {
             return L == o.L && k_req == o.k_req && control == o.control && keep_adj == o.keep_adj &&
-                   keep_int == o.keep_int && np == o.np && G == o.G;
+                   keep_int == o.keep_int && sort_every == o.sort_every && np == o.np && G == o.G;
         }
     } layout_;
 };
@@ -1186,7 +1433,8 @@ int dmpm_set_params(dmpm_ctx* ctx, const dmpm_params* p) {
     if (!ctx || !p) return DMPM_ERR_ARG;
     if (!(p->dt >= 0) || p->adjoint_mode < 0 || p->adjoint_mode > 1 || p->control_mode < 0 || p->control_mode > 1 ||
         p->loss_kind < 0 || p->loss_kind > 1 || p->checkpoint_every < 0 || p->block_size < 0 || p->block_size > 256 ||
-        (p->block_size % 32) != 0 || p->tile_cap < 0 || p->tile_cap > 1536) {
+        (p->block_size % 32) != 0 || p->tile_cap < 0 || p->tile_cap > 1536 || p->sort_every < 0 ||
+        p->warp_general < 0 || p->warp_general > 1) {
         ctx->err = "invalid dmpm_params";
         return DMPM_ERR_ARG;
     }
@@ -1276,6 +1524,17 @@ int dmpm_synchronize(dmpm_ctx* ctx) {
 }
 
 void* dmpm_stream(dmpm_ctx* ctx) { return ctx ? (void*)ctx->stream : nullptr; }
+
+int dmpm_cell_sort(dmpm_ctx* ctx, int layer, uint32_t* keys, uint32_t* order, uint32_t* item_start, int* n_items) {
+    return guarded(ctx, [&]() -> int {
+        if (ctx->precision != DMPM_FP32_MIXED) {
+            ctx->err = "the cell sort belongs to the FP32 path";
+            return DMPM_ERR_STATE;
+        }
+        static_cast<Engine<float>*>(ctx->eng.get())->debug_cell_sort(layer, keys, order, item_start, n_items);
+        return DMPM_OK;
+    });
+}
 
 int dmpm_set_profiling(dmpm_ctx* ctx, int on) {
     return with_engine(ctx, [&](auto& e) { e.set_profiling(on != 0); return DMPM_OK; });

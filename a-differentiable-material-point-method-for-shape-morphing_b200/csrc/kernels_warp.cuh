@@ -1,0 +1,670 @@
+// kernels_warp.cuh -- FP32 path kernels organised around cell-sorted warp items.
+//
+// GENERAL (a test switch) forces the per-lane reductions everywhere.
+//
+// A warp item is a run of at most 8 particles that share a cell in the sorted
+// order (sort.cuh).  One warp serves one item: lane = 4 q + s handles particle
+// slot q (0..7) and stencil slab s (0..3), i.e. the 16 nodes
+// (base_x + s, base_y + j, base_z + k), j, k in 0..3, fully unrolled with
+// compile-time j, k.  When all 8 particles of the warp share the cell (the
+// common case), scatters combine the 8 particles' contributions with a
+// butterfly reduce-scatter over the lanes of equal s, so each lane ends up
+// owning one node's complete sum and issues a single vector
+// red.global.add.v4.f32 per 8 nodes x 4 values; otherwise every lane issues
+// its own reductions.  Gathers sum the 16-node partial results of the 4 slab
+// lanes with two xor-shuffles.  The FP64 polar decomposition lives in the
+// per-particle kernels k_stress (forward) and k_adj_finalize (adjoint), so
+// the node loops keep a small register footprint.
+//
+// Math per stage is that of kernels.cuh (which cites the reference).
+#pragma once
+#include "sort.cuh"
+
+namespace dmpm {
+
+struct WarpItems {
+    const uint32_t* order;       // sorted particle indices
+    const uint32_t* item_start;  // n_items + 1 entries
+    int n_items;
+};
+
+struct ItemLane {
+    int p;       // particle index (slot 0's particle for idle lanes)
+    bool valid;  // lane carries a particle
+    int q, s;
+};
+
+__device__ __forceinline__ ItemLane item_lane(const WarpItems& it, int item) {
+    ItemLane r;
+    const int lane = threadIdx.x & 31;
+    r.q = lane >> 2;
+    r.s = lane & 3;
+    const uint32_t st = it.item_start[item];
+    const uint32_t cnt = it.item_start[item + 1] - st;
+    r.valid = (uint32_t)r.q < cnt;
+    r.p = (int)it.order[st + (r.valid ? r.q : 0)];
+    return r;
+}
+
+// true when every lane's stencil base equals lane 0's
+__device__ __forceinline__ bool warp_uniform_base(const int b[3]) {
+    const int b0 = __shfl_sync(0xffffffffu, b[0], 0), b1 = __shfl_sync(0xffffffffu, b[1], 0),
+              b2 = __shfl_sync(0xffffffffu, b[2], 0);
+    return __all_sync(0xffffffffu, b[0] == b0 && b[1] == b1 && b[2] == b2);
+}
+
+// Butterfly reduce-scatter over the 8 lanes that share lane & 3.  On return
+// v[0 .. N/8) hold the sums of the original entries off + i, with
+// off = (lane&16 ? N/2 : 0) + (lane&8 ? N/4 : 0) + (lane&4 ? N/8 : 0).
+template <int N> __device__ __forceinline__ void reduce_scatter8(float (&v)[N]) {
+    const int lane = threadIdx.x & 31;
+    {
+        const bool up = lane & 16;
+#pragma unroll
+        for (int i = 0; i < N / 2; i++) {
+            const float send = up ? v[i] : v[i + N / 2];
+            const float keep = up ? v[i + N / 2] : v[i];
+            v[i] = keep + __shfl_xor_sync(0xffffffffu, send, 16);
+        }
+    }
+    {
+        const bool up = lane & 8;
+#pragma unroll
+        for (int i = 0; i < N / 4; i++) {
+            const float send = up ? v[i] : v[i + N / 4];
+            const float keep = up ? v[i + N / 4] : v[i];
+            v[i] = keep + __shfl_xor_sync(0xffffffffu, send, 8);
+        }
+    }
+    {
+        const bool up = lane & 4;
+#pragma unroll
+        for (int i = 0; i < N / 8; i++) {
+            const float send = up ? v[i] : v[i + N / 8];
+            const float keep = up ? v[i + N / 8] : v[i];
+            v[i] = keep + __shfl_xor_sync(0xffffffffu, send, 4);
+        }
+    }
+}
+
+template <int N> __device__ __forceinline__ void reduce_slabs(float (&v)[N]) {
+#pragma unroll
+    for (int i = 0; i < N; i++) {
+        v[i] += __shfl_xor_sync(0xffffffffu, v[i], 1);
+        v[i] += __shfl_xor_sync(0xffffffffu, v[i], 2);
+    }
+}
+
+__device__ __forceinline__ bool in_grid(const GridGeom& g, int i, int j, int k) {
+    return i >= 0 && i < g.dim[0] && j >= 0 && j < g.dim[1] && k >= 0 && k < g.dim[2];
+}
+__device__ __forceinline__ size_t node_id(const GridGeom& g, int i, int j, int k) {
+    return ((size_t)i * g.dim[1] + j) * g.dim[2] + k;
+}
+
+// Node addressing of a lane's 16 stencil nodes (base_x + s, base_y + j, base_z + k):
+// node (j, k) = g00 + j * dim_z + k in 32-bit arithmetic (grids are limited to
+// 2^31 nodes) and bit 4j + k of mask says whether that node lies in the grid.
+// g00 may point outside the grid; it is only dereferenced under the mask.
+struct LaneNodes {
+    int g00, sj;
+    unsigned mask;
+};
+__device__ __forceinline__ LaneNodes lane_nodes(const GridGeom& g, const int base[3], int s) {
+    LaneNodes r;
+    const int gi = base[0] + s;
+    r.sj = g.dim[2];
+    r.g00 = (gi * g.dim[1] + base[1]) * g.dim[2] + base[2];
+    unsigned mj = 0, mk = 0;
+#pragma unroll
+    for (int t = 0; t < 4; t++) {
+        mj |= ((unsigned)(base[1] + t) < (unsigned)g.dim[1]) ? (1u << t) : 0u;
+        mk |= ((unsigned)(base[2] + t) < (unsigned)g.dim[2]) ? (1u << t) : 0u;
+    }
+    unsigned m = 0;
+#pragma unroll
+    for (int j = 0; j < 4; j++) m |= ((mj >> j) & 1u) ? (mk << (4 * j)) : 0u;
+    r.mask = ((unsigned)gi < (unsigned)g.dim[0]) ? m : 0u;
+    return r;
+}
+
+// Per-lane stencil weights: slab s of axis 0, all 4 nodes of axes 1 and 2.
+struct LaneW {
+    float d0, n0, s0;
+    float d1[4], n1[4], s1[4];
+    float d2[4], n2[4], s2[4];
+};
+// Branch-free cubic B-spline and slope (same piecewise polynomials as
+// Interpolation.h:5-30, evaluated with selects so divergent lanes do not
+// serialise).
+__device__ __forceinline__ float bsp(float q) {
+    const float a = fabsf(q);
+    const float inner = (0.5f * a - 1.f) * a * a + 2.f / 3.f;
+    const float t = 2.f - a;
+    const float outer = t * t * t * (1.f / 6.f);
+    return a < 1.f ? inner : (a < 2.f ? outer : 0.f);
+}
+__device__ __forceinline__ float bsp_slope(float q) {
+    const float a = fabsf(q);
+    const float inner = (1.5f * a - 2.f) * q;
+    const float outer = (-0.5f * a + 2.f - 2.f / a) * q;
+    return a < 1.f ? inner : (a < 2.f ? outer : 0.f);
+}
+
+// The 4 lanes of a particle (equal lane >> 2) each evaluate the weights of
+// stencil node s on all three axes; axis-1 and axis-2 values of the other
+// nodes come from the sibling lanes by shuffles.  Every lane of the warp must
+// call this (full-mask shuffles).
+__device__ __forceinline__ void lane_weights(const float x[3], const GridGeom& g, const int base[3], int s, LaneW& w,
+                                             bool slopes) {
+    const float dx = (float)g.dx, idx = 1.f / dx;
+    float d[3], n[3], sl[3];
+#pragma unroll
+    for (int c = 0; c < 3; c++) {
+        const float xg = (float)g.mn[c] + (float)(base[c] + s) * dx;
+        d[c] = xg - x[c];
+        const float q = d[c] * idx;
+        n[c] = bsp(q);
+        sl[c] = slopes ? bsp_slope(q) : 0.f;
+    }
+    w.d0 = d[0];
+    w.n0 = n[0];
+    w.s0 = sl[0];
+    const int grp = (threadIdx.x & 31) & ~3;
+#pragma unroll
+    for (int t = 0; t < 4; t++) {
+        w.d1[t] = __shfl_sync(0xffffffffu, d[1], grp + t);
+        w.n1[t] = __shfl_sync(0xffffffffu, n[1], grp + t);
+        w.d2[t] = __shfl_sync(0xffffffffu, d[2], grp + t);
+        w.n2[t] = __shfl_sync(0xffffffffu, n[2], grp + t);
+        if (slopes) {
+            w.s1[t] = __shfl_sync(0xffffffffu, sl[1], grp + t);
+            w.s2[t] = __shfl_sync(0xffffffffu, sl[2], grp + t);
+        } else {
+            w.s1[t] = 0.f;
+            w.s2[t] = 0.f;
+        }
+    }
+}
+
+__device__ __forceinline__ void load_x_base(const float* st, size_t np, int p, const GridGeom& g, float x[3],
+                                            int base[3]) {
+#pragma unroll
+    for (int c = 0; c < 3; c++) {
+        x[c] = st[(size_t)(PX + c) * np + p];
+        base[c] = stencil_base<float>(x[c] - (float)g.mn[c], (float)g.dx, g.dim[c]);
+    }
+}
+
+// ------------------------------------------------------------------ args
+struct WArgs {
+    int n;
+    size_t np;
+    GridGeom geo;
+    float dt, drag, s, fext[3];
+    WarpItems items;
+    const float* st;       // layer n state
+    float* st_next;        // layer n+1 state
+    const float* cst;      // constants
+    const float* dfc;      // dFc of layer n
+    float* G;              // [24][np] per layer: G (9), polar R (9), polar S (6: s00 s01 s02 s11 s12 s22)
+    node4<float>* grid;    // layer n grid: (p, m) after P2G, (v, m) after k_gop_inplace
+    float* P;              // debug: stress of layer n (or null)
+    unsigned* status;
+    // adjoint
+    const float* adj_next;
+    float* adj;
+    float* adjn;           // [12][np]: dLdv_next (3), dLdC_next (9)
+    float* gath;           // [18][np]: M (9), X (3), u (3), z (3)
+    node4<float>* gadj;    // (dLdv.xyz, 0)
+    node4<float>* gadj2;   // per node two records: (dLdp.xyz, dLdm), (v.xyz, m)
+    float* ctrl_grad;      // per-layer dL/d dFc [9][np] or null
+    double* ctrl_acc;      // tied FP64 accumulator or null
+    float* dbg_dLdP;
+    float* dbg_vnext;
+    float* dbg_Cnext;
+};
+
+// ------------------------------------------------------------------ forward
+// P = PK(F + dFc) in FP64;  G = -3/dx^2 dt vol P Fe^T + m C  (P_op_1 and the
+// particle-constant part of SingleParticle_to_grid, ForwardSimulation.cpp:6-9, 38)
+__global__ void __launch_bounds__(256) k_stress(WArgs a) {
+    const int p = blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= a.n) return;
+    const size_t np = a.np;
+    const m3<float> Fe = load_m3(a.st + (size_t)PF * np, np, p) + load_m3(a.dfc, np, p);
+    const m3<double> Fed = m3_cast<double>(Fe);
+    m3<double> Rd, Sd;
+    polar3(Fed, Rd, Sd);
+    const m3<double> Pd = pk_from_polar(Fed, Rd, (double)a.cst[(size_t)KLAM * np + p], (double)a.cst[(size_t)KMU * np + p]);
+    const m3<float> P = m3_cast<float>(Pd);
+    if (a.P) store_m3(a.P, np, p, P);
+    // polar factors for the adjoint (k_adj_finalize)
+    store_m3(a.G + 9 * np, np, p, m3_cast<float>(Rd));
+    a.G[18 * np + p] = (float)Sd.a[0][0];
+    a.G[19 * np + p] = (float)Sd.a[0][1];
+    a.G[20 * np + p] = (float)Sd.a[0][2];
+    a.G[21 * np + p] = (float)Sd.a[1][1];
+    a.G[22 * np + p] = (float)Sd.a[1][2];
+    a.G[23 * np + p] = (float)Sd.a[2][2];
+    const float dx = (float)a.geo.dx;
+    const float k = -3.f / (dx * dx) * a.dt * a.cst[(size_t)KVOL * np + p];
+    const m3<float> G = (k * P) * transpose(Fe) + a.cst[(size_t)KM * np + p] * load_m3(a.st + (size_t)PC * np, np, p);
+    store_m3(a.G, np, p, G);
+}
+
+// P2G: m_g += w m_p;  p_g += w (m_p v (1 - dt drag) + G (x_g - x_p))
+template <bool GENERAL> __global__ void __launch_bounds__(256, 3) k_p2g_w(WArgs a) {
+    const int item = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    if (item >= a.items.n_items) return;
+    const ItemLane L = item_lane(a.items, item);
+    const size_t np = a.np;
+    float x[3];
+    int base[3];
+    load_x_base(a.st, np, L.p, a.geo, x, base);
+    const bool uniform = !GENERAL && warp_uniform_base(base);
+    LaneW w;
+    lane_weights(x, a.geo, base, L.s, w, false);
+    const float mp = L.valid ? a.cst[(size_t)KM * np + L.p] : 0.f;
+    const float damp = 1.f - a.dt * a.drag;
+    float mvd[3], g0[3];
+    m3<float> G = load_m3(a.G, np, L.p);
+#pragma unroll
+    for (int c = 0; c < 3; c++) {
+        mvd[c] = mp * a.st[(size_t)(PV + c) * np + L.p] * damp;
+        g0[c] = G.a[c][0] * w.d0;
+    }
+    const LaneNodes N = lane_nodes(a.geo, base, L.s);
+#pragma unroll
+    for (int half = 0; half < 2; half++) {
+        float v[32];
+#pragma unroll
+        for (int jj = 0; jj < 2; jj++) {
+            const int j = 2 * half + jj;
+            float g1[3];
+#pragma unroll
+            for (int c = 0; c < 3; c++) g1[c] = g0[c] + G.a[c][1] * w.d1[j];
+            const float w01 = L.valid ? w.n0 * w.n1[j] : 0.f;
+#pragma unroll
+            for (int k = 0; k < 4; k++) {
+                const float wt = w01 * w.n2[k];
+                const int o = (jj * 4 + k) * 4;
+#pragma unroll
+                for (int c = 0; c < 3; c++) v[o + c] = wt * (mvd[c] + g1[c] + G.a[c][2] * w.d2[k]);
+                v[o + 3] = wt * mp;
+            }
+        }
+        if (uniform) {
+            reduce_scatter8<32>(v);
+            const int lane = threadIdx.x & 31;
+            const int nd = ((lane >> 4) & 1) * 4 + ((lane >> 3) & 1) * 2 + ((lane >> 2) & 1);
+            const int j = 2 * half + nd / 4, k = nd % 4;
+            if (((N.mask >> (4 * j + k)) & 1u) && (v[0] != 0.f || v[1] != 0.f || v[2] != 0.f || v[3] != 0.f))
+                red_add4(a.grid + (N.g00 + j * N.sj + k), v[0], v[1], v[2], v[3]);
+        } else if (L.valid) {
+#pragma unroll
+            for (int nd = 0; nd < 8; nd++) {
+                const int j = 2 * half + nd / 4, k = nd % 4;
+                if ((N.mask >> (4 * j + k)) & 1u)
+                    red_add4(a.grid + (N.g00 + j * N.sj + k), v[nd * 4], v[nd * 4 + 1], v[nd * 4 + 2], v[nd * 4 + 3]);
+            }
+        }
+    }
+}
+
+// G_op in place: (p, m) -> (v, m), v = p/m + dt f where |m| > FLT_EPSILON, else 0
+__global__ void k_gop_inplace(node4<float>* grid, size_t G, float dt, float f0, float f1, float f2) {
+    const size_t g = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (g >= G) return;
+    node4<float> nd = grid[g];
+    const float f[3] = {f0, f1, f2};
+    float v[3];
+    node_velocity(nd, dt, f, v);
+    nd.x = v[0];
+    nd.y = v[1];
+    nd.z = v[2];
+    grid[g] = nd;
+}
+
+// G2P + P_op_2: v' = sum w v_g;  C' = 3/dx^2 sum w v_g d^T;
+// F' = (1 - s)(I + dt C')(F + dFc) + s F;  x' = x + dt v'
+__global__ void __launch_bounds__(256, 4) k_g2p_w(WArgs a) {
+    const int item = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    if (item >= a.items.n_items) return;
+    const ItemLane L = item_lane(a.items, item);
+    const size_t np = a.np;
+    float x[3];
+    int base[3];
+    load_x_base(a.st, np, L.p, a.geo, x, base);
+    LaneW w;
+    lane_weights(x, a.geo, base, L.s, w, false);
+    float acc[12];  // v (3), C (9) row-major; C scaled by 3/dx^2 at the end
+#pragma unroll
+    for (int i = 0; i < 12; i++) acc[i] = 0.f;
+    const LaneNodes N = lane_nodes(a.geo, base, L.s);
+#pragma unroll
+    for (int j = 0; j < 4; j++) {
+        const float w01 = w.n0 * w.n1[j];
+#pragma unroll
+        for (int k = 0; k < 4; k++) {
+            if (!((N.mask >> (4 * j + k)) & 1u)) continue;
+            const node4<float> nd = a.grid[N.g00 + j * N.sj + k];
+            const float wt = w01 * w.n2[k];
+            const float vg[3] = {nd.x, nd.y, nd.z};
+            const float d[3] = {w.d0, w.d1[j], w.d2[k]};
+#pragma unroll
+            for (int r = 0; r < 3; r++) {
+                const float wv = wt * vg[r];
+                acc[r] += wv;
+#pragma unroll
+                for (int c = 0; c < 3; c++) acc[3 + 3 * r + c] += wv * d[c];
+            }
+        }
+    }
+    reduce_slabs<12>(acc);
+    if (!L.valid) return;
+    const float dx = (float)a.geo.dx;
+    const float k3 = 3.f / (dx * dx);
+    const int p = L.p;
+    m3<float> Cn;
+#pragma unroll
+    for (int r = 0; r < 3; r++)
+#pragma unroll
+        for (int c = 0; c < 3; c++) Cn.a[r][c] = k3 * acc[3 + 3 * r + c];
+    bool finite = true;
+    if (L.s == 0) {
+#pragma unroll
+        for (int c = 0; c < 3; c++) {
+            const float xn = x[c] + a.dt * acc[c];
+            a.st_next[(size_t)(PX + c) * np + p] = xn;
+            a.st_next[(size_t)(PV + c) * np + p] = acc[c];
+            finite &= isfinite(xn);
+        }
+    } else if (L.s == 1) {
+        store_m3(a.st_next + (size_t)PC * np, np, p, Cn);
+    } else {
+        // columns c of F' = (1-s)(I + dt C') Fe[:,c] + s F[:,c]; lane s=2 -> cols 0,1; s=3 -> col 2
+        const int c0 = L.s == 2 ? 0 : 2, c1 = L.s == 2 ? 2 : 3;
+        for (int c = c0; c < c1; c++) {
+            float Fc[3], Fec[3];
+#pragma unroll
+            for (int r = 0; r < 3; r++) {
+                Fc[r] = a.st[(size_t)(PF + r + 3 * c) * np + p];
+                Fec[r] = Fc[r] + a.dfc[(size_t)(r + 3 * c) * np + p];
+            }
+#pragma unroll
+            for (int r = 0; r < 3; r++) {
+                const float t = Fec[r] + a.dt * (Cn.a[r][0] * Fec[0] + Cn.a[r][1] * Fec[1] + Cn.a[r][2] * Fec[2]);
+                const float fn = (1.f - a.s) * t + a.s * Fc[r];
+                a.st_next[(size_t)(PF + r + 3 * c) * np + p] = fn;
+                finite &= isfinite(fn);
+            }
+        }
+    }
+    if (!finite) atomicOr(a.status, ST_NONFINITE_FWD);
+}
+
+// ------------------------------------------------------------------ adjoint
+// dLdv_next = dt dLdx' + dLdv';  dLdC_next = c dt dLdF' Fe^T + dLdC'
+// dLdv_g += w dLdv_next + 3/dx^2 w dLdC_next (x_g - x_p)   (BackPropagation.cpp:14-44)
+template <bool EXACT, bool GENERAL> __global__ void __launch_bounds__(256, 3) k_adj_scatter_w(WArgs a) {
+    const int item = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    if (item >= a.items.n_items) return;
+    const ItemLane L = item_lane(a.items, item);
+    const size_t np = a.np;
+    const int p = L.p;
+    float x[3];
+    int base[3];
+    load_x_base(a.st, np, p, a.geo, x, base);
+    const bool uniform = !GENERAL && warp_uniform_base(base);
+    LaneW w;
+    lane_weights(x, a.geo, base, L.s, w, false);
+    float vn[3];
+#pragma unroll
+    for (int c = 0; c < 3; c++) vn[c] = a.dt * a.adj_next[(size_t)(PX + c) * np + p] + a.adj_next[(size_t)(PV + c) * np + p];
+    const m3<float> Fe = load_m3(a.st + (size_t)PF * np, np, p) + load_m3(a.dfc, np, p);
+    const float cf = EXACT ? (1.f - a.s) * a.dt : a.dt;
+    const m3<float> Cn = (cf * load_m3(a.adj_next + (size_t)PF * np, np, p)) * transpose(Fe) +
+                         load_m3(a.adj_next + (size_t)PC * np, np, p);
+    if (L.valid) {
+        if (L.s == 0) {
+#pragma unroll
+            for (int c = 0; c < 3; c++) a.adjn[(size_t)c * np + p] = vn[c];
+            if (a.dbg_vnext) {
+#pragma unroll
+                for (int c = 0; c < 3; c++) a.dbg_vnext[(size_t)c * np + p] = vn[c];
+            }
+        } else if (L.s == 1) {
+            store_m3(a.adjn + 3 * np, np, p, Cn);
+            if (a.dbg_Cnext) store_m3(a.dbg_Cnext, np, p, Cn);
+        }
+    }
+    const float dx = (float)a.geo.dx;
+    const float k3 = 3.f / (dx * dx);
+    float c0[3];
+#pragma unroll
+    for (int r = 0; r < 3; r++) c0[r] = k3 * Cn.a[r][0] * w.d0;
+    const LaneNodes N = lane_nodes(a.geo, base, L.s);
+#pragma unroll
+    for (int half = 0; half < 2; half++) {
+        float v[32];
+#pragma unroll
+        for (int jj = 0; jj < 2; jj++) {
+            const int j = 2 * half + jj;
+            float c1[3];
+#pragma unroll
+            for (int r = 0; r < 3; r++) c1[r] = c0[r] + k3 * Cn.a[r][1] * w.d1[j];
+            const float w01 = L.valid ? w.n0 * w.n1[j] : 0.f;
+#pragma unroll
+            for (int k = 0; k < 4; k++) {
+                const float wt = w01 * w.n2[k];
+                const int o = (jj * 4 + k) * 4;
+#pragma unroll
+                for (int r = 0; r < 3; r++) v[o + r] = wt * (vn[r] + c1[r] + k3 * Cn.a[r][2] * w.d2[k]);
+                v[o + 3] = 0.f;
+            }
+        }
+        if (uniform) {
+            reduce_scatter8<32>(v);
+            const int lane = threadIdx.x & 31;
+            const int nd = ((lane >> 4) & 1) * 4 + ((lane >> 3) & 1) * 2 + ((lane >> 2) & 1);
+            const int j = 2 * half + nd / 4, k = nd % 4;
+            if (((N.mask >> (4 * j + k)) & 1u) && (v[0] != 0.f || v[1] != 0.f || v[2] != 0.f))
+                red_add4(a.gadj + (N.g00 + j * N.sj + k), v[0], v[1], v[2], 0.f);
+        } else if (L.valid) {
+#pragma unroll
+            for (int nd = 0; nd < 8; nd++) {
+                const int j = 2 * half + nd / 4, k = nd % 4;
+                if ((N.mask >> (4 * j + k)) & 1u)
+                    red_add4(a.gadj + (N.g00 + j * N.sj + k), v[nd * 4], v[nd * 4 + 1], v[nd * 4 + 2], 0.f);
+            }
+        }
+    }
+}
+
+// adjoint G_op per node: (dLdp, dLdm) from dLdv and the layer's (v, m)
+// The record pair (dLdp, dLdm), (v, m) of a node is stored contiguously (32 B)
+// so the gather reads one sector per node.
+template <bool EXACT>
+__global__ void k_adj_gop_w(const node4<float>* __restrict__ grid, const node4<float>* __restrict__ gadj,
+                            node4<float>* gadj2, size_t G, float dt, float f0, float f1, float f2) {
+    const size_t g = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (g >= G) return;
+    const node4<float> nd = grid[g];
+    const node4<float> dv = gadj[g];
+    node4<float> o{0.f, 0.f, 0.f, 0.f};
+    if (fabsf(nd.w) > (float)kFltEps) {
+        float v[3] = {nd.x, nd.y, nd.z};
+        if (EXACT) { v[0] -= dt * f0; v[1] -= dt * f1; v[2] -= dt * f2; }
+        o.x = dv.x / nd.w;
+        o.y = dv.y / nd.w;
+        o.z = dv.z / nd.w;
+        o.w = -1.f / nd.w * (v[0] * dv.x + v[1] * dv.y + v[2] * dv.z);
+    }
+    gadj2[2 * g] = o;
+    gadj2[2 * g + 1] = nd;
+}
+
+// adjoint P2G gather: per particle, over its 64 nodes,
+//   M += w d dLdp^T,  X += sigma (N'NN, NN'N, NNN'),  u += w dLdp,  z += w v_g
+//   sigma = m dLdm + dLdp.(m v c_d + G d) + v_g.(dLdv_next + 3/dx^2 dLdC_next d)
+// (the algebra of kernels.cuh:k_adj_gather); written to gath for k_adj_finalize.
+template <bool EXACT> __global__ void __launch_bounds__(256, 3) k_adj_gather_w(WArgs a) {
+    const int item = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    if (item >= a.items.n_items) return;
+    const ItemLane L = item_lane(a.items, item);
+    const size_t np = a.np;
+    const int p = L.p;
+    float x[3];
+    int base[3];
+    load_x_base(a.st, np, p, a.geo, x, base);
+    LaneW w;
+    lane_weights(x, a.geo, base, L.s, w, true);
+    const float mp = a.cst[(size_t)KM * np + p];
+    const float cd = EXACT ? (1.f - a.dt * a.drag) : 1.f;
+    const float dx = (float)a.geo.dx;
+    const float k3 = 3.f / (dx * dx);
+    float mvp[3], vn[3];
+#pragma unroll
+    for (int c = 0; c < 3; c++) {
+        mvp[c] = mp * a.st[(size_t)(PV + c) * np + p] * cd;
+        vn[c] = a.adjn[(size_t)c * np + p];
+    }
+    const m3<float> G = load_m3(a.G, np, p);
+    const m3<float> Cn = load_m3(a.adjn + 3 * np, np, p);
+    // sigma's node-dependent pieces: h_g = mvp + G d,  e_g = vn + k3 Cn d
+    float h0[3], e0[3];
+#pragma unroll
+    for (int r = 0; r < 3; r++) {
+        h0[r] = mvp[r] + G.a[r][0] * w.d0;
+        e0[r] = vn[r] + k3 * Cn.a[r][0] * w.d0;
+    }
+    float acc[18];  // M (9, row-major: M[r][c] = sum w d_r dLdp_c), X (3), u (3), z (3)
+#pragma unroll
+    for (int i = 0; i < 18; i++) acc[i] = 0.f;
+    const LaneNodes N = lane_nodes(a.geo, base, L.s);
+#pragma unroll
+    for (int j = 0; j < 4; j++) {
+        float h1[3], e1[3];
+#pragma unroll
+        for (int r = 0; r < 3; r++) {
+            h1[r] = h0[r] + G.a[r][1] * w.d1[j];
+            e1[r] = e0[r] + k3 * Cn.a[r][1] * w.d1[j];
+        }
+        const float n01 = w.n0 * w.n1[j], s01 = w.s0 * w.n1[j], n0s1 = w.n0 * w.s1[j];
+#pragma unroll
+        for (int k = 0; k < 4; k++) {
+            if (!((N.mask >> (4 * j + k)) & 1u)) continue;
+            const int g = N.g00 + j * N.sj + k;
+            const node4<float> o = a.gadj2[2 * g];
+            const node4<float> vg = a.gadj2[2 * g + 1];
+            const float wt = n01 * w.n2[k];
+            float sig = mp * o.w;
+            sig += o.x * (h1[0] + G.a[0][2] * w.d2[k]) + o.y * (h1[1] + G.a[1][2] * w.d2[k]) +
+                   o.z * (h1[2] + G.a[2][2] * w.d2[k]);
+            sig += vg.x * (e1[0] + k3 * Cn.a[0][2] * w.d2[k]) + vg.y * (e1[1] + k3 * Cn.a[1][2] * w.d2[k]) +
+                   vg.z * (e1[2] + k3 * Cn.a[2][2] * w.d2[k]);
+            acc[9] += sig * (s01 * w.n2[k]);
+            acc[10] += sig * (n0s1 * w.n2[k]);
+            acc[11] += sig * (n01 * w.s2[k]);
+            const float wo[3] = {wt * o.x, wt * o.y, wt * o.z};
+            acc[12] += wo[0];
+            acc[13] += wo[1];
+            acc[14] += wo[2];
+            acc[15] += wt * vg.x;
+            acc[16] += wt * vg.y;
+            acc[17] += wt * vg.z;
+            const float d[3] = {w.d0, w.d1[j], w.d2[k]};
+#pragma unroll
+            for (int r = 0; r < 3; r++)
+#pragma unroll
+                for (int c = 0; c < 3; c++) acc[3 * r + c] += d[r] * wo[c];
+        }
+    }
+    reduce_slabs<18>(acc);
+    if (!L.valid) return;
+    if (L.s == 0) {
+#pragma unroll
+        for (int i = 0; i < 9; i++) a.gath[(size_t)i * np + p] = acc[i];
+    } else if (L.s == 1) {
+#pragma unroll
+        for (int i = 9; i < 18; i++) a.gath[(size_t)i * np + p] = acc[i];
+    }
+}
+
+// per particle: P, polar factors and dP/dF in FP64, then the adjoint of layer n
+//   dLdP = -3/dx^2 dt vol M^T Fe,  dLdF(stress) = -3/dx^2 dt vol M P,  dLdC = m M^T
+//   dLdx = -X/dx - G^T u - 3/dx^2 dLdC_next^T z + dLdx',  dLdv = m (1 - dt drag) u
+//   REFCOMPAT: dLdF = (1-s)T + s dLdF' + stress + T + dP:dLdP,  T = (I + dt C')^T dLdF'
+//   EXACT:     dLdFe = (1-s)T + stress + dP:dLdP,  dLdF = dLdFe + s dLdF'
+template <bool EXACT> __global__ void __launch_bounds__(128) k_adj_finalize(WArgs a) {
+    const int p = blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= a.n) return;
+    const size_t np = a.np;
+    m3<float> M;
+#pragma unroll
+    for (int r = 0; r < 3; r++)
+#pragma unroll
+        for (int c = 0; c < 3; c++) M.a[r][c] = a.gath[(size_t)(3 * r + c) * np + p];
+    const m3<float> Fe = load_m3(a.st + (size_t)PF * np, np, p) + load_m3(a.dfc, np, p);
+    const m3<double> Fed = m3_cast<double>(Fe);
+    // polar factors computed in FP64 by k_stress for this layer
+    const m3<double> Rd = m3_cast<double>(load_m3(a.G + 9 * np, np, p));
+    m3<double> Sd;
+    Sd.a[0][0] = a.G[18 * np + p];
+    Sd.a[0][1] = Sd.a[1][0] = a.G[19 * np + p];
+    Sd.a[0][2] = Sd.a[2][0] = a.G[20 * np + p];
+    Sd.a[1][1] = a.G[21 * np + p];
+    Sd.a[1][2] = Sd.a[2][1] = a.G[22 * np + p];
+    Sd.a[2][2] = a.G[23 * np + p];
+    const double lam = (double)a.cst[(size_t)KLAM * np + p], mu = (double)a.cst[(size_t)KMU * np + p];
+    const m3<float> P = m3_cast<float>(pk_from_polar(Fed, Rd, lam, mu));
+    const float mp = a.cst[(size_t)KM * np + p], vol = a.cst[(size_t)KVOL * np + p];
+    const float dx = (float)a.geo.dx;
+    const float k3 = 3.f / (dx * dx);
+    const float kk = -k3 * a.dt * vol;
+    const m3<float> dLdP = kk * mtm(M, Fe);
+    const m3<float> dFstress = kk * (M * P);
+    const m3<float> G = load_m3(a.G, np, p);
+    const m3<float> Cn = load_m3(a.adjn + 3 * np, np, p);
+    float u[3], z[3], gtu[3], ctz[3];
+#pragma unroll
+    for (int c = 0; c < 3; c++) {
+        u[c] = a.gath[(size_t)(12 + c) * np + p];
+        z[c] = a.gath[(size_t)(15 + c) * np + p];
+    }
+    mtv(G, u, gtu);
+    mtv(Cn, z, ctz);
+#pragma unroll
+    for (int c = 0; c < 3; c++) {
+        const float X = a.gath[(size_t)(9 + c) * np + p];
+        a.adj[(size_t)(PX + c) * np + p] = -X / dx - gtu[c] - k3 * ctz[c] + a.adj_next[(size_t)(PX + c) * np + p];
+        a.adj[(size_t)(PV + c) * np + p] = mp * (1.f - a.dt * a.drag) * u[c];
+    }
+    store_m3(a.adj + (size_t)PC * np, np, p, mp * transpose(M));
+    const m3<float> Cnext = load_m3(a.st_next + (size_t)PC * np, np, p);
+    const m3<float> dFn = load_m3(a.adj_next + (size_t)PF * np, np, p);
+    const m3<float> Tr = mtm(m3_eye<float>() + a.dt * Cnext, dFn);
+    const m3<float> d2 = m3_cast<float>(d2_mult_from_polar<EXACT>(Fed, Rd, Sd, lam, mu, m3_cast<double>(dLdP)));
+    m3<float> dLdF, dLdFe;
+    if (EXACT) {
+        dLdFe = (1.f - a.s) * Tr + dFstress + d2;
+        dLdF = dLdFe + a.s * dFn;
+    } else {
+        dLdF = ((1.f - a.s) * Tr + a.s * dFn) + dFstress + Tr + d2;
+        dLdFe = dLdF;
+    }
+    store_m3(a.adj + (size_t)PF * np, np, p, dLdF);
+    if (a.ctrl_grad) store_m3(a.ctrl_grad, np, p, dLdFe);
+    if (a.ctrl_acc) {
+#pragma unroll
+        for (int c = 0; c < 3; c++)
+#pragma unroll
+            for (int r = 0; r < 3; r++) a.ctrl_acc[(size_t)(r + 3 * c) * np + p] += (double)dLdFe.a[r][c];
+    }
+    if (a.dbg_dLdP) store_m3(a.dbg_dLdP, np, p, dLdP);
+    if (!isfinite(dLdF.a[0][0] + dLdF.a[1][1] + dLdF.a[2][2] + a.adj[(size_t)PX * np + p]))
+        atomicOr(a.status, ST_NONFINITE_ADJ);
+}
+
+}  // namespace dmpm

@@ -207,15 +207,24 @@ template <class T> DMPM_HD void svd3(const m3<T>& A, m3<T>& U, T sig[3], m3<T>& 
         block = 1;
     }
     {
-        const int i = block, k = block + 1, o = block == 0 ? 2 : 0;
+        // two explicit branches keep every matrix index a compile-time constant
         givens_t<T> gu, gv;
         T s0, s1;
-        svd2(B.a[i][i], B.a[i][k], B.a[k][i], B.a[k][k], gu, s0, s1, gv);
-        rot_cols(U, i, k, gu);
-        rot_cols(V, i, k, gv);
-        sig[i] = s0;
-        sig[k] = s1;
-        sig[o] = B.a[o][o];
+        if (block == 0) {
+            svd2(B.a[0][0], B.a[0][1], B.a[1][0], B.a[1][1], gu, s0, s1, gv);
+            rot_cols(U, 0, 1, gu);
+            rot_cols(V, 0, 1, gv);
+            sig[0] = s0;
+            sig[1] = s1;
+            sig[2] = B.a[2][2];
+        } else {
+            svd2(B.a[1][1], B.a[1][2], B.a[2][1], B.a[2][2], gu, s0, s1, gv);
+            rot_cols(U, 1, 2, gu);
+            rot_cols(V, 1, 2, gv);
+            sig[1] = s0;
+            sig[2] = s1;
+            sig[0] = B.a[0][0];
+        }
     }
     // 4. order by decreasing magnitude (swaps keep U, V rotations)
 #pragma unroll

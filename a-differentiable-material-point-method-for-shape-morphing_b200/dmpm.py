@@ -30,7 +30,7 @@ FIELDS = {"x": 0, "v": 1, "F": 2, "C": 3, "P": 4, "m": 5, "vol": 6, "lam": 7, "m
 WIDTH = {"x": 3, "v": 3, "F": 9, "C": 9, "P": 9, "m": 1, "vol": 1, "lam": 1, "mu": 1, "dFc": 9, "dLdx": 3,
          "dLdv": 3, "dLdF": 9, "dLdC": 9, "dLdP": 9, "dLdv_next": 3, "dLdC_next": 9, "dLdFe": 9}
 GRID_FIELDS = {"grid_m": 0, "grid_v": 1, "grid_p": 2, "grid_dLdv": 3, "grid_dLdp": 4, "grid_dLdm": 5}
-NUM_KERNEL_IDS = 10
+NUM_KERNEL_IDS = 11
 GRID_WIDTH = {"grid_m": 1, "grid_v": 3, "grid_p": 3, "grid_dLdv": 3, "grid_dLdp": 3, "grid_dLdm": 1}
 
 
@@ -44,7 +44,8 @@ class Params(ctypes.Structure):
     _fields_ = [("dt", ctypes.c_double), ("drag", ctypes.c_double), ("f_ext", ctypes.c_double * 3),
                 ("smoothing", ctypes.c_double), ("adjoint_mode", ctypes.c_int), ("control_mode", ctypes.c_int),
                 ("loss_kind", ctypes.c_int), ("checkpoint_every", ctypes.c_int), ("keep_adjoints", ctypes.c_int),
-                ("keep_intermediates", ctypes.c_int), ("block_size", ctypes.c_int), ("tile_cap", ctypes.c_int)]
+                ("keep_intermediates", ctypes.c_int), ("block_size", ctypes.c_int), ("tile_cap", ctypes.c_int),
+                ("sort_every", ctypes.c_int), ("warp_general", ctypes.c_int)]
 
 
 _P = ctypes.c_void_p
@@ -91,6 +92,7 @@ def load_library(path: str = LIB_PATH) -> ctypes.CDLL:
     L.dmpm_launch_count.restype = ctypes.c_int64
     L.dmpm_set_profiling.argtypes = [_P, ctypes.c_int]
     L.dmpm_kernel_stats.argtypes = [_P, ctypes.c_int, ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_int64)]
+    L.dmpm_cell_sort.argtypes = [_P, ctypes.c_int, _P, _P, _P, ctypes.POINTER(ctypes.c_int)]
     L.dmpm_kernel_name.argtypes = [ctypes.c_int]
     L.dmpm_kernel_name.restype = ctypes.c_char_p
     _lib = L
@@ -199,7 +201,7 @@ class Context:
     def set_params(self, dt: float, drag: float = 0.0, f_ext=(0.0, 0.0, 0.0), smoothing: float = 0.0,
                    adjoint: str = "refcompat", control: str = "per_layer", loss: str = "ref",
                    checkpoint_every: int = 0, keep_adjoints: bool = False, keep_intermediates: bool = False,
-                   block_size: int = 0, tile_cap: int = 0):
+                   block_size: int = 0, tile_cap: int = 0, sort_every: int = 0, warp_general: bool = False):
         p = Params()
         self.lib.dmpm_default_params(ctypes.byref(p))
         p.dt, p.drag, p.smoothing = float(dt), float(drag), float(smoothing)
@@ -213,6 +215,8 @@ class Context:
         p.keep_intermediates = int(bool(keep_intermediates))
         p.block_size = int(block_size)
         p.tile_cap = int(tile_cap)
+        p.sort_every = int(sort_every)
+        p.warp_general = int(bool(warp_general))
         self._ck(self.lib.dmpm_set_params(self.h, ctypes.byref(p)), "set_params")
         self.params = p
 
@@ -322,6 +326,16 @@ class Context:
         out = ctypes.c_double()
         self._ck(self.lib.dmpm_dldf_norm(self.h, int(layer), ctypes.byref(out)), "dldf_norm")
         return float(out.value)
+
+    def cell_sort(self, layer: int):
+        """(sorted cell keys, stable order, item starts) of the FP32 path's cell sort on a layer."""
+        keys = np.empty(self.n, dtype=np.uint32)
+        order = np.empty(self.n, dtype=np.uint32)
+        items = np.empty(self.n + 1, dtype=np.uint32)
+        ni = ctypes.c_int()
+        self._ck(self.lib.dmpm_cell_sort(self.h, int(layer), keys.ctypes.data, order.ctypes.data, items.ctypes.data,
+                                         ctypes.byref(ni)), "cell_sort")
+        return keys, order, items[: ni.value + 1].copy()
 
     def get_points_ref(self, layer: int, points: np.ndarray) -> np.ndarray:
         assert points.dtype == np.float32 and points.shape == (self.n, 118) and points.flags.c_contiguous

@@ -124,6 +124,8 @@ typedef struct {
     int keep_intermediates;  /* keep P, dLdP, dLdv_next, dLdC_next and grid adjoints per layer */
     int block_size;          /* threads per CTA for particle kernels; 0 = default (256) */
     int tile_cap;            /* max nodes of a shared-memory tile; 0 = default */
+    int sort_every;          /* FP32 path: re-sort particles by cell every this many steps; 0 = default (8) */
+    int warp_general;        /* FP32 path: 1 disables the same-cell warp reduction (verification) */
 } dmpm_params;
 
 void dmpm_default_params(dmpm_params* p);
@@ -171,12 +173,17 @@ void* dmpm_stream(dmpm_ctx* ctx);
 /* Number of kernels this context has launched since creation. */
 int64_t dmpm_launch_count(const dmpm_ctx* ctx);
 
+/* The FP32 path's cell sort, run on a layer's state and returned for
+ * verification: keys[n] (sorted cell keys), order[n] (the stable permutation),
+ * item_start[n_items + 1] (warp items: runs of <= 8 same-cell particles). */
+int dmpm_cell_sort(dmpm_ctx* ctx, int layer, uint32_t* keys, uint32_t* order, uint32_t* item_start, int* n_items);
+
 /* Per-kernel device time.  With profiling on, every hot-path launch is
  * bracketed by CUDA events on the context's stream; dmpm_kernel_stats returns
  * the summed milliseconds and the launch count of one kernel since profiling
  * was (re)enabled.  Kernel ids run from 0 to DMPM_NUM_KERNEL_IDS - 1;
  * dmpm_kernel_name gives their names (p2g, g2p_p_op2, adj_p2g_gather, ...). */
-#define DMPM_NUM_KERNEL_IDS 10
+#define DMPM_NUM_KERNEL_IDS 11
 int dmpm_set_profiling(dmpm_ctx* ctx, int on);
 int dmpm_kernel_stats(dmpm_ctx* ctx, int kernel_id, double* total_ms, int64_t* launches);
 const char* dmpm_kernel_name(int kernel_id);

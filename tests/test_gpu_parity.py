@@ -149,12 +149,12 @@ def test_fp32_mixed_matches_fp64_oracle(gpu_ready, exact_case):
         assert normrel(c.get(0, "dLdx"), o.get(0, "dLdx")) < 1e-3
 
 
-def test_fp32_untiled_fallback_matches_tiled(gpu_ready, exact_case):
-    """tile_cap smaller than any stencil box forces every CTA onto the global path."""
+def test_fp32_general_path_matches_same_cell_reduction(gpu_ready, exact_case):
+    """warp_general disables the same-cell warp reduce-scatter; both paths agree."""
     sc, o, loss, L = exact_case
     res = []
-    for cap in (0, 8):
-        with make_ctx(sc, "fp32", o.target, adjoint="exact", tile_cap=cap) as c:
+    for general in (False, True):
+        with make_ctx(sc, "fp32", o.target, adjoint="exact", warp_general=general) as c:
             c.setup(L)
             c.forward(0)
             lo = c.loss()
@@ -163,6 +163,57 @@ def test_fp32_untiled_fallback_matches_tiled(gpu_ready, exact_case):
     assert relerr(res[0][0], res[1][0]) < 1e-5
     assert abs(res[0][1] - res[1][1]) / abs(res[1][1]) < 1e-5
     assert normrel(res[0][2], res[1][2]) < 1e-3
+
+
+@pytest.mark.parametrize("sort_every", [1, 3, 100])
+def test_fp32_sort_interval_does_not_change_results(gpu_ready, exact_case, sort_every):
+    sc, o, loss, L = exact_case
+    with make_ctx(sc, "fp32", o.target, adjoint="exact", sort_every=sort_every, keep_adjoints=True) as c:
+        c.setup(L)
+        c.forward(0)
+        assert relerr(c.get(L - 1, "x"), o.get(L - 1, "x")) < 1e-5
+        assert abs(c.loss() - loss) / abs(loss) < 1e-4
+        c.backward(0)
+        assert normrel(c.get(0, "dLdFe"), o.get(0, "dLdFe")) < 1e-3
+
+
+def _cpu_cell_keys(x, dims, dx=1.0, mn=(0.0, 0.0, 0.0)):
+    """Cell keys exactly as the engine defines them, in float32 on the CPU."""
+    x32 = np.asarray(x, dtype=np.float32)
+    q = np.floor((x32 - np.asarray(mn, dtype=np.float32)) / np.float32(dx)).astype(np.int64)
+    b = np.clip(np.clip(q, -8, np.asarray(dims) + 8) - 1, -4, np.asarray(dims))
+    c = b + 5
+    return ((c[:, 0] * (dims[1] + 8) + c[:, 1]) * (dims[2] + 8) + c[:, 2]).astype(np.uint32)
+
+
+@pytest.mark.parametrize("shuffle", [False, True])
+def test_cell_sort_is_bit_exact_stable_sort(gpu_ready, shuffle):
+    """Keys from the reference's floor division and the permutation of a stable
+    sort, bit-exact against numpy (argsort kind='stable'); items are runs of
+    at most 8 equal keys covering the sorted order."""
+    sc = scenes.small_scene(seed=21, res=24, radius=0.3, steps=4, v_std=2.0, dt=2e-4)
+    if shuffle:
+        perm = np.random.default_rng(3).permutation(sc.n)
+        for k in ("x", "v", "F", "C", "dFc", "m", "lam", "mu"):
+            setattr(sc, k, getattr(sc, k)[perm])
+    sc.vol = OracleGraph(sc, "f64").calc_volumes()
+    with make_ctx(sc, "fp32", np.zeros(int(np.prod(sc.dims))), sort_every=2) as c:
+        c.setup(5)
+        c.forward(0)
+        for layer in (0, 4):
+            keys, order, items = c.cell_sort(layer)
+            want_keys = _cpu_cell_keys(c.get(layer, "x"), sc.dims)
+            want_order = np.argsort(want_keys, kind="stable")
+            assert np.array_equal(order, want_order.astype(np.uint32))
+            assert np.array_equal(keys, want_keys[want_order])
+            assert items[0] == 0 and items[-1] == sc.n
+            sizes = np.diff(items.astype(np.int64))
+            assert np.all(sizes >= 1) and np.all(sizes <= 8)
+            for a, b in zip(items[:-1], items[1:]):
+                assert np.all(keys[a:b] == keys[a])
+            # an item boundary falls on every key change
+            changes = np.nonzero(np.diff(keys.astype(np.int64)))[0] + 1
+            assert set(changes.tolist()) <= set(items.tolist())
 
 
 def test_tied_controls_gradient_is_sum_over_layers(gpu_ready, exact_case):
