@@ -132,9 +132,15 @@ def max_over_ranks(value: float, world: int) -> float:
     import torch
     import torch.distributed as dist
 
-    t = torch.tensor([value], dtype=torch.float64, device="cuda")
+    dev = "cuda" if dist.get_backend() == "nccl" else "cpu"
+    t = torch.tensor([value], dtype=torch.float64, device=dev)
     dist.all_reduce(t, op=dist.ReduceOp.MAX)
     return float(t.item())
+
+
+def whole_job_value(units_per_rank_step: float, steps: int, world: int, ms_max: float) -> float:
+    """Units all ranks processed / the slowest rank's device time (weak scaling)."""
+    return units_per_rank_step * steps * world / (ms_max / 1000.0)
 
 
 def barrier(world: int):
@@ -353,7 +359,7 @@ def run_ours(args):
     kstats = c.kernel_stats()
     c.set_profiling(False)
     ms_max = max_over_ranks(ms, world)
-    value = units_per_step * args.steps * world / (ms_max / 1000.0)
+    value = whole_job_value(units_per_step, args.steps, world, ms_max)
     grad32 = c.control_grad()
 
     # e2e through the C ABI with pinned host buffers
@@ -374,7 +380,7 @@ def run_ours(args):
     e2e_step()
     barrier(world)
     ms_e2e = max_over_ranks(timed_steps(torch, c, args.steps, e2e_step), world)
-    e2e_value = units_per_step * args.steps * world / (ms_e2e / 1000.0)
+    e2e_value = whole_job_value(units_per_step, args.steps, world, ms_e2e)
     touched = int(np.count_nonzero(c.get_grid(0, "grid_m")))
     c.close()
 
