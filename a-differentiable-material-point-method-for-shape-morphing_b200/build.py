@@ -1,7 +1,7 @@
 """Build recipe for libdmpm.so (sm_100a) -- run by __graft_entry__.build().
 
     nvcc -gencode arch=compute_100a,code=sm_100a -lineinfo -O3 -std=c++17 \
-         -Xcompiler -fPIC -shared -I include -o <pkg>/libdmpm.so <pkg>/csrc/engine.cu
+         -Xcompiler -fPIC -shared -I include -o <pkg>/libdmpm.so <pkg>/csrc/*.cu
 
 The library is built in-tree so it travels with the repository snapshot.
 """
@@ -35,7 +35,8 @@ def build(force: bool = False, verbose: bool = False) -> str:
     srcs = _sources()
     if force or _stale(LIB, srcs):
         cmd = [NVCC, *ARCH, "-lineinfo", "-O3", "-std=c++17", "-Xcompiler", "-fPIC", "-shared",
-               "-I", os.path.join(REPO, "include"), "-o", LIB + ".tmp", os.path.join(CSRC, "engine.cu")]
+               "-I", os.path.join(REPO, "include"), "-o", LIB + ".tmp",
+               *[os.path.join(CSRC, f) for f in sorted(os.listdir(CSRC)) if f.endswith(".cu")]]
         if verbose:
             print(" ".join(cmd), file=sys.stderr)
         subprocess.check_call(cmd)

@@ -19,7 +19,7 @@ PKG_DIR = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(PKG_DIR, "libdmpm.so")
 
 # status codes / enums of include/dmpm.h
-OK, ERR_ARG, ERR_OOM, ERR_CUDA, ERR_NONFINITE, ERR_STATE = 0, 1, 2, 3, 4, 5
+OK, ERR_ARG, ERR_OOM, ERR_CUDA, ERR_NONFINITE, ERR_STATE, ERR_TOO_LARGE = 0, 1, 2, 3, 4, 5, 6
 FP64, FP32_MIXED = 0, 1
 ADJ_REFCOMPAT, ADJ_EXACT = 0, 1
 CTRL_PER_LAYER, CTRL_TIED = 0, 1
@@ -93,6 +93,8 @@ def load_library(path: str = LIB_PATH) -> ctypes.CDLL:
     L.dmpm_set_profiling.argtypes = [_P, ctypes.c_int]
     L.dmpm_kernel_stats.argtypes = [_P, ctypes.c_int, ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_int64)]
     L.dmpm_cell_sort.argtypes = [_P, ctypes.c_int, _P, _P, _P, ctypes.POINTER(ctypes.c_int)]
+    L.dmpm_compute_volumes_noalloc.argtypes = [ctypes.c_int, _P, _P, ctypes.c_int, ctypes.c_int, ctypes.c_int,
+                                               ctypes.c_float, _P, _P, _P]
     L.dmpm_kernel_name.argtypes = [ctypes.c_int]
     L.dmpm_kernel_name.restype = ctypes.c_char_p
     _lib = L

@@ -63,6 +63,7 @@ typedef struct dmpm_ctx dmpm_ctx;
 #define DMPM_ERR_CUDA 3      /* a CUDA runtime call failed */
 #define DMPM_ERR_NONFINITE 4 /* a stage produced NaN/inf (results still written, as the reference does) */
 #define DMPM_ERR_STATE 5     /* call order: e.g. backward before loss, or a layer that is not stored */
+#define DMPM_ERR_TOO_LARGE 6 /* size exceeds the fixed scratch capacity of dmpm_compute_volumes_noalloc */
 
 /* precision paths */
 #define DMPM_FP64 0       /* plain FP64 path: one kernel per reference stage, global atomics */
@@ -177,6 +178,25 @@ int64_t dmpm_launch_count(const dmpm_ctx* ctx);
  * verification: keys[n] (sorted cell keys), order[n] (the stable permutation),
  * item_start[n_items + 1] (warp items: runs of <= 8 same-cell particles). */
 int dmpm_cell_sort(dmpm_ctx* ctx, int layer, uint32_t* keys, uint32_t* order, uint32_t* item_start, int* n_items);
+
+/* Particle volumes without any device allocation.  No counterpart in the
+ * reference: it computes what dmpm_compute_volumes computes
+ * (CalculatePointCloudVolumes: vol_p = m_p / sum_g w m_g) for callers that
+ * cannot call cudaMalloc -- a frame loop that must not take the device-wide
+ * synchronisation of cudaMalloc/cudaFree, or a process whose device memory is
+ * already held by another framework's caching allocator.
+ *   x   device, n * 3 floats (x, y, z per particle, lattice units)
+ *   m   device, n floats;  vol: device, n floats (output)
+ *   min_point: host, 3 floats;  stream: a cudaStream_t (NULL = default stream)
+ * Its only scratch is a grid-mass array compiled into the library (every GPU
+ * that loads the library holds it until exit): grids above 1,048,576 nodes
+ * (dim_x * dim_y * dim_z) return DMPM_ERR_TOO_LARGE.  The array is shared by
+ * all calls on a device and cleared at the start of each call; calls whose GPU
+ * work overlaps race on it.  The first call on a device looks the array up
+ * with that device current; make it before any stream capture.  Asynchronous
+ * with respect to the host: results are ready when the stream is. */
+int dmpm_compute_volumes_noalloc(int n, const float* x, const float* m, int dim_x, int dim_y, int dim_z, float dx,
+                                 const float* min_point, float* vol, void* stream);
 
 /* Per-kernel device time.  With profiling on, every hot-path launch is
  * bracketed by CUDA events on the context's stream; dmpm_kernel_stats returns
