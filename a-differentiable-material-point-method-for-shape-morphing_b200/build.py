@@ -31,6 +31,27 @@ def _stale(target, sources):
     return any(os.path.getmtime(s) > t for s in sources)
 
 
+COMPAT = os.path.join(PKG_DIR, "compat")
+COMPAT_LIB = os.path.join(PKG_DIR, "libdmpm_compat.so")
+
+
+def build_compat(force: bool = False, verbose: bool = False) -> str:
+    """The DiffMPMLib3D-compatible C++ API over libdmpm.so (libdmpm_compat.so)."""
+    build(force=force, verbose=verbose)
+    srcs = [os.path.join(COMPAT, "dmpm_compat.cpp")] + [os.path.join(COMPAT, "DiffMPMLib3D", f)
+                                                         for f in os.listdir(os.path.join(COMPAT, "DiffMPMLib3D"))]
+    srcs.append(LIB)
+    if force or _stale(COMPAT_LIB, srcs):
+        cmd = ["g++", "-std=c++17", "-O2", "-fPIC", "-shared", "-I", COMPAT, "-I", os.path.join(REPO, "include"),
+               "-o", COMPAT_LIB + ".tmp", os.path.join(COMPAT, "dmpm_compat.cpp"), "-L", PKG_DIR, "-ldmpm",
+               "-Wl,-rpath,$ORIGIN"]
+        if verbose:
+            print(" ".join(cmd), file=sys.stderr)
+        subprocess.check_call(cmd)
+        os.replace(COMPAT_LIB + ".tmp", COMPAT_LIB)
+    return COMPAT_LIB
+
+
 def build(force: bool = False, verbose: bool = False) -> str:
     srcs = _sources()
     if force or _stale(LIB, srcs):
@@ -46,3 +67,4 @@ def build(force: bool = False, verbose: bool = False) -> str:
 
 if __name__ == "__main__":
     print(build(force="--force" in sys.argv, verbose=True))
+    print(build_compat(force="--force" in sys.argv, verbose=True))

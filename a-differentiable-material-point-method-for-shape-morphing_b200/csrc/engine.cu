@@ -1054,13 +1054,22 @@ template <class T> class Engine : public EngineBase {
 
     void backward(int control) {
         if (!loss_done_) throw StateError{"dmpm_loss must run before dmpm_backward"};
-        if (control < 0 || control > L_ - 1) throw ArgError{"control_layer out of range"};
+        backward_range(L_ - 1, control);
+    }
+
+    // Adjoint steps top-1 down to control, starting from the adjoint state of
+    // layer `top` (written by dmpm_loss, or by the caller for top < L-1).
+    void backward_range(int top, int control) {
+        if (!forward_done_ && L_ > 1) throw StateError{"dmpm_forward has not been run"};
+        if (top < 0 || top > L_ - 1) throw ArgError{"top layer out of range"};
+        if (control < 0 || control > top) throw ArgError{"control_layer out of range"};
+        if (top < L_ - 1 && !layers_[top].adj) throw StateError{"set keep_adjoints to start the adjoint below the last layer"};
         reset_status();
         if (ctrl_acc_) DMPM_CK(cudaMemsetAsync(ctrl_acc_, 0, 9 * np_ * sizeof(double), ctx_->stream));
         if (k_ == 1) {
-            for (int i = L_ - 2; i >= control; i--) adjoint_step(i);
+            for (int i = top - 1; i >= control; i--) adjoint_step(i);
         } else {
-            int i = L_ - 2;
+            int i = top - 1;
             while (i >= control) {
                 const int c = i - i % k_;
                 materialize_segment(c);
@@ -1132,6 +1141,12 @@ template <class T> class Engine : public EngineBase {
                 if (!layers_[l].st) throw StateError{"layer state is not stored (checkpointing)"};
                 const int off = field == DMPM_F_X ? PX : field == DMPM_F_V ? PV : field == DMPM_F_F ? PF : PC;
                 upload_planes(in, (field == DMPM_F_X || field == DMPM_F_V) ? 3 : 9, layers_[l].st + (size_t)off * np_);
+                break;
+            }
+            case DMPM_F_DLDX: case DMPM_F_DLDV: case DMPM_F_DLDF: case DMPM_F_DLDC: {
+                if (!layers_[l].adj) throw StateError{"adjoint fields can be set with keep_adjoints only"};
+                const int off = field == DMPM_F_DLDX ? PX : field == DMPM_F_DLDV ? PV : field == DMPM_F_DLDF ? PF : PC;
+                upload_planes(in, (field == DMPM_F_DLDX || field == DMPM_F_DLDV) ? 3 : 9, layers_[l].adj + (size_t)off * np_);
                 break;
             }
             default: throw ArgError{"field cannot be set per layer"};
@@ -1490,6 +1505,13 @@ int dmpm_loss(dmpm_ctx* ctx, double* loss) {
 int dmpm_backward(dmpm_ctx* ctx, int control_layer) {
     return with_engine(ctx, [&](auto& e) {
         e.backward(control_layer);
+        return (e.last_status() & ST_NONFINITE_ADJ) ? DMPM_ERR_NONFINITE : DMPM_OK;
+    });
+}
+
+int dmpm_backward_range(dmpm_ctx* ctx, int top_layer, int control_layer) {
+    return with_engine(ctx, [&](auto& e) {
+        e.backward_range(top_layer, control_layer);
         return (e.last_status() & ST_NONFINITE_ADJ) ? DMPM_ERR_NONFINITE : DMPM_OK;
     });
 }

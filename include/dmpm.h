@@ -157,6 +157,11 @@ int dmpm_setup(dmpm_ctx* ctx, int num_layers);
 int dmpm_forward(dmpm_ctx* ctx, int start_layer);
 int dmpm_loss(dmpm_ctx* ctx, double* loss);
 int dmpm_backward(dmpm_ctx* ctx, int control_layer);
+/* Adjoint steps from layer top_layer down to control_layer, starting from the
+ * adjoint state already in top_layer (set with dmpm_set_layer_particles when
+ * keep_adjoints is on): Back_Timestep applied top_layer - control_layer times
+ * (BackPropagation.h:7, BackPropagation.cpp:6-125). */
+int dmpm_backward_range(dmpm_ctx* ctx, int top_layer, int control_layer);
 
 int dmpm_get_particles(dmpm_ctx* ctx, int layer, int field, double* out);
 int dmpm_set_layer_particles(dmpm_ctx* ctx, int layer, int field, const double* in);
@@ -167,6 +172,22 @@ int dmpm_get_control_grad(dmpm_ctx* ctx, int layer, double* out);
 int dmpm_dldf_norm(dmpm_ctx* ctx, int layer, double* norm);
 /* Fill the state and gradient fields of an array of reference MaterialPoints for one layer. */
 int dmpm_get_points_ref(dmpm_ctx* ctx, int layer, void* points);
+
+/* Batched per-matrix functions of Elasticity.h, evaluated in FP64 on the
+ * current CUDA device with the hot path's device code.  Host arrays; F, dF and
+ * matrix outputs column-major, n matrices; lam, mu per matrix.
+ *   DMPM_ELEM_PK            out[9n]  PK_FixedCorotatedElasticity          (Elasticity.cpp:88-98)
+ *   DMPM_ELEM_D2_REFCOMPAT  out[9n]  d2_FCE_psi_dF2_mult_by_dF(F, dF)      (Elasticity.cpp:100-178)
+ *   DMPM_ELEM_D2_EXACT      out[9n]  the exact dP/dF : dF
+ *   DMPM_ELEM_POLAR         out[18n] R then S of JIXIE::polarDecomposition (ImplicitQRSVD.h:863-877)
+ *   DMPM_ELEM_ENERGY        out[n]   FixedCorotatedElasticity             (Elasticity.cpp:74-86) */
+#define DMPM_ELEM_PK 0
+#define DMPM_ELEM_D2_REFCOMPAT 1
+#define DMPM_ELEM_D2_EXACT 2
+#define DMPM_ELEM_POLAR 3
+#define DMPM_ELEM_ENERGY 4
+int dmpm_elementary(int kind, int n, const double* F, const double* lam, const double* mu, const double* dF,
+                    double* out);
 
 int dmpm_synchronize(dmpm_ctx* ctx);
 /* The context's CUDA stream (cudaStream_t) for callers that order their own work after it. */

@@ -209,6 +209,12 @@ void ref_scene_calc_volumes(void* h) {
     SingleThreadMPM::CalculatePointCloudVolumes(*s->pc, *s->grid);
 }
 
+// PointCloud::WriteEntirePointCloudToBinaryFile (PointCloud.cpp:334-346): the
+// reference's own .mpmbin writer, for pinning the on-disk format.
+void ref_scene_write_mpmbin(void* h, const char* path) {
+    static_cast<Scene*>(h)->pc->WriteEntirePointCloudToBinaryFile(path);
+}
+
 void ref_scene_get_particles(void* h, int field, real* out) {
     copy_out_particles(*static_cast<Scene*>(h)->pc, field, out);
 }

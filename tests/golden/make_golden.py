@@ -115,8 +115,25 @@ def make_rollout(prec):
     np.savez_compressed(os.path.join(HERE, "rollout_%s.npz" % prec), **out)
 
 
+def mpmbin_scene():
+    return scenes.small_scene(seed=77, res=8, radius=0.25, v_std=0.3)
+
+
+def make_mpmbin():
+    """cloud_ref.mpmbin: the reference's own PointCloud::WriteEntirePointCloudToBinaryFile
+    (PointCloud.cpp:334-346) of a small seeded cloud, to pin the .mpmbin format."""
+    import ctypes
+
+    sc = mpmbin_scene()
+    r = RefGraph(sc, "f32")
+    r.lib.ref_scene_write_mpmbin.argtypes = [ctypes.c_void_p, ctypes.c_char_p]
+    r.lib.ref_scene_write_mpmbin(r.h, os.path.join(HERE, "cloud_ref.mpmbin").encode())
+
+
 if __name__ == "__main__":
     for prec in ("f64", "f32"):
         make_elementary(prec)
         make_rollout(prec)
         print("wrote", prec)
+    make_mpmbin()
+    print("wrote cloud_ref.mpmbin")
