@@ -18,6 +18,7 @@
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <map>
 #include <memory>
 #include <string>
 #include <type_traits>
@@ -171,6 +172,39 @@ template <class T> __global__ void k_sqnorm9(const T* __restrict__ a, size_t np,
     double v = 0.0;
     if (p < n)
         for (int q = 0; q < 9; q++) { const double t = (double)a[(size_t)q * np + p]; v += t * t; }
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    if ((threadIdx.x & 31) == 0) s[threadIdx.x >> 5] = v;
+    __syncthreads();
+    if (threadIdx.x < 32) {
+        v = threadIdx.x < (blockDim.x >> 5) ? s[threadIdx.x] : 0.0;
+        for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+        if (threadIdx.x == 0) atomicAdd(out, v);
+    }
+}
+
+// Adam step on one set of controls (PointCloud::Descend_Adam, PointCloud.cpp:83-99):
+//   g = grad / norm;  m = b1 m + (1-b1) g;  v = b2 v + (1-b2) g^2;
+//   dFc -= lr (m / (1 - b1^t)) / (sqrt(v / (1 - b2^t)) + eps)
+// norm = ||grad|| from *norm2 (sum of squares) when normalising, else 1.
+template <class T, class G>
+__global__ void k_adam(T* dfc, const G* __restrict__ grad, T* mom, T* vec, size_t np, int n, const double* norm2,
+                       int normalize, float lr, float b1, float b2, float eps, float c1, float c2) {
+    const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= (size_t)9 * np) return;
+    if ((int)(i % np) >= n) return;
+    const float inv = normalize ? (float)(1.0 / sqrt(*norm2)) : 1.f;
+    const float g = (float)grad[i] * inv;
+    const float m = b1 * (float)mom[i] + (1.f - b1) * g;
+    const float v = b2 * (float)vec[i] + (1.f - b2) * g * g;
+    mom[i] = (T)m;
+    vec[i] = (T)v;
+    dfc[i] = (T)((float)dfc[i] - lr * ((m / c1) / (sqrtf(v / c2) + eps)));
+}
+template <class G> __global__ void k_sumsq(const G* __restrict__ a, size_t np, int n, double* out) {
+    __shared__ double s[32];
+    const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    double v = 0.0;
+    if (i < (size_t)9 * np && (int)(i % np) < n) { const double t = (double)a[i]; v = t * t; }
     for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
     if ((threadIdx.x & 31) == 0) s[threadIdx.x >> 5] = v;
     __syncthreads();
@@ -1153,6 +1187,52 @@ template <class T> class Engine : public EngineBase {
         }
     }
 
+    // one optimiser step on the controls of a layer (tied: the shared controls)
+    void adam_step(int l, double lr, double b1, double b2, double eps, int t, bool normalize) {
+        if (L_ <= 0) throw StateError{"dmpm_setup has not been called"};
+        if (t < 1) throw ArgError{"Adam timestep must be >= 1"};
+        T* dfc;
+        const void* grad;
+        bool grad_fp64;
+        if (ctrl_acc_) {
+            dfc = dfc0_;
+            grad = ctrl_acc_;
+            grad_fp64 = true;
+            l = -1;
+        } else {
+            if (l < 0 || l >= L_) throw ArgError{"layer out of range"};
+            dfc = layers_[l].dfc;
+            grad = layers_[l].ctrl_grad;
+            grad_fp64 = false;
+        }
+        auto it = adam_.find(l);
+        if (it == adam_.end()) {
+            T* st = (T*)misc_arena_.alloc(2 * 9 * np_ * sizeof(T));
+            DMPM_CK(cudaMemsetAsync(st, 0, 2 * 9 * np_ * sizeof(T), ctx_->stream));
+            it = adam_.emplace(l, st).first;
+        }
+        T* mom = it->second;
+        T* vec = it->second + 9 * np_;
+        double* norm2 = loss_acc_ + 1;
+        DMPM_CK(cudaMemsetAsync(norm2, 0, sizeof(double), ctx_->stream));
+        const unsigned blocks = (unsigned)((9 * np_ + 255) / 256);
+        if (grad_fp64) k_sumsq<double><<<blocks, 256, 0, ctx_->stream>>>((const double*)grad, np_, n_, norm2);
+        else k_sumsq<T><<<blocks, 256, 0, ctx_->stream>>>((const T*)grad, np_, n_, norm2);
+        launched();
+        const float c1 = 1.f - std::pow((float)b1, (float)t), c2 = 1.f - std::pow((float)b2, (float)t);
+        if (grad_fp64)
+            k_adam<T, double><<<blocks, 256, 0, ctx_->stream>>>(dfc, (const double*)grad, mom, vec, np_, n_, norm2,
+                                                                  normalize ? 1 : 0, (float)lr, (float)b1, (float)b2,
+                                                                  (float)eps, c1, c2);
+        else
+            k_adam<T, T><<<blocks, 256, 0, ctx_->stream>>>(dfc, (const T*)grad, mom, vec, np_, n_, norm2,
+                                                            normalize ? 1 : 0, (float)lr, (float)b1, (float)b2,
+                                                            (float)eps, c1, c2);
+        launched();
+        // per-layer controls of later layers are copies made by setup; the
+        // reference descends only the control layer, so nothing else changes
+    }
+
     void get_control_grad(int l, double* out) {
         if (!out) throw ArgError{"out is NULL"};
         if (ctrl_acc_) {
@@ -1327,6 +1407,7 @@ template <class T> class Engine : public EngineBase {
     uint32_t* tile_tot_ = nullptr;
     uint32_t* nitems_dev_ = nullptr;
     int sorted_ = 0;
+    std::map<int, T*> adam_;  // Adam moment buffers per control set (layer, or -1 for tied controls)
     double* ctrl_acc_ = nullptr;
     bool forward_done_ = false, loss_done_ = false;
     int backward_lo_ = 0;
@@ -1526,6 +1607,11 @@ int dmpm_set_layer_particles(dmpm_ctx* ctx, int layer, int field, const double* 
 
 int dmpm_get_grid(dmpm_ctx* ctx, int layer, int field, double* out) {
     return with_engine(ctx, [&](auto& e) { e.get_grid(layer, field, out); return DMPM_OK; });
+}
+
+int dmpm_adam_step(dmpm_ctx* ctx, int layer, double lr, double beta1, double beta2, double eps, int t,
+                   int normalize) {
+    return with_engine(ctx, [&](auto& e) { e.adam_step(layer, lr, beta1, beta2, eps, t, normalize != 0); return DMPM_OK; });
 }
 
 int dmpm_get_control_grad(dmpm_ctx* ctx, int layer, double* out) {

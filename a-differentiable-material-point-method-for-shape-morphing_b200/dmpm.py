@@ -85,6 +85,8 @@ def load_library(path: str = LIB_PATH) -> ctypes.CDLL:
     L.dmpm_get_control_grad.argtypes = [_P, ctypes.c_int, _P]
     L.dmpm_dldf_norm.argtypes = [_P, ctypes.c_int, ctypes.POINTER(ctypes.c_double)]
     L.dmpm_get_points_ref.argtypes = [_P, ctypes.c_int, _P]
+    L.dmpm_adam_step.argtypes = [_P, ctypes.c_int, ctypes.c_double, ctypes.c_double, ctypes.c_double,
+                                 ctypes.c_double, ctypes.c_int, ctypes.c_int]
     L.dmpm_synchronize.argtypes = [_P]
     L.dmpm_stream.argtypes = [_P]
     L.dmpm_stream.restype = _P
@@ -323,6 +325,12 @@ class Context:
         a = np.empty(self.n * 9, dtype=np.float64)
         self._ck(self.lib.dmpm_get_control_grad(self.h, int(layer), a.ctypes.data), "control_grad")
         return _from_cm(a)
+
+    def adam_step(self, t: int, lr: float = 1e-2, beta1: float = 0.9, beta2: float = 0.999, eps: float = 1e-5,
+                  layer: int = 0, normalize: bool = True):
+        """Descend_Adam on the controls (device); t is the 1-based step count."""
+        self._ck(self.lib.dmpm_adam_step(self.h, int(layer), lr, beta1, beta2, eps, int(t), int(normalize)),
+                 "adam_step")
 
     def dldf_norm(self, layer: int = 0) -> float:
         out = ctypes.c_double()

@@ -438,6 +438,165 @@ def run_ours(args):
     return 0
 
 
+# ---------------------------------------------------------------- configs 0, 2, 4
+def _cfl_dt(sc):
+    """Configured dt, or half the explicit CFL limit when the configured dt exceeds it."""
+    lim = sc.cfl_dt()
+    return (sc.dt, None) if sc.dt <= lim else (0.5 * lim, sc.dt)
+
+
+def _scene_inputs(dmpm, sc, device):
+    with dmpm.Context("fp64", device) as c64:
+        c64.load_scene(sc)
+        c64.set_params(dt=sc.dt)
+        c64.setup(1)
+        return c64.get(0, "vol"), c64.target_mass()
+
+
+def _mem_used_gb(torch, device):
+    free, total = torch.cuda.mem_get_info(device)
+    return (total - free) / 1e9
+
+
+def run_config0(args):
+    """Config 0 at full size: the plain FP64 GPU path against the reference's own
+    FP64 build (oracle/_ref) on the same scene -- forward state, loss and the
+    reference-compatible adjoint -- plus both throughputs."""
+    import torch
+
+    import dmpm
+    from oracle import lib as olib
+
+    sc = scenes.config_scene(0)
+    sc.dt, dt_sub = _cfl_dt(sc)
+    vol, target = _scene_inputs(dmpm, sc, 0)
+    sc.vol = vol
+    L = sc.steps + 1
+    out = {"mode": "config0", "particles": sc.n, "grid": list(sc.dims), "steps": sc.steps, "dt": sc.dt,
+           "dt_substituted_from": dt_sub, "loss": "reference log-mass + penalty", "adjoint": "refcompat"}
+    c = setup_ctx(dmpm, sc, "fp64", 0, vol, target, sc.dt, 1)
+    c.set_params(dt=sc.dt, drag=sc.drag, f_ext=sc.f_ext, smoothing=sc.smoothing, adjoint="refcompat",
+                 control="per_layer", keep_adjoints=True)
+    c.setup(L)
+    gradient_step(c)
+    ms = timed_steps(torch, c, 1, lambda: gradient_step(c))
+    g_loss = c.loss()
+    c.backward(0)
+    out["gpu_fp64_particle_steps_per_s"] = sc.n * sc.steps / (ms / 1000.0)
+    if olib.ref_available("f64"):
+        r = olib.RefGraph(sc, "f64", target_m=target)
+        r.setup(L, sc.dt, sc.drag, sc.f_ext, sc.smoothing)
+        t0 = time.perf_counter()
+        r.forward(0)
+        r_loss = r.loss()
+        r.backward(0)
+        t_ref = time.perf_counter() - t0
+        rel = lambda a, b: float(np.max(np.abs(a - b)) / np.max(np.abs(b)))
+        out.update({"ref_fp64_particle_steps_per_s": sc.n * sc.steps / t_ref,
+                    "relerr_x_last": rel(c.get(L - 1, "x"), r.get(L - 1, "x")),
+                    "relerr_loss": abs(g_loss - r_loss) / abs(r_loss),
+                    "relerr_dLdF_layer0": rel(c.get(0, "dLdF"), r.get(0, "dLdF")),
+                    "relerr_dLdx_layer0": rel(c.get(0, "dLdx"), r.get(0, "dLdx")),
+                    "parity_bar": 1e-10})
+    else:
+        out["ref_fp64"] = "unavailable: oracle/_ref not built"
+    c.close()
+    print(json.dumps(out), flush=True)
+    return 0
+
+
+def run_config2(args):
+    """Config 2: union of 3 spheres, 128^3, 500 steps -- store-all vs checkpoint
+    every 25 steps (peak HBM, recompute overhead), FP32-mixed, exact adjoint."""
+    import torch
+
+    import dmpm
+
+    sc = scenes.config_scene(2)
+    if args.rollout_steps:
+        sc.steps = args.rollout_steps
+    sc.dt, dt_sub = _cfl_dt(sc)
+    vol, target = _scene_inputs(dmpm, sc, 0)
+    out = {"mode": "config2", "particles": sc.n, "grid": list(sc.dims), "steps": sc.steps, "dt": sc.dt,
+           "dt_substituted_from": dt_sub}
+    grads = {}
+    for ckpt in (1, 25):
+        torch.cuda.synchronize()
+        base = _mem_used_gb(torch, 0)
+        c = setup_ctx(dmpm, sc, "fp32", 0, vol, target, sc.dt, ckpt)
+        gradient_step(c)
+        used = _mem_used_gb(torch, 0) - base
+        n = max(1, args.steps // 4)
+        ms = timed_steps(torch, c, n, lambda: gradient_step(c)) / n
+        grads[ckpt] = c.control_grad()
+        out["ckpt%d" % ckpt] = {"ms_per_gradient": ms, "particle_steps_per_s": sc.n * sc.steps / (ms / 1000.0),
+                                "hbm_gb": used, "engine_bytes_gb": c.info()["device_bytes"] / 1e9,
+                                "checkpoint_every": c.info()["checkpoint_every"]}
+        c.close()
+    out["recompute_overhead"] = out["ckpt25"]["ms_per_gradient"] / out["ckpt1"]["ms_per_gradient"] - 1.0
+    out["grad_relerr_ckpt25_vs_store_all"] = float(np.linalg.norm(grads[25] - grads[1]) / np.linalg.norm(grads[1]))
+    if not args.no_fp64:
+        c64 = setup_ctx(dmpm, sc, "fp64", 0, vol, target, sc.dt, 25)
+        t0 = time.perf_counter()
+        gradient_step(c64)
+        g64 = c64.control_grad()
+        out["fp64_ckpt25_s"] = time.perf_counter() - t0
+        out["grad_relerr_fp32_vs_fp64"] = float(np.linalg.norm(grads[25] - g64) / np.linalg.norm(g64))
+        c64.close()
+    print(json.dumps(out), flush=True)
+    return 0
+
+
+def run_config4(args):
+    """Config 4: sphere -> torus at 256^3 (~8M particles), 400 steps, checkpoint
+    every 20, 30 device Adam iterations (lr 1e-2) on tied controls; loss curve,
+    per-iteration time, FP32 gradient error vs the FP64 GPU path at iterations
+    1 and the last."""
+    import torch
+
+    import dmpm
+
+    sc = scenes.config_scene(4)
+    if args.rollout_steps:
+        sc.steps = args.rollout_steps
+    sc.dt, dt_sub = _cfl_dt(sc)
+    vol, target = _scene_inputs(dmpm, sc, 0)
+    iters = args.iters
+    out = {"mode": "config4", "particles": sc.n, "grid": list(sc.dims), "steps": sc.steps, "dt": sc.dt,
+           "dt_substituted_from": dt_sub, "checkpoint_every": 20, "iterations": iters, "lr": 1e-2}
+    torch.cuda.synchronize()
+    base = _mem_used_gb(torch, 0)
+    c = setup_ctx(dmpm, sc, "fp32", 0, vol, target, sc.dt, 20)
+    out["hbm_gb_fp32"] = _mem_used_gb(torch, 0) - base
+    losses, times, relerrs = [], [], {}
+
+    def fp64_relerr(grad32):
+        c64 = setup_ctx(dmpm, sc, "fp64", 0, vol, target, sc.dt, 20)
+        d = c.get(0, "dFc")
+        c64.set_layer(0, "dFc", d)
+        gradient_step(c64)
+        g64 = c64.control_grad()
+        c64.close()
+        return float(np.linalg.norm(grad32 - g64) / np.linalg.norm(g64))
+
+    for it in range(1, iters + 1):
+        holder = {}
+        ms = timed_steps(torch, c, 1, lambda: holder.update(loss=gradient_step(c)))
+        losses.append(holder["loss"])
+        if it in (1, iters) and not args.no_fp64:
+            relerrs[it] = fp64_relerr(c.control_grad())
+        t0 = time.perf_counter()
+        c.adam_step(t=it, lr=1e-2)
+        c.synchronize()
+        times.append(ms + 1000.0 * (time.perf_counter() - t0))
+    out.update({"loss_curve": losses, "ms_per_iteration": times,
+                "particle_steps_per_s": sc.n * sc.steps / (float(np.median(times)) / 1000.0),
+                "grad_relerr_vs_fp64": relerrs})
+    c.close()
+    print(json.dumps(out), flush=True)
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser(description=__doc__, formatter_class=argparse.RawDescriptionHelpFormatter)
     ap.add_argument("--gpus", type=int, default=1)
@@ -450,11 +609,19 @@ def main():
     ap.add_argument("--rollout-steps", type=int, default=0, help="override the 200 time steps (profiling runs)")
     ap.add_argument("--no-fp64", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--config", type=int, default=1, help="1 = headline workload; 0, 2, 4 = extra measurements")
+    ap.add_argument("--iters", type=int, default=30, help="config 4: Adam iterations")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
     if args.impl == "reference":
         return run_reference(args)
+    if args.config == 0:
+        return run_config0(args)
+    if args.config == 2:
+        return run_config2(args)
+    if args.config == 4:
+        return run_config4(args)
     return run_ours(args)
 
 

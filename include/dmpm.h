@@ -170,6 +170,13 @@ int dmpm_get_grid(dmpm_ctx* ctx, int layer, int field, double* out);
  * sum over layers (layer ignored). */
 int dmpm_get_control_grad(dmpm_ctx* ctx, int layer, double* out);
 int dmpm_dldf_norm(dmpm_ctx* ctx, int layer, double* norm);
+/* One Adam step on the controls, on the device: PointCloud::Descend_Adam
+ * (PointCloud.cpp:83-99) applied to the control gradient of `layer` (tied
+ * controls: the summed gradient; layer ignored).  normalize = 1 divides the
+ * gradient by its norm first, as the reference does with Compute_dLdF_Norm.
+ * Moment buffers live in the context; t is the 1-based step count. */
+int dmpm_adam_step(dmpm_ctx* ctx, int layer, double lr, double beta1, double beta2, double eps, int t,
+                   int normalize);
 /* Fill the state and gradient fields of an array of reference MaterialPoints for one layer. */
 int dmpm_get_points_ref(dmpm_ctx* ctx, int layer, void* points);
 

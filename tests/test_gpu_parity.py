@@ -344,3 +344,30 @@ def test_nonfinite_is_flagged_not_faulted(gpu_ready):
             c.setup(4)
             assert c.forward(0) == dmpm.OK
             assert np.all(np.isfinite(c.get(3, "x")))
+
+
+def test_device_adam_step_matches_reference_formula(gpu_ready, exact_case):
+    """dmpm_adam_step = PointCloud::Descend_Adam on the tied control gradient,
+    with the gradient divided by its norm (PointCloud.cpp:83-99)."""
+    sc, o, loss, L = exact_case
+    with make_ctx(sc, "fp32", o.target, adjoint="exact", control="tied") as c:
+        c.setup(L)
+        c.forward(0)
+        c.loss()
+        c.backward(0)
+        g = c.control_grad()
+        d0 = c.get(0, "dFc")
+        c.adam_step(t=1, lr=1e-2, beta1=0.9, beta2=0.999, eps=1e-5)
+        d1 = c.get(0, "dFc")
+        # a second step reuses the moments
+        c.adam_step(t=2, lr=1e-2, beta1=0.9, beta2=0.999, eps=1e-5)
+        d2 = c.get(0, "dFc")
+    gn = g / np.linalg.norm(g)
+    m = 0.1 * gn
+    v = 0.001 * gn * gn
+    want1 = d0 - 1e-2 * (m / (1 - 0.9)) / (np.sqrt(v / (1 - 0.999)) + 1e-5)
+    m2 = 0.9 * m + 0.1 * gn
+    v2 = 0.999 * v + 0.001 * gn * gn
+    want2 = want1 - 1e-2 * (m2 / (1 - 0.81)) / (np.sqrt(v2 / (1 - 0.999 ** 2)) + 1e-5)
+    assert relerr(d1 - d0, want1 - d0) < 1e-4
+    assert relerr(d2 - d0, want2 - d0) < 1e-4
