@@ -27,8 +27,10 @@
 #include "dmpm.h"
 #include "kernels.cuh"
 #include "kernels_warp.cuh"
+#include "host_common.cuh"
 
 using namespace dmpm;
+using namespace dmpm_host;
 
 namespace {
 
@@ -48,73 +50,6 @@ constexpr int kDefaultSortEvery = 8;
 // per-layer auxiliary planes of the FP32 path: G (9), polar R (9), polar S (6)
 constexpr int kAuxPlanes = 24;
 
-struct CudaError {
-    cudaError_t code;
-    std::string what;
-};
-
-#define DMPM_CK(call)                                                                        \
-    do {                                                                                     \
-        cudaError_t e_ = (call);                                                             \
-        if (e_ != cudaSuccess) throw CudaError{e_, std::string(#call) + ": " + cudaGetErrorString(e_)}; \
-    } while (0)
-
-struct ArgError {
-    std::string what;
-};
-struct StateError {
-    std::string what;
-};
-
-size_t round_up(size_t a, size_t b) { return (a + b - 1) / b * b; }
-
-// Device allocation owner.
-class Arena {
-   public:
-    ~Arena() { release(); }
-    void* alloc(size_t bytes) {
-        if (bytes == 0) return nullptr;
-        void* p = nullptr;
-        cudaError_t e = cudaMalloc(&p, round_up(bytes, 256));
-        if (e != cudaSuccess) {
-            cudaGetLastError();
-            throw CudaError{e, "cudaMalloc(" + std::to_string(bytes) + " bytes): " + cudaGetErrorString(e)};
-        }
-        ptrs_.push_back(p);
-        bytes_ += round_up(bytes, 256);
-        return p;
-    }
-    void release() {
-        for (void* p : ptrs_) cudaFree(p);
-        ptrs_.clear();
-        bytes_ = 0;
-    }
-    size_t bytes() const { return bytes_; }
-
-   private:
-    std::vector<void*> ptrs_;
-    size_t bytes_ = 0;
-};
-
-// ---------------------------------------------------------------- layout kernels
-template <class T> __global__ void k_unpack(const double* __restrict__ src, int width, int n, T* dst, size_t np) {
-    const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= (size_t)n * width) return;
-    const int p = (int)(i / width), q = (int)(i % width);
-    dst[(size_t)q * np + p] = (T)src[i];
-}
-template <class T> __global__ void k_pack(const T* __restrict__ src, size_t np, int width, int n, double* dst) {
-    const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= (size_t)n * width) return;
-    const int p = (int)(i / width), q = (int)(i % width);
-    dst[i] = (double)src[(size_t)q * np + p];
-}
-template <class T> __global__ void k_pack_acc(const double* __restrict__ src, size_t np, int n, double* dst) {
-    const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= (size_t)n * 9) return;
-    const int p = (int)(i / 9), q = (int)(i % 9);
-    dst[i] = src[(size_t)q * np + p];
-}
 // Reference MaterialPoint (118 floats): x 0, v 3, F 6, C 15, P 24, m 33, vol 34,
 // lam 35, mu 36, dFc 37 (MaterialPoint.h:18-46).
 template <class T>
@@ -373,7 +308,7 @@ template <class T> class Engine : public EngineBase {
     LossArgs<T> loss_args() const {
         LossArgs<T> a{};
         a.n = n_;
-        a.np = np_;
+        a.np = a.npc = np_;
         a.geo = geo_;
         a.cst = cst_;
         a.target = target_;
@@ -519,7 +454,7 @@ template <class T> class Engine : public EngineBase {
             launched();
             LossArgs<T> a = loss_args();
             a.n = n;
-            a.np = npt;
+            a.np = a.npc = npt;
             a.st = st;
             a.cst = cst;
             a.grid = scratch_grid_;
@@ -534,6 +469,17 @@ template <class T> class Engine : public EngineBase {
 
     // ---------------------------------------------------------- layers
     bool stored(int l) const { return k_ == 1 || l % k_ == 0 || l == L_ - 1; }
+    int control_stride() const { return ctx_->prm.control_stride > 1 ? ctx_->prm.control_stride : 1; }
+    // per-layer controls: does layer l own its dFc and gradient (a control frame)?
+    bool owns_controls(int l) const {
+        return ctx_->prm.control_mode == DMPM_CTRL_PER_LAYER &&
+               (control_stride() == 1 || (l % control_stride() == 0 && l < L_ - 1));
+    }
+    int num_control_layers() const {
+        int c = 0;
+        for (int l = 0; l < L_; l++) c += owns_controls(l) ? 1 : 0;
+        return c;
+    }
 
     void setup(int num_layers) {
         check_scene();
@@ -544,6 +490,7 @@ template <class T> class Engine : public EngineBase {
         want.L = num_layers; want.k_req = P.checkpoint_every; want.control = P.control_mode;
         want.keep_adj = P.keep_adjoints; want.keep_int = P.keep_intermediates; want.np = np_; want.G = G_;
         want.sort_every = P.sort_every;
+        want.stride = control_stride();
         if (want == layout_ && (int)layers_.size() == num_layers) {
             reset_layers();
             return;
@@ -560,7 +507,7 @@ template <class T> class Engine : public EngineBase {
             size_t free_b = 0, total_b = 0;
             DMPM_CK(cudaMemGetInfo(&free_b, &total_b));
             const double need = (double)L_ * (st_bytes + gr_bytes) +
-                                (per_layer ? 2.0 * L_ * 9 * np_ * sizeof(T) : 0.0) +
+                                (per_layer ? 2.0 * num_control_layers() * 9 * np_ * sizeof(T) : 0.0) +
                                 (P.keep_adjoints ? (double)L_ * st_bytes : 0.0);
             k = need < 0.8 * (double)free_b ? 1 : std::max(2, (int)std::ceil(std::sqrt((double)L_)));
         }
@@ -585,11 +532,20 @@ template <class T> class Engine : public EngineBase {
         }
         // controls
         if (per_layer) {
-            T* dbase = (T*)layer_arena_.alloc((size_t)L_ * 9 * np_ * sizeof(T));
-            T* gbase = (T*)layer_arena_.alloc((size_t)L_ * 9 * np_ * sizeof(T));
-            for (int l = 0; l < L_; l++) {
-                layers_[l].dfc = dbase + (size_t)l * 9 * np_;
-                layers_[l].ctrl_grad = gbase + (size_t)l * 9 * np_;
+            // control frames own a dFc copy and a gradient; the other layers read
+            // the uploaded dFc, which nothing writes
+            const size_t nc = (size_t)num_control_layers();
+            T* dbase = (T*)layer_arena_.alloc(nc * 9 * np_ * sizeof(T));
+            T* gbase = (T*)layer_arena_.alloc(nc * 9 * np_ * sizeof(T));
+            for (int l = 0, c = 0; l < L_; l++) {
+                if (owns_controls(l)) {
+                    layers_[l].dfc = dbase + (size_t)c * 9 * np_;
+                    layers_[l].ctrl_grad = gbase + (size_t)c * 9 * np_;
+                    c++;
+                } else {
+                    layers_[l].dfc = dfc0_;
+                    layers_[l].ctrl_grad = nullptr;
+                }
             }
             ctrl_acc_ = nullptr;
         } else {
@@ -660,6 +616,7 @@ template <class T> class Engine : public EngineBase {
         DMPM_CK(cudaMemcpyAsync(layers_[0].st, st0_, st_bytes, cudaMemcpyDeviceToDevice, ctx_->stream));
         if (ctx_->prm.control_mode == DMPM_CTRL_PER_LAYER) {
             for (int l = 0; l < L_; l++) {
+                if (!owns_controls(l)) continue;
                 DMPM_CK(cudaMemcpyAsync(layers_[l].dfc, dfc0_, 9 * np_ * sizeof(T), cudaMemcpyDeviceToDevice, ctx_->stream));
                 DMPM_CK(cudaMemsetAsync(layers_[l].ctrl_grad, 0, 9 * np_ * sizeof(T), ctx_->stream));
             }
@@ -779,7 +736,7 @@ template <class T> class Engine : public EngineBase {
         WArgs a{};
         const dmpm_params& P = ctx_->prm;
         a.n = n_;
-        a.np = np_;
+        a.np = a.npl = a.npn = np_;
         a.geo = geo_;
         a.dt = (float)P.dt;
         a.drag = (float)P.drag;
@@ -827,8 +784,8 @@ template <class T> class Engine : public EngineBase {
             pend();
             if (wg) {
                 pbeg(K_P2G);
-                if (ctx_->prm.warp_general) k_p2g_w<true><<<wg, 256, 0, ctx_->stream>>>(a);
-                else k_p2g_w<false><<<wg, 256, 0, ctx_->stream>>>(a);
+                if (ctx_->prm.warp_general) k_p2g_w<true, false><<<wg, 256, 0, ctx_->stream>>>(a);
+                else k_p2g_w<false, false><<<wg, 256, 0, ctx_->stream>>>(a);
                 launched();
                 pend();
             }
@@ -838,7 +795,7 @@ template <class T> class Engine : public EngineBase {
             pend();
             if (wg) {
                 pbeg(K_G2P);
-                k_g2p_w<<<wg, 256, 0, ctx_->stream>>>(a);
+                k_g2p_w<false><<<wg, 256, 0, ctx_->stream>>>(a);
                 launched();
                 pend();
             }
@@ -997,11 +954,11 @@ template <class T> class Engine : public EngineBase {
             if (wg) {
                 pbeg(K_ADJ_SCATTER);
                 if (P.warp_general) {
-                    if (ex) k_adj_scatter_w<true, true><<<wg, 256, 0, ctx_->stream>>>(a);
-                    else k_adj_scatter_w<false, true><<<wg, 256, 0, ctx_->stream>>>(a);
+                    if (ex) k_adj_scatter_w<true, true, false><<<wg, 256, 0, ctx_->stream>>>(a);
+                    else k_adj_scatter_w<false, true, false><<<wg, 256, 0, ctx_->stream>>>(a);
                 } else {
-                    if (ex) k_adj_scatter_w<true, false><<<wg, 256, 0, ctx_->stream>>>(a);
-                    else k_adj_scatter_w<false, false><<<wg, 256, 0, ctx_->stream>>>(a);
+                    if (ex) k_adj_scatter_w<true, false, false><<<wg, 256, 0, ctx_->stream>>>(a);
+                    else k_adj_scatter_w<false, false, false><<<wg, 256, 0, ctx_->stream>>>(a);
                 }
                 launched();
                 pend();
@@ -1018,8 +975,8 @@ template <class T> class Engine : public EngineBase {
             }
             if (wg) {
                 pbeg(K_ADJ_GATHER);
-                if (ex) k_adj_gather_w<true><<<wg, 256, 0, ctx_->stream>>>(a);
-                else k_adj_gather_w<false><<<wg, 256, 0, ctx_->stream>>>(a);
+                if (ex) k_adj_gather_w<true, false><<<wg, 256, 0, ctx_->stream>>>(a);
+                else k_adj_gather_w<false, false><<<wg, 256, 0, ctx_->stream>>>(a);
                 launched();
                 pend();
             }
@@ -1159,7 +1116,8 @@ template <class T> class Engine : public EngineBase {
             case DMPM_F_DLDV_NEXT: download_planes(need_dbg(layers_[l].dbgvn), 3, out); break;
             case DMPM_F_DLDC_NEXT: download_planes(need_dbg(layers_[l].dbgCn), 9, out); break;
             case DMPM_F_DLDFE:
-                if (!layers_[l].ctrl_grad) throw StateError{"tied controls: use dmpm_get_control_grad"};
+                if (ctrl_acc_) throw StateError{"tied controls: use dmpm_get_control_grad"};
+                if (!layers_[l].ctrl_grad) throw ArgError{"layer is not a control frame (control_stride)"};
                 download_planes(layers_[l].ctrl_grad, 9, out);
                 break;
             default: throw ArgError{"unknown particle field"};
@@ -1170,7 +1128,10 @@ template <class T> class Engine : public EngineBase {
         if (l < 0 || l >= L_) throw ArgError{"layer out of range"};
         if (!in) throw ArgError{"in is NULL"};
         switch (field) {
-            case DMPM_F_DFC: upload_planes(in, 9, layers_[l].dfc); break;
+            case DMPM_F_DFC:
+                if (!ctrl_acc_ && !owns_controls(l)) throw ArgError{"layer is not a control frame (control_stride)"};
+                upload_planes(in, 9, layers_[l].dfc);
+                break;
             case DMPM_F_X: case DMPM_F_V: case DMPM_F_F: case DMPM_F_C: {
                 if (!layers_[l].st) throw StateError{"layer state is not stored (checkpointing)"};
                 const int off = field == DMPM_F_X ? PX : field == DMPM_F_V ? PV : field == DMPM_F_F ? PF : PC;
@@ -1201,6 +1162,7 @@ template <class T> class Engine : public EngineBase {
             l = -1;
         } else {
             if (l < 0 || l >= L_) throw ArgError{"layer out of range"};
+            if (!owns_controls(l)) throw ArgError{"layer is not a control frame (control_stride)"};
             dfc = layers_[l].dfc;
             grad = layers_[l].ctrl_grad;
             grad_fp64 = false;
@@ -1244,6 +1206,7 @@ template <class T> class Engine : public EngineBase {
             return;
         }
         if (l < 0 || l >= L_) throw ArgError{"layer out of range"};
+        if (!layers_[l].ctrl_grad) throw ArgError{"layer is not a control frame (control_stride)"};
         download_planes(layers_[l].ctrl_grad, 9, out);
     }
 
@@ -1424,11 +1387,12 @@ template <class T> class Engine : public EngineBase {
     int64_t prof_cnt_[K_COUNT] = {};
     // the layout the layer storage was allocated for (setup reuses it when unchanged)
     struct Layout {
-        int L = -1, k_req = -1, control = -1, keep_adj = -1, keep_int = -1, sort_every = -1;
+        int L = -1, k_req = -1, control = -1, keep_adj = -1, keep_int = -1, sort_every = -1, stride = -1;
         size_t np = 0, G = 0;
         bool operator==(const Layout& o) const {
             return L == o.L && k_req == o.k_req && control == o.control && keep_adj == o.keep_adj &&
-                   keep_int == o.keep_int && sort_every == o.sort_every && np == o.np && G == o.G;
+                   keep_int == o.keep_int && sort_every == o.sort_every && stride == o.stride && np == o.np &&
+                   G == o.G;
         }
     } layout_;
 };
@@ -1530,7 +1494,7 @@ int dmpm_set_params(dmpm_ctx* ctx, const dmpm_params* p) {
     if (!(p->dt >= 0) || p->adjoint_mode < 0 || p->adjoint_mode > 1 || p->control_mode < 0 || p->control_mode > 1 ||
         p->loss_kind < 0 || p->loss_kind > 1 || p->checkpoint_every < 0 || p->block_size < 0 || p->block_size > 256 ||
         (p->block_size % 32) != 0 || p->tile_cap < 0 || p->tile_cap > 1536 || p->sort_every < 0 ||
-        p->warp_general < 0 || p->warp_general > 1) {
+        p->warp_general < 0 || p->warp_general > 1 || p->control_stride < 0) {
         ctx->err = "invalid dmpm_params";
         return DMPM_ERR_ARG;
     }

@@ -1,0 +1,80 @@
+// host_common.cuh -- host-side helpers shared by the one-scene engine
+// (engine.cu) and the batch engine (batch.cu): error types, the CUDA call
+// check, the device allocation owner and the SoA <-> row-major copy kernels.
+#pragma once
+#include <cuda_runtime.h>
+
+#include <string>
+#include <vector>
+
+namespace dmpm_host {
+
+struct CudaError {
+    cudaError_t code;
+    std::string what;
+};
+
+#define DMPM_CK(call)                                                                        \
+    do {                                                                                     \
+        cudaError_t e_ = (call);                                                             \
+        if (e_ != cudaSuccess) throw CudaError{e_, std::string(#call) + ": " + cudaGetErrorString(e_)}; \
+    } while (0)
+
+struct ArgError {
+    std::string what;
+};
+struct StateError {
+    std::string what;
+};
+
+inline size_t round_up(size_t a, size_t b) { return (a + b - 1) / b * b; }
+
+// Device allocation owner.
+class Arena {
+   public:
+    ~Arena() { release(); }
+    void* alloc(size_t bytes) {
+        if (bytes == 0) return nullptr;
+        void* p = nullptr;
+        cudaError_t e = cudaMalloc(&p, round_up(bytes, 256));
+        if (e != cudaSuccess) {
+            cudaGetLastError();
+            throw CudaError{e, "cudaMalloc(" + std::to_string(bytes) + " bytes): " + cudaGetErrorString(e)};
+        }
+        ptrs_.push_back(p);
+        bytes_ += round_up(bytes, 256);
+        return p;
+    }
+    void release() {
+        for (void* p : ptrs_) cudaFree(p);
+        ptrs_.clear();
+        bytes_ = 0;
+    }
+    size_t bytes() const { return bytes_; }
+
+   private:
+    std::vector<void*> ptrs_;
+    size_t bytes_ = 0;
+};
+
+
+// ---------------------------------------------------------------- layout kernels
+template <class T> __global__ void k_unpack(const double* __restrict__ src, int width, int n, T* dst, size_t np) {
+    const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= (size_t)n * width) return;
+    const int p = (int)(i / width), q = (int)(i % width);
+    dst[(size_t)q * np + p] = (T)src[i];
+}
+template <class T> __global__ void k_pack(const T* __restrict__ src, size_t np, int width, int n, double* dst) {
+    const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= (size_t)n * width) return;
+    const int p = (int)(i / width), q = (int)(i % width);
+    dst[i] = (double)src[(size_t)q * np + p];
+}
+template <class T> __global__ void k_pack_acc(const double* __restrict__ src, size_t np, int n, double* dst) {
+    const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= (size_t)n * 9) return;
+    const int p = (int)(i / 9), q = (int)(i % 9);
+    dst[i] = src[(size_t)q * np + p];
+}
+}  // namespace dmpm_host

@@ -357,7 +357,8 @@ template <class T, bool TILED> __global__ void __launch_bounds__(256) k_g2p(FwdA
 // ------------------------------------------------------------------ loss
 template <class T> struct LossArgs {
     int n;
-    size_t np;
+    size_t np;           // plane stride of st and adj
+    size_t npc;          // plane stride of cst
     GridGeom geo;
     const T* st;         // last layer state
     const T* cst;
@@ -386,7 +387,7 @@ template <class T, bool TILED> __global__ void __launch_bounds__(256) k_p2g_mass
             x[c] = a.st[(size_t)(PX + c) * a.np + p];
             base[c] = stencil_base<T>(x[c] - (T)a.geo.mn[c], dx, a.geo.dim[c]);
         }
-        mp = a.cst[(size_t)KM * a.np + p];
+        mp = a.cst[(size_t)KM * a.npc + p];
     }
     axis_w<T> w[3];
 #pragma unroll
@@ -484,7 +485,7 @@ template <class T> __global__ void __launch_bounds__(256) k_loss_dldx(LossArgs<T
     axis_w<T> w[3];
 #pragma unroll
     for (int c = 0; c < 3; c++) axis_weights(x[c], (T)a.geo.mn[c], dx, base[c], w[c], true);
-    const T mp = a.cst[(size_t)KM * a.np + p];
+    const T mp = a.cst[(size_t)KM * a.npc + p];
     T acc[3] = {0, 0, 0};
     const T ndx = -T(1) / dx;
 #pragma unroll 2
@@ -830,7 +831,7 @@ template <class T> __global__ void k_volumes(LossArgs<T> a, T* vol_out) {
         if (gi < 0 || gi >= a.geo.dim[0] || gj < 0 || gj >= a.geo.dim[1] || gk < 0 || gk >= a.geo.dim[2]) continue;
         mg += w[0].n[di] * w[1].n[dj] * w[2].n[dk] * a.grid[((size_t)gi * a.geo.dim[1] + gj) * a.geo.dim[2] + gk].w;
     }
-    const T mp = a.cst[(size_t)KM * a.np + p];
+    const T mp = a.cst[(size_t)KM * a.npc + p];
     vol_out[p] = (fabs(mg) > (T)kFltEps) ? mp / mg : T(0);
 }
 

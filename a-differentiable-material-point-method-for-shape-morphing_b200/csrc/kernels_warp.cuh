@@ -197,17 +197,49 @@ __device__ __forceinline__ void load_x_base(const float* st, size_t np, int p, c
 }
 
 // ------------------------------------------------------------------ args
+// Minimum resident blocks per SM (the register cap the compiler works to) for
+// the per-particle FP64 kernels: k_stress at 256 threads per block (2: 128
+// registers, no spills; 1 lets it take 132 and run one block per SM),
+// k_adj_finalize at 128 (4: 128 registers with a 32-byte spill, 11 % faster
+// than the 168-register build on the 64^3, 267k-particle workload).
+#ifndef DMPM_STRESS_MIN_BLOCKS
+#define DMPM_STRESS_MIN_BLOCKS 2
+#endif
+#ifndef DMPM_FINALIZE_MIN_BLOCKS
+#define DMPM_FINALIZE_MIN_BLOCKS 4
+#endif
+// and for the adjoint gather (256 threads per block)
+#ifndef DMPM_GATHER_MIN_BLOCKS
+#define DMPM_GATHER_MIN_BLOCKS 3
+#endif
+
+// Grid of one instance of a batch: its geometry, the offset of its first node
+// in the batch's concatenated grids and of its first cell key.
+struct InstGeo {
+    GridGeom g;
+    int goff;
+    uint32_t koff;
+};
+
+// Plane strides: np for the per-particle constants, controls and adjoint
+// scratch; npl for the state, affine/polar planes and adjoint of layer n;
+// npn for the state and adjoint of layer n + 1.  One scene: all three equal.
+// A batch stores each layer for the instances still running, so its layers
+// have their own strides.
 struct WArgs {
     int n;
-    size_t np;
+    size_t np, npl, npn;
     GridGeom geo;
     float dt, drag, s, fext[3];
     WarpItems items;
+    const uint32_t* n_items_dev;  // item count on the device (grid-stride launches), or null: items.n_items
+    const InstGeo* ig;            // batch: per-instance grids, indexed by item_inst
+    const uint16_t* item_inst;
     const float* st;       // layer n state
     float* st_next;        // layer n+1 state
     const float* cst;      // constants
     const float* dfc;      // dFc of layer n
-    float* G;              // [24][np] per layer: G (9), polar R (9), polar S (6: s00 s01 s02 s11 s12 s22)
+    float* G;              // [24][npl] per layer: G (9), polar R (9), polar S (6: s00 s01 s02 s11 s12 s22)
     node4<float>* grid;    // layer n grid: (p, m) after P2G, (v, m) after k_gop_inplace
     float* P;              // debug: stress of layer n (or null)
     unsigned* status;
@@ -225,95 +257,152 @@ struct WArgs {
     float* dbg_Cnext;
 };
 
+// Warp items are visited by a loop over the launch's warps: a batch launch
+// has a persistent grid sized to the SMs, a one-scene launch one warp per item.
+__device__ __forceinline__ int item_count(const WArgs& a) {
+    return a.n_items_dev ? (int)*a.n_items_dev : a.items.n_items;
+}
+__device__ __forceinline__ int first_warp() { return (int)((blockIdx.x * blockDim.x + threadIdx.x) >> 5); }
+// batch launches are persistent (grid-stride over the items); one-scene
+// launches give every item its own warp, so their loop body runs once
+template <bool BATCH> __device__ __forceinline__ int next_item(int item, int nit) {
+    return BATCH ? item + (int)((gridDim.x * blockDim.x) >> 5) : nit;
+}
+template <bool BATCH> __device__ __forceinline__ void item_grid(const WArgs& a, int item, GridGeom& g, int& goff) {
+    if constexpr (BATCH) {
+        const InstGeo& ig = a.ig[a.item_inst[item]];
+        g = ig.g;
+        goff = ig.goff;
+    } else {
+        g = a.geo;
+        goff = 0;
+    }
+}
+
+// Gathers over a warp whose 32 lanes share one stencil base (all 8 particles
+// of the item in one cell, the common case after the cell sort) first copy
+// the item's 64 stencil nodes, R consecutive node4 records each, from global
+// memory into the warp's shared-memory slice: 2R independent 16-byte loads per
+// lane, all in flight together, instead of 16 R dependent loads per lane.
+// Record r of stencil node (s, j, k) lands at dst[R (16 s + 4 j + k) + r];
+// nodes outside the grid are stored as zeros.  Warp kernels run 256-thread
+// blocks (8 warps), one slice per warp.
+#ifndef DMPM_STAGE_NODES
+#define DMPM_STAGE_NODES 1
+#endif
+template <int R>
+__device__ __forceinline__ void stage_stencil(const node4<float>* __restrict__ src, const GridGeom& g, int goff,
+                                              const int base[3], node4<float>* dst) {
+    const int lane = threadIdx.x & 31;
+    __syncwarp();  // the previous item's readers are done with the slice
+#pragma unroll
+    for (int i = 0; i < 2 * R; i++) {
+        const int t = lane + 32 * i;
+        const int n = t / R, r = t % R;
+        const int gi = base[0] + (n >> 4), gj = base[1] + ((n >> 2) & 3), gk = base[2] + (n & 3);
+        const bool in = (unsigned)gi < (unsigned)g.dim[0] && (unsigned)gj < (unsigned)g.dim[1] &&
+                        (unsigned)gk < (unsigned)g.dim[2];
+        dst[t] = in ? src[(size_t)R * (unsigned)((gi * g.dim[1] + gj) * g.dim[2] + gk + goff) + r]
+                    : node4<float>{0.f, 0.f, 0.f, 0.f};
+    }
+    __syncwarp();
+}
+
 // ------------------------------------------------------------------ forward
 // P = PK(F + dFc) in FP64;  G = -3/dx^2 dt vol P Fe^T + m C  (P_op_1 and the
 // particle-constant part of SingleParticle_to_grid, ForwardSimulation.cpp:6-9, 38)
-__global__ void __launch_bounds__(256) k_stress(WArgs a) {
+static __global__ void __launch_bounds__(256, DMPM_STRESS_MIN_BLOCKS) k_stress(WArgs a) {
+    const size_t np = a.np, npl = a.npl;
     const int p = blockIdx.x * blockDim.x + threadIdx.x;
-    if (p >= a.n) return;
-    const size_t np = a.np;
-    const m3<float> Fe = load_m3(a.st + (size_t)PF * np, np, p) + load_m3(a.dfc, np, p);
-    const m3<double> Fed = m3_cast<double>(Fe);
-    m3<double> Rd, Sd;
-    polar3(Fed, Rd, Sd);
-    const m3<double> Pd = pk_from_polar(Fed, Rd, (double)a.cst[(size_t)KLAM * np + p], (double)a.cst[(size_t)KMU * np + p]);
-    const m3<float> P = m3_cast<float>(Pd);
-    if (a.P) store_m3(a.P, np, p, P);
-    // polar factors for the adjoint (k_adj_finalize)
-    store_m3(a.G + 9 * np, np, p, m3_cast<float>(Rd));
-    a.G[18 * np + p] = (float)Sd.a[0][0];
-    a.G[19 * np + p] = (float)Sd.a[0][1];
-    a.G[20 * np + p] = (float)Sd.a[0][2];
-    a.G[21 * np + p] = (float)Sd.a[1][1];
-    a.G[22 * np + p] = (float)Sd.a[1][2];
-    a.G[23 * np + p] = (float)Sd.a[2][2];
-    const float dx = (float)a.geo.dx;
-    const float k = -3.f / (dx * dx) * a.dt * a.cst[(size_t)KVOL * np + p];
-    const m3<float> G = (k * P) * transpose(Fe) + a.cst[(size_t)KM * np + p] * load_m3(a.st + (size_t)PC * np, np, p);
-    store_m3(a.G, np, p, G);
+    if (p < a.n) {
+        const m3<float> Fe = load_m3(a.st + (size_t)PF * npl, npl, p) + load_m3(a.dfc, np, p);
+        const m3<double> Fed = m3_cast<double>(Fe);
+        m3<double> Rd, Sd;
+        polar3(Fed, Rd, Sd);
+        const m3<double> Pd = pk_from_polar(Fed, Rd, (double)a.cst[(size_t)KLAM * np + p], (double)a.cst[(size_t)KMU * np + p]);
+        const m3<float> P = m3_cast<float>(Pd);
+        if (a.P) store_m3(a.P, npl, p, P);
+        // polar factors for the adjoint (k_adj_finalize)
+        store_m3(a.G + 9 * npl, npl, p, m3_cast<float>(Rd));
+        a.G[18 * npl + p] = (float)Sd.a[0][0];
+        a.G[19 * npl + p] = (float)Sd.a[0][1];
+        a.G[20 * npl + p] = (float)Sd.a[0][2];
+        a.G[21 * npl + p] = (float)Sd.a[1][1];
+        a.G[22 * npl + p] = (float)Sd.a[1][2];
+        a.G[23 * npl + p] = (float)Sd.a[2][2];
+        const float dx = (float)a.geo.dx;
+        const float k = -3.f / (dx * dx) * a.dt * a.cst[(size_t)KVOL * np + p];
+        const m3<float> G = (k * P) * transpose(Fe) + a.cst[(size_t)KM * np + p] * load_m3(a.st + (size_t)PC * npl, npl, p);
+        store_m3(a.G, npl, p, G);
+    }
 }
 
 // P2G: m_g += w m_p;  p_g += w (m_p v (1 - dt drag) + G (x_g - x_p))
-template <bool GENERAL> __global__ void __launch_bounds__(256, 3) k_p2g_w(WArgs a) {
-    const int item = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-    if (item >= a.items.n_items) return;
-    const ItemLane L = item_lane(a.items, item);
-    const size_t np = a.np;
-    float x[3];
-    int base[3];
-    load_x_base(a.st, np, L.p, a.geo, x, base);
-    const bool uniform = !GENERAL && warp_uniform_base(base);
-    LaneW w;
-    lane_weights(x, a.geo, base, L.s, w, false);
-    const float mp = L.valid ? a.cst[(size_t)KM * np + L.p] : 0.f;
-    const float damp = 1.f - a.dt * a.drag;
-    float mvd[3], g0[3];
-    m3<float> G = load_m3(a.G, np, L.p);
+template <bool GENERAL, bool BATCH> __global__ void __launch_bounds__(256, 3) k_p2g_w(WArgs a) {
+    const int nit = item_count(a);
+    const size_t np = a.np, npl = a.npl;
+    for (int item = first_warp(); item < nit; item = next_item<BATCH>(item, nit)) {
+        GridGeom geo;
+        int goff;
+        item_grid<BATCH>(a, item, geo, goff);
+        const ItemLane L = item_lane(a.items, item);
+        float x[3];
+        int base[3];
+        load_x_base(a.st, npl, L.p, geo, x, base);
+        const bool uniform = !GENERAL && warp_uniform_base(base);
+        LaneW w;
+        lane_weights(x, geo, base, L.s, w, false);
+        const float mp = L.valid ? a.cst[(size_t)KM * np + L.p] : 0.f;
+        const float damp = 1.f - a.dt * a.drag;
+        float mvd[3], g0[3];
+        m3<float> G = load_m3(a.G, npl, L.p);
 #pragma unroll
-    for (int c = 0; c < 3; c++) {
-        mvd[c] = mp * a.st[(size_t)(PV + c) * np + L.p] * damp;
-        g0[c] = G.a[c][0] * w.d0;
-    }
-    const LaneNodes N = lane_nodes(a.geo, base, L.s);
-#pragma unroll
-    for (int half = 0; half < 2; half++) {
-        float v[32];
-#pragma unroll
-        for (int jj = 0; jj < 2; jj++) {
-            const int j = 2 * half + jj;
-            float g1[3];
-#pragma unroll
-            for (int c = 0; c < 3; c++) g1[c] = g0[c] + G.a[c][1] * w.d1[j];
-            const float w01 = L.valid ? w.n0 * w.n1[j] : 0.f;
-#pragma unroll
-            for (int k = 0; k < 4; k++) {
-                const float wt = w01 * w.n2[k];
-                const int o = (jj * 4 + k) * 4;
-#pragma unroll
-                for (int c = 0; c < 3; c++) v[o + c] = wt * (mvd[c] + g1[c] + G.a[c][2] * w.d2[k]);
-                v[o + 3] = wt * mp;
-            }
+        for (int c = 0; c < 3; c++) {
+            mvd[c] = mp * a.st[(size_t)(PV + c) * npl + L.p] * damp;
+            g0[c] = G.a[c][0] * w.d0;
         }
-        if (uniform) {
-            reduce_scatter8<32>(v);
-            const int lane = threadIdx.x & 31;
-            const int nd = ((lane >> 4) & 1) * 4 + ((lane >> 3) & 1) * 2 + ((lane >> 2) & 1);
-            const int j = 2 * half + nd / 4, k = nd % 4;
-            if (((N.mask >> (4 * j + k)) & 1u) && (v[0] != 0.f || v[1] != 0.f || v[2] != 0.f || v[3] != 0.f))
-                red_add4(a.grid + (N.g00 + j * N.sj + k), v[0], v[1], v[2], v[3]);
-        } else if (L.valid) {
+        LaneNodes N = lane_nodes(geo, base, L.s);
+        N.g00 += goff;
 #pragma unroll
-            for (int nd = 0; nd < 8; nd++) {
+        for (int half = 0; half < 2; half++) {
+            float v[32];
+#pragma unroll
+            for (int jj = 0; jj < 2; jj++) {
+                const int j = 2 * half + jj;
+                float g1[3];
+#pragma unroll
+                for (int c = 0; c < 3; c++) g1[c] = g0[c] + G.a[c][1] * w.d1[j];
+                const float w01 = L.valid ? w.n0 * w.n1[j] : 0.f;
+#pragma unroll
+                for (int k = 0; k < 4; k++) {
+                    const float wt = w01 * w.n2[k];
+                    const int o = (jj * 4 + k) * 4;
+#pragma unroll
+                    for (int c = 0; c < 3; c++) v[o + c] = wt * (mvd[c] + g1[c] + G.a[c][2] * w.d2[k]);
+                    v[o + 3] = wt * mp;
+                }
+            }
+            if (uniform) {
+                reduce_scatter8<32>(v);
+                const int lane = threadIdx.x & 31;
+                const int nd = ((lane >> 4) & 1) * 4 + ((lane >> 3) & 1) * 2 + ((lane >> 2) & 1);
                 const int j = 2 * half + nd / 4, k = nd % 4;
-                if ((N.mask >> (4 * j + k)) & 1u)
-                    red_add4(a.grid + (N.g00 + j * N.sj + k), v[nd * 4], v[nd * 4 + 1], v[nd * 4 + 2], v[nd * 4 + 3]);
+                if (((N.mask >> (4 * j + k)) & 1u) && (v[0] != 0.f || v[1] != 0.f || v[2] != 0.f || v[3] != 0.f))
+                    red_add4(a.grid + (N.g00 + j * N.sj + k), v[0], v[1], v[2], v[3]);
+            } else if (L.valid) {
+#pragma unroll
+                for (int nd = 0; nd < 8; nd++) {
+                    const int j = 2 * half + nd / 4, k = nd % 4;
+                    if ((N.mask >> (4 * j + k)) & 1u)
+                        red_add4(a.grid + (N.g00 + j * N.sj + k), v[nd * 4], v[nd * 4 + 1], v[nd * 4 + 2], v[nd * 4 + 3]);
+                }
             }
         }
     }
 }
 
 // G_op in place: (p, m) -> (v, m), v = p/m + dt f where |m| > FLT_EPSILON, else 0
-__global__ void k_gop_inplace(node4<float>* grid, size_t G, float dt, float f0, float f1, float f2) {
+static __global__ void k_gop_inplace(node4<float>* grid, size_t G, float dt, float f0, float f1, float f2) {
     const size_t g = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (g >= G) return;
     node4<float> nd = grid[g];
@@ -328,28 +417,24 @@ __global__ void k_gop_inplace(node4<float>* grid, size_t G, float dt, float f0, 
 
 // G2P + P_op_2: v' = sum w v_g;  C' = 3/dx^2 sum w v_g d^T;
 // F' = (1 - s)(I + dt C')(F + dFc) + s F;  x' = x + dt v'
-__global__ void __launch_bounds__(256, 4) k_g2p_w(WArgs a) {
-    const int item = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-    if (item >= a.items.n_items) return;
-    const ItemLane L = item_lane(a.items, item);
-    const size_t np = a.np;
-    float x[3];
-    int base[3];
-    load_x_base(a.st, np, L.p, a.geo, x, base);
-    LaneW w;
-    lane_weights(x, a.geo, base, L.s, w, false);
-    float acc[12];  // v (3), C (9) row-major; C scaled by 3/dx^2 at the end
+template <bool BATCH> __global__ void __launch_bounds__(256, 4) k_g2p_w(WArgs a) {
+    const int nit = item_count(a);
+    const size_t np = a.np, npl = a.npl, npn = a.npn;
+    for (int item = first_warp(); item < nit; item = next_item<BATCH>(item, nit)) {
+        GridGeom geo;
+        int goff;
+        item_grid<BATCH>(a, item, geo, goff);
+        const ItemLane L = item_lane(a.items, item);
+        float x[3];
+        int base[3];
+        load_x_base(a.st, npl, L.p, geo, x, base);
+        LaneW w;
+        lane_weights(x, geo, base, L.s, w, false);
+        float acc[12];  // v (3), C (9) row-major; C scaled by 3/dx^2 at the end
 #pragma unroll
-    for (int i = 0; i < 12; i++) acc[i] = 0.f;
-    const LaneNodes N = lane_nodes(a.geo, base, L.s);
-#pragma unroll
-    for (int j = 0; j < 4; j++) {
-        const float w01 = w.n0 * w.n1[j];
-#pragma unroll
-        for (int k = 0; k < 4; k++) {
-            if (!((N.mask >> (4 * j + k)) & 1u)) continue;
-            const node4<float> nd = a.grid[N.g00 + j * N.sj + k];
-            const float wt = w01 * w.n2[k];
+        for (int i = 0; i < 12; i++) acc[i] = 0.f;
+        auto node = [&](const node4<float>& nd, int j, int k) {
+            const float wt = w.n0 * w.n1[j] * w.n2[k];
             const float vg[3] = {nd.x, nd.y, nd.z};
             const float d[3] = {w.d0, w.d1[j], w.d2[k]};
 #pragma unroll
@@ -359,124 +444,154 @@ __global__ void __launch_bounds__(256, 4) k_g2p_w(WArgs a) {
 #pragma unroll
                 for (int c = 0; c < 3; c++) acc[3 + 3 * r + c] += wv * d[c];
             }
-        }
-    }
-    reduce_slabs<12>(acc);
-    if (!L.valid) return;
-    const float dx = (float)a.geo.dx;
-    const float k3 = 3.f / (dx * dx);
-    const int p = L.p;
-    m3<float> Cn;
+        };
+        if (DMPM_STAGE_NODES && warp_uniform_base(base)) {
+            __shared__ node4<float> s_nodes[8][64];
+            node4<float>* sw = s_nodes[threadIdx.x >> 5];
+            stage_stencil<1>(a.grid, geo, goff, base, sw);
 #pragma unroll
-    for (int r = 0; r < 3; r++)
+            for (int j = 0; j < 4; j++)
 #pragma unroll
-        for (int c = 0; c < 3; c++) Cn.a[r][c] = k3 * acc[3 + 3 * r + c];
-    bool finite = true;
-    if (L.s == 0) {
+                for (int k = 0; k < 4; k++) node(sw[16 * L.s + 4 * j + k], j, k);
+        } else {
+            LaneNodes N = lane_nodes(geo, base, L.s);
+            N.g00 += goff;
 #pragma unroll
-        for (int c = 0; c < 3; c++) {
-            const float xn = x[c] + a.dt * acc[c];
-            a.st_next[(size_t)(PX + c) * np + p] = xn;
-            a.st_next[(size_t)(PV + c) * np + p] = acc[c];
-            finite &= isfinite(xn);
-        }
-    } else if (L.s == 1) {
-        store_m3(a.st_next + (size_t)PC * np, np, p, Cn);
-    } else {
-        // columns c of F' = (1-s)(I + dt C') Fe[:,c] + s F[:,c]; lane s=2 -> cols 0,1; s=3 -> col 2
-        const int c0 = L.s == 2 ? 0 : 2, c1 = L.s == 2 ? 2 : 3;
-        for (int c = c0; c < c1; c++) {
-            float Fc[3], Fec[3];
+            for (int j = 0; j < 4; j++) {
+                // the row's four node records are loaded before any is used (more loads in
+                // flight); nodes outside the grid read as zero and contribute nothing
+                node4<float> row[4];
 #pragma unroll
-            for (int r = 0; r < 3; r++) {
-                Fc[r] = a.st[(size_t)(PF + r + 3 * c) * np + p];
-                Fec[r] = Fc[r] + a.dfc[(size_t)(r + 3 * c) * np + p];
-            }
+                for (int k = 0; k < 4; k++)
+                    row[k] = ((N.mask >> (4 * j + k)) & 1u) ? a.grid[N.g00 + j * N.sj + k]
+                                                             : node4<float>{0.f, 0.f, 0.f, 0.f};
 #pragma unroll
-            for (int r = 0; r < 3; r++) {
-                const float t = Fec[r] + a.dt * (Cn.a[r][0] * Fec[0] + Cn.a[r][1] * Fec[1] + Cn.a[r][2] * Fec[2]);
-                const float fn = (1.f - a.s) * t + a.s * Fc[r];
-                a.st_next[(size_t)(PF + r + 3 * c) * np + p] = fn;
-                finite &= isfinite(fn);
+                for (int k = 0; k < 4; k++) node(row[k], j, k);
             }
         }
+        reduce_slabs<12>(acc);
+        if (!L.valid) continue;
+        const float dx = (float)geo.dx;
+        const float k3 = 3.f / (dx * dx);
+        const int p = L.p;
+        m3<float> Cn;
+#pragma unroll
+        for (int r = 0; r < 3; r++)
+#pragma unroll
+            for (int c = 0; c < 3; c++) Cn.a[r][c] = k3 * acc[3 + 3 * r + c];
+        bool finite = true;
+        if (L.s == 0) {
+#pragma unroll
+            for (int c = 0; c < 3; c++) {
+                const float xn = x[c] + a.dt * acc[c];
+                a.st_next[(size_t)(PX + c) * npn + p] = xn;
+                a.st_next[(size_t)(PV + c) * npn + p] = acc[c];
+                finite &= isfinite(xn);
+            }
+        } else if (L.s == 1) {
+            store_m3(a.st_next + (size_t)PC * npn, npn, p, Cn);
+        } else {
+            // columns c of F' = (1-s)(I + dt C') Fe[:,c] + s F[:,c]; lane s=2 -> cols 0,1; s=3 -> col 2
+            const int c0 = L.s == 2 ? 0 : 2, c1 = L.s == 2 ? 2 : 3;
+            for (int c = c0; c < c1; c++) {
+                float Fc[3], Fec[3];
+#pragma unroll
+                for (int r = 0; r < 3; r++) {
+                    Fc[r] = a.st[(size_t)(PF + r + 3 * c) * npl + p];
+                    Fec[r] = Fc[r] + a.dfc[(size_t)(r + 3 * c) * np + p];
+                }
+#pragma unroll
+                for (int r = 0; r < 3; r++) {
+                    const float t = Fec[r] + a.dt * (Cn.a[r][0] * Fec[0] + Cn.a[r][1] * Fec[1] + Cn.a[r][2] * Fec[2]);
+                    const float fn = (1.f - a.s) * t + a.s * Fc[r];
+                    a.st_next[(size_t)(PF + r + 3 * c) * npn + p] = fn;
+                    finite &= isfinite(fn);
+                }
+            }
+        }
+        if (!finite) atomicOr(a.status, ST_NONFINITE_FWD);
     }
-    if (!finite) atomicOr(a.status, ST_NONFINITE_FWD);
 }
 
 // ------------------------------------------------------------------ adjoint
 // dLdv_next = dt dLdx' + dLdv';  dLdC_next = c dt dLdF' Fe^T + dLdC'
 // dLdv_g += w dLdv_next + 3/dx^2 w dLdC_next (x_g - x_p)   (BackPropagation.cpp:14-44)
-template <bool EXACT, bool GENERAL> __global__ void __launch_bounds__(256, 3) k_adj_scatter_w(WArgs a) {
-    const int item = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-    if (item >= a.items.n_items) return;
-    const ItemLane L = item_lane(a.items, item);
-    const size_t np = a.np;
-    const int p = L.p;
-    float x[3];
-    int base[3];
-    load_x_base(a.st, np, p, a.geo, x, base);
-    const bool uniform = !GENERAL && warp_uniform_base(base);
-    LaneW w;
-    lane_weights(x, a.geo, base, L.s, w, false);
-    float vn[3];
+template <bool EXACT, bool GENERAL, bool BATCH> __global__ void __launch_bounds__(256, 3) k_adj_scatter_w(WArgs a) {
+    const int nit = item_count(a);
+    const size_t np = a.np, npl = a.npl, npn = a.npn;
+    for (int item = first_warp(); item < nit; item = next_item<BATCH>(item, nit)) {
+        GridGeom geo;
+        int goff;
+        item_grid<BATCH>(a, item, geo, goff);
+        const ItemLane L = item_lane(a.items, item);
+        const int p = L.p;
+        float x[3];
+        int base[3];
+        load_x_base(a.st, npl, p, geo, x, base);
+        const bool uniform = !GENERAL && warp_uniform_base(base);
+        LaneW w;
+        lane_weights(x, geo, base, L.s, w, false);
+        float vn[3];
 #pragma unroll
-    for (int c = 0; c < 3; c++) vn[c] = a.dt * a.adj_next[(size_t)(PX + c) * np + p] + a.adj_next[(size_t)(PV + c) * np + p];
-    const m3<float> Fe = load_m3(a.st + (size_t)PF * np, np, p) + load_m3(a.dfc, np, p);
-    const float cf = EXACT ? (1.f - a.s) * a.dt : a.dt;
-    const m3<float> Cn = (cf * load_m3(a.adj_next + (size_t)PF * np, np, p)) * transpose(Fe) +
-                         load_m3(a.adj_next + (size_t)PC * np, np, p);
-    if (L.valid) {
-        if (L.s == 0) {
+        for (int c = 0; c < 3; c++)
+            vn[c] = a.dt * a.adj_next[(size_t)(PX + c) * npn + p] + a.adj_next[(size_t)(PV + c) * npn + p];
+        const m3<float> Fe = load_m3(a.st + (size_t)PF * npl, npl, p) + load_m3(a.dfc, np, p);
+        const float cf = EXACT ? (1.f - a.s) * a.dt : a.dt;
+        const m3<float> Cn = (cf * load_m3(a.adj_next + (size_t)PF * npn, npn, p)) * transpose(Fe) +
+                             load_m3(a.adj_next + (size_t)PC * npn, npn, p);
+        if (L.valid) {
+            if (L.s == 0) {
 #pragma unroll
-            for (int c = 0; c < 3; c++) a.adjn[(size_t)c * np + p] = vn[c];
-            if (a.dbg_vnext) {
+                for (int c = 0; c < 3; c++) a.adjn[(size_t)c * np + p] = vn[c];
+                if (a.dbg_vnext) {
 #pragma unroll
-                for (int c = 0; c < 3; c++) a.dbg_vnext[(size_t)c * np + p] = vn[c];
-            }
-        } else if (L.s == 1) {
-            store_m3(a.adjn + 3 * np, np, p, Cn);
-            if (a.dbg_Cnext) store_m3(a.dbg_Cnext, np, p, Cn);
-        }
-    }
-    const float dx = (float)a.geo.dx;
-    const float k3 = 3.f / (dx * dx);
-    float c0[3];
-#pragma unroll
-    for (int r = 0; r < 3; r++) c0[r] = k3 * Cn.a[r][0] * w.d0;
-    const LaneNodes N = lane_nodes(a.geo, base, L.s);
-#pragma unroll
-    for (int half = 0; half < 2; half++) {
-        float v[32];
-#pragma unroll
-        for (int jj = 0; jj < 2; jj++) {
-            const int j = 2 * half + jj;
-            float c1[3];
-#pragma unroll
-            for (int r = 0; r < 3; r++) c1[r] = c0[r] + k3 * Cn.a[r][1] * w.d1[j];
-            const float w01 = L.valid ? w.n0 * w.n1[j] : 0.f;
-#pragma unroll
-            for (int k = 0; k < 4; k++) {
-                const float wt = w01 * w.n2[k];
-                const int o = (jj * 4 + k) * 4;
-#pragma unroll
-                for (int r = 0; r < 3; r++) v[o + r] = wt * (vn[r] + c1[r] + k3 * Cn.a[r][2] * w.d2[k]);
-                v[o + 3] = 0.f;
+                    for (int c = 0; c < 3; c++) a.dbg_vnext[(size_t)c * np + p] = vn[c];
+                }
+            } else if (L.s == 1) {
+                store_m3(a.adjn + 3 * np, np, p, Cn);
+                if (a.dbg_Cnext) store_m3(a.dbg_Cnext, np, p, Cn);
             }
         }
-        if (uniform) {
-            reduce_scatter8<32>(v);
-            const int lane = threadIdx.x & 31;
-            const int nd = ((lane >> 4) & 1) * 4 + ((lane >> 3) & 1) * 2 + ((lane >> 2) & 1);
-            const int j = 2 * half + nd / 4, k = nd % 4;
-            if (((N.mask >> (4 * j + k)) & 1u) && (v[0] != 0.f || v[1] != 0.f || v[2] != 0.f))
-                red_add4(a.gadj + (N.g00 + j * N.sj + k), v[0], v[1], v[2], 0.f);
-        } else if (L.valid) {
+        const float dx = (float)geo.dx;
+        const float k3 = 3.f / (dx * dx);
+        float c0[3];
 #pragma unroll
-            for (int nd = 0; nd < 8; nd++) {
+        for (int r = 0; r < 3; r++) c0[r] = k3 * Cn.a[r][0] * w.d0;
+        LaneNodes N = lane_nodes(geo, base, L.s);
+        N.g00 += goff;
+#pragma unroll
+        for (int half = 0; half < 2; half++) {
+            float v[32];
+#pragma unroll
+            for (int jj = 0; jj < 2; jj++) {
+                const int j = 2 * half + jj;
+                float c1[3];
+#pragma unroll
+                for (int r = 0; r < 3; r++) c1[r] = c0[r] + k3 * Cn.a[r][1] * w.d1[j];
+                const float w01 = L.valid ? w.n0 * w.n1[j] : 0.f;
+#pragma unroll
+                for (int k = 0; k < 4; k++) {
+                    const float wt = w01 * w.n2[k];
+                    const int o = (jj * 4 + k) * 4;
+#pragma unroll
+                    for (int r = 0; r < 3; r++) v[o + r] = wt * (vn[r] + c1[r] + k3 * Cn.a[r][2] * w.d2[k]);
+                    v[o + 3] = 0.f;
+                }
+            }
+            if (uniform) {
+                reduce_scatter8<32>(v);
+                const int lane = threadIdx.x & 31;
+                const int nd = ((lane >> 4) & 1) * 4 + ((lane >> 3) & 1) * 2 + ((lane >> 2) & 1);
                 const int j = 2 * half + nd / 4, k = nd % 4;
-                if ((N.mask >> (4 * j + k)) & 1u)
-                    red_add4(a.gadj + (N.g00 + j * N.sj + k), v[nd * 4], v[nd * 4 + 1], v[nd * 4 + 2], 0.f);
+                if (((N.mask >> (4 * j + k)) & 1u) && (v[0] != 0.f || v[1] != 0.f || v[2] != 0.f))
+                    red_add4(a.gadj + (N.g00 + j * N.sj + k), v[0], v[1], v[2], 0.f);
+            } else if (L.valid) {
+#pragma unroll
+                for (int nd = 0; nd < 8; nd++) {
+                    const int j = 2 * half + nd / 4, k = nd % 4;
+                    if ((N.mask >> (4 * j + k)) & 1u)
+                        red_add4(a.gadj + (N.g00 + j * N.sj + k), v[nd * 4], v[nd * 4 + 1], v[nd * 4 + 2], 0.f);
+                }
             }
         }
     }
@@ -509,63 +624,54 @@ __global__ void k_adj_gop_w(const node4<float>* __restrict__ grid, const node4<f
 //   M += w d dLdp^T,  X += sigma (N'NN, NN'N, NNN'),  u += w dLdp,  z += w v_g
 //   sigma = m dLdm + dLdp.(m v c_d + G d) + v_g.(dLdv_next + 3/dx^2 dLdC_next d)
 // (the algebra of kernels.cuh:k_adj_gather); written to gath for k_adj_finalize.
-template <bool EXACT> __global__ void __launch_bounds__(256, 3) k_adj_gather_w(WArgs a) {
-    const int item = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-    if (item >= a.items.n_items) return;
-    const ItemLane L = item_lane(a.items, item);
-    const size_t np = a.np;
-    const int p = L.p;
-    float x[3];
-    int base[3];
-    load_x_base(a.st, np, p, a.geo, x, base);
-    LaneW w;
-    lane_weights(x, a.geo, base, L.s, w, true);
-    const float mp = a.cst[(size_t)KM * np + p];
-    const float cd = EXACT ? (1.f - a.dt * a.drag) : 1.f;
-    const float dx = (float)a.geo.dx;
-    const float k3 = 3.f / (dx * dx);
-    float mvp[3], vn[3];
+template <bool EXACT, bool BATCH> __global__ void __launch_bounds__(256, DMPM_GATHER_MIN_BLOCKS) k_adj_gather_w(WArgs a) {
+    const int nit = item_count(a);
+    const size_t np = a.np, npl = a.npl;
+    for (int item = first_warp(); item < nit; item = next_item<BATCH>(item, nit)) {
+        GridGeom geo;
+        int goff;
+        item_grid<BATCH>(a, item, geo, goff);
+        const ItemLane L = item_lane(a.items, item);
+        const int p = L.p;
+        float x[3];
+        int base[3];
+        load_x_base(a.st, npl, p, geo, x, base);
+        LaneW w;
+        lane_weights(x, geo, base, L.s, w, true);
+        const float mp = a.cst[(size_t)KM * np + p];
+        const float cd = EXACT ? (1.f - a.dt * a.drag) : 1.f;
+        const float dx = (float)geo.dx;
+        const float k3 = 3.f / (dx * dx);
+        float mvp[3], vn[3];
 #pragma unroll
-    for (int c = 0; c < 3; c++) {
-        mvp[c] = mp * a.st[(size_t)(PV + c) * np + p] * cd;
-        vn[c] = a.adjn[(size_t)c * np + p];
-    }
-    const m3<float> G = load_m3(a.G, np, p);
-    const m3<float> Cn = load_m3(a.adjn + 3 * np, np, p);
-    // sigma's node-dependent pieces: h_g = mvp + G d,  e_g = vn + k3 Cn d
-    float h0[3], e0[3];
-#pragma unroll
-    for (int r = 0; r < 3; r++) {
-        h0[r] = mvp[r] + G.a[r][0] * w.d0;
-        e0[r] = vn[r] + k3 * Cn.a[r][0] * w.d0;
-    }
-    float acc[18];  // M (9, row-major: M[r][c] = sum w d_r dLdp_c), X (3), u (3), z (3)
-#pragma unroll
-    for (int i = 0; i < 18; i++) acc[i] = 0.f;
-    const LaneNodes N = lane_nodes(a.geo, base, L.s);
-#pragma unroll
-    for (int j = 0; j < 4; j++) {
-        float h1[3], e1[3];
+        for (int c = 0; c < 3; c++) {
+            mvp[c] = mp * a.st[(size_t)(PV + c) * npl + p] * cd;
+            vn[c] = a.adjn[(size_t)c * np + p];
+        }
+        const m3<float> G = load_m3(a.G, npl, p);
+        const m3<float> Cn = load_m3(a.adjn + 3 * np, np, p);
+        // sigma's node-dependent pieces: h_g = mvp + G d,  e_g = vn + k3 Cn d
+        float h0[3], e0[3];
 #pragma unroll
         for (int r = 0; r < 3; r++) {
-            h1[r] = h0[r] + G.a[r][1] * w.d1[j];
-            e1[r] = e0[r] + k3 * Cn.a[r][1] * w.d1[j];
+            h0[r] = mvp[r] + G.a[r][0] * w.d0;
+            e0[r] = vn[r] + k3 * Cn.a[r][0] * w.d0;
         }
-        const float n01 = w.n0 * w.n1[j], s01 = w.s0 * w.n1[j], n0s1 = w.n0 * w.s1[j];
+        float acc[18];  // M (9, row-major: M[r][c] = sum w d_r dLdp_c), X (3), u (3), z (3)
 #pragma unroll
-        for (int k = 0; k < 4; k++) {
-            if (!((N.mask >> (4 * j + k)) & 1u)) continue;
-            const int g = N.g00 + j * N.sj + k;
-            const node4<float> o = a.gadj2[2 * g];
-            const node4<float> vg = a.gadj2[2 * g + 1];
+        for (int i = 0; i < 18; i++) acc[i] = 0.f;
+        auto node = [&](const node4<float>& o, const node4<float>& vg, int j, int k) {
+            float h[3], e[3];
+#pragma unroll
+            for (int r = 0; r < 3; r++) {
+                h[r] = h0[r] + G.a[r][1] * w.d1[j] + G.a[r][2] * w.d2[k];
+                e[r] = e0[r] + k3 * Cn.a[r][1] * w.d1[j] + k3 * Cn.a[r][2] * w.d2[k];
+            }
+            const float n01 = w.n0 * w.n1[j];
             const float wt = n01 * w.n2[k];
-            float sig = mp * o.w;
-            sig += o.x * (h1[0] + G.a[0][2] * w.d2[k]) + o.y * (h1[1] + G.a[1][2] * w.d2[k]) +
-                   o.z * (h1[2] + G.a[2][2] * w.d2[k]);
-            sig += vg.x * (e1[0] + k3 * Cn.a[0][2] * w.d2[k]) + vg.y * (e1[1] + k3 * Cn.a[1][2] * w.d2[k]) +
-                   vg.z * (e1[2] + k3 * Cn.a[2][2] * w.d2[k]);
-            acc[9] += sig * (s01 * w.n2[k]);
-            acc[10] += sig * (n0s1 * w.n2[k]);
+            const float sig = mp * o.w + o.x * h[0] + o.y * h[1] + o.z * h[2] + vg.x * e[0] + vg.y * e[1] + vg.z * e[2];
+            acc[9] += sig * (w.s0 * w.n1[j] * w.n2[k]);
+            acc[10] += sig * (w.n0 * w.s1[j] * w.n2[k]);
             acc[11] += sig * (n01 * w.s2[k]);
             const float wo[3] = {wt * o.x, wt * o.y, wt * o.z};
             acc[12] += wo[0];
@@ -579,16 +685,39 @@ template <bool EXACT> __global__ void __launch_bounds__(256, 3) k_adj_gather_w(W
             for (int r = 0; r < 3; r++)
 #pragma unroll
                 for (int c = 0; c < 3; c++) acc[3 * r + c] += d[r] * wo[c];
+        };
+        if (DMPM_STAGE_NODES && warp_uniform_base(base)) {
+            __shared__ node4<float> s_rec[8][128];
+            node4<float>* sw = s_rec[threadIdx.x >> 5];
+            stage_stencil<2>(a.gadj2, geo, goff, base, sw);
+#pragma unroll
+            for (int j = 0; j < 4; j++)
+#pragma unroll
+                for (int k = 0; k < 4; k++) {
+                    const int n = 16 * L.s + 4 * j + k;
+                    node(sw[2 * n], sw[2 * n + 1], j, k);
+                }
+        } else {
+            LaneNodes N = lane_nodes(geo, base, L.s);
+            N.g00 += goff;
+#pragma unroll
+            for (int j = 0; j < 4; j++)
+#pragma unroll
+                for (int k = 0; k < 4; k++) {
+                    if (!((N.mask >> (4 * j + k)) & 1u)) continue;
+                    const int g = N.g00 + j * N.sj + k;
+                    node(a.gadj2[2 * g], a.gadj2[2 * g + 1], j, k);
+                }
         }
-    }
-    reduce_slabs<18>(acc);
-    if (!L.valid) return;
-    if (L.s == 0) {
+        reduce_slabs<18>(acc);
+        if (!L.valid) continue;
+        if (L.s == 0) {
 #pragma unroll
-        for (int i = 0; i < 9; i++) a.gath[(size_t)i * np + p] = acc[i];
-    } else if (L.s == 1) {
+            for (int i = 0; i < 9; i++) a.gath[(size_t)i * np + p] = acc[i];
+        } else if (L.s == 1) {
 #pragma unroll
-        for (int i = 9; i < 18; i++) a.gath[(size_t)i * np + p] = acc[i];
+            for (int i = 9; i < 18; i++) a.gath[(size_t)i * np + p] = acc[i];
+        }
     }
 }
 
@@ -597,74 +726,78 @@ template <bool EXACT> __global__ void __launch_bounds__(256, 3) k_adj_gather_w(W
 //   dLdx = -X/dx - G^T u - 3/dx^2 dLdC_next^T z + dLdx',  dLdv = m (1 - dt drag) u
 //   REFCOMPAT: dLdF = (1-s)T + s dLdF' + stress + T + dP:dLdP,  T = (I + dt C')^T dLdF'
 //   EXACT:     dLdFe = (1-s)T + stress + dP:dLdP,  dLdF = dLdFe + s dLdF'
-template <bool EXACT> __global__ void __launch_bounds__(128) k_adj_finalize(WArgs a) {
+// (the REFCOMPAT variant, with its finite-difference dJFit, keeps the
+// compiler's own register budget)
+template <bool EXACT>
+__global__ void __launch_bounds__(128, EXACT ? DMPM_FINALIZE_MIN_BLOCKS : 1) k_adj_finalize(WArgs a) {
+    const size_t np = a.np, npl = a.npl, npn = a.npn;
     const int p = blockIdx.x * blockDim.x + threadIdx.x;
-    if (p >= a.n) return;
-    const size_t np = a.np;
-    m3<float> M;
+    if (p < a.n) {
+        m3<float> M;
 #pragma unroll
-    for (int r = 0; r < 3; r++)
+        for (int r = 0; r < 3; r++)
 #pragma unroll
-        for (int c = 0; c < 3; c++) M.a[r][c] = a.gath[(size_t)(3 * r + c) * np + p];
-    const m3<float> Fe = load_m3(a.st + (size_t)PF * np, np, p) + load_m3(a.dfc, np, p);
-    const m3<double> Fed = m3_cast<double>(Fe);
-    // polar factors computed in FP64 by k_stress for this layer
-    const m3<double> Rd = m3_cast<double>(load_m3(a.G + 9 * np, np, p));
-    m3<double> Sd;
-    Sd.a[0][0] = a.G[18 * np + p];
-    Sd.a[0][1] = Sd.a[1][0] = a.G[19 * np + p];
-    Sd.a[0][2] = Sd.a[2][0] = a.G[20 * np + p];
-    Sd.a[1][1] = a.G[21 * np + p];
-    Sd.a[1][2] = Sd.a[2][1] = a.G[22 * np + p];
-    Sd.a[2][2] = a.G[23 * np + p];
-    const double lam = (double)a.cst[(size_t)KLAM * np + p], mu = (double)a.cst[(size_t)KMU * np + p];
-    const m3<float> P = m3_cast<float>(pk_from_polar(Fed, Rd, lam, mu));
-    const float mp = a.cst[(size_t)KM * np + p], vol = a.cst[(size_t)KVOL * np + p];
-    const float dx = (float)a.geo.dx;
-    const float k3 = 3.f / (dx * dx);
-    const float kk = -k3 * a.dt * vol;
-    const m3<float> dLdP = kk * mtm(M, Fe);
-    const m3<float> dFstress = kk * (M * P);
-    const m3<float> G = load_m3(a.G, np, p);
-    const m3<float> Cn = load_m3(a.adjn + 3 * np, np, p);
-    float u[3], z[3], gtu[3], ctz[3];
+            for (int c = 0; c < 3; c++) M.a[r][c] = a.gath[(size_t)(3 * r + c) * np + p];
+        const m3<float> Fe = load_m3(a.st + (size_t)PF * npl, npl, p) + load_m3(a.dfc, np, p);
+        const m3<double> Fed = m3_cast<double>(Fe);
+        // polar factors computed in FP64 by k_stress for this layer
+        const m3<double> Rd = m3_cast<double>(load_m3(a.G + 9 * npl, npl, p));
+        m3<double> Sd;
+        Sd.a[0][0] = a.G[18 * npl + p];
+        Sd.a[0][1] = Sd.a[1][0] = a.G[19 * npl + p];
+        Sd.a[0][2] = Sd.a[2][0] = a.G[20 * npl + p];
+        Sd.a[1][1] = a.G[21 * npl + p];
+        Sd.a[1][2] = Sd.a[2][1] = a.G[22 * npl + p];
+        Sd.a[2][2] = a.G[23 * npl + p];
+        const double lam = (double)a.cst[(size_t)KLAM * np + p], mu = (double)a.cst[(size_t)KMU * np + p];
+        const m3<float> P = m3_cast<float>(pk_from_polar(Fed, Rd, lam, mu));
+        const float mp = a.cst[(size_t)KM * np + p], vol = a.cst[(size_t)KVOL * np + p];
+        const float dx = (float)a.geo.dx;
+        const float k3 = 3.f / (dx * dx);
+        const float kk = -k3 * a.dt * vol;
+        const m3<float> dLdP = kk * mtm(M, Fe);
+        const m3<float> dFstress = kk * (M * P);
+        const m3<float> G = load_m3(a.G, npl, p);
+        const m3<float> Cn = load_m3(a.adjn + 3 * np, np, p);
+        float u[3], z[3], gtu[3], ctz[3];
 #pragma unroll
-    for (int c = 0; c < 3; c++) {
-        u[c] = a.gath[(size_t)(12 + c) * np + p];
-        z[c] = a.gath[(size_t)(15 + c) * np + p];
+        for (int c = 0; c < 3; c++) {
+            u[c] = a.gath[(size_t)(12 + c) * np + p];
+            z[c] = a.gath[(size_t)(15 + c) * np + p];
+        }
+        mtv(G, u, gtu);
+        mtv(Cn, z, ctz);
+#pragma unroll
+        for (int c = 0; c < 3; c++) {
+            const float X = a.gath[(size_t)(9 + c) * np + p];
+            a.adj[(size_t)(PX + c) * npl + p] = -X / dx - gtu[c] - k3 * ctz[c] + a.adj_next[(size_t)(PX + c) * npn + p];
+            a.adj[(size_t)(PV + c) * npl + p] = mp * (1.f - a.dt * a.drag) * u[c];
+        }
+        store_m3(a.adj + (size_t)PC * npl, npl, p, mp * transpose(M));
+        const m3<float> Cnext = load_m3(a.st_next + (size_t)PC * npn, npn, p);
+        const m3<float> dFn = load_m3(a.adj_next + (size_t)PF * npn, npn, p);
+        const m3<float> Tr = mtm(m3_eye<float>() + a.dt * Cnext, dFn);
+        const m3<float> d2 = m3_cast<float>(d2_mult_from_polar<EXACT>(Fed, Rd, Sd, lam, mu, m3_cast<double>(dLdP)));
+        m3<float> dLdF, dLdFe;
+        if (EXACT) {
+            dLdFe = (1.f - a.s) * Tr + dFstress + d2;
+            dLdF = dLdFe + a.s * dFn;
+        } else {
+            dLdF = ((1.f - a.s) * Tr + a.s * dFn) + dFstress + Tr + d2;
+            dLdFe = dLdF;
+        }
+        store_m3(a.adj + (size_t)PF * npl, npl, p, dLdF);
+        if (a.ctrl_grad) store_m3(a.ctrl_grad, np, p, dLdFe);
+        if (a.ctrl_acc) {
+#pragma unroll
+            for (int c = 0; c < 3; c++)
+#pragma unroll
+                for (int r = 0; r < 3; r++) a.ctrl_acc[(size_t)(r + 3 * c) * np + p] += (double)dLdFe.a[r][c];
+        }
+        if (a.dbg_dLdP) store_m3(a.dbg_dLdP, np, p, dLdP);
+        if (!isfinite(dLdF.a[0][0] + dLdF.a[1][1] + dLdF.a[2][2] + a.adj[(size_t)PX * npl + p]))
+            atomicOr(a.status, ST_NONFINITE_ADJ);
     }
-    mtv(G, u, gtu);
-    mtv(Cn, z, ctz);
-#pragma unroll
-    for (int c = 0; c < 3; c++) {
-        const float X = a.gath[(size_t)(9 + c) * np + p];
-        a.adj[(size_t)(PX + c) * np + p] = -X / dx - gtu[c] - k3 * ctz[c] + a.adj_next[(size_t)(PX + c) * np + p];
-        a.adj[(size_t)(PV + c) * np + p] = mp * (1.f - a.dt * a.drag) * u[c];
-    }
-    store_m3(a.adj + (size_t)PC * np, np, p, mp * transpose(M));
-    const m3<float> Cnext = load_m3(a.st_next + (size_t)PC * np, np, p);
-    const m3<float> dFn = load_m3(a.adj_next + (size_t)PF * np, np, p);
-    const m3<float> Tr = mtm(m3_eye<float>() + a.dt * Cnext, dFn);
-    const m3<float> d2 = m3_cast<float>(d2_mult_from_polar<EXACT>(Fed, Rd, Sd, lam, mu, m3_cast<double>(dLdP)));
-    m3<float> dLdF, dLdFe;
-    if (EXACT) {
-        dLdFe = (1.f - a.s) * Tr + dFstress + d2;
-        dLdF = dLdFe + a.s * dFn;
-    } else {
-        dLdF = ((1.f - a.s) * Tr + a.s * dFn) + dFstress + Tr + d2;
-        dLdFe = dLdF;
-    }
-    store_m3(a.adj + (size_t)PF * np, np, p, dLdF);
-    if (a.ctrl_grad) store_m3(a.ctrl_grad, np, p, dLdFe);
-    if (a.ctrl_acc) {
-#pragma unroll
-        for (int c = 0; c < 3; c++)
-#pragma unroll
-            for (int r = 0; r < 3; r++) a.ctrl_acc[(size_t)(r + 3 * c) * np + p] += (double)dLdFe.a[r][c];
-    }
-    if (a.dbg_dLdP) store_m3(a.dbg_dLdP, np, p, dLdP);
-    if (!isfinite(dLdF.a[0][0] + dLdF.a[1][1] + dLdF.a[2][2] + a.adj[(size_t)PX * np + p]))
-        atomicOr(a.status, ST_NONFINITE_ADJ);
 }
 
 }  // namespace dmpm

@@ -154,7 +154,7 @@ template <class Op> __global__ void __launch_bounds__(SCAN_THREADS) k_scan_add(u
 }
 
 // ------------------------------------------------------------------ radix sort
-__global__ void __launch_bounds__(RS_THREADS) k_rs_upsweep(const uint32_t* __restrict__ keys, int n, int shift,
+static __global__ void __launch_bounds__(RS_THREADS) k_rs_upsweep(const uint32_t* __restrict__ keys, int n, int shift,
                                                           uint32_t* counts, int ntiles) {
     __shared__ uint32_t hist[256];
     hist[threadIdx.x] = 0;
@@ -168,7 +168,7 @@ __global__ void __launch_bounds__(RS_THREADS) k_rs_upsweep(const uint32_t* __res
     counts[(size_t)threadIdx.x * ntiles + blockIdx.x] = hist[threadIdx.x];
 }
 
-__global__ void __launch_bounds__(RS_THREADS) k_rs_downsweep(const uint32_t* __restrict__ keys_in,
+static __global__ void __launch_bounds__(RS_THREADS) k_rs_downsweep(const uint32_t* __restrict__ keys_in,
                                                             const uint32_t* __restrict__ vals_in, uint32_t* keys_out,
                                                             uint32_t* vals_out, int n, int shift,
                                                             const uint32_t* __restrict__ offsets, int ntiles) {
@@ -221,14 +221,14 @@ __global__ void __launch_bounds__(RS_THREADS) k_rs_downsweep(const uint32_t* __r
 
 // ------------------------------------------------------------------ warp items
 // head[i] = i if a run of equal keys starts at i, else 0 (max-scan -> run start)
-__global__ void k_run_heads(const uint32_t* __restrict__ keys, int n, uint32_t* head) {
+static __global__ void k_run_heads(const uint32_t* __restrict__ keys, int n, uint32_t* head) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     head[i] = (i == 0 || keys[i] != keys[i - 1]) ? (uint32_t)i : 0u;
 }
 // after an inclusive max-scan of head (exclusive scan combined with the own
 // value), flag item starts: every 8th element of a run.
-__global__ void k_item_flags(const uint32_t* __restrict__ keys, const uint32_t* __restrict__ run_excl, int n,
+static __global__ void k_item_flags(const uint32_t* __restrict__ keys, const uint32_t* __restrict__ run_excl, int n,
                              uint32_t* flags) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
@@ -237,7 +237,7 @@ __global__ void k_item_flags(const uint32_t* __restrict__ keys, const uint32_t* 
     flags[i] = ((uint32_t)i - start) % 8u == 0u ? 1u : 0u;
 }
 // flags has been exclusive-sum-scanned into idx; write item starts.
-__global__ void k_item_starts(const uint32_t* __restrict__ keys, const uint32_t* __restrict__ run_excl,
+static __global__ void k_item_starts(const uint32_t* __restrict__ keys, const uint32_t* __restrict__ run_excl,
                               const uint32_t* __restrict__ idx, int n, uint32_t* item_start) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i > n) return;
@@ -248,7 +248,7 @@ __global__ void k_item_starts(const uint32_t* __restrict__ keys, const uint32_t*
     const uint32_t start = run_excl[i] > own ? run_excl[i] : own;
     if (((uint32_t)i - start) % 8u == 0u) item_start[idx[i]] = (uint32_t)i;
 }
-__global__ void k_item_sentinel(uint32_t* item_start, const uint32_t* n_items, int n) {
+static __global__ void k_item_sentinel(uint32_t* item_start, const uint32_t* n_items, int n) {
     item_start[*n_items] = (uint32_t)n;
 }
 

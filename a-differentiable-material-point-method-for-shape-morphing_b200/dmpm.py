@@ -45,7 +45,17 @@ class Params(ctypes.Structure):
                 ("smoothing", ctypes.c_double), ("adjoint_mode", ctypes.c_int), ("control_mode", ctypes.c_int),
                 ("loss_kind", ctypes.c_int), ("checkpoint_every", ctypes.c_int), ("keep_adjoints", ctypes.c_int),
                 ("keep_intermediates", ctypes.c_int), ("block_size", ctypes.c_int), ("tile_cap", ctypes.c_int),
-                ("sort_every", ctypes.c_int), ("warp_general", ctypes.c_int)]
+                ("sort_every", ctypes.c_int), ("warp_general", ctypes.c_int), ("control_stride", ctypes.c_int)]
+
+
+class Instance(ctypes.Structure):
+    _fields_ = [("n", ctypes.c_int), ("dim_x", ctypes.c_int), ("dim_y", ctypes.c_int), ("dim_z", ctypes.c_int),
+                ("dx", ctypes.c_double), ("min_point", ctypes.c_double * 3), ("steps", ctypes.c_int)]
+
+
+class BatchLaunch(ctypes.Structure):
+    _fields_ = [("sort_every", ctypes.c_int), ("ctas_per_sm", ctypes.c_int), ("particle_block", ctypes.c_int),
+                ("use_graph", ctypes.c_int)]
 
 
 _P = ctypes.c_void_p
@@ -99,6 +109,22 @@ def load_library(path: str = LIB_PATH) -> ctypes.CDLL:
                                                ctypes.c_float, _P, _P, _P]
     L.dmpm_kernel_name.argtypes = [ctypes.c_int]
     L.dmpm_kernel_name.restype = ctypes.c_char_p
+    L.dmpm_batch_create.argtypes = [ctypes.c_int, ctypes.c_int, _P, ctypes.POINTER(_P)]
+    L.dmpm_batch_destroy.argtypes = [_P]
+    L.dmpm_batch_last_error.argtypes = [_P]
+    L.dmpm_batch_last_error.restype = ctypes.c_char_p
+    L.dmpm_batch_set_params.argtypes = [_P, ctypes.POINTER(Params)]
+    L.dmpm_batch_set_particles.argtypes = [_P, ctypes.c_int] + [_P] * 9
+    L.dmpm_batch_set_target_mass.argtypes = [_P, ctypes.c_int, _P]
+    L.dmpm_batch_set_launch.argtypes = [_P, ctypes.POINTER(BatchLaunch)]
+    L.dmpm_batch_get_launch.argtypes = [_P, ctypes.POINTER(BatchLaunch)]
+    L.dmpm_batch_setup.argtypes = [_P]
+    L.dmpm_batch_gradient.argtypes = [_P, _P]
+    L.dmpm_batch_autotune.argtypes = [_P, ctypes.c_int, ctypes.POINTER(ctypes.c_double)]
+    L.dmpm_batch_get_control_grad.argtypes = [_P, ctypes.c_int, _P]
+    L.dmpm_batch_get_particles.argtypes = [_P, ctypes.c_int, ctypes.c_int, ctypes.c_int, _P]
+    L.dmpm_batch_info.argtypes = [_P, ctypes.POINTER(ctypes.c_int64), ctypes.c_int]
+    L.dmpm_batch_stream.argtypes = [_P, ctypes.POINTER(_P)]
     _lib = L
     return L
 
@@ -205,7 +231,8 @@ class Context:
     def set_params(self, dt: float, drag: float = 0.0, f_ext=(0.0, 0.0, 0.0), smoothing: float = 0.0,
                    adjoint: str = "refcompat", control: str = "per_layer", loss: str = "ref",
                    checkpoint_every: int = 0, keep_adjoints: bool = False, keep_intermediates: bool = False,
-                   block_size: int = 0, tile_cap: int = 0, sort_every: int = 0, warp_general: bool = False):
+                   block_size: int = 0, tile_cap: int = 0, sort_every: int = 0, warp_general: bool = False,
+                   control_stride: int = 0):
         p = Params()
         self.lib.dmpm_default_params(ctypes.byref(p))
         p.dt, p.drag, p.smoothing = float(dt), float(drag), float(smoothing)
@@ -221,6 +248,7 @@ class Context:
         p.tile_cap = int(tile_cap)
         p.sort_every = int(sort_every)
         p.warp_general = int(bool(warp_general))
+        p.control_stride = int(control_stride)
         self._ck(self.lib.dmpm_set_params(self.h, ctypes.byref(p)), "set_params")
         self.params = p
 
@@ -351,3 +379,118 @@ class Context:
         assert points.dtype == np.float32 and points.shape == (self.n, 118) and points.flags.c_contiguous
         self._ck(self.lib.dmpm_get_points_ref(self.h, int(layer), points.ctypes.data), "get_points_ref")
         return points
+
+
+class Batch:
+    """Many independent scenes advanced together (dmpm_batch_*): FP32-mixed,
+    every layer kept, tied controls, one launch per stage per time step,
+    optionally replayed as a CUDA graph."""
+
+    def __init__(self, specs: Sequence[dict], device: int = 0):
+        """specs: per instance {"n", "dims", "dx", "min_point", "steps"}."""
+        self.lib = load_library()
+        arr = (Instance * len(specs))()
+        for i, sp in enumerate(specs):
+            arr[i].n = int(sp["n"])
+            arr[i].dim_x, arr[i].dim_y, arr[i].dim_z = (int(d) for d in sp["dims"])
+            arr[i].dx = float(sp.get("dx", 1.0))
+            for c in range(3):
+                arr[i].min_point[c] = float(sp.get("min_point", (0.0, 0.0, 0.0))[c])
+            arr[i].steps = int(sp["steps"])
+        h = _P()
+        st = self.lib.dmpm_batch_create(device, len(specs), ctypes.cast(arr, _P), ctypes.byref(h))
+        if st != OK:
+            raise DmpmError(st, "dmpm_batch_create failed (no CUDA device, or invalid instances)")
+        self.h = h
+        self.specs = [dict(sp) for sp in specs]
+        self.count = len(specs)
+
+    def _ck(self, st: int, what: str, allow_nonfinite: bool = False) -> int:
+        if st == OK or (allow_nonfinite and st == ERR_NONFINITE):
+            return st
+        msg = self.lib.dmpm_batch_last_error(self.h)
+        raise DmpmError(st, "%s: %s" % (what, msg.decode() if msg else ""))
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.lib.dmpm_batch_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        self.close()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def set_params(self, dt: float, drag: float = 0.0, f_ext=(0.0, 0.0, 0.0), smoothing: float = 0.0,
+                   adjoint: str = "exact", loss: str = "ref"):
+        p = Params()
+        self.lib.dmpm_default_params(ctypes.byref(p))
+        p.dt, p.drag, p.smoothing = float(dt), float(drag), float(smoothing)
+        for i in range(3):
+            p.f_ext[i] = float(f_ext[i])
+        p.adjoint_mode = ADJ_EXACT if adjoint == "exact" else ADJ_REFCOMPAT
+        p.control_mode = CTRL_TIED
+        p.loss_kind = LOSS_L2 if loss == "l2" else LOSS_REF_LOGMASS
+        self._ck(self.lib.dmpm_batch_set_params(self.h, ctypes.byref(p)), "batch_set_params")
+
+    def set_particles(self, inst: int, x, m, lam, mu, v=None, F=None, C=None, dFc=None, vol=None):
+        a = [np.ascontiguousarray(x, dtype=np.float64), None if v is None else np.ascontiguousarray(v, dtype=np.float64),
+             None if F is None else _cm(F), None if C is None else _cm(C), None if dFc is None else _cm(dFc),
+             np.ascontiguousarray(m, dtype=np.float64), None if vol is None else np.ascontiguousarray(vol, dtype=np.float64),
+             np.ascontiguousarray(lam, dtype=np.float64), np.ascontiguousarray(mu, dtype=np.float64)]
+        self._ck(self.lib.dmpm_batch_set_particles(self.h, int(inst), *[_ptr(t) for t in a]), "batch_set_particles")
+
+    def set_target_mass(self, inst: int, target):
+        t = np.ascontiguousarray(target, dtype=np.float64)
+        self._ck(self.lib.dmpm_batch_set_target_mass(self.h, int(inst), t.ctypes.data), "batch_set_target_mass")
+
+    def set_launch(self, sort_every: int = 0, ctas_per_sm: int = 0, particle_block: int = 0, use_graph: bool = True):
+        c = BatchLaunch(int(sort_every), int(ctas_per_sm), int(particle_block), int(bool(use_graph)))
+        self._ck(self.lib.dmpm_batch_set_launch(self.h, ctypes.byref(c)), "batch_set_launch")
+
+    def launch(self) -> dict:
+        c = BatchLaunch()
+        self._ck(self.lib.dmpm_batch_get_launch(self.h, ctypes.byref(c)), "batch_get_launch")
+        return {"sort_every": c.sort_every, "ctas_per_sm": c.ctas_per_sm, "particle_block": c.particle_block,
+                "use_graph": bool(c.use_graph)}
+
+    def setup(self):
+        self._ck(self.lib.dmpm_batch_setup(self.h), "batch_setup")
+
+    def gradient(self, allow_nonfinite: bool = False) -> np.ndarray:
+        out = np.empty(self.count, dtype=np.float64)
+        self._ck(self.lib.dmpm_batch_gradient(self.h, out.ctypes.data), "batch_gradient", allow_nonfinite)
+        return out
+
+    def autotune(self, reps: int = 2) -> float:
+        ms = ctypes.c_double()
+        self._ck(self.lib.dmpm_batch_autotune(self.h, int(reps), ctypes.byref(ms)), "batch_autotune")
+        return float(ms.value)
+
+    def control_grad(self, inst: int) -> np.ndarray:
+        a = np.empty(int(self.specs[inst]["n"]) * 9, dtype=np.float64)
+        self._ck(self.lib.dmpm_batch_get_control_grad(self.h, int(inst), a.ctypes.data), "batch_control_grad")
+        return _from_cm(a)
+
+    def get(self, inst: int, layer: int, field: str) -> np.ndarray:
+        w = WIDTH[field]
+        out = np.empty(int(self.specs[inst]["n"]) * w, dtype=np.float64)
+        self._ck(self.lib.dmpm_batch_get_particles(self.h, int(inst), int(layer), FIELDS[field], out.ctypes.data),
+                 "batch_get " + field)
+        return _from_cm(out) if w == 9 else out.reshape(-1, 3)
+
+    def info(self) -> dict:
+        a = (ctypes.c_int64 * 6)()
+        self._ck(self.lib.dmpm_batch_info(self.h, a, 6), "batch_info")
+        return {"instances": a[0], "particles": a[1], "nodes": a[2], "device_bytes": a[3],
+                "launches_per_gradient": a[4], "graph": bool(a[5])}
+
+    @property
+    def stream(self) -> int:
+        s = _P()
+        self._ck(self.lib.dmpm_batch_stream(self.h, ctypes.byref(s)), "batch_stream")
+        return s.value or 0

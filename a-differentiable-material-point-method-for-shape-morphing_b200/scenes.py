@@ -191,6 +191,20 @@ def _bb(c, h):
     return (c - h, c + h)
 
 
+# Density of the 128^3 and 256^3 scenes: the reference's default p_density
+# (DiffMPMAnimator3D/MPMPolyscope.h:37).  With density 1, the value the small
+# scenes use, a fully covered node of a 256^3 unit box holds 1/256^3 = 6e-8,
+# below the FLT_EPSILON node-mass threshold of the grid update
+# (ForwardSimulation.cpp:55, BackPropagation.cpp:55) and of the volume
+# estimate (ForwardSimulation.cpp:288): every node would count as empty, every
+# volume would be zero and the rollout would not move.  At 128^3 a full node
+# holds 4.8e-7, so the partly covered surface nodes cross the threshold from
+# step to step: the 500-step gradient of the three-sphere scene then changes
+# by 1e-6 (relative) between two FP64 runs that differ only in atomic
+# summation order, against 2e-11 at density 40.
+LARGE_SCENE_DENSITY = 40.0
+
+
 def config_scene(config: int, instance: int = 0, ppc_root: Optional[int] = None) -> Scene:
     """The five benchmark configurations as seeded scenes (seed = 1000*config + instance)."""
     seed = 1000 * config + instance
@@ -210,11 +224,12 @@ def config_scene(config: int, instance: int = 0, ppc_root: Optional[int] = None)
         lo = np.min(cs - rs[:, None], 0)
         hi = np.max(cs + rs[:, None], 0)
         return make_scene("3spheres_128^3", shp, capsule(c, 0.5, 0.15), 128, ppc_root or 2, 5e4, 0.35,
-                          2.5e-4, 500, seed, checkpoint_every=25, bbox=(lo, hi),
+                          2.5e-4, 500, seed, rho=LARGE_SCENE_DENSITY, checkpoint_every=25, bbox=(lo, hi),
                           target_bbox=_bb(c, (0.4, 0.15, 0.15)))
     if config == 4:
         return make_scene("sphere_r0.2423_256^3", sphere(c, 0.2423), torus(c, 0.3, 0.1), 256, ppc_root or 2,
-                          1e4, 0.3, 1.25e-4, 400, seed, checkpoint_every=20, bbox=_bb(c, 0.2423),
+                          1e4, 0.3, 1.25e-4, 400, seed, rho=LARGE_SCENE_DENSITY, checkpoint_every=20,
+                          bbox=_bb(c, 0.2423),
                           target_bbox=_bb(c, (0.4, 0.4, 0.1)))
     raise ValueError("config %d is not a single-instance scene; see batch_scenes" % config)
 

@@ -156,13 +156,13 @@ def build_scene(instance: int, ppc_root: int):
     return sc
 
 
-def setup_ctx(dmpm, sc, prec, device, vol, target, dt, checkpoint_every):
+def setup_ctx(dmpm, sc, prec, device, vol, target, dt, checkpoint_every, control="tied", control_stride=0):
     c = dmpm.Context(prec, device)
     c.set_grid(sc.dims, sc.dx, sc.min_point)
     c.set_particles(sc.x, sc.m, sc.lam, sc.mu, v=sc.v, F=sc.F, C=sc.C, dFc=sc.dFc, vol=vol)
     c.set_target_mass(target)
-    c.set_params(dt=dt, drag=sc.drag, f_ext=sc.f_ext, smoothing=sc.smoothing, adjoint="exact", control="tied",
-                 loss="ref", checkpoint_every=checkpoint_every)
+    c.set_params(dt=dt, drag=sc.drag, f_ext=sc.f_ext, smoothing=sc.smoothing, adjoint="exact", control=control,
+                 loss="ref", checkpoint_every=checkpoint_every, control_stride=control_stride)
     c.setup(sc.steps + 1)
     return c
 
@@ -197,15 +197,28 @@ def timed_steps(torch, c, steps, fn):
     return e0.elapsed_time(e1)
 
 
-# algorithmic bytes per launch of each kernel, FP32 tiled path
-def algorithmic_bytes(kernel: str, n: int, touched: int) -> float:
-    per_particle = {
-        "p2g": 37 * 4, "g2p_p_op2": (21 + 24) * 4, "adj_g2p_scatter": 45 * 4,
-        "adj_p2g_gather": 70 * 4 + 24 * 4 + 9 * 8 * 2, "p2g_mass": 4 * 4, "loss_dldx": 4 * 4 + 24 * 4,
-    }
-    per_node = {"p2g": 16, "g2p_p_op2": 16, "adj_g2p_scatter": 16, "adj_p2g_gather": 32, "p2g_mass": 4,
-                "loss_dldx": 4}
-    return per_particle.get(kernel, 0) * n + per_node.get(kernel, 0) * touched
+# Algorithmic bytes per launch of each kernel of the FP32 path: every particle
+# plane it must read or write once (4 B per FP32 value, the FP64 tied-control
+# accumulator 8 B), the sorted-order index of the warp-item kernels (4 B per
+# particle), and its grid records: per touched node for the particle-parallel
+# kernels, per grid node for the node-parallel ones.
+PER_PARTICLE_BYTES = {
+    "p_op1": (9 + 9 + 4 + 9) * 4 + 24 * 4,                  # F, dFc, m/vol/lam/mu, C -> G, R, S
+    "p2g": (3 + 1 + 3 + 9 + 1) * 4,                         # x, m, v, G, order
+    "g2p_p_op2": (3 + 9 + 9 + 1) * 4 + 24 * 4,              # x, F, dFc, order -> x, v, C, F
+    "adj_g2p_scatter": (3 + 24 + 9 + 9 + 1) * 4 + 12 * 4,   # x, adjoint', F, dFc, order -> dLdv', dLdC'
+    "adj_p2g_gather": (3 + 1 + 3 + 12 + 9 + 1) * 4 + 18 * 4,  # x, m, v, dLdv'/dLdC', G, order -> M, X, u, z
+    "adj_finalize": (18 + 9 + 9 + 9 + 6 + 4 + 9 + 9 + 3 + 9 + 9) * 4 + 24 * 4 + 9 * 8 * 2,
+    "p2g_mass": 4 * 4, "loss_dldx": 4 * 4 + 24 * 4,
+}
+PER_TOUCHED_NODE_BYTES = {"p2g": 16, "g2p_p_op2": 16, "adj_g2p_scatter": 16, "adj_p2g_gather": 32,
+                          "p2g_mass": 4, "loss_dldx": 4}
+PER_GRID_NODE_BYTES = {"g_op": 32, "adj_g_op": 64}
+
+
+def algorithmic_bytes(kernel: str, n: int, touched: int, nodes: int) -> float:
+    return (PER_PARTICLE_BYTES.get(kernel, 0) * n + PER_TOUCHED_NODE_BYTES.get(kernel, 0) * touched
+            + PER_GRID_NODE_BYTES.get(kernel, 0) * nodes)
 
 
 def committed_traffic(kernel: str):
@@ -382,6 +395,7 @@ def run_ours(args):
     ms_e2e = max_over_ranks(timed_steps(torch, c, args.steps, e2e_step), world)
     e2e_value = whole_job_value(units_per_step, args.steps, world, ms_e2e)
     touched = int(np.count_nonzero(c.get_grid(0, "grid_m")))
+    nodes = int(np.prod(sc.dims))
     c.close()
 
     # plain FP64 GPU path on the same workload
@@ -405,14 +419,14 @@ def run_ours(args):
     top = max(kern, key=lambda k: kern[k]["total_ms"]) if kern else None
     roof = None
     if top:
-        alg = algorithmic_bytes(top, sc.n, touched)
+        alg = algorithmic_bytes(top, sc.n, touched, nodes)
         achieved = alg / (kern[top]["avg_us"] * 1e-6) / 1e9
         roof = {"kernel": top, "bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                 "frac": achieved / peak, "peak_source": peak_kind + " (MEASURED_PEAKS.json hbm_gbs)",
                 "traffic": committed_traffic(top), "algorithmic_bytes_per_launch": alg,
                 "avg_launch_us": kern[top]["avg_us"]}
         for k in kern:
-            b = algorithmic_bytes(k, sc.n, touched)
+            b = algorithmic_bytes(k, sc.n, touched, nodes)
             if b:
                 kern[k]["hbm_frac"] = b / (kern[k]["avg_us"] * 1e-6) / 1e9 / peak
 
@@ -525,33 +539,138 @@ def run_config2(args):
         base = _mem_used_gb(torch, 0)
         c = setup_ctx(dmpm, sc, "fp32", 0, vol, target, sc.dt, ckpt)
         gradient_step(c)
+        first = c.control_grad()
         used = _mem_used_gb(torch, 0) - base
         n = max(1, args.steps // 4)
         ms = timed_steps(torch, c, n, lambda: gradient_step(c)) / n
         grads[ckpt] = c.control_grad()
+        if ckpt == 1:  # same inputs twice: the FP32 run-to-run spread (atomic summation order)
+            out["grad_relerr_fp32_repeat"] = float(np.linalg.norm(grads[1] - first) / np.linalg.norm(first))
         out["ckpt%d" % ckpt] = {"ms_per_gradient": ms, "particle_steps_per_s": sc.n * sc.steps / (ms / 1000.0),
                                 "hbm_gb": used, "engine_bytes_gb": c.info()["device_bytes"] / 1e9,
                                 "checkpoint_every": c.info()["checkpoint_every"]}
         c.close()
     out["recompute_overhead"] = out["ckpt25"]["ms_per_gradient"] / out["ckpt1"]["ms_per_gradient"] - 1.0
-    out["grad_relerr_ckpt25_vs_store_all"] = float(np.linalg.norm(grads[25] - grads[1]) / np.linalg.norm(grads[1]))
+    rel = lambda a, b: float(np.linalg.norm(a - b) / np.linalg.norm(b))
+    out["grad_relerr_ckpt25_vs_store_all"] = rel(grads[25], grads[1])
     if not args.no_fp64:
+        # the FP64 path twice on the same inputs: its spread is FP64 rounding
+        # (atomic summation order) amplified by the adjoint of this rollout
         c64 = setup_ctx(dmpm, sc, "fp64", 0, vol, target, sc.dt, 25)
         t0 = time.perf_counter()
         gradient_step(c64)
         g64 = c64.control_grad()
         out["fp64_ckpt25_s"] = time.perf_counter() - t0
-        out["grad_relerr_fp32_vs_fp64"] = float(np.linalg.norm(grads[25] - g64) / np.linalg.norm(g64))
+        gradient_step(c64)
+        out["grad_relerr_fp64_repeat"] = rel(c64.control_grad(), g64)
         c64.close()
+        out["grad_relerr_fp32_store_all_vs_fp64"] = rel(grads[1], g64)
+        out["grad_relerr_fp32_ckpt25_vs_fp64"] = rel(grads[25], g64)
+    print(json.dumps(out), flush=True)
+    return 0
+
+
+def run_config3(args):
+    """Config 3: 48 seeded instances (sphere / ellipsoid / box, 5k-150k
+    particles, 32^3 or 64^3, 100-300 steps) in one batch: one launch per stage
+    per time step, the gradient evaluation replayed as a CUDA graph, launch
+    settings autotuned; against the same batch without the graph and against
+    one engine context per instance run one after another."""
+    import torch
+
+    import dmpm
+
+    scs = scenes.batch_scenes(48)
+    lim = min(sc.cfl_dt() for sc in scs)
+    dt0 = scs[0].dt
+    dt = dt0 if dt0 <= lim else 0.5 * lim
+    units = float(sum(sc.n * sc.steps for sc in scs))  # particle-steps of one gradient evaluation
+    inputs = [_scene_inputs(dmpm, sc, 0) for sc in scs]
+    out = {"mode": "config3", "instances": len(scs), "particles": int(sum(sc.n for sc in scs)),
+           "particle_range": [int(min(sc.n for sc in scs)), int(max(sc.n for sc in scs))],
+           "steps_range": [int(min(sc.steps for sc in scs)), int(max(sc.steps for sc in scs))],
+           "grids": sorted({int(sc.dims[0]) for sc in scs}), "particle_steps_per_gradient": units, "dt": dt,
+           "dt_substituted_from": dt0 if dt != dt0 else None}
+    torch.cuda.synchronize()
+    base = _mem_used_gb(torch, 0)
+    b = dmpm.Batch([{"n": sc.n, "dims": sc.dims, "dx": sc.dx, "min_point": sc.min_point, "steps": sc.steps}
+                    for sc in scs])
+    b.set_params(dt=dt, drag=scs[0].drag, f_ext=scs[0].f_ext, smoothing=scs[0].smoothing, adjoint="exact")
+    for i, sc in enumerate(scs):
+        vol, target = inputs[i]
+        b.set_particles(i, sc.x, sc.m, sc.lam, sc.mu, v=sc.v, F=sc.F, C=sc.C, dFc=sc.dFc, vol=vol)
+        b.set_target_mass(i, target)
+    b.set_launch(use_graph=True)
+    b.setup()
+    out["hbm_gb"] = _mem_used_gb(torch, 0) - base
+    t0 = time.perf_counter()
+    out["autotune_best_ms"] = b.autotune(reps=1)
+    out["autotune_s"] = time.perf_counter() - t0
+    out["launch"] = b.launch()
+    stream = torch.cuda.ExternalStream(b.stream)
+    reps = max(2, args.steps // 4)
+
+    def timed(fn):
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        fn()
+        torch.cuda.synchronize()
+        e0.record(stream)
+        for _ in range(reps):
+            fn()
+        e1.record(stream)
+        e1.synchronize()
+        return e0.elapsed_time(e1) / reps
+
+    losses = b.gradient()
+    ms_graph = timed(lambda: b.gradient())
+    info = b.info()
+    grads = {i: b.control_grad(i) for i in (0, 1, len(scs) - 1)}
+    cfg = b.launch()
+    b.set_launch(sort_every=cfg["sort_every"], ctas_per_sm=cfg["ctas_per_sm"],
+                 particle_block=cfg["particle_block"], use_graph=False)
+    ms_eager = timed(lambda: b.gradient())
+    b.close()
+    out["batched_graph"] = {"ms_per_gradient": ms_graph, "particle_steps_per_s": units / (ms_graph / 1e3),
+                            "launches_per_gradient": info["launches_per_gradient"]}
+    out["batched_eager"] = {"ms_per_gradient": ms_eager, "particle_steps_per_s": units / (ms_eager / 1e3)}
+    # one engine context per instance, one after another (each with its own launches and syncs)
+    tot_ms, relerr_loss, relerr_grad = 0.0, 0.0, 0.0
+    for i, sc in enumerate(scs):
+        vol, target = inputs[i]
+        c = setup_ctx(dmpm, sc, "fp32", 0, vol, target, dt, 1)
+        s_i = torch.cuda.ExternalStream(c.stream)
+        gradient_step(c)
+        torch.cuda.synchronize()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(s_i)
+        for _ in range(reps):
+            lo = gradient_step(c)
+        e1.record(s_i)
+        e1.synchronize()
+        tot_ms += e0.elapsed_time(e1) / reps
+        relerr_loss = max(relerr_loss, abs(lo - losses[i]) / abs(lo))
+        if i in grads:
+            g = c.control_grad()
+            relerr_grad = max(relerr_grad, float(np.linalg.norm(grads[i] - g) / np.linalg.norm(g)))
+        c.close()
+    out["one_context_per_instance"] = {"ms_per_gradient": tot_ms, "particle_steps_per_s": units / (tot_ms / 1e3)}
+    out["speedup_graph_over_per_instance"] = tot_ms / ms_graph
+    out["speedup_graph_over_eager"] = ms_eager / ms_graph
+    out["max_loss_relerr_batch_vs_per_instance"] = relerr_loss
+    out["max_grad_relerr_batch_vs_per_instance"] = relerr_grad
     print(json.dumps(out), flush=True)
     return 0
 
 
 def run_config4(args):
     """Config 4: sphere -> torus at 256^3 (~8M particles), 400 steps, checkpoint
-    every 20, 30 device Adam iterations (lr 1e-2) on tied controls; loss curve,
-    per-iteration time, FP32 gradient error vs the FP64 GPU path at iterations
-    1 and the last."""
+    every 20, 30 device Adam iterations (lr 1e-2) on the per-particle controls of
+    the first control frame (layer 0; the reference's optimiser descends one
+    frame's dFc at a time, CompGraph.cpp:352-420, with the gradient divided by
+    its norm, PointCloud.cpp:83-99); loss curve, per-iteration time, FP32
+    gradient error vs the FP64 GPU path at iterations 1 and the last."""
     import torch
 
     import dmpm
@@ -566,31 +685,58 @@ def run_config4(args):
            "dt_substituted_from": dt_sub, "checkpoint_every": 20, "iterations": iters, "lr": 1e-2}
     torch.cuda.synchronize()
     base = _mem_used_gb(torch, 0)
-    c = setup_ctx(dmpm, sc, "fp32", 0, vol, target, sc.dt, 20)
+    frame = dict(control="per_layer", control_stride=sc.steps)  # layer 0 is the only control frame
+    c = setup_ctx(dmpm, sc, "fp32", 0, vol, target, sc.dt, 20, **frame)
     out["hbm_gb_fp32"] = _mem_used_gb(torch, 0) - base
+    out["controls"] = "per-particle dFc of layer 0 (one control frame), exact adjoint"
     losses, times, relerrs = [], [], {}
 
-    def fp64_relerr(grad32):
-        c64 = setup_ctx(dmpm, sc, "fp64", 0, vol, target, sc.dt, 20)
-        d = c.get(0, "dFc")
-        c64.set_layer(0, "dFc", d)
+    def fp64_relerr(grad32, dfc):
+        c64 = setup_ctx(dmpm, sc, "fp64", 0, vol, target, sc.dt, 20, **frame)
+        c64.set_layer(0, "dFc", dfc)
         gradient_step(c64)
-        g64 = c64.control_grad()
+        g64 = c64.control_grad(0)
         c64.close()
         return float(np.linalg.norm(grad32 - g64) / np.linalg.norm(g64))
 
+    # Adam with the reference optimiser's line search (CompGraph.cpp:388-420): step, re-run the
+    # forward pass, keep the step if the loss fell, else step back (Descend_Adam with -alpha, which
+    # updates the moments again, as the reference does) and halve alpha; a frame whose line search
+    # finds no decrease ends its descent.
+    max_ls = 6
+    ls_trials, grad_ms, stopped, last = [], [], None, None
     for it in range(1, iters + 1):
         holder = {}
         ms = timed_steps(torch, c, 1, lambda: holder.update(loss=gradient_step(c)))
-        losses.append(holder["loss"])
-        if it in (1, iters) and not args.no_fp64:
-            relerrs[it] = fp64_relerr(c.control_grad())
+        loss = holder["loss"]
+        losses.append(loss)
+        grad_ms.append(ms)
+        if not args.no_fp64:  # the controls and FP32 gradient of this iteration (host copies)
+            last = (it, c.control_grad(0), c.get(0, "dFc"))
+            if it == 1:
+                relerrs[1] = fp64_relerr(last[1], last[2])
         t0 = time.perf_counter()
-        c.adam_step(t=it, lr=1e-2)
+        alpha, found = 1e-2, False
+        for ls in range(max_ls):
+            c.adam_step(t=it, lr=alpha, layer=0)
+            c.forward(0)
+            if c.loss() < loss:
+                found = True
+                break
+            c.adam_step(t=it, lr=-alpha, layer=0)
+            alpha *= 0.5
         c.synchronize()
+        ls_trials.append(ls + 1)
         times.append(ms + 1000.0 * (time.perf_counter() - t0))
-    out.update({"loss_curve": losses, "ms_per_iteration": times,
-                "particle_steps_per_s": sc.n * sc.steps / (float(np.median(times)) / 1000.0),
+        if not found:
+            stopped = it
+            break
+    if last is not None and last[0] not in relerrs:
+        relerrs[last[0]] = fp64_relerr(last[1], last[2])
+    out.update({"loss_curve": losses, "ms_per_iteration": times, "ms_per_gradient": grad_ms,
+                "line_search_trials": ls_trials, "max_line_search_trials": max_ls,
+                "stopped_at_iteration_without_decrease": stopped,
+                "particle_steps_per_s": sc.n * sc.steps / (float(np.median(grad_ms)) / 1000.0),
                 "grad_relerr_vs_fp64": relerrs})
     c.close()
     print(json.dumps(out), flush=True)
@@ -609,7 +755,7 @@ def main():
     ap.add_argument("--rollout-steps", type=int, default=0, help="override the 200 time steps (profiling runs)")
     ap.add_argument("--no-fp64", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--config", type=int, default=1, help="1 = headline workload; 0, 2, 4 = extra measurements")
+    ap.add_argument("--config", type=int, default=1, help="1 = headline workload; 0, 2, 3, 4 = extra measurements")
     ap.add_argument("--iters", type=int, default=30, help="config 4: Adam iterations")
     args = ap.parse_args()
     if args.warmup < 3:
@@ -620,6 +766,8 @@ def main():
         return run_config0(args)
     if args.config == 2:
         return run_config2(args)
+    if args.config == 3:
+        return run_config3(args)
     if args.config == 4:
         return run_config4(args)
     return run_ours(args)

@@ -127,6 +127,11 @@ typedef struct {
     int tile_cap;            /* max nodes of a shared-memory tile; 0 = default */
     int sort_every;          /* FP32 path: re-sort particles by cell every this many steps; 0 = default (8) */
     int warp_general;        /* FP32 path: 1 disables the same-cell warp reduction (verification) */
+    int control_stride;      /* DMPM_CTRL_PER_LAYER: layers 0, s, 2s, ... below the last own their
+                                controls and gradients (OptInput::control_stride, the control frames
+                                of CompGraph::OptimizeDefGradControlSequence, CompGraph.cpp:352);
+                                the other layers read the uploaded dFc, as the reference's copies made
+                                by SetUpCompGraph stay unchanged there.  0 or 1 = every layer. */
 } dmpm_params;
 
 void dmpm_default_params(dmpm_params* p);
@@ -235,6 +240,63 @@ int dmpm_compute_volumes_noalloc(int n, const float* x, const float* m, int dim_
 int dmpm_set_profiling(dmpm_ctx* ctx, int on);
 int dmpm_kernel_stats(dmpm_ctx* ctx, int kernel_id, double* total_ms, int64_t* launches);
 const char* dmpm_kernel_name(int kernel_id);
+
+/* ------------------------------------------------------------------------
+ * Batched instances.  No reference counterpart: the reference drives one
+ * CompGraph per process (CompGraph.h:17-66).  A batch holds many independent
+ * scenes (each its own point cloud, grid, target and number of time steps)
+ * and advances all of them with one launch per stage per time step; a
+ * gradient evaluation (ComputeForwardPass(0), EndLayerMassLoss and
+ * ComputeBackwardPass(0) of every instance, CompGraph.cpp:246-267, 110-244)
+ * can be captured once and replayed as a CUDA graph.  FP32-mixed arithmetic
+ * (the FP32_MIXED path), every layer kept, tied controls (one dFc per
+ * particle, gradient summed over the instance's layers).  Instances share
+ * dt, drag, f_ext, smoothing, adjoint mode and loss kind (dmpm_params).
+ * One batch = one CUDA stream; not thread-safe.
+ * ------------------------------------------------------------------------ */
+typedef struct dmpm_batch dmpm_batch;
+typedef struct {
+    int n;                   /* particles */
+    int dim_x, dim_y, dim_z; /* grid nodes per axis */
+    double dx;
+    double min_point[3];
+    int steps;               /* time steps of the rollout (layers = steps + 1), >= 1 */
+} dmpm_instance;
+typedef struct {
+    int sort_every;     /* re-sort particles by cell every this many steps; 0 = 8 */
+    int ctas_per_sm;    /* persistent grid of the warp-item kernels, CTAs per SM (1..8); 0 = 3 */
+    int particle_block; /* threads per block of the per-particle kernels: 128 or 256; 0 = 256 */
+    int use_graph;      /* 1 = capture the gradient evaluation once, replay it as a CUDA graph */
+} dmpm_batch_launch;
+int dmpm_batch_create(int device, int count, const dmpm_instance* instances, dmpm_batch** out);
+int dmpm_batch_destroy(dmpm_batch* b);
+const char* dmpm_batch_last_error(const dmpm_batch* b);
+int dmpm_batch_set_params(dmpm_batch* b, const dmpm_params* params);
+/* Instance `inst` (0-based, creation order): host arrays as dmpm_set_particles. */
+int dmpm_batch_set_particles(dmpm_batch* b, int inst, const double* x, const double* v, const double* F,
+                             const double* C, const double* dFc, const double* m, const double* vol,
+                             const double* lam, const double* mu);
+int dmpm_batch_set_target_mass(dmpm_batch* b, int inst, const double* target_m);
+int dmpm_batch_set_launch(dmpm_batch* b, const dmpm_batch_launch* cfg);
+int dmpm_batch_get_launch(const dmpm_batch* b, dmpm_batch_launch* cfg);
+/* Allocate every layer of every instance (store-all); fails with DMPM_ERR_OOM
+ * when the batch does not fit. */
+int dmpm_batch_setup(dmpm_batch* b);
+/* One gradient evaluation of every instance; losses: host, count doubles
+ * (EndLayerMassLoss of each instance's last layer). */
+int dmpm_batch_gradient(dmpm_batch* b, double* losses);
+/* Time each launch configuration of a small grid (sort interval, CTAs per SM,
+ * particle block) over `reps` gradient evaluations, keep the fastest and
+ * report its milliseconds per evaluation. */
+int dmpm_batch_autotune(dmpm_batch* b, int reps, double* best_ms);
+/* dL/d dFc of instance `inst` (tied: summed over its layers), host n * 9 doubles. */
+int dmpm_batch_get_control_grad(dmpm_batch* b, int inst, double* out);
+/* DMPM_F_X, _V, _F or _C of instance `inst` at `layer` (0..steps), host doubles. */
+int dmpm_batch_get_particles(dmpm_batch* b, int inst, int layer, int field, double* out);
+/* info: [0] instances, [1] particles, [2] grid nodes, [3] device bytes,
+ * [4] kernel launches of one gradient evaluation, [5] 1 if a graph is captured */
+int dmpm_batch_info(const dmpm_batch* b, int64_t* info, int count);
+int dmpm_batch_stream(const dmpm_batch* b, void** stream);
 
 #ifdef __cplusplus
 }

@@ -35,6 +35,22 @@ def test_params_struct_matches_header():
     assert abs(p.dt - 1.0 / 120.0) < 1e-15 and p.drag == 0.5 and abs(p.smoothing - 0.1) < 1e-15
 
 
+def test_params_layout_matches_c(tmp_path):
+    """Every field of the ctypes Params sits at the offset the C compiler gives dmpm_params."""
+    fields = [f for f, _ in dmpm.Params._fields_]
+    prog = tmp_path / "layout.c"
+    prog.write_text('#include <stddef.h>\n#include <stdio.h>\n#include "dmpm.h"\nint main(void) {\n'
+                    '  printf("%zu\\n", sizeof(dmpm_params));\n'
+                    + "".join('  printf("%%zu\\n", offsetof(dmpm_params, %s));\n' % f for f in fields)
+                    + "  return 0;\n}\n")
+    exe = tmp_path / "layout"
+    subprocess.check_call(["gcc", "-I", os.path.join(REPO, "include"), str(prog), "-o", str(exe)])
+    vals = [int(v) for v in subprocess.run([str(exe)], capture_output=True, text=True, check=True).stdout.split()]
+    import ctypes
+    assert vals[0] == ctypes.sizeof(dmpm.Params)
+    assert vals[1:] == [getattr(dmpm.Params, f).offset for f in fields]
+
+
 def test_null_arguments_are_rejected_without_gpu():
     lib = dmpm.load_library()
     assert lib.dmpm_create(0, 7, None) == dmpm.ERR_ARG

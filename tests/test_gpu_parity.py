@@ -371,3 +371,38 @@ def test_device_adam_step_matches_reference_formula(gpu_ready, exact_case):
     want2 = want1 - 1e-2 * (m2 / (1 - 0.81)) / (np.sqrt(v2 / (1 - 0.999 ** 2)) + 1e-5)
     assert relerr(d1 - d0, want1 - d0) < 1e-4
     assert relerr(d2 - d0, want2 - d0) < 1e-4
+
+
+def test_control_stride_keeps_controls_on_frames_only(gpu_ready, exact_case):
+    """control_stride = 3 with 7 layers: layers 0 and 3 own dFc and its gradient
+    (the control frames of OptimizeDefGradControlSequence, CompGraph.cpp:352);
+    the others read the uploaded dFc.  Same losses and frame gradients as
+    per-layer storage of every layer, before and after editing a frame's dFc."""
+    sc, o, loss, L = exact_case
+    rng = np.random.default_rng(11)
+    with make_ctx(sc, "fp64", o.target, adjoint="exact") as c1, \
+            make_ctx(sc, "fp64", o.target, adjoint="exact", control_stride=3) as c3:
+        for c in (c1, c3):
+            c.setup(L)
+        for it in range(2):
+            res = []
+            for c in (c1, c3):
+                c.forward(0)
+                lo = c.loss()
+                c.backward(0)
+                res.append((lo, c.control_grad(0), c.control_grad(3)))
+            assert abs(res[0][0] - res[1][0]) <= 1e-13 * abs(res[0][0])
+            assert relerr(res[1][1], res[0][1]) < 1e-12 and relerr(res[1][2], res[0][2]) < 1e-12
+            if it == 0:
+                assert relerr(res[1][1], o.get(0, "dLdFe")) < 1e-9
+                assert relerr(res[1][2], o.get(3, "dLdFe")) < 1e-9
+                d = c3.get(3, "dFc") + 1e-3 * rng.normal(size=(sc.n, 3, 3))
+                c1.set_layer(3, "dFc", d)
+                c3.set_layer(3, "dFc", d)
+        with pytest.raises(dmpm.DmpmError):
+            c3.set_layer(1, "dFc", d)
+        with pytest.raises(dmpm.DmpmError):
+            c3.control_grad(2)
+        with pytest.raises(dmpm.DmpmError):
+            c3.adam_step(t=1, layer=4)
+        c3.adam_step(t=1, layer=3)
