@@ -561,9 +561,7 @@ struct dmpm_batch::Impl {
         if (ex) k_adj_gather_w<true, true><<<wb, 256, 0, b->stream>>>(a);
         else k_adj_gather_w<false, true><<<wb, 256, 0, b->stream>>>(a);
         launched();
-        const unsigned fb = (unsigned)((a.n + 127) / 128);
-        if (ex) k_adj_finalize<true><<<fb, 128, 0, b->stream>>>(a);
-        else k_adj_finalize<false><<<fb, 128, 0, b->stream>>>(a);
+        launch_finalize(a, ex, b->stream);
         launched();
     }
 

@@ -981,8 +981,7 @@ template <class T> class Engine : public EngineBase {
                 pend();
             }
             pbeg(K_ADJ_FINALIZE);
-            if (ex) k_adj_finalize<true><<<(n_ + 127) / 128, 128, 0, ctx_->stream>>>(a);
-            else k_adj_finalize<false><<<(n_ + 127) / 128, 128, 0, ctx_->stream>>>(a);
+            launch_finalize(a, ex, ctx_->stream);
             launched();
             pend();
             return;

@@ -279,11 +279,12 @@ template <bool BATCH> __device__ __forceinline__ void item_grid(const WArgs& a, 
     }
 }
 
-// Gathers over a warp whose 32 lanes share one stencil base (all 8 particles
-// of the item in one cell, the common case after the cell sort) first copy
-// the item's 64 stencil nodes, R consecutive node4 records each, from global
-// memory into the warp's shared-memory slice: 2R independent 16-byte loads per
-// lane, all in flight together, instead of 16 R dependent loads per lane.
+// The adjoint gather over a warp whose 32 lanes share one stencil base (all 8
+// particles of the item in one cell, the common case after the cell sort)
+// first copies the item's 64 stencil nodes, R consecutive node4 records each,
+// from global memory into the warp's shared-memory slice: 2R independent
+// 16-byte loads per lane, all in flight together, instead of 16 R dependent
+// loads per lane (1.6 % faster on the 64^3, 267k-particle workload).
 // Record r of stencil node (s, j, k) lands at dst[R (16 s + 4 j + k) + r];
 // nodes outside the grid are stored as zeros.  Warp kernels run 256-thread
 // blocks (8 warps), one slice per warp.
@@ -430,44 +431,50 @@ template <bool BATCH> __global__ void __launch_bounds__(256, 4) k_g2p_w(WArgs a)
         load_x_base(a.st, npl, L.p, geo, x, base);
         LaneW w;
         lane_weights(x, geo, base, L.s, w, false);
-        float acc[12];  // v (3), C (9) row-major; C scaled by 3/dx^2 at the end
+        // v = sum w v_g and C = sum w v_g d^T (scaled by 3/dx^2 at the end), with the
+        // weight w = n0 n1[j] n2[k] and d = (d0, d1[j], d2[k]) factored per stencil row:
+        // the node loop accumulates only the k-dependent sums, the row applies n0 n1[j]
+        // and d1[j], and the d0 column is d0 v.
+        float nd2[4];
 #pragma unroll
-        for (int i = 0; i < 12; i++) acc[i] = 0.f;
-        auto node = [&](const node4<float>& nd, int j, int k) {
-            const float wt = w.n0 * w.n1[j] * w.n2[k];
-            const float vg[3] = {nd.x, nd.y, nd.z};
-            const float d[3] = {w.d0, w.d1[j], w.d2[k]};
+        for (int k = 0; k < 4; k++) nd2[k] = w.n2[k] * w.d2[k];
+        float V[3] = {0.f, 0.f, 0.f}, C1[3] = {0.f, 0.f, 0.f}, C2[3] = {0.f, 0.f, 0.f};
+        LaneNodes N = lane_nodes(geo, base, L.s);
+        N.g00 += goff;
+#pragma unroll
+        for (int j = 0; j < 4; j++) {
+            // the row's four node records are loaded before any is used (more loads in
+            // flight); nodes outside the grid read as zero and contribute nothing
+            node4<float> row[4];
+#pragma unroll
+            for (int k = 0; k < 4; k++)
+                row[k] = ((N.mask >> (4 * j + k)) & 1u) ? a.grid[N.g00 + j * N.sj + k]
+                                                         : node4<float>{0.f, 0.f, 0.f, 0.f};
+            float Vj[3] = {0.f, 0.f, 0.f}, Wj[3] = {0.f, 0.f, 0.f};
+#pragma unroll
+            for (int k = 0; k < 4; k++) {
+                const float vg[3] = {row[k].x, row[k].y, row[k].z};
+#pragma unroll
+                for (int r = 0; r < 3; r++) {
+                    Vj[r] += w.n2[k] * vg[r];
+                    Wj[r] += nd2[k] * vg[r];
+                }
+            }
+            const float w01 = w.n0 * w.n1[j], w01d = w01 * w.d1[j];
 #pragma unroll
             for (int r = 0; r < 3; r++) {
-                const float wv = wt * vg[r];
-                acc[r] += wv;
-#pragma unroll
-                for (int c = 0; c < 3; c++) acc[3 + 3 * r + c] += wv * d[c];
+                V[r] += w01 * Vj[r];
+                C1[r] += w01d * Vj[r];
+                C2[r] += w01 * Wj[r];
             }
-        };
-        if (DMPM_STAGE_NODES && warp_uniform_base(base)) {
-            __shared__ node4<float> s_nodes[8][64];
-            node4<float>* sw = s_nodes[threadIdx.x >> 5];
-            stage_stencil<1>(a.grid, geo, goff, base, sw);
+        }
+        float acc[12];  // v (3), C (9) row-major
 #pragma unroll
-            for (int j = 0; j < 4; j++)
-#pragma unroll
-                for (int k = 0; k < 4; k++) node(sw[16 * L.s + 4 * j + k], j, k);
-        } else {
-            LaneNodes N = lane_nodes(geo, base, L.s);
-            N.g00 += goff;
-#pragma unroll
-            for (int j = 0; j < 4; j++) {
-                // the row's four node records are loaded before any is used (more loads in
-                // flight); nodes outside the grid read as zero and contribute nothing
-                node4<float> row[4];
-#pragma unroll
-                for (int k = 0; k < 4; k++)
-                    row[k] = ((N.mask >> (4 * j + k)) & 1u) ? a.grid[N.g00 + j * N.sj + k]
-                                                             : node4<float>{0.f, 0.f, 0.f, 0.f};
-#pragma unroll
-                for (int k = 0; k < 4; k++) node(row[k], j, k);
-            }
+        for (int r = 0; r < 3; r++) {
+            acc[r] = V[r];
+            acc[3 + 3 * r] = w.d0 * V[r];
+            acc[4 + 3 * r] = C1[r];
+            acc[5 + 3 * r] = C2[r];
         }
         reduce_slabs<12>(acc);
         if (!L.valid) continue;
@@ -721,83 +728,150 @@ template <bool EXACT, bool BATCH> __global__ void __launch_bounds__(256, DMPM_GA
     }
 }
 
+// ------------------------------------------------------------------ finalize
 // per particle: P, polar factors and dP/dF in FP64, then the adjoint of layer n
 //   dLdP = -3/dx^2 dt vol M^T Fe,  dLdF(stress) = -3/dx^2 dt vol M P,  dLdC = m M^T
 //   dLdx = -X/dx - G^T u - 3/dx^2 dLdC_next^T z + dLdx',  dLdv = m (1 - dt drag) u
 //   REFCOMPAT: dLdF = (1-s)T + s dLdF' + stress + T + dP:dLdP,  T = (I + dt C')^T dLdF'
 //   EXACT:     dLdFe = (1-s)T + stress + dP:dLdP,  dLdF = dLdFe + s dLdF'
-// (the REFCOMPAT variant, with its finite-difference dJFit, keeps the
-// compiler's own register budget)
-template <bool EXACT>
-__global__ void __launch_bounds__(128, EXACT ? DMPM_FINALIZE_MIN_BLOCKS : 1) k_adj_finalize(WArgs a) {
-    const size_t np = a.np, npl = a.npl, npn = a.npn;
-    const int p = blockIdx.x * blockDim.x + threadIdx.x;
-    if (p < a.n) {
-        m3<float> M;
+//
+// Its inputs are 94 FP32 planes per particle (slots below) and, with tied
+// controls, the 9 FP64 planes of the control-gradient accumulator.
+enum : int {
+    FS_GATH = 0,    // 18: M (9, row-major), X (3), u (3), z (3)
+    FS_F = 18,      // 9: F of layer n
+    FS_DFC = 27,    // 9: dFc
+    FS_AUX = 36,    // 24: G (9), polar R (9), polar S (6)
+    FS_CST = 60,    // 4: m, vol, lam, mu
+    FS_CN = 64,     // 9: dLdC_next
+    FS_AX = 73,     // 3: dLdx of layer n+1
+    FS_AF = 76,     // 9: dLdF of layer n+1
+    FS_CNEXT = 85,  // 9: C of layer n+1
+    FS_COUNT = 94
+};
+
+// first element and stride of a slot's plane
+__device__ __forceinline__ const float* fin_plane(const WArgs& a, int slot, size_t& stride) {
+    if (slot < FS_F) { stride = a.np; return a.gath + (size_t)slot * a.np; }
+    if (slot < FS_DFC) { stride = a.npl; return a.st + (size_t)(PF + slot - FS_F) * a.npl; }
+    if (slot < FS_AUX) { stride = a.np; return a.dfc + (size_t)(slot - FS_DFC) * a.np; }
+    if (slot < FS_CST) { stride = a.npl; return a.G + (size_t)(slot - FS_AUX) * a.npl; }
+    if (slot < FS_CN) { stride = a.np; return a.cst + (size_t)(slot - FS_CST) * a.np; }
+    if (slot < FS_AX) { stride = a.np; return a.adjn + (size_t)(3 + slot - FS_CN) * a.np; }
+    if (slot < FS_AF) { stride = a.npn; return a.adj_next + (size_t)(PX + slot - FS_AX) * a.npn; }
+    if (slot < FS_CNEXT) { stride = a.npn; return a.adj_next + (size_t)(PF + slot - FS_AF) * a.npn; }
+    stride = a.npn;
+    return a.st_next + (size_t)(PC + slot - FS_CNEXT) * a.npn;
+}
+
+// the finalize inputs of particle p, read from global memory
+struct FinGlobal {
+    const WArgs* a;
+    int p;
+    __device__ __forceinline__ float operator()(int slot) const {
+        size_t st;
+        return fin_plane(*a, slot, st)[p];
+    }
+    __device__ __forceinline__ double acc(int i) const { return a->ctrl_acc[(size_t)i * a->np + p]; }
+};
+template <bool EXACT, class In> __device__ __forceinline__ void finalize_particle(const WArgs& a, int p, const In& in) {
+    const size_t np = a.np, npl = a.npl;
+    auto mat = [&](int slot) {  // 9 column-major planes -> m3
+        m3<float> m;
 #pragma unroll
         for (int r = 0; r < 3; r++)
 #pragma unroll
-            for (int c = 0; c < 3; c++) M.a[r][c] = a.gath[(size_t)(3 * r + c) * np + p];
-        const m3<float> Fe = load_m3(a.st + (size_t)PF * npl, npl, p) + load_m3(a.dfc, np, p);
-        const m3<double> Fed = m3_cast<double>(Fe);
-        // polar factors computed in FP64 by k_stress for this layer
-        const m3<double> Rd = m3_cast<double>(load_m3(a.G + 9 * npl, npl, p));
-        m3<double> Sd;
-        Sd.a[0][0] = a.G[18 * npl + p];
-        Sd.a[0][1] = Sd.a[1][0] = a.G[19 * npl + p];
-        Sd.a[0][2] = Sd.a[2][0] = a.G[20 * npl + p];
-        Sd.a[1][1] = a.G[21 * npl + p];
-        Sd.a[1][2] = Sd.a[2][1] = a.G[22 * npl + p];
-        Sd.a[2][2] = a.G[23 * npl + p];
-        const double lam = (double)a.cst[(size_t)KLAM * np + p], mu = (double)a.cst[(size_t)KMU * np + p];
-        const m3<float> P = m3_cast<float>(pk_from_polar(Fed, Rd, lam, mu));
-        const float mp = a.cst[(size_t)KM * np + p], vol = a.cst[(size_t)KVOL * np + p];
-        const float dx = (float)a.geo.dx;
-        const float k3 = 3.f / (dx * dx);
-        const float kk = -k3 * a.dt * vol;
-        const m3<float> dLdP = kk * mtm(M, Fe);
-        const m3<float> dFstress = kk * (M * P);
-        const m3<float> G = load_m3(a.G, npl, p);
-        const m3<float> Cn = load_m3(a.adjn + 3 * np, np, p);
-        float u[3], z[3], gtu[3], ctz[3];
+            for (int c = 0; c < 3; c++) m.a[r][c] = in(slot + r + 3 * c);
+        return m;
+    };
+    m3<float> M;
 #pragma unroll
-        for (int c = 0; c < 3; c++) {
-            u[c] = a.gath[(size_t)(12 + c) * np + p];
-            z[c] = a.gath[(size_t)(15 + c) * np + p];
-        }
-        mtv(G, u, gtu);
-        mtv(Cn, z, ctz);
+    for (int r = 0; r < 3; r++)
 #pragma unroll
-        for (int c = 0; c < 3; c++) {
-            const float X = a.gath[(size_t)(9 + c) * np + p];
-            a.adj[(size_t)(PX + c) * npl + p] = -X / dx - gtu[c] - k3 * ctz[c] + a.adj_next[(size_t)(PX + c) * npn + p];
-            a.adj[(size_t)(PV + c) * npl + p] = mp * (1.f - a.dt * a.drag) * u[c];
-        }
-        store_m3(a.adj + (size_t)PC * npl, npl, p, mp * transpose(M));
-        const m3<float> Cnext = load_m3(a.st_next + (size_t)PC * npn, npn, p);
-        const m3<float> dFn = load_m3(a.adj_next + (size_t)PF * npn, npn, p);
-        const m3<float> Tr = mtm(m3_eye<float>() + a.dt * Cnext, dFn);
-        const m3<float> d2 = m3_cast<float>(d2_mult_from_polar<EXACT>(Fed, Rd, Sd, lam, mu, m3_cast<double>(dLdP)));
-        m3<float> dLdF, dLdFe;
-        if (EXACT) {
-            dLdFe = (1.f - a.s) * Tr + dFstress + d2;
-            dLdF = dLdFe + a.s * dFn;
-        } else {
-            dLdF = ((1.f - a.s) * Tr + a.s * dFn) + dFstress + Tr + d2;
-            dLdFe = dLdF;
-        }
-        store_m3(a.adj + (size_t)PF * npl, npl, p, dLdF);
-        if (a.ctrl_grad) store_m3(a.ctrl_grad, np, p, dLdFe);
-        if (a.ctrl_acc) {
+        for (int c = 0; c < 3; c++) M.a[r][c] = in(FS_GATH + 3 * r + c);
+    const m3<float> Fe = mat(FS_F) + mat(FS_DFC);
+    const m3<double> Fed = m3_cast<double>(Fe);
+    // polar factors computed in FP64 by k_stress for this layer
+    const m3<double> Rd = m3_cast<double>(mat(FS_AUX + 9));
+    m3<double> Sd;
+    Sd.a[0][0] = in(FS_AUX + 18);
+    Sd.a[0][1] = Sd.a[1][0] = in(FS_AUX + 19);
+    Sd.a[0][2] = Sd.a[2][0] = in(FS_AUX + 20);
+    Sd.a[1][1] = in(FS_AUX + 21);
+    Sd.a[1][2] = Sd.a[2][1] = in(FS_AUX + 22);
+    Sd.a[2][2] = in(FS_AUX + 23);
+    const double lam = (double)in(FS_CST + KLAM), mu = (double)in(FS_CST + KMU);
+    const m3<float> P = m3_cast<float>(pk_from_polar(Fed, Rd, lam, mu));
+    const float mp = in(FS_CST + KM), vol = in(FS_CST + KVOL);
+    const float dx = (float)a.geo.dx;
+    const float k3 = 3.f / (dx * dx);
+    const float kk = -k3 * a.dt * vol;
+    const m3<float> dLdP = kk * mtm(M, Fe);
+    const m3<float> dFstress = kk * (M * P);
+    const m3<float> G = mat(FS_AUX);
+    const m3<float> Cn = mat(FS_CN);
+    float u[3], z[3], gtu[3], ctz[3];
 #pragma unroll
-            for (int c = 0; c < 3; c++)
-#pragma unroll
-                for (int r = 0; r < 3; r++) a.ctrl_acc[(size_t)(r + 3 * c) * np + p] += (double)dLdFe.a[r][c];
-        }
-        if (a.dbg_dLdP) store_m3(a.dbg_dLdP, np, p, dLdP);
-        if (!isfinite(dLdF.a[0][0] + dLdF.a[1][1] + dLdF.a[2][2] + a.adj[(size_t)PX * npl + p]))
-            atomicOr(a.status, ST_NONFINITE_ADJ);
+    for (int c = 0; c < 3; c++) {
+        u[c] = in(FS_GATH + 12 + c);
+        z[c] = in(FS_GATH + 15 + c);
     }
+    mtv(G, u, gtu);
+    mtv(Cn, z, ctz);
+    float ax0 = 0.f;
+#pragma unroll
+    for (int c = 0; c < 3; c++) {
+        const float X = in(FS_GATH + 9 + c);
+        const float ax = -X / dx - gtu[c] - k3 * ctz[c] + in(FS_AX + c);
+        if (c == 0) ax0 = ax;
+        a.adj[(size_t)(PX + c) * npl + p] = ax;
+        a.adj[(size_t)(PV + c) * npl + p] = mp * (1.f - a.dt * a.drag) * u[c];
+    }
+    store_m3(a.adj + (size_t)PC * npl, npl, p, mp * transpose(M));
+    const m3<float> Cnext = mat(FS_CNEXT);
+    const m3<float> dFn = mat(FS_AF);
+    const m3<float> Tr = mtm(m3_eye<float>() + a.dt * Cnext, dFn);
+    const m3<float> d2 = m3_cast<float>(d2_mult_from_polar<EXACT>(Fed, Rd, Sd, lam, mu, m3_cast<double>(dLdP)));
+    m3<float> dLdF, dLdFe;
+    if (EXACT) {
+        dLdFe = (1.f - a.s) * Tr + dFstress + d2;
+        dLdF = dLdFe + a.s * dFn;
+    } else {
+        dLdF = ((1.f - a.s) * Tr + a.s * dFn) + dFstress + Tr + d2;
+        dLdFe = dLdF;
+    }
+    store_m3(a.adj + (size_t)PF * npl, npl, p, dLdF);
+    if (a.ctrl_grad) store_m3(a.ctrl_grad, np, p, dLdFe);
+    if (a.ctrl_acc) {
+#pragma unroll
+        for (int c = 0; c < 3; c++)
+#pragma unroll
+            for (int r = 0; r < 3; r++)
+                a.ctrl_acc[(size_t)(r + 3 * c) * np + p] = in.acc(r + 3 * c) + (double)dLdFe.a[r][c];
+    }
+    if (a.dbg_dLdP) store_m3(a.dbg_dLdP, np, p, dLdP);
+    if (!isfinite(dLdF.a[0][0] + dLdF.a[1][1] + dLdF.a[2][2] + ax0)) atomicOr(a.status, ST_NONFINITE_ADJ);
+}
+
+// one thread per particle, inputs read from global memory (the REFCOMPAT
+// variant, with its finite-difference dJFit, keeps the compiler's own
+// register budget)
+template <bool EXACT>
+__global__ void __launch_bounds__(128, EXACT ? DMPM_FINALIZE_MIN_BLOCKS : 1) k_adj_finalize(WArgs a) {
+    const int p = blockIdx.x * blockDim.x + threadIdx.x;
+    if (p < a.n) finalize_particle<EXACT>(a, p, FinGlobal{&a, p});
+}
+
+// host side: one thread per particle (a variant that first staged each
+// block's 94 input planes in shared memory with cp.async.bulk copies measured
+// 7 % slower on the 64^3, 267k-particle workload -- 57 KB of shared memory
+// per 128 particles cut residency to 12 warps per SM, and the kernel is bound
+// by its dependent FP64 chains, not by load latency -- so it was dropped)
+inline void launch_finalize(const WArgs& a, bool exact, cudaStream_t st) {
+    if (a.n <= 0) return;
+    const unsigned b = (unsigned)((a.n + 127) / 128);
+    if (exact) k_adj_finalize<true><<<b, 128, 0, st>>>(a);
+    else k_adj_finalize<false><<<b, 128, 0, st>>>(a);
 }
 
 }  // namespace dmpm

@@ -138,6 +138,19 @@ def max_over_ranks(value: float, world: int) -> float:
     return float(t.item())
 
 
+def shard_instances(work, world: int, rank: int):
+    """Instances of this rank: longest-processing-time-first assignment of the
+    per-instance work (particles x steps) to the least-loaded rank; every
+    instance goes to exactly one rank and no data crosses ranks."""
+    load = [0.0] * world
+    owner = {}
+    for i in sorted(range(len(work)), key=lambda i: (-work[i], i)):
+        r = min(range(world), key=lambda r: (load[r], r))
+        owner[i] = r
+        load[r] += work[i]
+    return [i for i in range(len(work)) if owner[i] == rank]
+
+
 def whole_job_value(units_per_rank_step: float, steps: int, world: int, ms_max: float) -> float:
     """Units all ranks processed / the slowest rank's device time (weak scaling)."""
     return units_per_rank_step * steps * world / (ms_max / 1000.0)
@@ -472,6 +485,57 @@ def _mem_used_gb(torch, device):
     return (total - free) / 1e9
 
 
+def run_fd(args):
+    """Config 1 at full size: the adjoint's directional derivatives g.d (plain
+    FP64 path and FP32-mixed path, exact adjoint, tied controls) against FP64
+    central differences (L(dFc + h d) - L(dFc - h d)) / 2h along 16 seeded
+    directions d with N(0, 1) entries, for h = 1e-3 (the configured step) and
+    smaller steps (truncation error shrinks with h until the loss's rounding
+    dominates)."""
+    import dmpm
+
+    sc = build_scene(0, args.ppc_root)
+    if args.rollout_steps:
+        sc.steps = args.rollout_steps
+    sc.dt, dt_sub = _cfl_dt(sc)
+    vol, target = _scene_inputs(dmpm, sc, 0)
+    hs = [float(x) for x in args.fd_h.split(",")]
+    ndir = 16
+    rng = np.random.default_rng(12345)
+    dirs = [rng.normal(size=(sc.n, 3, 3)) for _ in range(ndir)]
+    c64 = setup_ctx(dmpm, sc, "fp64", 0, vol, target, sc.dt, 1)
+    gradient_step(c64)
+    g64 = c64.control_grad()
+    c32 = setup_ctx(dmpm, sc, "fp32", 0, vol, target, sc.dt, 1)
+    gradient_step(c32)
+    g32 = c32.control_grad()
+    c32.close()
+    base = c64.get(0, "dFc")
+    a64 = [float(np.sum(g64 * d)) for d in dirs]
+    a32 = [float(np.sum(g32 * d)) for d in dirs]
+    per_h = {}
+    for h in hs:
+        fds = []
+        for d in dirs:
+            lp = []
+            for sgn in (1.0, -1.0):
+                c64.set_layer(0, "dFc", base + sgn * h * d)
+                c64.forward(0)
+                lp.append(c64.loss())
+            fds.append((lp[0] - lp[1]) / (2 * h))
+        e64 = [abs(a - f) / abs(f) for a, f in zip(a64, fds)]
+        e32 = [abs(a - f) / abs(f) for a, f in zip(a32, fds)]
+        per_h["%g" % h] = {"relerr_fp64_median": float(np.median(e64)), "relerr_fp64_max": float(np.max(e64)),
+                           "relerr_fp32_median": float(np.median(e32)), "relerr_fp32_max": float(np.max(e32)),
+                           "fd": fds}
+    c64.close()
+    out = {"mode": "fd", "workload": "ellipsoid -> torus, 64^3, %d particles, %d steps" % (sc.n, sc.steps),
+           "dt": sc.dt, "dt_substituted_from": dt_sub, "directions": ndir, "adjoint_fp64": a64, "adjoint_fp32": a32,
+           "grad_relerr_fp32_vs_fp64": float(np.linalg.norm(g32 - g64) / np.linalg.norm(g64)), "per_h": per_h}
+    print(json.dumps(out), flush=True)
+    return 0
+
+
 def run_config0(args):
     """Config 0 at full size: the plain FP64 GPU path against the reference's own
     FP64 build (oracle/_ref) on the same scene -- forward state, loss and the
@@ -580,21 +644,26 @@ def run_config3(args):
 
     import dmpm
 
-    scs = scenes.batch_scenes(48)
-    lim = min(sc.cfl_dt() for sc in scs)
-    dt0 = scs[0].dt
+    world, rank, local = dist_setup(args.gpus)
+    all_scs = scenes.batch_scenes(args.instances)
+    lim = min(sc.cfl_dt() for sc in all_scs)  # one dt for every instance: the smallest limit
+    dt0 = all_scs[0].dt
     dt = dt0 if dt0 <= lim else 0.5 * lim
+    units_all = float(sum(sc.n * sc.steps for sc in all_scs))
+    mine = shard_instances([sc.n * sc.steps for sc in all_scs], world, rank)
+    scs = [all_scs[i] for i in mine]
     units = float(sum(sc.n * sc.steps for sc in scs))  # particle-steps of one gradient evaluation
-    inputs = [_scene_inputs(dmpm, sc, 0) for sc in scs]
-    out = {"mode": "config3", "instances": len(scs), "particles": int(sum(sc.n for sc in scs)),
+    inputs = [_scene_inputs(dmpm, sc, local) for sc in scs]
+    out = {"mode": "config3", "n_gpus": world, "scaling": "strong", "instances": len(all_scs),
+           "instances_on_rank0": len(scs), "particles": int(sum(sc.n for sc in all_scs)),
            "particle_range": [int(min(sc.n for sc in scs)), int(max(sc.n for sc in scs))],
            "steps_range": [int(min(sc.steps for sc in scs)), int(max(sc.steps for sc in scs))],
            "grids": sorted({int(sc.dims[0]) for sc in scs}), "particle_steps_per_gradient": units, "dt": dt,
            "dt_substituted_from": dt0 if dt != dt0 else None}
     torch.cuda.synchronize()
-    base = _mem_used_gb(torch, 0)
+    base = _mem_used_gb(torch, local)
     b = dmpm.Batch([{"n": sc.n, "dims": sc.dims, "dx": sc.dx, "min_point": sc.min_point, "steps": sc.steps}
-                    for sc in scs])
+                    for sc in scs], device=local)
     b.set_params(dt=dt, drag=scs[0].drag, f_ext=scs[0].f_ext, smoothing=scs[0].smoothing, adjoint="exact")
     for i, sc in enumerate(scs):
         vol, target = inputs[i]
@@ -602,7 +671,7 @@ def run_config3(args):
         b.set_target_mass(i, target)
     b.set_launch(use_graph=True)
     b.setup()
-    out["hbm_gb"] = _mem_used_gb(torch, 0) - base
+    out["hbm_gb"] = _mem_used_gb(torch, local) - base
     t0 = time.perf_counter()
     out["autotune_best_ms"] = b.autotune(reps=1)
     out["autotune_s"] = time.perf_counter() - t0
@@ -623,22 +692,25 @@ def run_config3(args):
         return e0.elapsed_time(e1) / reps
 
     losses = b.gradient()
-    ms_graph = timed(lambda: b.gradient())
+    barrier(world)
+    ms_graph = max_over_ranks(timed(lambda: b.gradient()), world)
     info = b.info()
-    grads = {i: b.control_grad(i) for i in (0, 1, len(scs) - 1)}
+    grads = {i: b.control_grad(i) for i in sorted({0, min(1, len(scs) - 1), len(scs) - 1})}
     cfg = b.launch()
     b.set_launch(sort_every=cfg["sort_every"], ctas_per_sm=cfg["ctas_per_sm"],
                  particle_block=cfg["particle_block"], use_graph=False)
-    ms_eager = timed(lambda: b.gradient())
+    barrier(world)
+    ms_eager = max_over_ranks(timed(lambda: b.gradient()), world)
     b.close()
-    out["batched_graph"] = {"ms_per_gradient": ms_graph, "particle_steps_per_s": units / (ms_graph / 1e3),
+    # whole job: every rank's particle-steps over the slowest rank's device time
+    out["batched_graph"] = {"ms_per_gradient": ms_graph, "particle_steps_per_s": units_all / (ms_graph / 1e3),
                             "launches_per_gradient": info["launches_per_gradient"]}
-    out["batched_eager"] = {"ms_per_gradient": ms_eager, "particle_steps_per_s": units / (ms_eager / 1e3)}
+    out["batched_eager"] = {"ms_per_gradient": ms_eager, "particle_steps_per_s": units_all / (ms_eager / 1e3)}
     # one engine context per instance, one after another (each with its own launches and syncs)
     tot_ms, relerr_loss, relerr_grad = 0.0, 0.0, 0.0
     for i, sc in enumerate(scs):
         vol, target = inputs[i]
-        c = setup_ctx(dmpm, sc, "fp32", 0, vol, target, dt, 1)
+        c = setup_ctx(dmpm, sc, "fp32", local, vol, target, dt, 1)
         s_i = torch.cuda.ExternalStream(c.stream)
         gradient_step(c)
         torch.cuda.synchronize()
@@ -655,12 +727,18 @@ def run_config3(args):
             g = c.control_grad()
             relerr_grad = max(relerr_grad, float(np.linalg.norm(grads[i] - g) / np.linalg.norm(g)))
         c.close()
-    out["one_context_per_instance"] = {"ms_per_gradient": tot_ms, "particle_steps_per_s": units / (tot_ms / 1e3)}
+    tot_ms = max_over_ranks(tot_ms, world)
+    out["one_context_per_instance"] = {"ms_per_gradient": tot_ms, "particle_steps_per_s": units_all / (tot_ms / 1e3)}
     out["speedup_graph_over_per_instance"] = tot_ms / ms_graph
     out["speedup_graph_over_eager"] = ms_eager / ms_graph
     out["max_loss_relerr_batch_vs_per_instance"] = relerr_loss
     out["max_grad_relerr_batch_vs_per_instance"] = relerr_grad
-    print(json.dumps(out), flush=True)
+    if rank == 0:
+        print(json.dumps(out), flush=True)
+    if world > 1:
+        import torch.distributed as dist
+
+        dist.destroy_process_group()
     return 0
 
 
@@ -757,11 +835,16 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--config", type=int, default=1, help="1 = headline workload; 0, 2, 3, 4 = extra measurements")
     ap.add_argument("--iters", type=int, default=30, help="config 4: Adam iterations")
+    ap.add_argument("--fd", action="store_true", help="config 1: adjoint vs central differences, 16 directions")
+    ap.add_argument("--instances", type=int, default=48, help="config 3: number of batched instances")
+    ap.add_argument("--fd-h", default="1e-3,1e-4,1e-5,1e-6", help="--fd: central-difference steps")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
     if args.impl == "reference":
         return run_reference(args)
+    if args.fd:
+        return run_fd(args)
     if args.config == 0:
         return run_config0(args)
     if args.config == 2:

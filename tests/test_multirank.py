@@ -58,3 +58,16 @@ def test_reference_arm_skips_nonzero_ranks(monkeypatch):
         steps, warmup, ppc_root, dt, rollout_steps = 1, 3, 2, 0.0, 0
 
     assert bench.run_reference(A()) == 0
+
+
+def test_instance_sharding_covers_every_instance_once():
+    import scenes
+
+    work = [sc.n * sc.steps for sc in scenes.batch_scenes(48)]
+    for world in (1, 2, 3, 8):
+        shards = [bench.shard_instances(work, world, r) for r in range(world)]
+        flat = sorted(i for sh in shards for i in sh)
+        assert flat == list(range(len(work)))
+        loads = [sum(work[i] for i in sh) for sh in shards]
+        # longest-processing-time-first: no rank exceeds the mean by more than one instance
+        assert max(loads) - sum(work) / world <= max(work)
