@@ -570,12 +570,27 @@ def run_config0(args):
         r.backward(0)
         t_ref = time.perf_counter() - t0
         rel = lambda a, b: float(np.max(np.abs(a - b)) / np.max(np.abs(b)))
+        nrel = lambda a, b: float(np.linalg.norm(a - b) / np.linalg.norm(b))
+        rF, rx = r.get(0, "dLdF"), r.get(0, "dLdx")
+        gF, gx = c.get(0, "dLdF"), c.get(0, "dLdx")
         out.update({"ref_fp64_particle_steps_per_s": sc.n * sc.steps / t_ref,
                     "relerr_x_last": rel(c.get(L - 1, "x"), r.get(L - 1, "x")),
                     "relerr_loss": abs(g_loss - r_loss) / abs(r_loss),
-                    "relerr_dLdF_layer0": rel(c.get(0, "dLdF"), r.get(0, "dLdF")),
-                    "relerr_dLdx_layer0": rel(c.get(0, "dLdx"), r.get(0, "dLdx")),
+                    "relerr_dLdF_layer0": rel(gF, rF), "relerr_dLdx_layer0": rel(gx, rx),
+                    "normrel_dLdF_layer0": nrel(gF, rF), "normrel_dLdx_layer0": nrel(gx, rx),
                     "parity_bar": 1e-10})
+        # the reference against itself, positions perturbed by one ulp: its
+        # finite-difference d(J F^-T)/dF (delta 1e-6, Elasticity.cpp:7-72) turns
+        # rounding-level input changes into ~1e-10 changes of the adjoint
+        sc_ulp = scenes.Scene(**{**sc.__dict__, "x": sc.x * (1.0 + 2.0 ** -52)})
+        r2 = olib.RefGraph(sc_ulp, "f64", target_m=target)
+        r2.setup(L, sc.dt, sc.drag, sc.f_ext, sc.smoothing)
+        r2.forward(0)
+        r2.loss()
+        r2.backward(0)
+        out.update({"ref_vs_ref_ulp_relerr_dLdF_layer0": rel(r2.get(0, "dLdF"), rF),
+                    "ref_vs_ref_ulp_relerr_dLdx_layer0": rel(r2.get(0, "dLdx"), rx),
+                    "ref_vs_ref_ulp_normrel_dLdF_layer0": nrel(r2.get(0, "dLdF"), rF)})
     else:
         out["ref_fp64"] = "unavailable: oracle/_ref not built"
     c.close()
