@@ -501,12 +501,12 @@ struct dmpm_batch::Impl {
         DMPM_CK(cudaMemsetAsync(grid[t], 0, Gt * sizeof(node4<float>), b->stream));
         k_stress<<<(unsigned)((a.n + pb - 1) / pb), pb, 0, b->stream>>>(a);
         launched();
-        k_p2g_w<false, true><<<wb, 256, 0, b->stream>>>(a);
+        k_p2g_w<false, ITEMS_BATCH><<<wb, 256, 0, b->stream>>>(a);
         launched();
         k_gop_inplace<<<(unsigned)((Gt + 255) / 256), 256, 0, b->stream>>>(grid[t], Gt, a.dt, a.fext[0], a.fext[1],
                                                                              a.fext[2]);
         launched();
-        k_g2p_w<true><<<wb, 256, 0, b->stream>>>(a);
+        k_g2p_w<ITEMS_BATCH><<<wb, 256, 0, b->stream>>>(a);
         launched();
     }
 
@@ -551,15 +551,15 @@ struct dmpm_batch::Impl {
         const unsigned wb = warp_blocks(t);
         const bool ex = prm.adjoint_mode == DMPM_ADJ_EXACT;
         DMPM_CK(cudaMemsetAsync(gadj, 0, Gt * sizeof(node4<float>), b->stream));
-        if (ex) k_adj_scatter_w<true, false, true><<<wb, 256, 0, b->stream>>>(a);
-        else k_adj_scatter_w<false, false, true><<<wb, 256, 0, b->stream>>>(a);
+        if (ex) k_adj_scatter_w<true, false, ITEMS_BATCH><<<wb, 256, 0, b->stream>>>(a);
+        else k_adj_scatter_w<false, false, ITEMS_BATCH><<<wb, 256, 0, b->stream>>>(a);
         launched();
         const unsigned gb = (unsigned)((Gt + 255) / 256);
         if (ex) k_adj_gop_w<true><<<gb, 256, 0, b->stream>>>(grid[t], gadj, gadj2, Gt, a.dt, a.fext[0], a.fext[1], a.fext[2]);
         else k_adj_gop_w<false><<<gb, 256, 0, b->stream>>>(grid[t], gadj, gadj2, Gt, a.dt, a.fext[0], a.fext[1], a.fext[2]);
         launched();
-        if (ex) k_adj_gather_w<true, true><<<wb, 256, 0, b->stream>>>(a);
-        else k_adj_gather_w<false, true><<<wb, 256, 0, b->stream>>>(a);
+        if (ex) k_adj_gather_w<true, ITEMS_BATCH><<<wb, 256, 0, b->stream>>>(a);
+        else k_adj_gather_w<false, ITEMS_BATCH><<<wb, 256, 0, b->stream>>>(a);
         launched();
         launch_finalize(a, ex, b->stream);
         launched();

@@ -163,6 +163,7 @@ struct dmpm_ctx {
     cudaStream_t stream = nullptr;
     std::string err;
     dmpm_params prm{};
+    int64_t prm_gen = 0;  // bumped by dmpm_set_params (captured graphs hold the parameters)
     int64_t launches = 0;
     std::unique_ptr<EngineBase> eng;
 };
@@ -179,7 +180,7 @@ template <class T> class Engine : public EngineBase {
     struct Epoch {
         uint32_t* order = nullptr;
         uint32_t* items = nullptr;
-        int n_items = 0;
+        uint32_t* n_items = nullptr;  // device scalar: the warp kernels read it, the host never does
         bool valid = false;
     };
 
@@ -190,6 +191,7 @@ template <class T> class Engine : public EngineBase {
         if (dx_ <= 0 || dy_ <= 0 || dz_ <= 0 || !(h > 0)) throw ArgError{"grid dims and dx must be positive"};
         if ((double)dx_ * dy_ * dz_ > 2e9) throw ArgError{"grid has more than 2e9 nodes"};
         const bool same = grid_set_ && geo_.dim[0] == dx_ && geo_.dim[1] == dy_ && geo_.dim[2] == dz_;
+        drop_graphs();  // the grid geometry is a kernel argument of every captured launch
         geo_.dim[0] = dx_; geo_.dim[1] = dy_; geo_.dim[2] = dz_;
         geo_.dx = h;
         for (int a = 0; a < 3; a++) geo_.mn[a] = mn ? mn[a] : 0.0;
@@ -215,6 +217,7 @@ template <class T> class Engine : public EngineBase {
             DMPM_CK(cudaMemsetAsync(dfc0_, 0, 9 * np_ * sizeof(T), ctx_->stream));
             return;
         }
+        drop_graphs();
         n_ = n;
         np_ = round_up((size_t)n, 64);
         layers_.clear();
@@ -323,6 +326,17 @@ template <class T> class Engine : public EngineBase {
     int tile_cap() const { return ctx_->prm.tile_cap > 0 ? ctx_->prm.tile_cap : kDefaultTileCap; }
     unsigned pgrid() const { return (unsigned)((n_ + block() - 1) / block()); }
     unsigned pgrid256() const { return (unsigned)((n_ + 255) / 256); }
+    // persistent grid of the warp-item kernels: 3 CTAs of 256 threads per SM, fewer
+    // when the particles could not fill them (at most one item per particle)
+    unsigned warp_blocks() {
+        if (sms_ == 0) {
+            int dev = 0;
+            DMPM_CK(cudaGetDevice(&dev));
+            DMPM_CK(cudaDeviceGetAttribute(&sms_, cudaDevAttrMultiProcessorCount, dev));
+        }
+        const size_t most = ((size_t)n_ * 32 + 255) / 256;
+        return (unsigned)std::max<size_t>(1, std::min<size_t>(most, (size_t)sms_ * 3));
+    }
     unsigned ggrid() const { return (unsigned)((G_ + 255) / 256); }
 
     void launched() {
@@ -495,6 +509,7 @@ template <class T> class Engine : public EngineBase {
             reset_layers();
             return;
         }
+        drop_graphs();
         L_ = num_layers;
         layer_arena_.release();
         layers_.assign(L_, LayerSlots{});
@@ -639,6 +654,7 @@ template <class T> class Engine : public EngineBase {
         for (Epoch& e : epochs_) {
             e.order = (uint32_t*)layer_arena_.alloc((size_t)n_ * sizeof(uint32_t));
             e.items = (uint32_t*)layer_arena_.alloc(((size_t)n_ + 1) * sizeof(uint32_t));
+            e.n_items = (uint32_t*)layer_arena_.alloc(16);
         }
         const size_t n = (size_t)n_;
         sk_[0] = (uint32_t*)layer_arena_.alloc(n * 4);
@@ -651,7 +667,6 @@ template <class T> class Engine : public EngineBase {
         counts_ = (uint32_t*)layer_arena_.alloc(256 * rs_tiles * 4);
         const size_t mx = std::max(n, 256 * rs_tiles);
         tile_tot_ = (uint32_t*)layer_arena_.alloc(((mx + SCAN_TILE - 1) / SCAN_TILE + 1) * 4);
-        nitems_dev_ = (uint32_t*)layer_arena_.alloc(16);
     }
 
     template <class Op> void device_scan(uint32_t* data, size_t n, uint32_t* grand) {
@@ -698,15 +713,11 @@ template <class T> class Engine : public EngineBase {
         device_scan<OpMax>(sh_, (size_t)n, nullptr);
         k_item_flags<<<(n + 255) / 256, 256, 0, ctx_->stream>>>(sk_[cur], sh_, n, sf_);
         launched();
-        device_scan<OpSum>(sf_, (size_t)n, nitems_dev_);
+        device_scan<OpSum>(sf_, (size_t)n, e.n_items);
         k_item_starts<<<(n + 255) / 256, 256, 0, ctx_->stream>>>(sk_[cur], sh_, sf_, n, e.items);
         launched();
-        k_item_sentinel<<<1, 1, 0, ctx_->stream>>>(e.items, nitems_dev_, n);
+        k_item_sentinel<<<1, 1, 0, ctx_->stream>>>(e.items, e.n_items, n);
         launched();
-        DMPM_CK(cudaMemcpyAsync((char*)host_misc_ + 24, nitems_dev_, 4, cudaMemcpyDeviceToHost, ctx_->stream));
-        DMPM_CK(cudaStreamSynchronize(ctx_->stream));
-        harvest();
-        e.n_items = (int)*(uint32_t*)((char*)host_misc_ + 24);
         e.valid = true;
     }
 
@@ -724,12 +735,16 @@ template <class T> class Engine : public EngineBase {
         Arena tmp;
         e.order = (uint32_t*)tmp.alloc((size_t)n_ * 4);
         e.items = (uint32_t*)tmp.alloc(((size_t)n_ + 1) * 4);
+        e.n_items = (uint32_t*)tmp.alloc(16);
         cell_sort(materialize_state(l), e);
+        uint32_t ni = 0;
+        DMPM_CK(cudaMemcpyAsync(&ni, e.n_items, 4, cudaMemcpyDeviceToHost, ctx_->stream));
+        DMPM_CK(cudaStreamSynchronize(ctx_->stream));
         if (keys) DMPM_CK(cudaMemcpyAsync(keys, sk_[sorted_], (size_t)n_ * 4, cudaMemcpyDeviceToHost, ctx_->stream));
         if (order) DMPM_CK(cudaMemcpyAsync(order, e.order, (size_t)n_ * 4, cudaMemcpyDeviceToHost, ctx_->stream));
-        if (items) DMPM_CK(cudaMemcpyAsync(items, e.items, ((size_t)e.n_items + 1) * 4, cudaMemcpyDeviceToHost, ctx_->stream));
+        if (items) DMPM_CK(cudaMemcpyAsync(items, e.items, ((size_t)ni + 1) * 4, cudaMemcpyDeviceToHost, ctx_->stream));
         DMPM_CK(cudaStreamSynchronize(ctx_->stream));
-        if (n_items) *n_items = e.n_items;
+        if (n_items) *n_items = (int)ni;
     }
 
     WArgs warp_args() const {
@@ -769,7 +784,8 @@ template <class T> class Engine : public EngineBase {
         if constexpr (kWarp) {
             Epoch& ep = epoch_for(l, st, allow_sort);
             WArgs a = warp_args();
-            a.items = WarpItems{ep.order, ep.items, ep.n_items};
+            a.items = WarpItems{ep.order, ep.items, 0};
+            a.n_items_dev = ep.n_items;
             a.st = (const float*)st;
             a.st_next = (float*)out;
             a.dfc = (const float*)layers_[l].dfc;
@@ -777,28 +793,24 @@ template <class T> class Engine : public EngineBase {
             a.grid = (node4<float>*)g;
             a.P = ctx_->prm.keep_intermediates ? (float*)layers_[l].dbgP : nullptr;
             DMPM_CK(cudaMemsetAsync(g, 0, G_ * sizeof(node4<T>), ctx_->stream));
-            const unsigned wg = (unsigned)((ep.n_items + 7) / 8);
+            const unsigned wg = warp_blocks();
             pbeg(K_P_OP1);
             k_stress<<<pgrid256(), 256, 0, ctx_->stream>>>(a);
             launched();
             pend();
-            if (wg) {
-                pbeg(K_P2G);
-                if (ctx_->prm.warp_general) k_p2g_w<true, false><<<wg, 256, 0, ctx_->stream>>>(a);
-                else k_p2g_w<false, false><<<wg, 256, 0, ctx_->stream>>>(a);
-                launched();
-                pend();
-            }
+            pbeg(K_P2G);
+            if (ctx_->prm.warp_general) k_p2g_w<true, ITEMS_PERSISTENT><<<wg, 256, 0, ctx_->stream>>>(a);
+            else k_p2g_w<false, ITEMS_PERSISTENT><<<wg, 256, 0, ctx_->stream>>>(a);
+            launched();
+            pend();
             pbeg(K_GOP);
             k_gop_inplace<<<ggrid(), 256, 0, ctx_->stream>>>((node4<float>*)g, G_, a.dt, a.fext[0], a.fext[1], a.fext[2]);
             launched();
             pend();
-            if (wg) {
-                pbeg(K_G2P);
-                k_g2p_w<false><<<wg, 256, 0, ctx_->stream>>>(a);
-                launched();
-                pend();
-            }
+            pbeg(K_G2P);
+            k_g2p_w<ITEMS_PERSISTENT><<<wg, 256, 0, ctx_->stream>>>(a);
+            launched();
+            pend();
             return;
         }
         FwdArgs<T> a = fwd_args();
@@ -837,13 +849,68 @@ template <class T> class Engine : public EngineBase {
         DMPM_CK(cudaMemsetAsync(status_, 0, sizeof(unsigned), ctx_->stream));
     }
 
+    // ---------------------------------------------------------- CUDA graphs
+    // The FP32 store-all forward and backward passes enqueue a fixed sequence
+    // of ~1,100 launches with no host read-back; each is captured once per
+    // (start / top, control) and replayed.  Graphs are dropped whenever a
+    // captured pointer or parameter can change: new particle or layer storage,
+    // a new grid, dmpm_set_params.
+    bool graphs_ok() const { return kWarp && k_ == 1 && !prof_ && !ctx_->prm.eager; }
+    void drop_graphs() {
+        for (auto& kv : graphs_)
+            if (kv.second.exec) cudaGraphExecDestroy(kv.second.exec);
+        graphs_.clear();
+    }
+    template <class Fn> void run_graph(std::pair<int64_t, int64_t> key, Fn enqueue) {
+        if (graph_gen_ != ctx_->prm_gen) {
+            drop_graphs();
+            graph_gen_ = ctx_->prm_gen;
+        }
+        auto it = graphs_.find(key);
+        if (it != graphs_.end()) {
+            DMPM_CK(cudaGraphLaunch(it->second.exec, ctx_->stream));
+            ctx_->launches += it->second.launches;
+            return;
+        }
+        const int64_t l0 = ctx_->launches;
+        DMPM_CK(cudaStreamBeginCapture(ctx_->stream, cudaStreamCaptureModeThreadLocal));
+        try {
+            enqueue();
+        } catch (...) {
+            cudaGraph_t g = nullptr;
+            cudaStreamEndCapture(ctx_->stream, &g);
+            if (g) cudaGraphDestroy(g);
+            cudaGetLastError();
+            throw;
+        }
+        cudaGraph_t g = nullptr;
+        DMPM_CK(cudaStreamEndCapture(ctx_->stream, &g));
+        Graph gr;
+        gr.launches = ctx_->launches - l0;  // counted once here for the replay below
+        const cudaError_t e = cudaGraphInstantiate(&gr.exec, g, 0);
+        cudaGraphDestroy(g);
+        if (e != cudaSuccess) throw CudaError{e, std::string("cudaGraphInstantiate: ") + cudaGetErrorString(e)};
+        graphs_.emplace(key, gr);
+        DMPM_CK(cudaGraphLaunch(gr.exec, ctx_->stream));
+    }
+
     void forward(int start) {
         if (L_ <= 0) throw StateError{"dmpm_setup has not been called"};
         if (start < 0 || start >= L_) throw ArgError{"start_layer out of range"};
         reset_status();
         if (k_ == 1) {
-            for (int l = start; l + 1 < L_; l++)
-                step(l, layers_[l].st, layers_[l + 1].st, layers_[l].grid, layers_[l].G, true);
+            auto body = [&]() {
+                for (int l = start; l + 1 < L_; l++)
+                    step(l, layers_[l].st, layers_[l + 1].st, layers_[l].grid, layers_[l].G, true);
+            };
+            if (graphs_ok()) {
+                run_graph({0, start}, body);
+                if constexpr (kWarp)  // the replayed sorts refreshed every epoch the pass touches
+                    for (int l = start; l + 1 < L_; l++)
+                        epochs_[std::min((int)epochs_.size() - 1, l / sort_every())].valid = true;
+            } else {
+                body();
+            }
         } else {
             const T* cur = materialize_state(start);
             int r = 0;
@@ -930,7 +997,8 @@ template <class T> class Engine : public EngineBase {
         if constexpr (kWarp) {
             Epoch& ep = epoch_for(i, state_of(i), false);
             WArgs a = warp_args();
-            a.items = WarpItems{ep.order, ep.items, ep.n_items};
+            a.items = WarpItems{ep.order, ep.items, 0};
+            a.n_items_dev = ep.n_items;
             a.st = (const float*)state_of(i);
             a.st_next = (float*)state_of(i + 1);
             a.dfc = (const float*)layers_[i].dfc;
@@ -950,19 +1018,17 @@ template <class T> class Engine : public EngineBase {
             if (!a.st || !a.st_next || !a.grid || !a.G) throw StateError{"internal: layer not materialised"};
             DMPM_CK(cudaMemsetAsync(gadj_, 0, G_ * sizeof(node4<T>), ctx_->stream));
             const bool ex = P.adjoint_mode == DMPM_ADJ_EXACT;
-            const unsigned wg = (unsigned)((ep.n_items + 7) / 8);
-            if (wg) {
-                pbeg(K_ADJ_SCATTER);
-                if (P.warp_general) {
-                    if (ex) k_adj_scatter_w<true, true, false><<<wg, 256, 0, ctx_->stream>>>(a);
-                    else k_adj_scatter_w<false, true, false><<<wg, 256, 0, ctx_->stream>>>(a);
-                } else {
-                    if (ex) k_adj_scatter_w<true, false, false><<<wg, 256, 0, ctx_->stream>>>(a);
-                    else k_adj_scatter_w<false, false, false><<<wg, 256, 0, ctx_->stream>>>(a);
-                }
-                launched();
-                pend();
+            const unsigned wg = warp_blocks();
+            pbeg(K_ADJ_SCATTER);
+            if (P.warp_general) {
+                if (ex) k_adj_scatter_w<true, true, ITEMS_PERSISTENT><<<wg, 256, 0, ctx_->stream>>>(a);
+                else k_adj_scatter_w<false, true, ITEMS_PERSISTENT><<<wg, 256, 0, ctx_->stream>>>(a);
+            } else {
+                if (ex) k_adj_scatter_w<true, false, ITEMS_PERSISTENT><<<wg, 256, 0, ctx_->stream>>>(a);
+                else k_adj_scatter_w<false, false, ITEMS_PERSISTENT><<<wg, 256, 0, ctx_->stream>>>(a);
             }
+            launched();
+            pend();
             pbeg(K_ADJ_GOP);
             if (ex) k_adj_gop_w<true><<<ggrid(), 256, 0, ctx_->stream>>>(a.grid, a.gadj, a.gadj2, G_, a.dt, a.fext[0], a.fext[1], a.fext[2]);
             else k_adj_gop_w<false><<<ggrid(), 256, 0, ctx_->stream>>>(a.grid, a.gadj, a.gadj2, G_, a.dt, a.fext[0], a.fext[1], a.fext[2]);
@@ -973,13 +1039,11 @@ template <class T> class Engine : public EngineBase {
                 DMPM_CK(cudaMemcpy2DAsync(layers_[i].dbggdp, sizeof(node4<T>), gadj2_, 2 * sizeof(node4<T>),
                                           sizeof(node4<T>), G_, cudaMemcpyDeviceToDevice, ctx_->stream));
             }
-            if (wg) {
-                pbeg(K_ADJ_GATHER);
-                if (ex) k_adj_gather_w<true, false><<<wg, 256, 0, ctx_->stream>>>(a);
-                else k_adj_gather_w<false, false><<<wg, 256, 0, ctx_->stream>>>(a);
-                launched();
-                pend();
-            }
+            pbeg(K_ADJ_GATHER);
+            if (ex) k_adj_gather_w<true, ITEMS_PERSISTENT><<<wg, 256, 0, ctx_->stream>>>(a);
+            else k_adj_gather_w<false, ITEMS_PERSISTENT><<<wg, 256, 0, ctx_->stream>>>(a);
+            launched();
+            pend();
             pbeg(K_ADJ_FINALIZE);
             launch_finalize(a, ex, ctx_->stream);
             launched();
@@ -1057,7 +1121,15 @@ template <class T> class Engine : public EngineBase {
         reset_status();
         if (ctrl_acc_) DMPM_CK(cudaMemsetAsync(ctrl_acc_, 0, 9 * np_ * sizeof(double), ctx_->stream));
         if (k_ == 1) {
-            for (int i = top - 1; i >= control; i--) adjoint_step(i);
+            auto body = [&]() {
+                for (int i = top - 1; i >= control; i--) adjoint_step(i);
+            };
+            bool sorted = true;  // a captured backward pass must not contain sorts
+            if constexpr (kWarp)
+                for (int i = top - 1; i >= control; i--)
+                    sorted &= epochs_[std::min((int)epochs_.size() - 1, i / sort_every())].valid;
+            if (graphs_ok() && sorted) run_graph({1 + (int64_t)top, control}, body);
+            else body();
         } else {
             int i = top - 1;
             while (i >= control) {
@@ -1305,6 +1377,7 @@ template <class T> class Engine : public EngineBase {
 
     ~Engine() override {
         cudaStreamSynchronize(ctx_->stream);
+        drop_graphs();
         harvest();
         for (cudaEvent_t e : event_pool_) cudaEventDestroy(e);
         if (host_misc_) cudaFreeHost(host_misc_);
@@ -1367,7 +1440,6 @@ template <class T> class Engine : public EngineBase {
     uint32_t* sf_ = nullptr;
     uint32_t* counts_ = nullptr;
     uint32_t* tile_tot_ = nullptr;
-    uint32_t* nitems_dev_ = nullptr;
     int sorted_ = 0;
     std::map<int, T*> adam_;  // Adam moment buffers per control set (layer, or -1 for tied controls)
     double* ctrl_acc_ = nullptr;
@@ -1380,6 +1452,15 @@ template <class T> class Engine : public EngineBase {
         cudaEvent_t e0, e1;
     };
     bool prof_ = false;
+    int sms_ = 0;
+    // CUDA graphs of the FP32 store-all forward pass (per start layer) and
+    // backward pass (per top and control layer), with the kernel launches each holds
+    struct Graph {
+        cudaGraphExec_t exec = nullptr;
+        int64_t launches = 0;
+    };
+    std::map<std::pair<int64_t, int64_t>, Graph> graphs_;
+    int64_t graph_gen_ = -1;
     std::vector<Pending> pend_;
     std::vector<cudaEvent_t> event_pool_;
     double prof_ms_[K_COUNT] = {};
@@ -1493,11 +1574,12 @@ int dmpm_set_params(dmpm_ctx* ctx, const dmpm_params* p) {
     if (!(p->dt >= 0) || p->adjoint_mode < 0 || p->adjoint_mode > 1 || p->control_mode < 0 || p->control_mode > 1 ||
         p->loss_kind < 0 || p->loss_kind > 1 || p->checkpoint_every < 0 || p->block_size < 0 || p->block_size > 256 ||
         (p->block_size % 32) != 0 || p->tile_cap < 0 || p->tile_cap > 1536 || p->sort_every < 0 ||
-        p->warp_general < 0 || p->warp_general > 1 || p->control_stride < 0) {
+        p->warp_general < 0 || p->warp_general > 1 || p->control_stride < 0 || p->eager < 0 || p->eager > 1) {
         ctx->err = "invalid dmpm_params";
         return DMPM_ERR_ARG;
     }
     ctx->prm = *p;
+    ctx->prm_gen++;
     return DMPM_OK;
 }
 

@@ -257,19 +257,21 @@ struct WArgs {
     float* dbg_Cnext;
 };
 
-// Warp items are visited by a loop over the launch's warps: a batch launch
-// has a persistent grid sized to the SMs, a one-scene launch one warp per item.
+// How a warp-item launch walks its items:
+//   ITEMS_PER_WARP   one warp per item, the grid sized on the host from the item count
+//   ITEMS_PERSISTENT a persistent grid sized to the SMs loops over the items, whose
+//                    count stays on the device (no host read-back, so capturable)
+//   ITEMS_BATCH      persistent, items of several instances, each item's grid looked up
+enum : int { ITEMS_PER_WARP = 0, ITEMS_PERSISTENT = 1, ITEMS_BATCH = 2 };
 __device__ __forceinline__ int item_count(const WArgs& a) {
     return a.n_items_dev ? (int)*a.n_items_dev : a.items.n_items;
 }
 __device__ __forceinline__ int first_warp() { return (int)((blockIdx.x * blockDim.x + threadIdx.x) >> 5); }
-// batch launches are persistent (grid-stride over the items); one-scene
-// launches give every item its own warp, so their loop body runs once
-template <bool BATCH> __device__ __forceinline__ int next_item(int item, int nit) {
-    return BATCH ? item + (int)((gridDim.x * blockDim.x) >> 5) : nit;
+template <int MODE> __device__ __forceinline__ int next_item(int item, int nit) {
+    return MODE != ITEMS_PER_WARP ? item + (int)((gridDim.x * blockDim.x) >> 5) : nit;
 }
-template <bool BATCH> __device__ __forceinline__ void item_grid(const WArgs& a, int item, GridGeom& g, int& goff) {
-    if constexpr (BATCH) {
+template <int MODE> __device__ __forceinline__ void item_grid(const WArgs& a, int item, GridGeom& g, int& goff) {
+    if constexpr (MODE == ITEMS_BATCH) {
         const InstGeo& ig = a.ig[a.item_inst[item]];
         g = ig.g;
         goff = ig.goff;
@@ -339,13 +341,13 @@ static __global__ void __launch_bounds__(256, DMPM_STRESS_MIN_BLOCKS) k_stress(W
 }
 
 // P2G: m_g += w m_p;  p_g += w (m_p v (1 - dt drag) + G (x_g - x_p))
-template <bool GENERAL, bool BATCH> __global__ void __launch_bounds__(256, 3) k_p2g_w(WArgs a) {
+template <bool GENERAL, int MODE> __global__ void __launch_bounds__(256, 3) k_p2g_w(WArgs a) {
     const int nit = item_count(a);
     const size_t np = a.np, npl = a.npl;
-    for (int item = first_warp(); item < nit; item = next_item<BATCH>(item, nit)) {
+    for (int item = first_warp(); item < nit; item = next_item<MODE>(item, nit)) {
         GridGeom geo;
         int goff;
-        item_grid<BATCH>(a, item, geo, goff);
+        item_grid<MODE>(a, item, geo, goff);
         const ItemLane L = item_lane(a.items, item);
         float x[3];
         int base[3];
@@ -418,13 +420,13 @@ static __global__ void k_gop_inplace(node4<float>* grid, size_t G, float dt, flo
 
 // G2P + P_op_2: v' = sum w v_g;  C' = 3/dx^2 sum w v_g d^T;
 // F' = (1 - s)(I + dt C')(F + dFc) + s F;  x' = x + dt v'
-template <bool BATCH> __global__ void __launch_bounds__(256, 4) k_g2p_w(WArgs a) {
+template <int MODE> __global__ void __launch_bounds__(256, 4) k_g2p_w(WArgs a) {
     const int nit = item_count(a);
     const size_t np = a.np, npl = a.npl, npn = a.npn;
-    for (int item = first_warp(); item < nit; item = next_item<BATCH>(item, nit)) {
+    for (int item = first_warp(); item < nit; item = next_item<MODE>(item, nit)) {
         GridGeom geo;
         int goff;
-        item_grid<BATCH>(a, item, geo, goff);
+        item_grid<MODE>(a, item, geo, goff);
         const ItemLane L = item_lane(a.items, item);
         float x[3];
         int base[3];
@@ -523,13 +525,13 @@ template <bool BATCH> __global__ void __launch_bounds__(256, 4) k_g2p_w(WArgs a)
 // ------------------------------------------------------------------ adjoint
 // dLdv_next = dt dLdx' + dLdv';  dLdC_next = c dt dLdF' Fe^T + dLdC'
 // dLdv_g += w dLdv_next + 3/dx^2 w dLdC_next (x_g - x_p)   (BackPropagation.cpp:14-44)
-template <bool EXACT, bool GENERAL, bool BATCH> __global__ void __launch_bounds__(256, 3) k_adj_scatter_w(WArgs a) {
+template <bool EXACT, bool GENERAL, int MODE> __global__ void __launch_bounds__(256, 3) k_adj_scatter_w(WArgs a) {
     const int nit = item_count(a);
     const size_t np = a.np, npl = a.npl, npn = a.npn;
-    for (int item = first_warp(); item < nit; item = next_item<BATCH>(item, nit)) {
+    for (int item = first_warp(); item < nit; item = next_item<MODE>(item, nit)) {
         GridGeom geo;
         int goff;
-        item_grid<BATCH>(a, item, geo, goff);
+        item_grid<MODE>(a, item, geo, goff);
         const ItemLane L = item_lane(a.items, item);
         const int p = L.p;
         float x[3];
@@ -631,13 +633,13 @@ __global__ void k_adj_gop_w(const node4<float>* __restrict__ grid, const node4<f
 //   M += w d dLdp^T,  X += sigma (N'NN, NN'N, NNN'),  u += w dLdp,  z += w v_g
 //   sigma = m dLdm + dLdp.(m v c_d + G d) + v_g.(dLdv_next + 3/dx^2 dLdC_next d)
 // (the algebra of kernels.cuh:k_adj_gather); written to gath for k_adj_finalize.
-template <bool EXACT, bool BATCH> __global__ void __launch_bounds__(256, DMPM_GATHER_MIN_BLOCKS) k_adj_gather_w(WArgs a) {
+template <bool EXACT, int MODE> __global__ void __launch_bounds__(256, DMPM_GATHER_MIN_BLOCKS) k_adj_gather_w(WArgs a) {
     const int nit = item_count(a);
     const size_t np = a.np, npl = a.npl;
-    for (int item = first_warp(); item < nit; item = next_item<BATCH>(item, nit)) {
+    for (int item = first_warp(); item < nit; item = next_item<MODE>(item, nit)) {
         GridGeom geo;
         int goff;
-        item_grid<BATCH>(a, item, geo, goff);
+        item_grid<MODE>(a, item, geo, goff);
         const ItemLane L = item_lane(a.items, item);
         const int p = L.p;
         float x[3];

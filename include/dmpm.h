@@ -67,7 +67,7 @@ typedef struct dmpm_ctx dmpm_ctx;
 
 /* precision paths */
 #define DMPM_FP64 0       /* plain FP64 path: one kernel per reference stage, global atomics */
-#define DMPM_FP32_MIXED 1 /* FP32 state and grid, shared-memory tiles; FP64 polar/SVD, stress
+#define DMPM_FP32_MIXED 1 /* FP32 state and grid, cell-sorted warp items; FP64 polar/SVD, stress
                              derivative, loss and control-gradient sums */
 
 /* adjoint modes */
@@ -132,6 +132,9 @@ typedef struct {
                                 of CompGraph::OptimizeDefGradControlSequence, CompGraph.cpp:352);
                                 the other layers read the uploaded dFc, as the reference's copies made
                                 by SetUpCompGraph stay unchanged there.  0 or 1 = every layer. */
+    int eager;               /* FP32 path with every layer kept: 0 = capture dmpm_forward / dmpm_backward
+                                once per start (top, control) layer and replay them as CUDA graphs;
+                                1 = launch kernel by kernel (per-kernel profiling also does) */
 } dmpm_params;
 
 void dmpm_default_params(dmpm_params* p);

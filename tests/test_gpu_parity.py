@@ -406,3 +406,30 @@ def test_control_stride_keeps_controls_on_frames_only(gpu_ready, exact_case):
         with pytest.raises(dmpm.DmpmError):
             c3.adam_step(t=1, layer=4)
         c3.adam_step(t=1, layer=3)
+
+
+def test_graph_replay_matches_eager_launches(gpu_ready, exact_case):
+    """The FP32 store-all passes are captured once and replayed as CUDA graphs;
+    replays give the eager launches' results, and dmpm_set_params (here a new
+    dt) drops the captured graphs so the next pass runs with the new values."""
+    sc, o, loss, L = exact_case
+    out = {}
+    for eager in (True, False):
+        with make_ctx(sc, "fp32", o.target, adjoint="exact", control="tied", eager=eager) as c:
+            c.setup(L)
+            res = []
+            for dt in (sc.dt, sc.dt, 0.5 * sc.dt):
+                c.set_params(dt=dt, drag=sc.drag, f_ext=sc.f_ext, smoothing=sc.smoothing, adjoint="exact",
+                             control="tied", eager=eager)
+                for _ in range(2):  # capture, then replay
+                    c.forward(0)
+                    lo = c.loss()
+                    c.backward(0)
+                    res.append((lo, c.control_grad(), c.get(L - 1, "x")))
+            out[eager] = res
+    for (l_e, g_e, x_e), (l_g, g_g, x_g) in zip(out[True], out[False]):
+        assert abs(l_g - l_e) <= 1e-6 * abs(l_e)
+        assert relerr(g_g, g_e) < 1e-4
+        assert relerr(x_g, x_e) < 1e-6
+    # the halved dt changed the result (the graph of the old dt was not replayed)
+    assert relerr(out[False][4][2], out[False][0][2]) > 1e-6
