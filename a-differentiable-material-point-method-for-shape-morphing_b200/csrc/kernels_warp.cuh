@@ -187,6 +187,44 @@ __device__ __forceinline__ void lane_weights(const float x[3], const GridGeom& g
     }
 }
 
+// As lane_weights, but axis 1 is left to the caller: it gets this lane's own
+// axis-1 offset, weight and slope in own1 and fetches row j's values with
+// row_weights (three shuffles) when it reaches that row, so only one row's
+// values are live at a time.  Fills d0, n0, s0 and the axis-2 arrays of w.
+__device__ __forceinline__ void lane_weights_k(const float x[3], const GridGeom& g, const int base[3], int s,
+                                               LaneW& w, float own1[3], bool slopes) {
+    const float dx = (float)g.dx, idx = 1.f / dx;
+    float d[3], n[3], sl[3];
+#pragma unroll
+    for (int c = 0; c < 3; c++) {
+        const float xg = (float)g.mn[c] + (float)(base[c] + s) * dx;
+        d[c] = xg - x[c];
+        const float q = d[c] * idx;
+        n[c] = bsp(q);
+        sl[c] = slopes ? bsp_slope(q) : 0.f;
+    }
+    w.d0 = d[0];
+    w.n0 = n[0];
+    w.s0 = sl[0];
+    own1[0] = d[1];
+    own1[1] = n[1];
+    own1[2] = sl[1];
+    const int grp = (threadIdx.x & 31) & ~3;
+#pragma unroll
+    for (int t = 0; t < 4; t++) {
+        w.d2[t] = __shfl_sync(0xffffffffu, d[2], grp + t);
+        w.n2[t] = __shfl_sync(0xffffffffu, n[2], grp + t);
+        w.s2[t] = slopes ? __shfl_sync(0xffffffffu, sl[2], grp + t) : 0.f;
+    }
+}
+// row j's axis-1 (offset, weight, slope) from the lane of slab j; every lane must call it
+__device__ __forceinline__ void row_weights(const float own1[3], int j, float& d1, float& n1, float& s1) {
+    const int src = ((threadIdx.x & 31) & ~3) + j;
+    d1 = __shfl_sync(0xffffffffu, own1[0], src);
+    n1 = __shfl_sync(0xffffffffu, own1[1], src);
+    s1 = __shfl_sync(0xffffffffu, own1[2], src);
+}
+
 __device__ __forceinline__ void load_x_base(const float* st, size_t np, int p, const GridGeom& g, float x[3],
                                             int base[3]) {
 #pragma unroll
@@ -208,9 +246,13 @@ __device__ __forceinline__ void load_x_base(const float* st, size_t np, int p, c
 #ifndef DMPM_FINALIZE_MIN_BLOCKS
 #define DMPM_FINALIZE_MIN_BLOCKS 4
 #endif
-// and for the adjoint gather (256 threads per block)
+// and for the adjoint gather and the two scatters, P2G and the adjoint G2P
+// (256 threads per block)
 #ifndef DMPM_GATHER_MIN_BLOCKS
 #define DMPM_GATHER_MIN_BLOCKS 3
+#endif
+#ifndef DMPM_SCATTER_MIN_BLOCKS
+#define DMPM_SCATTER_MIN_BLOCKS 3
 #endif
 
 // Grid of one instance of a batch: its geometry, the offset of its first node
@@ -341,7 +383,7 @@ static __global__ void __launch_bounds__(256, DMPM_STRESS_MIN_BLOCKS) k_stress(W
 }
 
 // P2G: m_g += w m_p;  p_g += w (m_p v (1 - dt drag) + G (x_g - x_p))
-template <bool GENERAL, int MODE> __global__ void __launch_bounds__(256, 3) k_p2g_w(WArgs a) {
+template <bool GENERAL, int MODE> __global__ void __launch_bounds__(256, DMPM_SCATTER_MIN_BLOCKS) k_p2g_w(WArgs a) {
     const int nit = item_count(a);
     const size_t np = a.np, npl = a.npl;
     for (int item = first_warp(); item < nit; item = next_item<MODE>(item, nit)) {
@@ -354,7 +396,8 @@ template <bool GENERAL, int MODE> __global__ void __launch_bounds__(256, 3) k_p2
         load_x_base(a.st, npl, L.p, geo, x, base);
         const bool uniform = !GENERAL && warp_uniform_base(base);
         LaneW w;
-        lane_weights(x, geo, base, L.s, w, false);
+        float own1[3];
+        lane_weights_k(x, geo, base, L.s, w, own1, false);
         const float mp = L.valid ? a.cst[(size_t)KM * np + L.p] : 0.f;
         const float damp = 1.f - a.dt * a.drag;
         float mvd[3], g0[3];
@@ -372,10 +415,12 @@ template <bool GENERAL, int MODE> __global__ void __launch_bounds__(256, 3) k_p2
 #pragma unroll
             for (int jj = 0; jj < 2; jj++) {
                 const int j = 2 * half + jj;
+                float d1, n1, s1;
+                row_weights(own1, j, d1, n1, s1);
                 float g1[3];
 #pragma unroll
-                for (int c = 0; c < 3; c++) g1[c] = g0[c] + G.a[c][1] * w.d1[j];
-                const float w01 = L.valid ? w.n0 * w.n1[j] : 0.f;
+                for (int c = 0; c < 3; c++) g1[c] = g0[c] + G.a[c][1] * d1;
+                const float w01 = L.valid ? w.n0 * n1 : 0.f;
 #pragma unroll
                 for (int k = 0; k < 4; k++) {
                     const float wt = w01 * w.n2[k];
@@ -432,7 +477,8 @@ template <int MODE> __global__ void __launch_bounds__(256, 4) k_g2p_w(WArgs a) {
         int base[3];
         load_x_base(a.st, npl, L.p, geo, x, base);
         LaneW w;
-        lane_weights(x, geo, base, L.s, w, false);
+        float own1[3];
+        lane_weights_k(x, geo, base, L.s, w, own1, false);
         // v = sum w v_g and C = sum w v_g d^T (scaled by 3/dx^2 at the end), with the
         // weight w = n0 n1[j] n2[k] and d = (d0, d1[j], d2[k]) factored per stencil row:
         // the node loop accumulates only the k-dependent sums, the row applies n0 n1[j]
@@ -462,7 +508,9 @@ template <int MODE> __global__ void __launch_bounds__(256, 4) k_g2p_w(WArgs a) {
                     Wj[r] += nd2[k] * vg[r];
                 }
             }
-            const float w01 = w.n0 * w.n1[j], w01d = w01 * w.d1[j];
+            float d1, n1, s1;
+            row_weights(own1, j, d1, n1, s1);
+            const float w01 = w.n0 * n1, w01d = w01 * d1;
 #pragma unroll
             for (int r = 0; r < 3; r++) {
                 V[r] += w01 * Vj[r];
@@ -525,7 +573,7 @@ template <int MODE> __global__ void __launch_bounds__(256, 4) k_g2p_w(WArgs a) {
 // ------------------------------------------------------------------ adjoint
 // dLdv_next = dt dLdx' + dLdv';  dLdC_next = c dt dLdF' Fe^T + dLdC'
 // dLdv_g += w dLdv_next + 3/dx^2 w dLdC_next (x_g - x_p)   (BackPropagation.cpp:14-44)
-template <bool EXACT, bool GENERAL, int MODE> __global__ void __launch_bounds__(256, 3) k_adj_scatter_w(WArgs a) {
+template <bool EXACT, bool GENERAL, int MODE> __global__ void __launch_bounds__(256, DMPM_SCATTER_MIN_BLOCKS) k_adj_scatter_w(WArgs a) {
     const int nit = item_count(a);
     const size_t np = a.np, npl = a.npl, npn = a.npn;
     for (int item = first_warp(); item < nit; item = next_item<MODE>(item, nit)) {
@@ -539,7 +587,8 @@ template <bool EXACT, bool GENERAL, int MODE> __global__ void __launch_bounds__(
         load_x_base(a.st, npl, p, geo, x, base);
         const bool uniform = !GENERAL && warp_uniform_base(base);
         LaneW w;
-        lane_weights(x, geo, base, L.s, w, false);
+        float own1[3];
+        lane_weights_k(x, geo, base, L.s, w, own1, false);
         float vn[3];
 #pragma unroll
         for (int c = 0; c < 3; c++)
@@ -574,10 +623,12 @@ template <bool EXACT, bool GENERAL, int MODE> __global__ void __launch_bounds__(
 #pragma unroll
             for (int jj = 0; jj < 2; jj++) {
                 const int j = 2 * half + jj;
+                float d1, n1, s1;
+                row_weights(own1, j, d1, n1, s1);
                 float c1[3];
 #pragma unroll
-                for (int r = 0; r < 3; r++) c1[r] = c0[r] + k3 * Cn.a[r][1] * w.d1[j];
-                const float w01 = L.valid ? w.n0 * w.n1[j] : 0.f;
+                for (int r = 0; r < 3; r++) c1[r] = c0[r] + k3 * Cn.a[r][1] * d1;
+                const float w01 = L.valid ? w.n0 * n1 : 0.f;
 #pragma unroll
                 for (int k = 0; k < 4; k++) {
                     const float wt = w01 * w.n2[k];
@@ -646,7 +697,8 @@ template <bool EXACT, int MODE> __global__ void __launch_bounds__(256, DMPM_GATH
         int base[3];
         load_x_base(a.st, npl, p, geo, x, base);
         LaneW w;
-        lane_weights(x, geo, base, L.s, w, true);
+        float own1[3];
+        lane_weights_k(x, geo, base, L.s, w, own1, true);
         const float mp = a.cst[(size_t)KM * np + p];
         const float cd = EXACT ? (1.f - a.dt * a.drag) : 1.f;
         const float dx = (float)geo.dx;
@@ -669,18 +721,19 @@ template <bool EXACT, int MODE> __global__ void __launch_bounds__(256, DMPM_GATH
         float acc[18];  // M (9, row-major: M[r][c] = sum w d_r dLdp_c), X (3), u (3), z (3)
 #pragma unroll
         for (int i = 0; i < 18; i++) acc[i] = 0.f;
-        auto node = [&](const node4<float>& o, const node4<float>& vg, int j, int k) {
+        // one node (j, k) of the lane's slab, with row j's axis-1 values d1, n1, s1
+        auto node = [&](const node4<float>& o, const node4<float>& vg, float d1, float n1, float s1, int k) {
             float h[3], e[3];
 #pragma unroll
             for (int r = 0; r < 3; r++) {
-                h[r] = h0[r] + G.a[r][1] * w.d1[j] + G.a[r][2] * w.d2[k];
-                e[r] = e0[r] + k3 * Cn.a[r][1] * w.d1[j] + k3 * Cn.a[r][2] * w.d2[k];
+                h[r] = h0[r] + G.a[r][1] * d1 + G.a[r][2] * w.d2[k];
+                e[r] = e0[r] + k3 * Cn.a[r][1] * d1 + k3 * Cn.a[r][2] * w.d2[k];
             }
-            const float n01 = w.n0 * w.n1[j];
+            const float n01 = w.n0 * n1;
             const float wt = n01 * w.n2[k];
             const float sig = mp * o.w + o.x * h[0] + o.y * h[1] + o.z * h[2] + vg.x * e[0] + vg.y * e[1] + vg.z * e[2];
-            acc[9] += sig * (w.s0 * w.n1[j] * w.n2[k]);
-            acc[10] += sig * (w.n0 * w.s1[j] * w.n2[k]);
+            acc[9] += sig * (w.s0 * n1 * w.n2[k]);
+            acc[10] += sig * (w.n0 * s1 * w.n2[k]);
             acc[11] += sig * (n01 * w.s2[k]);
             const float wo[3] = {wt * o.x, wt * o.y, wt * o.z};
             acc[12] += wo[0];
@@ -689,7 +742,7 @@ template <bool EXACT, int MODE> __global__ void __launch_bounds__(256, DMPM_GATH
             acc[15] += wt * vg.x;
             acc[16] += wt * vg.y;
             acc[17] += wt * vg.z;
-            const float d[3] = {w.d0, w.d1[j], w.d2[k]};
+            const float d[3] = {w.d0, d1, w.d2[k]};
 #pragma unroll
             for (int r = 0; r < 3; r++)
 #pragma unroll
@@ -700,23 +753,29 @@ template <bool EXACT, int MODE> __global__ void __launch_bounds__(256, DMPM_GATH
             node4<float>* sw = s_rec[threadIdx.x >> 5];
             stage_stencil<2>(a.gadj2, geo, goff, base, sw);
 #pragma unroll
-            for (int j = 0; j < 4; j++)
+            for (int j = 0; j < 4; j++) {
+                float d1, n1, s1;
+                row_weights(own1, j, d1, n1, s1);
 #pragma unroll
                 for (int k = 0; k < 4; k++) {
                     const int n = 16 * L.s + 4 * j + k;
-                    node(sw[2 * n], sw[2 * n + 1], j, k);
+                    node(sw[2 * n], sw[2 * n + 1], d1, n1, s1, k);
                 }
+            }
         } else {
             LaneNodes N = lane_nodes(geo, base, L.s);
             N.g00 += goff;
 #pragma unroll
-            for (int j = 0; j < 4; j++)
+            for (int j = 0; j < 4; j++) {
+                float d1, n1, s1;
+                row_weights(own1, j, d1, n1, s1);
 #pragma unroll
                 for (int k = 0; k < 4; k++) {
                     if (!((N.mask >> (4 * j + k)) & 1u)) continue;
                     const int g = N.g00 + j * N.sj + k;
-                    node(a.gadj2[2 * g], a.gadj2[2 * g + 1], j, k);
+                    node(a.gadj2[2 * g], a.gadj2[2 * g + 1], d1, n1, s1, k);
                 }
+            }
         }
         reduce_slabs<18>(acc);
         if (!L.valid) continue;
