@@ -240,6 +240,12 @@ __device__ __forceinline__ void load_x_base(const float* st, size_t np, int p, c
 // registers, no spills; 1 lets it take 132 and run one block per SM),
 // k_adj_finalize at 128 (4: 128 registers with a 32-byte spill, 11 % faster
 // than the 168-register build on the 64^3, 267k-particle workload).
+// k_stress takes the FP64 polar factors from the scaled Newton iteration
+// (polar_newton) where det(F + dFc) > 0 and from the SVD (polar3) otherwise;
+// 0 uses the SVD everywhere
+#ifndef DMPM_NEWTON_POLAR
+#define DMPM_NEWTON_POLAR 1
+#endif
 #ifndef DMPM_STRESS_MIN_BLOCKS
 #define DMPM_STRESS_MIN_BLOCKS 2
 #endif
@@ -369,7 +375,7 @@ static __global__ void __launch_bounds__(256, DMPM_STRESS_MIN_BLOCKS) k_stress(W
         const m3<float> Fe = load_m3(a.st + (size_t)PF * npl, npl, p) + load_m3(a.dfc, np, p);
         const m3<double> Fed = m3_cast<double>(Fe);
         m3<double> Rd, Sd;
-        polar3(Fed, Rd, Sd);
+        if (!DMPM_NEWTON_POLAR || !polar_newton(Fed, Rd, Sd)) polar3(Fed, Rd, Sd);
         const m3<double> Pd = pk_from_polar(Fed, Rd, (double)a.cst[(size_t)KLAM * np + p], (double)a.cst[(size_t)KMU * np + p]);
         const m3<float> P = m3_cast<float>(Pd);
         if (a.P) store_m3(a.P, npl, p, P);

@@ -263,4 +263,42 @@ template <class T> DMPM_HD void polar3(const m3<T>& F, m3<T>& R, m3<T>& S) {
             S.a[i][j] = V.a[i][0] * s[0] * V.a[j][0] + V.a[i][1] * s[1] * V.a[j][1] + V.a[i][2] * s[2] * V.a[j][2];
 }
 
+// Polar decomposition F = R S of a matrix with det F > 0 by the scaled Newton
+// iteration  X <- (z X + X^{-T} / z) / 2,  z = det(X)^{-1/3}  (Higham 1986,
+// determinant scaling), which converges quadratically to the rotation of the
+// polar decomposition -- for det F > 0 the same R that polar3 obtains from
+// the SVD -- in a few inverse-transposes instead of an SVD.  Returns false,
+// leaving R and S unset, when det F is not comfortably positive or the
+// iteration has not converged in 24 steps; the caller then uses polar3, whose
+// rotation-variant convention the reference relies on for inverted F.
+template <class T> DMPM_HD bool polar_newton(const m3<T>& F, m3<T>& R, m3<T>& S) {
+    if (!(det3(F) > T(1e-6))) return false;
+    m3<T> X = F;
+    bool done = false;
+    for (int it = 0; it < 24 && !done; it++) {
+        const m3<T> Xit = inv_transpose3(X);
+        const T c = cbrt(det3(X));  // z = 1 / c
+        const T z = T(1) / c;
+        T diff = T(0), nrm = T(0);
+#pragma unroll
+        for (int i = 0; i < 3; i++)
+#pragma unroll
+            for (int j = 0; j < 3; j++) {
+                const T y = T(0.5) * (z * X.a[i][j] + c * Xit.a[i][j]);
+                diff += (y - X.a[i][j]) * (y - X.a[i][j]);
+                nrm += y * y;
+                X.a[i][j] = y;
+            }
+        done = diff <= T(1e-30) * nrm;  // relative change below 1e-15: converged to rounding
+    }
+    if (!done) return false;
+    R = X;
+    const m3<T> M = mtm(R, F);  // R^T F, symmetric up to rounding
+#pragma unroll
+    for (int i = 0; i < 3; i++)
+#pragma unroll
+        for (int j = 0; j < 3; j++) S.a[i][j] = T(0.5) * (M.a[i][j] + M.a[j][i]);
+    return true;
+}
+
 }  // namespace dmpm

@@ -21,6 +21,9 @@ template <class T> static void st(const m3<T>& m, T* a) {
         m3<T> Um, Vm; svd3(ld(F), Um, s, Vm); st(Um, U); st(Vm, V); }                                 \
     extern "C" void mh_polar_##SFX(const T* F, T* R, T* S) {                                          \
         m3<T> Rm, Sm; polar3(ld(F), Rm, Sm); st(Rm, R); st(Sm, S); }                                  \
+    extern "C" int mh_polar_newton_##SFX(const T* F, T* R, T* S) {                                    \
+        m3<T> Rm, Sm; const bool ok = polar_newton(ld(F), Rm, Sm); if (ok) { st(Rm, R); st(Sm, S); }   \
+        return ok ? 1 : 0; }                                                                          \
     extern "C" void mh_pk_##SFX(const T* F, T lam, T mu, T* P) { st(pk_stress(ld(F), lam, mu), P); } \
     extern "C" void mh_d2_##SFX(const T* F, T lam, T mu, const T* dF, int exact, T* out) {            \
         st(exact ? d2_mult<true>(ld(F), lam, mu, ld(dF)) : d2_mult<false>(ld(F), lam, mu, ld(dF)), out); }

@@ -113,3 +113,46 @@ def test_exact_stress_derivative_matches_fd(mh):
         h = 1e-6
         fd = (ref.pk(F + h * dF, lam, mu) - ref.pk(F - h * dF, lam, mu)) / (2 * h)
         assert relerr(un(out), fd) < 1e-7
+
+
+def test_newton_polar_matches_svd_polar(mh):
+    """polar_newton (the FP32 path's k_stress, det F > 0) gives polar3's R and S
+    to rounding, and declines inverted or near-singular F (left to the SVD)."""
+    mh.mh_polar_newton_f64.restype = ctypes.c_int
+    rng = np.random.default_rng(2024)
+    cases = []
+    for t in range(400):
+        k = t % 4
+        if k == 0:
+            F = np.eye(3) + 1e-3 * rng.normal(size=(3, 3))
+        elif k == 1:
+            F = np.eye(3) + 0.3 * rng.normal(size=(3, 3))
+        elif k == 2:
+            Q, _ = np.linalg.qr(rng.normal(size=(3, 3)))
+            Q *= np.sign(np.linalg.det(Q))
+            F = Q @ np.diag(rng.uniform(0.2, 5.0, 3)) @ Q.T
+        else:
+            Q1, _ = np.linalg.qr(rng.normal(size=(3, 3)))
+            Q1 *= np.sign(np.linalg.det(Q1))
+            Q2, _ = np.linalg.qr(rng.normal(size=(3, 3)))
+            Q2 *= np.sign(np.linalg.det(Q2))
+            F = Q1 @ np.diag(rng.uniform(0.05, 20.0, 3)) @ Q2
+        cases.append(F)
+    used = 0
+    for F in cases:
+        R = np.zeros(9)
+        S = np.zeros(9)
+        ok = mh.mh_polar_newton_f64(cm(F).ctypes.data_as(P), R.ctypes.data_as(P), S.ctypes.data_as(P))
+        if np.linalg.det(F) > 1e-3:
+            assert ok == 1
+        if not ok:
+            continue
+        used += 1
+        R0, S0 = polar(mh, F)
+        assert np.abs(un(R) - R0).max() < 1e-12
+        assert np.abs(un(S) - S0).max() < 1e-12 * max(1.0, np.abs(S0).max())
+    assert used >= 380
+    for F in (np.diag([1.0, 1.0, -1.0]), np.diag([1.0, 1.0, 1e-9]), -np.eye(3)):
+        R = np.zeros(9)
+        S = np.zeros(9)
+        assert mh.mh_polar_newton_f64(cm(F).ctypes.data_as(P), R.ctypes.data_as(P), S.ctypes.data_as(P)) == 0
