@@ -19,6 +19,7 @@
 #include "DiffMPMLib3D/CompGraph.h"
 #include "DiffMPMLib3D/Elasticity.h"
 #include "DiffMPMLib3D/ForwardSimulation.h"
+#include "DiffMPMLib3D/GeometryLoading.h"
 #include "dmpm.h"
 
 namespace DiffMPMLib3D {
@@ -807,6 +808,25 @@ void CompGraph::OptimizeDefGradControlSequence(int num_steps, float _dt, float _
     std::cout << "Final loss = " << final_loss << std::endl;
     std::ofstream ofs("gradient_norm_log.csv");
     for (size_t i = 0; i < gradientNormHistory.size(); i++) ofs << i << "," << gradientNormHistory[i] << "\n";
+}
+
+// ---- GeometryLoading (GeometryLoading.cpp:10-83) ----
+
+std::vector<Vec3> GeometryLoading::GeneratePointCloudFromTriangleArrays(const float* V, int nv, const int* F, int nf,
+                                                                        Vec3 min_point, Vec3 max_point,
+                                                                        float sampling_dx) {
+    int dims[3];
+    check(nullptr, dmpm_mesh_lattice_dims(min_point.data(), max_point.data(), sampling_dx, dims),
+          "dmpm_mesh_lattice_dims");
+    const int64_t cap = (int64_t)dims[0] * dims[1] * dims[2];
+    std::vector<float> buf((size_t)cap * 3);
+    int64_t n = 0;
+    check(nullptr, dmpm_mesh_lattice_points(V, nv, F, nf, min_point.data(), max_point.data(), sampling_dx,
+                                            buf.data(), cap, &n),
+          "dmpm_mesh_lattice_points");
+    std::vector<Vec3> pts((size_t)n);
+    for (int64_t i = 0; i < n; i++) pts[(size_t)i] = Vec3(buf[3 * i], buf[3 * i + 1], buf[3 * i + 2]);
+    return pts;
 }
 
 }  // namespace DiffMPMLib3D

@@ -126,6 +126,9 @@ def load_library(path: str = LIB_PATH) -> ctypes.CDLL:
     L.dmpm_batch_get_particles.argtypes = [_P, ctypes.c_int, ctypes.c_int, ctypes.c_int, _P]
     L.dmpm_batch_info.argtypes = [_P, ctypes.POINTER(ctypes.c_int64), ctypes.c_int]
     L.dmpm_batch_stream.argtypes = [_P, ctypes.POINTER(_P)]
+    L.dmpm_mesh_lattice_dims.argtypes = [_P, _P, ctypes.c_float, _P]
+    L.dmpm_mesh_lattice_points.argtypes = [_P, ctypes.c_int, _P, ctypes.c_int, _P, _P, ctypes.c_float, _P,
+                                           ctypes.c_int64, ctypes.POINTER(ctypes.c_int64)]
     _lib = L
     return L
 
@@ -496,3 +499,63 @@ class Batch:
         s = _P()
         self._ck(self.lib.dmpm_batch_stream(self.h, ctypes.byref(s)), "batch_stream")
         return s.value or 0
+
+
+def mesh_lattice_points(V, F, point_dx: float, min_point=None, max_point=None) -> np.ndarray:
+    """Point cloud of a watertight, outward-oriented triangle mesh on the GPU
+    (dmpm_mesh_lattice_points): the lattice points of spacing point_dx over
+    [min_point, max_point] (default: the vertices' float32 bounding box, as
+    LoadMPMPointCloudFromObj takes it) whose winding number is >= 1/2, in the
+    reference's lattice order.  V: (nv, 3), F: (nf, 3) 0-based; returns
+    (n, 3) float32."""
+    lib = load_library()
+    V = np.ascontiguousarray(V, dtype=np.float32)
+    F = np.ascontiguousarray(F, dtype=np.int32)
+    mn = np.ascontiguousarray(V.min(axis=0) if min_point is None else min_point, dtype=np.float32)
+    mx = np.ascontiguousarray(V.max(axis=0) if max_point is None else max_point, dtype=np.float32)
+    dims = np.zeros(3, dtype=np.int32)
+    st = lib.dmpm_mesh_lattice_dims(mn.ctypes.data, mx.ctypes.data, float(point_dx), dims.ctypes.data)
+    if st != OK:
+        raise DmpmError(st, "mesh_lattice_dims: invalid bounds or spacing")
+    cap = int(np.prod(dims.astype(np.int64)))
+    out = np.empty((cap, 3), dtype=np.float32)
+    n = ctypes.c_int64()
+    st = lib.dmpm_mesh_lattice_points(V.ctypes.data, len(V), F.ctypes.data, len(F), mn.ctypes.data, mx.ctypes.data,
+                                      float(point_dx), out.ctypes.data, cap, ctypes.byref(n))
+    if st != OK:
+        raise DmpmError(st, "mesh_lattice_points failed")
+    return out[: n.value].copy()
+
+
+def read_obj(path: str):
+    """Vertices (float32) and triangles (0-based) of the 'v' and 'f' lines of an
+    OBJ file; 'f' entries may be v, v/vt, v//vn or v/vt/vn, negative indices
+    count from the end, polygons are split into a fan of triangles."""
+    V, F = [], []
+    with open(path) as f:
+        for line in f:
+            t = line.split()
+            if not t:
+                continue
+            if t[0] == "v":
+                V.append([float(x) for x in t[1:4]])
+            elif t[0] == "f":
+                idx = [int(x.split("/")[0]) for x in t[1:]]
+                idx = [i - 1 if i > 0 else len(V) + i for i in idx]
+                for k in range(1, len(idx) - 1):
+                    F.append([idx[0], idx[k], idx[k + 1]])
+    return np.asarray(V, dtype=np.float32), np.asarray(F, dtype=np.int32)
+
+
+def point_cloud_from_obj(path: str, point_dx: float, density: float, lam: float, mu: float) -> dict:
+    """LoadMPMPointCloudFromObj (MPMPolyscope.cpp:10-60): the mesh's lattice
+    points (mesh_lattice_points over the vertices' bounding box), v = 0, F = I,
+    m = point_dx^3 density, the given lam and mu.  Returns the arrays
+    Context.set_particles takes."""
+    V, F = read_obj(path)
+    x = mesh_lattice_points(V, F, point_dx).astype(np.float64)
+    n = len(x)
+    pdx = np.float32(point_dx)
+    m = float(np.float32(pdx * pdx * pdx * np.float32(density)))
+    return {"x": x, "v": np.zeros((n, 3)), "F": np.broadcast_to(np.eye(3), (n, 3, 3)).copy(),
+            "m": np.full(n, m), "lam": np.full(n, float(np.float32(lam))), "mu": np.full(n, float(np.float32(mu)))}

@@ -6,10 +6,10 @@ holding the fields in declaration order, each Vec3 as
 cereal_eigen.h writes the row count, then the coefficients).
 
 A caller holding an input.json of the reference sets up an engine context
-from it with grid_dims / point_mass / params below.  The OBJ meshes it names
-are not loaded here (mesh voxelisation is outside this library); the point
-clouds come from .mpmbin files (the C++ PointCloud of compat/ reads and
-writes them) or from the caller.
+from it with grid_dims / point_mass / params below, and turns the OBJ meshes
+it names into point clouds with dmpm.point_cloud_from_obj(path, point_dx(opt),
+opt.p_density, opt.lam, opt.mu) (the GPU lattice sampler); .mpmbin point
+clouds are read and written by the C++ PointCloud of compat/.
 """
 from __future__ import annotations
 

@@ -63,7 +63,7 @@ typedef struct dmpm_ctx dmpm_ctx;
 #define DMPM_ERR_CUDA 3      /* a CUDA runtime call failed */
 #define DMPM_ERR_NONFINITE 4 /* a stage produced NaN/inf (results still written, as the reference does) */
 #define DMPM_ERR_STATE 5     /* call order: e.g. backward before loss, or a layer that is not stored */
-#define DMPM_ERR_TOO_LARGE 6 /* size exceeds the fixed scratch capacity of dmpm_compute_volumes_noalloc */
+#define DMPM_ERR_TOO_LARGE 6 /* a size exceeds a fixed capacity: dmpm_compute_volumes_noalloc's scratch, an output buffer */
 
 /* precision paths */
 #define DMPM_FP64 0       /* plain FP64 path: one kernel per reference stage, global atomics */
@@ -300,6 +300,26 @@ int dmpm_batch_get_particles(dmpm_batch* b, int inst, int layer, int field, doub
  * [4] kernel launches of one gradient evaluation, [5] 1 if a graph is captured */
 int dmpm_batch_info(const dmpm_batch* b, int64_t* info, int count);
 int dmpm_batch_stream(const dmpm_batch* b, void** stream);
+
+/* ------------------------------------------------------------------------
+ * Scene setup: point cloud of a watertight, outward-oriented triangle mesh,
+ * computed on the current CUDA device.  GeometryLoading::
+ * GeneratePointCloudFromWatertightTriangleMesh (GeometryLoading.cpp:10-83),
+ * as LoadMPMPointCloudFromObj calls it (MPMPolyscope.cpp:10-60, min_point and
+ * max_point the vertices' bounding box): the lattice min_point +
+ * sampling_dx (i, j, k), i < ceil((max - min) / sampling_dx) + 1 per axis,
+ * i outermost, keeping the points whose winding number is >= 1/2 (the
+ * reference's libigl signed distance with winding-number sign is <= 0
+ * there).  The reference also keeps a lattice point that lies exactly on a
+ * face, which this function leaves out when its winding number is below 1/2.
+ *   V: nv * 3 floats;  F: nf * 3 vertex indices (0-based)
+ *   out: capacity * 3 floats (NULL with capacity 0 to count only)
+ *   *count: the number of points kept; DMPM_ERR_TOO_LARGE when > capacity
+ * ------------------------------------------------------------------------ */
+int dmpm_mesh_lattice_dims(const float* min_point, const float* max_point, float sampling_dx, int* dims);
+int dmpm_mesh_lattice_points(const float* V, int nv, const int* F, int nf, const float* min_point,
+                             const float* max_point, float sampling_dx, float* out, int64_t capacity,
+                             int64_t* count);
 
 #ifdef __cplusplus
 }
