@@ -326,16 +326,17 @@ template <class T> class Engine : public EngineBase {
     int tile_cap() const { return ctx_->prm.tile_cap > 0 ? ctx_->prm.tile_cap : kDefaultTileCap; }
     unsigned pgrid() const { return (unsigned)((n_ + block() - 1) / block()); }
     unsigned pgrid256() const { return (unsigned)((n_ + 255) / 256); }
-    // persistent grid of the warp-item kernels: 3 CTAs of 256 threads per SM, fewer
-    // when the particles could not fill them (at most one item per particle)
-    unsigned warp_blocks() {
+    // persistent grid of a warp-item kernel: ctas CTAs of 256 threads per SM (the
+    // residency its register budget allows), fewer when the particles could not
+    // fill them (at most one item per particle)
+    unsigned warp_blocks(int ctas = 3) {
         if (sms_ == 0) {
             int dev = 0;
             DMPM_CK(cudaGetDevice(&dev));
             DMPM_CK(cudaDeviceGetAttribute(&sms_, cudaDevAttrMultiProcessorCount, dev));
         }
         const size_t most = ((size_t)n_ * 32 + 255) / 256;
-        return (unsigned)std::max<size_t>(1, std::min<size_t>(most, (size_t)sms_ * 3));
+        return (unsigned)std::max<size_t>(1, std::min<size_t>(most, (size_t)sms_ * ctas));
     }
     unsigned ggrid() const { return (unsigned)((G_ + 255) / 256); }
 
@@ -793,14 +794,14 @@ template <class T> class Engine : public EngineBase {
             a.grid = (node4<float>*)g;
             a.P = ctx_->prm.keep_intermediates ? (float*)layers_[l].dbgP : nullptr;
             DMPM_CK(cudaMemsetAsync(g, 0, G_ * sizeof(node4<T>), ctx_->stream));
-            const unsigned wg = warp_blocks();
+            const unsigned ws = warp_blocks(DMPM_SCATTER_CTAS);
             pbeg(K_P_OP1);
             k_stress<<<pgrid256(), 256, 0, ctx_->stream>>>(a);
             launched();
             pend();
             pbeg(K_P2G);
-            if (ctx_->prm.warp_general) k_p2g_w<true, ITEMS_PERSISTENT><<<wg, 256, 0, ctx_->stream>>>(a);
-            else k_p2g_w<false, ITEMS_PERSISTENT><<<wg, 256, 0, ctx_->stream>>>(a);
+            if (ctx_->prm.warp_general) k_p2g_w<true, ITEMS_PERSISTENT><<<ws, 256, 0, ctx_->stream>>>(a);
+            else k_p2g_w<false, ITEMS_PERSISTENT><<<ws, 256, 0, ctx_->stream>>>(a);
             launched();
             pend();
             pbeg(K_GOP);
@@ -808,7 +809,7 @@ template <class T> class Engine : public EngineBase {
             launched();
             pend();
             pbeg(K_G2P);
-            k_g2p_w<ITEMS_PERSISTENT><<<wg, 256, 0, ctx_->stream>>>(a);
+            k_g2p_w<ITEMS_PERSISTENT><<<warp_blocks(DMPM_G2P_CTAS), 256, 0, ctx_->stream>>>(a);
             launched();
             pend();
             return;
@@ -1018,14 +1019,14 @@ template <class T> class Engine : public EngineBase {
             if (!a.st || !a.st_next || !a.grid || !a.G) throw StateError{"internal: layer not materialised"};
             DMPM_CK(cudaMemsetAsync(gadj_, 0, G_ * sizeof(node4<T>), ctx_->stream));
             const bool ex = P.adjoint_mode == DMPM_ADJ_EXACT;
-            const unsigned wg = warp_blocks();
+            const unsigned ws = warp_blocks(DMPM_SCATTER_CTAS), wg = warp_blocks(DMPM_GATHER_CTAS);
             pbeg(K_ADJ_SCATTER);
             if (P.warp_general) {
-                if (ex) k_adj_scatter_w<true, true, ITEMS_PERSISTENT><<<wg, 256, 0, ctx_->stream>>>(a);
-                else k_adj_scatter_w<false, true, ITEMS_PERSISTENT><<<wg, 256, 0, ctx_->stream>>>(a);
+                if (ex) k_adj_scatter_w<true, true, ITEMS_PERSISTENT><<<ws, 256, 0, ctx_->stream>>>(a);
+                else k_adj_scatter_w<false, true, ITEMS_PERSISTENT><<<ws, 256, 0, ctx_->stream>>>(a);
             } else {
-                if (ex) k_adj_scatter_w<true, false, ITEMS_PERSISTENT><<<wg, 256, 0, ctx_->stream>>>(a);
-                else k_adj_scatter_w<false, false, ITEMS_PERSISTENT><<<wg, 256, 0, ctx_->stream>>>(a);
+                if (ex) k_adj_scatter_w<true, false, ITEMS_PERSISTENT><<<ws, 256, 0, ctx_->stream>>>(a);
+                else k_adj_scatter_w<false, false, ITEMS_PERSISTENT><<<ws, 256, 0, ctx_->stream>>>(a);
             }
             launched();
             pend();

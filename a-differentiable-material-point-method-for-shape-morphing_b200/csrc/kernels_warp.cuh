@@ -53,38 +53,28 @@ __device__ __forceinline__ bool warp_uniform_base(const int b[3]) {
     return __all_sync(0xffffffffu, b[0] == b0 && b[1] == b1 && b[2] == b2);
 }
 
-// Butterfly reduce-scatter over the 8 lanes that share lane & 3.  On return
-// v[0 .. N/8) hold the sums of the original entries off + i, with
-// off = (lane&16 ? N/2 : 0) + (lane&8 ? N/4 : 0) + (lane&4 ? N/8 : 0).
+// Butterfly reduce-scatter over the 8 lanes that share lane & 3, for vectors
+// whose 8 blocks of N/8 entries the lanes hold in a lane-permuted order: lane
+// L's block b holds stencil node b ^ perm(L), perm(L) = 4 (L>>4 & 1) +
+// 2 (L>>3 & 1) + (L>>2 & 1) (scatter_perm).  Then at every stage each lane
+// keeps the lower half and sends the upper half -- the partner holds the same
+// nodes there -- with no per-lane selects.  On return v[0 .. N/8) of lane L
+// hold the sums of node perm(L)'s entries over the 8 lanes.
 template <int N> __device__ __forceinline__ void reduce_scatter8(float (&v)[N]) {
+#pragma unroll
+    for (int i = 0; i < N / 2; i++) v[i] += __shfl_xor_sync(0xffffffffu, v[i + N / 2], 16);
+#pragma unroll
+    for (int i = 0; i < N / 4; i++) v[i] += __shfl_xor_sync(0xffffffffu, v[i + N / 4], 8);
+#pragma unroll
+    for (int i = 0; i < N / 8; i++) v[i] += __shfl_xor_sync(0xffffffffu, v[i + N / 8], 4);
+}
+// this lane's node permutation for reduce_scatter8: row bit (jp) and axis-2 bits (kp)
+struct ScatterPerm {
+    int jp, kp;
+};
+__device__ __forceinline__ ScatterPerm scatter_perm() {
     const int lane = threadIdx.x & 31;
-    {
-        const bool up = lane & 16;
-#pragma unroll
-        for (int i = 0; i < N / 2; i++) {
-            const float send = up ? v[i] : v[i + N / 2];
-            const float keep = up ? v[i + N / 2] : v[i];
-            v[i] = keep + __shfl_xor_sync(0xffffffffu, send, 16);
-        }
-    }
-    {
-        const bool up = lane & 8;
-#pragma unroll
-        for (int i = 0; i < N / 4; i++) {
-            const float send = up ? v[i] : v[i + N / 4];
-            const float keep = up ? v[i + N / 4] : v[i];
-            v[i] = keep + __shfl_xor_sync(0xffffffffu, send, 8);
-        }
-    }
-    {
-        const bool up = lane & 4;
-#pragma unroll
-        for (int i = 0; i < N / 8; i++) {
-            const float send = up ? v[i] : v[i + N / 8];
-            const float keep = up ? v[i + N / 8] : v[i];
-            v[i] = keep + __shfl_xor_sync(0xffffffffu, send, 4);
-        }
-    }
+    return ScatterPerm{(lane >> 4) & 1, ((lane >> 3) & 1) * 2 + ((lane >> 2) & 1)};
 }
 
 template <int N> __device__ __forceinline__ void reduce_slabs(float (&v)[N]) {
@@ -190,9 +180,10 @@ __device__ __forceinline__ void lane_weights(const float x[3], const GridGeom& g
 // As lane_weights, but axis 1 is left to the caller: it gets this lane's own
 // axis-1 offset, weight and slope in own1 and fetches row j's values with
 // row_weights (three shuffles) when it reaches that row, so only one row's
-// values are live at a time.  Fills d0, n0, s0 and the axis-2 arrays of w.
+// values are live at a time.  Fills d0, n0, s0 and the axis-2 arrays of w,
+// the latter in the order of node k ^ kperm (reduce_scatter8's permutation).
 __device__ __forceinline__ void lane_weights_k(const float x[3], const GridGeom& g, const int base[3], int s,
-                                               LaneW& w, float own1[3], bool slopes) {
+                                               LaneW& w, float own1[3], bool slopes, int kperm = 0) {
     const float dx = (float)g.dx, idx = 1.f / dx;
     float d[3], n[3], sl[3];
 #pragma unroll
@@ -211,10 +202,10 @@ __device__ __forceinline__ void lane_weights_k(const float x[3], const GridGeom&
     own1[2] = sl[1];
     const int grp = (threadIdx.x & 31) & ~3;
 #pragma unroll
-    for (int t = 0; t < 4; t++) {
-        w.d2[t] = __shfl_sync(0xffffffffu, d[2], grp + t);
-        w.n2[t] = __shfl_sync(0xffffffffu, n[2], grp + t);
-        w.s2[t] = slopes ? __shfl_sync(0xffffffffu, sl[2], grp + t) : 0.f;
+    for (int t = 0; t < 4; t++) {  // entry t holds axis-2 node t ^ kperm
+        w.d2[t] = __shfl_sync(0xffffffffu, d[2], grp + (t ^ kperm));
+        w.n2[t] = __shfl_sync(0xffffffffu, n[2], grp + (t ^ kperm));
+        w.s2[t] = slopes ? __shfl_sync(0xffffffffu, sl[2], grp + (t ^ kperm)) : 0.f;
     }
 }
 // row j's axis-1 (offset, weight, slope) from the lane of slab j; every lane must call it
@@ -259,6 +250,13 @@ __device__ __forceinline__ void load_x_base(const float* st, size_t np, int p, c
 #endif
 #ifndef DMPM_SCATTER_MIN_BLOCKS
 #define DMPM_SCATTER_MIN_BLOCKS 3
+#endif
+// CTAs per SM of the persistent grids (no more than the register budget above lets reside)
+#ifndef DMPM_GATHER_CTAS
+#define DMPM_GATHER_CTAS DMPM_GATHER_MIN_BLOCKS
+#endif
+#ifndef DMPM_SCATTER_CTAS
+#define DMPM_SCATTER_CTAS DMPM_SCATTER_MIN_BLOCKS
 #endif
 
 // Grid of one instance of a batch: its geometry, the offset of its first node
@@ -407,9 +405,11 @@ template <bool GENERAL, int MODE> __global__ void __launch_bounds__(256, DMPM_SC
         int base[3];
         load_x_base(a.st, npl, L.p, geo, x, base);
         const bool uniform = !GENERAL && warp_uniform_base(base);
+        // slot (jj, kk) of each half holds node (2 half + (jj ^ P.jp), kk ^ P.kp)
+        const ScatterPerm P = scatter_perm();
         LaneW w;
         float own1[3];
-        lane_weights_k(x, geo, base, L.s, w, own1, false);
+        lane_weights_k(x, geo, base, L.s, w, own1, false, P.kp);
         const float mp = L.valid ? a.cst[(size_t)KM * np + L.p] : 0.f;
         const float damp = 1.f - a.dt * a.drag;
         float mvd[3], g0[3];
@@ -426,33 +426,30 @@ template <bool GENERAL, int MODE> __global__ void __launch_bounds__(256, DMPM_SC
             float v[32];
 #pragma unroll
             for (int jj = 0; jj < 2; jj++) {
-                const int j = 2 * half + jj;
                 float d1, n1, s1;
-                row_weights(own1, j, d1, n1, s1);
+                row_weights(own1, 2 * half + (jj ^ P.jp), d1, n1, s1);
                 float g1[3];
 #pragma unroll
                 for (int c = 0; c < 3; c++) g1[c] = g0[c] + G.a[c][1] * d1;
                 const float w01 = L.valid ? w.n0 * n1 : 0.f;
 #pragma unroll
-                for (int k = 0; k < 4; k++) {
-                    const float wt = w01 * w.n2[k];
-                    const int o = (jj * 4 + k) * 4;
+                for (int kk = 0; kk < 4; kk++) {
+                    const float wt = w01 * w.n2[kk];
+                    const int o = (jj * 4 + kk) * 4;
 #pragma unroll
-                    for (int c = 0; c < 3; c++) v[o + c] = wt * (mvd[c] + g1[c] + G.a[c][2] * w.d2[k]);
+                    for (int c = 0; c < 3; c++) v[o + c] = wt * (mvd[c] + g1[c] + G.a[c][2] * w.d2[kk]);
                     v[o + 3] = wt * mp;
                 }
             }
             if (uniform) {
                 reduce_scatter8<32>(v);
-                const int lane = threadIdx.x & 31;
-                const int nd = ((lane >> 4) & 1) * 4 + ((lane >> 3) & 1) * 2 + ((lane >> 2) & 1);
-                const int j = 2 * half + nd / 4, k = nd % 4;
+                const int j = 2 * half + P.jp, k = P.kp;
                 if (((N.mask >> (4 * j + k)) & 1u) && (v[0] != 0.f || v[1] != 0.f || v[2] != 0.f || v[3] != 0.f))
                     red_add4(a.grid + (N.g00 + j * N.sj + k), v[0], v[1], v[2], v[3]);
             } else if (L.valid) {
 #pragma unroll
                 for (int nd = 0; nd < 8; nd++) {
-                    const int j = 2 * half + nd / 4, k = nd % 4;
+                    const int j = 2 * half + ((nd >> 2) ^ P.jp), k = (nd & 3) ^ P.kp;
                     if ((N.mask >> (4 * j + k)) & 1u)
                         red_add4(a.grid + (N.g00 + j * N.sj + k), v[nd * 4], v[nd * 4 + 1], v[nd * 4 + 2], v[nd * 4 + 3]);
                 }
@@ -477,6 +474,10 @@ static __global__ void k_gop_inplace(node4<float>* grid, size_t G, float dt, flo
 
 // G2P + P_op_2: v' = sum w v_g;  C' = 3/dx^2 sum w v_g d^T;
 // F' = (1 - s)(I + dt C')(F + dFc) + s F;  x' = x + dt v'
+// G2P keeps 64 registers without spills, so four 256-thread CTAs reside per SM
+#ifndef DMPM_G2P_CTAS
+#define DMPM_G2P_CTAS 4
+#endif
 template <int MODE> __global__ void __launch_bounds__(256, 4) k_g2p_w(WArgs a) {
     const int nit = item_count(a);
     const size_t np = a.np, npl = a.npl, npn = a.npn;
@@ -499,24 +500,8 @@ template <int MODE> __global__ void __launch_bounds__(256, 4) k_g2p_w(WArgs a) {
 #pragma unroll
         for (int k = 0; k < 4; k++) nd2[k] = w.n2[k] * w.d2[k];
         float V[3] = {0.f, 0.f, 0.f}, C1[3] = {0.f, 0.f, 0.f}, C2[3] = {0.f, 0.f, 0.f};
-        // a uniform item stages its 64 stencil nodes in shared memory (stage_stencil);
-        // otherwise each lane loads its slab's nodes, a row at a time
-        const bool staged = DMPM_STAGE_NODES && warp_uniform_base(base);
-        __shared__ node4<float> s_nodes[8][StageRecords<1>::value];
-        node4<float>* sw = s_nodes[threadIdx.x >> 5];
-        if (staged) stage_stencil<1>(a.grid, geo, goff, base, sw);
-        LaneNodes N = lane_nodes(geo, base, L.s);
-        N.g00 += goff;
-#pragma unroll
-        for (int j = 0; j < 4; j++) {
-            // the row's four node records are loaded before any is used (more loads in
-            // flight); nodes outside the grid read as zero and contribute nothing
-            node4<float> row[4];
-#pragma unroll
-            for (int k = 0; k < 4; k++)
-                row[k] = staged ? sw[stage_index<1>(16 * L.s + 4 * j + k, 0)]
-                                : (((N.mask >> (4 * j + k)) & 1u) ? a.grid[N.g00 + j * N.sj + k]
-                                                                  : node4<float>{0.f, 0.f, 0.f, 0.f});
+        // one stencil row j from its four node records
+        auto row_sum = [&](int j, const node4<float> (&row)[4]) {
             float Vj[3] = {0.f, 0.f, 0.f}, Wj[3] = {0.f, 0.f, 0.f};
 #pragma unroll
             for (int k = 0; k < 4; k++) {
@@ -535,6 +520,33 @@ template <int MODE> __global__ void __launch_bounds__(256, 4) k_g2p_w(WArgs a) {
                 V[r] += w01 * Vj[r];
                 C1[r] += w01d * Vj[r];
                 C2[r] += w01 * Wj[r];
+            }
+        };
+        // a uniform item stages its 64 stencil nodes in shared memory (stage_stencil);
+        // otherwise each lane loads its slab's nodes, a row at a time (the row's four
+        // records before any is used; nodes outside the grid read as zero)
+        __shared__ node4<float> s_nodes[8][StageRecords<1>::value];
+        if (DMPM_STAGE_NODES && warp_uniform_base(base)) {
+            node4<float>* sw = s_nodes[threadIdx.x >> 5];
+            stage_stencil<1>(a.grid, geo, goff, base, sw);
+#pragma unroll
+            for (int j = 0; j < 4; j++) {
+                node4<float> row[4];
+#pragma unroll
+                for (int k = 0; k < 4; k++) row[k] = sw[stage_index<1>(16 * L.s + 4 * j + k, 0)];
+                row_sum(j, row);
+            }
+        } else {
+            LaneNodes N = lane_nodes(geo, base, L.s);
+            N.g00 += goff;
+#pragma unroll
+            for (int j = 0; j < 4; j++) {
+                node4<float> row[4];
+#pragma unroll
+                for (int k = 0; k < 4; k++)
+                    row[k] = ((N.mask >> (4 * j + k)) & 1u) ? a.grid[N.g00 + j * N.sj + k]
+                                                            : node4<float>{0.f, 0.f, 0.f, 0.f};
+                row_sum(j, row);
             }
         }
         float acc[12];  // v (3), C (9) row-major
@@ -555,6 +567,8 @@ template <int MODE> __global__ void __launch_bounds__(256, 4) k_g2p_w(WArgs a) {
         for (int r = 0; r < 3; r++)
 #pragma unroll
             for (int c = 0; c < 3; c++) Cn.a[r][c] = k3 * acc[3 + 3 * r + c];
+        // lane s = 0 stores x' and v', s = 1 C'; lanes s = 0, 2, 3 each one column
+        // c of F' = (1-s)(I + dt C') Fe[:,c] + s F[:,c]
         bool finite = true;
         if (L.s == 0) {
 #pragma unroll
@@ -564,25 +578,23 @@ template <int MODE> __global__ void __launch_bounds__(256, 4) k_g2p_w(WArgs a) {
                 a.st_next[(size_t)(PV + c) * npn + p] = acc[c];
                 finite &= isfinite(xn);
             }
-        } else if (L.s == 1) {
+        }
+        if (L.s == 1) {
             store_m3(a.st_next + (size_t)PC * npn, npn, p, Cn);
         } else {
-            // columns c of F' = (1-s)(I + dt C') Fe[:,c] + s F[:,c]; lane s=2 -> cols 0,1; s=3 -> col 2
-            const int c0 = L.s == 2 ? 0 : 2, c1 = L.s == 2 ? 2 : 3;
-            for (int c = c0; c < c1; c++) {
-                float Fc[3], Fec[3];
+            const int c = L.s == 0 ? 0 : L.s - 1;
+            float Fc[3], Fec[3];
 #pragma unroll
-                for (int r = 0; r < 3; r++) {
-                    Fc[r] = a.st[(size_t)(PF + r + 3 * c) * npl + p];
-                    Fec[r] = Fc[r] + a.dfc[(size_t)(r + 3 * c) * np + p];
-                }
+            for (int r = 0; r < 3; r++) {
+                Fc[r] = a.st[(size_t)(PF + r + 3 * c) * npl + p];
+                Fec[r] = Fc[r] + a.dfc[(size_t)(r + 3 * c) * np + p];
+            }
 #pragma unroll
-                for (int r = 0; r < 3; r++) {
-                    const float t = Fec[r] + a.dt * (Cn.a[r][0] * Fec[0] + Cn.a[r][1] * Fec[1] + Cn.a[r][2] * Fec[2]);
-                    const float fn = (1.f - a.s) * t + a.s * Fc[r];
-                    a.st_next[(size_t)(PF + r + 3 * c) * npn + p] = fn;
-                    finite &= isfinite(fn);
-                }
+            for (int r = 0; r < 3; r++) {
+                const float t = Fec[r] + a.dt * (Cn.a[r][0] * Fec[0] + Cn.a[r][1] * Fec[1] + Cn.a[r][2] * Fec[2]);
+                const float fn = (1.f - a.s) * t + a.s * Fc[r];
+                a.st_next[(size_t)(PF + r + 3 * c) * npn + p] = fn;
+                finite &= isfinite(fn);
             }
         }
         if (!finite) atomicOr(a.status, ST_NONFINITE_FWD);
@@ -605,9 +617,10 @@ template <bool EXACT, bool GENERAL, int MODE> __global__ void __launch_bounds__(
         int base[3];
         load_x_base(a.st, npl, p, geo, x, base);
         const bool uniform = !GENERAL && warp_uniform_base(base);
+        const ScatterPerm P = scatter_perm();  // as in k_p2g_w
         LaneW w;
         float own1[3];
-        lane_weights_k(x, geo, base, L.s, w, own1, false);
+        lane_weights_k(x, geo, base, L.s, w, own1, false, P.kp);
         float vn[3];
 #pragma unroll
         for (int c = 0; c < 3; c++)
@@ -638,38 +651,34 @@ template <bool EXACT, bool GENERAL, int MODE> __global__ void __launch_bounds__(
         N.g00 += goff;
 #pragma unroll
         for (int half = 0; half < 2; half++) {
-            float v[32];
+            float v[24];  // 8 nodes x dLdv_g (3)
 #pragma unroll
             for (int jj = 0; jj < 2; jj++) {
-                const int j = 2 * half + jj;
                 float d1, n1, s1;
-                row_weights(own1, j, d1, n1, s1);
+                row_weights(own1, 2 * half + (jj ^ P.jp), d1, n1, s1);
                 float c1[3];
 #pragma unroll
                 for (int r = 0; r < 3; r++) c1[r] = c0[r] + k3 * Cn.a[r][1] * d1;
                 const float w01 = L.valid ? w.n0 * n1 : 0.f;
 #pragma unroll
-                for (int k = 0; k < 4; k++) {
-                    const float wt = w01 * w.n2[k];
-                    const int o = (jj * 4 + k) * 4;
+                for (int kk = 0; kk < 4; kk++) {
+                    const float wt = w01 * w.n2[kk];
+                    const int o = (jj * 4 + kk) * 3;
 #pragma unroll
-                    for (int r = 0; r < 3; r++) v[o + r] = wt * (vn[r] + c1[r] + k3 * Cn.a[r][2] * w.d2[k]);
-                    v[o + 3] = 0.f;
+                    for (int r = 0; r < 3; r++) v[o + r] = wt * (vn[r] + c1[r] + k3 * Cn.a[r][2] * w.d2[kk]);
                 }
             }
             if (uniform) {
-                reduce_scatter8<32>(v);
-                const int lane = threadIdx.x & 31;
-                const int nd = ((lane >> 4) & 1) * 4 + ((lane >> 3) & 1) * 2 + ((lane >> 2) & 1);
-                const int j = 2 * half + nd / 4, k = nd % 4;
+                reduce_scatter8<24>(v);
+                const int j = 2 * half + P.jp, k = P.kp;
                 if (((N.mask >> (4 * j + k)) & 1u) && (v[0] != 0.f || v[1] != 0.f || v[2] != 0.f))
                     red_add4(a.gadj + (N.g00 + j * N.sj + k), v[0], v[1], v[2], 0.f);
             } else if (L.valid) {
 #pragma unroll
                 for (int nd = 0; nd < 8; nd++) {
-                    const int j = 2 * half + nd / 4, k = nd % 4;
+                    const int j = 2 * half + ((nd >> 2) ^ P.jp), k = (nd & 3) ^ P.kp;
                     if ((N.mask >> (4 * j + k)) & 1u)
-                        red_add4(a.gadj + (N.g00 + j * N.sj + k), v[nd * 4], v[nd * 4 + 1], v[nd * 4 + 2], 0.f);
+                        red_add4(a.gadj + (N.g00 + j * N.sj + k), v[nd * 3], v[nd * 3 + 1], v[nd * 3 + 2], 0.f);
                 }
             }
         }
