@@ -749,32 +749,40 @@ template <bool EXACT, int MODE> __global__ void __launch_bounds__(256, DMPM_GATH
         float acc[18];  // M (9, row-major: M[r][c] = sum w d_r dLdp_c), X (3), u (3), z (3)
 #pragma unroll
         for (int i = 0; i < 18; i++) acc[i] = 0.f;
-        // one node (j, k) of the lane's slab, with row j's axis-1 values d1, n1, s1
-        auto node = [&](const node4<float>& o, const node4<float>& vg, float d1, float n1, float s1, int k) {
+        // Factored sums: on this lane d0, n0 and s0 are constant and on a row d1, n1, s1, so
+        //   M[0][c] = d0 u_c (formed after the loop),
+        //   X0 = s0 sum_j n1 S_j,  X1 = n0 sum_j s1 S_j,  X2 = n0 sum_j n1 T_j,
+        // with the row sums S_j = sum_k n2_k sigma, T_j = sum_k s2_k sigma.
+        float S = 0.f, T = 0.f;
+        // one node (j, k) of the lane's slab, with row j's axis-1 values d1, n1
+        auto node = [&](const node4<float>& o, const node4<float>& vg, float d1, float n1, int k) {
             float h[3], e[3];
 #pragma unroll
             for (int r = 0; r < 3; r++) {
                 h[r] = h0[r] + G.a[r][1] * d1 + G.a[r][2] * w.d2[k];
                 e[r] = e0[r] + k3 * Cn.a[r][1] * d1 + k3 * Cn.a[r][2] * w.d2[k];
             }
-            const float n01 = w.n0 * n1;
-            const float wt = n01 * w.n2[k];
+            const float wt = (w.n0 * n1) * w.n2[k];
             const float sig = mp * o.w + o.x * h[0] + o.y * h[1] + o.z * h[2] + vg.x * e[0] + vg.y * e[1] + vg.z * e[2];
-            acc[9] += sig * (w.s0 * n1 * w.n2[k]);
-            acc[10] += sig * (w.n0 * s1 * w.n2[k]);
-            acc[11] += sig * (n01 * w.s2[k]);
+            S += w.n2[k] * sig;
+            T += w.s2[k] * sig;
             const float wo[3] = {wt * o.x, wt * o.y, wt * o.z};
-            acc[12] += wo[0];
-            acc[13] += wo[1];
-            acc[14] += wo[2];
             acc[15] += wt * vg.x;
             acc[16] += wt * vg.y;
             acc[17] += wt * vg.z;
-            const float d[3] = {w.d0, d1, w.d2[k]};
 #pragma unroll
-            for (int r = 0; r < 3; r++)
-#pragma unroll
-                for (int c = 0; c < 3; c++) acc[3 * r + c] += d[r] * wo[c];
+            for (int c = 0; c < 3; c++) {
+                acc[12 + c] += wo[c];
+                acc[3 + c] += d1 * wo[c];
+                acc[6 + c] += w.d2[k] * wo[c];
+            }
+        };
+        auto end_row = [&](float n1, float s1) {
+            acc[9] += n1 * S;
+            acc[10] += s1 * S;
+            acc[11] += n1 * T;
+            S = 0.f;
+            T = 0.f;
         };
         if (DMPM_STAGE_NODES && warp_uniform_base(base)) {
             __shared__ node4<float> s_rec[8][StageRecords<2>::value];
@@ -787,8 +795,9 @@ template <bool EXACT, int MODE> __global__ void __launch_bounds__(256, DMPM_GATH
 #pragma unroll
                 for (int k = 0; k < 4; k++) {
                     const int n = 16 * L.s + 4 * j + k;
-                    node(sw[stage_index<2>(n, 0)], sw[stage_index<2>(n, 1)], d1, n1, s1, k);
+                    node(sw[stage_index<2>(n, 0)], sw[stage_index<2>(n, 1)], d1, n1, k);
                 }
+                end_row(n1, s1);
             }
         } else {
             LaneNodes N = lane_nodes(geo, base, L.s);
@@ -801,10 +810,16 @@ template <bool EXACT, int MODE> __global__ void __launch_bounds__(256, DMPM_GATH
                 for (int k = 0; k < 4; k++) {
                     if (!((N.mask >> (4 * j + k)) & 1u)) continue;
                     const int g = N.g00 + j * N.sj + k;
-                    node(a.gadj2[2 * g], a.gadj2[2 * g + 1], d1, n1, s1, k);
+                    node(a.gadj2[2 * g], a.gadj2[2 * g + 1], d1, n1, k);
                 }
+                end_row(n1, s1);
             }
         }
+        acc[9] *= w.s0;
+        acc[10] *= w.n0;
+        acc[11] *= w.n0;
+#pragma unroll
+        for (int c = 0; c < 3; c++) acc[c] = w.d0 * acc[12 + c];
         reduce_slabs<18>(acc);
         if (!L.valid) continue;
         if (L.s == 0) {

@@ -82,3 +82,37 @@ def test_compat_cpp_geometry_loading(gpu_ready, tmp_path):
     subprocess.check_call([exe, obj, repr(dx), str(out)])
     pts = np.fromfile(out, dtype=np.float32).reshape(-1, 3)
     assert np.array_equal(pts, ref)
+
+
+@pytest.mark.gpu
+def test_input_file_and_mesh_drive_a_gradient(gpu_ready, tmp_path):
+    """An OptInput file naming OBJ meshes, turned into a context the way the
+    reference's animator sets up its CompGraph (LoadMPMPointCloudFromObj for
+    the input and target meshes, grid from the file, volumes, target mass
+    raster, simulation parameters), runs forward + loss + backward."""
+    import optinput
+
+    obj, _, _ = _golden("sphere")
+    opt = optinput.OptInput(mpm_input_mesh_path=obj, mpm_target_mesh_path=obj, grid_dx=0.05,
+                            grid_min_point=(-1.0, -1.0, -1.0), grid_max_point=(1.0, 1.0, 1.0), dt=1e-4,
+                            num_timesteps=4, control_stride=2)
+    path = str(tmp_path / "input.json")
+    optinput.save(opt, path)
+    opt = optinput.load(path)
+    pc = dmpm.point_cloud_from_obj(opt.mpm_input_mesh_path, optinput.point_dx(opt), opt.p_density, opt.lam, opt.mu)
+    assert abs(pc["m"][0] - optinput.point_mass(opt)) <= 1e-6 * optinput.point_mass(opt)
+    with dmpm.Context("fp32") as c:
+        c.set_grid(optinput.grid_dims(opt), opt.grid_dx, opt.grid_min_point)
+        c.set_particles(pc["x"], pc["m"], pc["lam"], pc["mu"], v=pc["v"], F=pc["F"])
+        c.compute_volumes()  # CalculatePointCloudVolumes, as LoadCompGraph does
+        tpc = dmpm.point_cloud_from_obj(opt.mpm_target_mesh_path, optinput.point_dx(opt), opt.p_density, opt.lam,
+                                        opt.mu)
+        c.rasterize_target(tpc["x"], optinput.point_mass(opt))
+        c.set_params(**optinput.params(opt), adjoint="exact")
+        c.setup(opt.num_timesteps + 1)
+        assert c.forward(0) == dmpm.OK
+        loss = c.loss()
+        assert c.backward(0) == dmpm.OK
+        g = c.control_grad(0)
+    assert np.isfinite(loss) and loss > 0
+    assert g.shape == (len(pc["x"]), 3, 3) and np.all(np.isfinite(g)) and np.abs(g).max() > 0
