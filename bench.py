@@ -805,13 +805,23 @@ def run_config4(args):
     # updates the moments again, as the reference does) and halve alpha; a frame whose line search
     # finds no decrease ends its descent.
     max_ls = 6
-    ls_trials, grad_ms, stopped, last = [], [], None, None
+    ls_trials, grad_ms, stopped, last, nonfinite = [], [], None, None, None
+
+    def statused_gradient(holder):
+        st_f = c.forward(0)
+        holder["loss"] = c.loss()
+        st_b = c.backward(0)
+        holder["finite"] = st_f == dmpm.OK and st_b == dmpm.OK and math.isfinite(holder["loss"])
+
     for it in range(1, iters + 1):
         holder = {}
-        ms = timed_steps(torch, c, 1, lambda: holder.update(loss=gradient_step(c)))
+        ms = timed_steps(torch, c, 1, lambda: statused_gradient(holder))
         loss = holder["loss"]
         losses.append(loss)
         grad_ms.append(ms)
+        if not holder["finite"]:  # the rollout or its adjoint went non-finite at these controls
+            nonfinite = it
+            break
         if not args.no_fp64:  # the controls and FP32 gradient of this iteration (host copies)
             last = (it, c.control_grad(0), c.get(0, "dFc"))
             if it == 1:
@@ -820,8 +830,9 @@ def run_config4(args):
         alpha, found = 1e-2, False
         for ls in range(max_ls):
             c.adam_step(t=it, lr=alpha, layer=0)
-            c.forward(0)
-            if c.loss() < loss:
+            st = c.forward(0)
+            trial = c.loss()
+            if st == dmpm.OK and math.isfinite(trial) and trial < loss:
                 found = True
                 break
             c.adam_step(t=it, lr=-alpha, layer=0)
@@ -837,6 +848,7 @@ def run_config4(args):
     out.update({"loss_curve": losses, "ms_per_iteration": times, "ms_per_gradient": grad_ms,
                 "line_search_trials": ls_trials, "max_line_search_trials": max_ls,
                 "stopped_at_iteration_without_decrease": stopped,
+                "stopped_at_iteration_nonfinite": nonfinite,
                 "particle_steps_per_s": sc.n * sc.steps / (float(np.median(grad_ms)) / 1000.0),
                 "grad_relerr_vs_fp64": relerrs})
     c.close()
