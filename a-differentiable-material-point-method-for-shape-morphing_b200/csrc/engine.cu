@@ -135,6 +135,49 @@ __global__ void k_adam(T* dfc, const G* __restrict__ grad, T* mom, T* vec, size_
     vec[i] = (T)v;
     dfc[i] = (T)((float)dfc[i] - lr * ((m / c1) / (sqrtf(v / c2) + eps)));
 }
+// The other descent rules of PointCloud (PointCloud.cpp:101-204), one element of
+// one control matrix per thread, g = grad / norm as in k_adam:
+//   AMSGRAD  m, v as Adam; vmax = max(vmax, v / (1 - b2^t)); dFc -= lr (m / (1 - b1^t)) / (sqrt(vmax) + eps)
+//   LION     m = b1 m + (1 - b1) sign(g); dFc -= lr m           (sign(0) = 0, SignFloat)
+//   GD       dFc -= lr g
+//   DLDF     d = g clipped to [-1, 1] with |d| >= 1e-3 (sign kept, 0 -> +1e-3);
+//            m = 0.9 m + lr d; dFc -= m                           (Descend_dLdF)
+template <class T, class G>
+__global__ void k_descend(int kind, T* dfc, const G* __restrict__ grad, T* mom, T* vec, T* vmax, size_t np, int n,
+                          const double* norm2, int normalize, float lr, float b1, float b2, float eps, float c1,
+                          float c2) {
+    const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= (size_t)9 * np) return;
+    if ((int)(i % np) >= n) return;
+    const float inv = normalize ? (float)(1.0 / sqrt(*norm2)) : 1.f;
+    const float g = (float)grad[i] * inv;
+    float d = (float)dfc[i];
+    if (kind == DMPM_DESCEND_AMSGRAD) {
+        const float m = b1 * (float)mom[i] + (1.f - b1) * g;
+        const float v = b2 * (float)vec[i] + (1.f - b2) * g * g;
+        const float vm = fmaxf((float)vmax[i], v / c2);
+        mom[i] = (T)m;
+        vec[i] = (T)v;
+        vmax[i] = (T)vm;
+        d -= lr * ((m / c1) / (sqrtf(vm) + eps));
+    } else if (kind == DMPM_DESCEND_LION) {
+        const float sg = g > 0.f ? 1.f : (g < 0.f ? -1.f : 0.f);
+        const float m = b1 * (float)mom[i] + (1.f - b1) * sg;
+        mom[i] = (T)m;
+        d -= lr * m;
+    } else if (kind == DMPM_DESCEND_GD) {
+        d -= lr * g;
+    } else {  // DMPM_DESCEND_DLDF
+        float c = g;
+        if (c > 1.f) c = 1.f;
+        if (c < -1.f) c = -1.f;
+        if (fabsf(c) < 1e-3f) c = c < 0.f ? -1e-3f : 1e-3f;
+        const float m = 0.9f * (float)mom[i] + lr * c;
+        mom[i] = (T)m;
+        d -= m;
+    }
+    dfc[i] = (T)d;
+}
 template <class G> __global__ void k_sumsq(const G* __restrict__ a, size_t np, int n, double* out) {
     __shared__ double s[32];
     const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
@@ -1222,8 +1265,13 @@ template <class T> class Engine : public EngineBase {
 
     // one optimiser step on the controls of a layer (tied: the shared controls)
     void adam_step(int l, double lr, double b1, double b2, double eps, int t, bool normalize) {
+        descend(l, DMPM_DESCEND_ADAM, lr, b1, b2, eps, t, normalize);
+    }
+    void descend(int l, int kind, double lr, double b1, double b2, double eps, int t, bool normalize) {
         if (L_ <= 0) throw StateError{"dmpm_setup has not been called"};
-        if (t < 1) throw ArgError{"Adam timestep must be >= 1"};
+        if (kind < DMPM_DESCEND_ADAM || kind > DMPM_DESCEND_DLDF) throw ArgError{"unknown descent rule"};
+        if ((kind == DMPM_DESCEND_ADAM || kind == DMPM_DESCEND_AMSGRAD) && t < 1)
+            throw ArgError{"Adam timestep must be >= 1"};
         T* dfc;
         const void* grad;
         bool grad_fp64;
@@ -1240,13 +1288,14 @@ template <class T> class Engine : public EngineBase {
             grad_fp64 = false;
         }
         auto it = adam_.find(l);
-        if (it == adam_.end()) {
-            T* st = (T*)misc_arena_.alloc(2 * 9 * np_ * sizeof(T));
-            DMPM_CK(cudaMemsetAsync(st, 0, 2 * 9 * np_ * sizeof(T), ctx_->stream));
+        if (it == adam_.end()) {  // momentum, vector, vector_max of MaterialPoint, shared by the rules
+            T* st = (T*)misc_arena_.alloc(3 * 9 * np_ * sizeof(T));
+            DMPM_CK(cudaMemsetAsync(st, 0, 3 * 9 * np_ * sizeof(T), ctx_->stream));
             it = adam_.emplace(l, st).first;
         }
         T* mom = it->second;
         T* vec = it->second + 9 * np_;
+        T* vmax = it->second + 18 * np_;
         double* norm2 = loss_acc_ + 1;
         DMPM_CK(cudaMemsetAsync(norm2, 0, sizeof(double), ctx_->stream));
         const unsigned blocks = (unsigned)((9 * np_ + 255) / 256);
@@ -1254,14 +1303,24 @@ template <class T> class Engine : public EngineBase {
         else k_sumsq<T><<<blocks, 256, 0, ctx_->stream>>>((const T*)grad, np_, n_, norm2);
         launched();
         const float c1 = 1.f - std::pow((float)b1, (float)t), c2 = 1.f - std::pow((float)b2, (float)t);
-        if (grad_fp64)
-            k_adam<T, double><<<blocks, 256, 0, ctx_->stream>>>(dfc, (const double*)grad, mom, vec, np_, n_, norm2,
-                                                                  normalize ? 1 : 0, (float)lr, (float)b1, (float)b2,
-                                                                  (float)eps, c1, c2);
-        else
-            k_adam<T, T><<<blocks, 256, 0, ctx_->stream>>>(dfc, (const T*)grad, mom, vec, np_, n_, norm2,
-                                                            normalize ? 1 : 0, (float)lr, (float)b1, (float)b2,
-                                                            (float)eps, c1, c2);
+        if (kind == DMPM_DESCEND_ADAM) {
+            if (grad_fp64)
+                k_adam<T, double><<<blocks, 256, 0, ctx_->stream>>>(dfc, (const double*)grad, mom, vec, np_, n_,
+                                                                      norm2, normalize ? 1 : 0, (float)lr, (float)b1,
+                                                                      (float)b2, (float)eps, c1, c2);
+            else
+                k_adam<T, T><<<blocks, 256, 0, ctx_->stream>>>(dfc, (const T*)grad, mom, vec, np_, n_, norm2,
+                                                                normalize ? 1 : 0, (float)lr, (float)b1, (float)b2,
+                                                                (float)eps, c1, c2);
+        } else if (grad_fp64) {
+            k_descend<T, double><<<blocks, 256, 0, ctx_->stream>>>(kind, dfc, (const double*)grad, mom, vec, vmax,
+                                                                     np_, n_, norm2, normalize ? 1 : 0, (float)lr,
+                                                                     (float)b1, (float)b2, (float)eps, c1, c2);
+        } else {
+            k_descend<T, T><<<blocks, 256, 0, ctx_->stream>>>(kind, dfc, (const T*)grad, mom, vec, vmax, np_, n_,
+                                                               norm2, normalize ? 1 : 0, (float)lr, (float)b1,
+                                                               (float)b2, (float)eps, c1, c2);
+        }
         launched();
         // per-layer controls of later layers are copies made by setup; the
         // reference descends only the control layer, so nothing else changes
@@ -1658,6 +1717,14 @@ int dmpm_get_grid(dmpm_ctx* ctx, int layer, int field, double* out) {
 int dmpm_adam_step(dmpm_ctx* ctx, int layer, double lr, double beta1, double beta2, double eps, int t,
                    int normalize) {
     return with_engine(ctx, [&](auto& e) { e.adam_step(layer, lr, beta1, beta2, eps, t, normalize != 0); return DMPM_OK; });
+}
+
+int dmpm_descend(dmpm_ctx* ctx, int layer, int rule, double lr, double beta1, double beta2, double eps, int t,
+                 int normalize) {
+    return with_engine(ctx, [&](auto& e) {
+        e.descend(layer, rule, lr, beta1, beta2, eps, t, normalize != 0);
+        return DMPM_OK;
+    });
 }
 
 int dmpm_get_control_grad(dmpm_ctx* ctx, int layer, double* out) {

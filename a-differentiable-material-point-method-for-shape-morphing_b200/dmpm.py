@@ -24,6 +24,7 @@ FP64, FP32_MIXED = 0, 1
 ADJ_REFCOMPAT, ADJ_EXACT = 0, 1
 CTRL_PER_LAYER, CTRL_TIED = 0, 1
 LOSS_REF_LOGMASS, LOSS_L2 = 0, 1
+DESCEND = {"adam": 0, "amsgrad": 1, "lion": 2, "gd": 3, "dldf": 4}
 
 FIELDS = {"x": 0, "v": 1, "F": 2, "C": 3, "P": 4, "m": 5, "vol": 6, "lam": 7, "mu": 8, "dFc": 9, "dLdx": 10,
           "dLdv": 11, "dLdF": 12, "dLdC": 13, "dLdP": 14, "dLdv_next": 15, "dLdC_next": 16, "dLdFe": 19}
@@ -98,6 +99,8 @@ def load_library(path: str = LIB_PATH) -> ctypes.CDLL:
     L.dmpm_get_points_ref.argtypes = [_P, ctypes.c_int, _P]
     L.dmpm_adam_step.argtypes = [_P, ctypes.c_int, ctypes.c_double, ctypes.c_double, ctypes.c_double,
                                  ctypes.c_double, ctypes.c_int, ctypes.c_int]
+    L.dmpm_descend.argtypes = [_P, ctypes.c_int, ctypes.c_int, ctypes.c_double, ctypes.c_double, ctypes.c_double,
+                               ctypes.c_double, ctypes.c_int, ctypes.c_int]
     L.dmpm_synchronize.argtypes = [_P]
     L.dmpm_stream.argtypes = [_P]
     L.dmpm_stream.restype = _P
@@ -365,6 +368,14 @@ class Context:
         self._ck(self.lib.dmpm_adam_step(self.h, int(layer), lr, beta1, beta2, eps, int(t), int(normalize)),
                  "adam_step")
 
+    def descend(self, rule: str, lr: float, t: int = 1, beta1: float = 0.9, beta2: float = 0.999, eps: float = 1e-5,
+                layer: int = 0, normalize: bool = True):
+        """One of PointCloud's descent rules on the controls (device): "adam",
+        "amsgrad", "lion" (beta1 = its beta), "gd" or "dldf" (Descend_dLdF)."""
+        r = DESCEND[rule]
+        self._ck(self.lib.dmpm_descend(self.h, int(layer), r, lr, beta1, beta2, eps, int(t), int(normalize)),
+                 "descend " + rule)
+
     def dldf_norm(self, layer: int = 0) -> float:
         out = ctypes.c_double()
         self._ck(self.lib.dmpm_dldf_norm(self.h, int(layer), ctypes.byref(out)), "dldf_norm")
@@ -559,3 +570,118 @@ def point_cloud_from_obj(path: str, point_dx: float, density: float, lam: float,
     m = float(np.float32(pdx * pdx * pdx * np.float32(density)))
     return {"x": x, "v": np.zeros((n, 3)), "F": np.broadcast_to(np.eye(3), (n, 3, 3)).copy(),
             "m": np.full(n, m), "lam": np.full(n, float(np.float32(lam))), "mu": np.full(n, float(np.float32(mu)))}
+
+
+# ---------------------------------------------------------------- surfaces
+def _surf_lib():
+    lib = load_library()
+    I64 = ctypes.c_int64
+    lib.dmpm_surface_grid_dims.argtypes = [_P, _P, ctypes.c_float, _P]
+    lib.dmpm_surface_p2g_mass.argtypes = [_P, I64, ctypes.c_float, _P, ctypes.c_float, _P, _P]
+    lib.dmpm_surface_g2g_mass.argtypes = [_P, _P, ctypes.c_float, _P, _P, ctypes.c_float, _P, _P]
+    lib.dmpm_surface_sphere_field.argtypes = [_P, I64, ctypes.c_float, ctypes.c_int, _P, ctypes.c_float, _P, _P]
+    lib.dmpm_surface_extract.argtypes = [_P, _P, ctypes.c_float, _P, ctypes.c_float, _P, I64, _P, I64,
+                                         ctypes.POINTER(I64), ctypes.POINTER(I64)]
+    return lib
+
+
+def _f32(a, shape=None):
+    a = np.ascontiguousarray(a, dtype=np.float32)
+    return a if shape is None else a.reshape(shape)
+
+
+def _dims(d):
+    return np.ascontiguousarray([int(v) for v in d], dtype=np.int32)
+
+
+def _surf_ck(st, what):
+    if st != OK:
+        raise DmpmError(st, what)
+
+
+def surface_grid_dims(min_point, max_point, dx: float):
+    """ceil((max_x - min_x) / dx) nodes per axis (dmpm_surface_grid_dims)."""
+    lib = _surf_lib()
+    mn, mx = _f32(min_point), _f32(max_point)  # held here for the duration of the call
+    d = np.zeros(3, dtype=np.int32)
+    _surf_ck(lib.dmpm_surface_grid_dims(mn.ctypes.data, mx.ctypes.data, float(dx), d.ctypes.data), "surface_grid_dims")
+    return tuple(int(v) for v in d)
+
+
+def p2g_mass(points, mp_m: float, dims, dx: float, min_point) -> np.ndarray:
+    """SingleThreadMPM::P2G_Mass on the GPU: node masses, flat in node order."""
+    lib = _surf_lib()
+    p, d, mn = _f32(points, (-1, 3)), _dims(dims), _f32(min_point)
+    out = np.empty(int(np.prod(dims)), dtype=np.float32)
+    _surf_ck(lib.dmpm_surface_p2g_mass(p.ctypes.data, len(p), float(mp_m), d.ctypes.data, float(dx), mn.ctypes.data,
+                                       out.ctypes.data), "p2g_mass")
+    return out
+
+
+def g2g_mass(mass1, dims1, dx1: float, min1, dims2, dx2: float, min2) -> np.ndarray:
+    """SingleThreadMPM::G2G_Mass on the GPU."""
+    lib = _surf_lib()
+    m1, d1, mn1, d2, mn2 = _f32(mass1), _dims(dims1), _f32(min1), _dims(dims2), _f32(min2)
+    out = np.empty(int(np.prod(dims2)), dtype=np.float32)
+    _surf_ck(lib.dmpm_surface_g2g_mass(m1.ctypes.data, d1.ctypes.data, float(dx1), mn1.ctypes.data, d2.ctypes.data,
+                                       float(dx2), mn2.ctypes.data, out.ctypes.data), "g2g_mass")
+    return out
+
+
+def sphere_field(points, radius: float, blur_iterations: int, dims, dx: float, min_point) -> np.ndarray:
+    """The sphere-union field of SphereUnionMarchingCubesSurfaceFromPointCloud on the GPU."""
+    lib = _surf_lib()
+    p, d, mn = _f32(points, (-1, 3)), _dims(dims), _f32(min_point)
+    out = np.empty(int(np.prod(dims)), dtype=np.float32)
+    _surf_ck(lib.dmpm_surface_sphere_field(p.ctypes.data, len(p), float(radius), int(blur_iterations), d.ctypes.data,
+                                           float(dx), mn.ctypes.data, out.ctypes.data), "sphere_field")
+    return out
+
+
+def extract_surface(field, dims, dx: float, min_point, iso: float):
+    """Triangle mesh (V float32 (n, 3), F int32 (m, 3)) of {field = iso} (dmpm_surface_extract)."""
+    lib = _surf_lib()
+    f = _f32(field)
+    d, mn = _dims(dims), _f32(min_point)
+    nv, nf = ctypes.c_int64(), ctypes.c_int64()
+    st = lib.dmpm_surface_extract(f.ctypes.data, d.ctypes.data, float(dx), mn.ctypes.data, float(iso), None, 0, None,
+                                  0, ctypes.byref(nv), ctypes.byref(nf))
+    if st not in (OK, ERR_TOO_LARGE):
+        raise DmpmError(st, "extract_surface")
+    V = np.empty((nv.value, 3), dtype=np.float32)
+    F = np.empty((nf.value, 3), dtype=np.int32)
+    _surf_ck(lib.dmpm_surface_extract(f.ctypes.data, d.ctypes.data, float(dx), mn.ctypes.data, float(iso),
+                                      V.ctypes.data, nv.value, F.ctypes.data, nf.value, ctypes.byref(nv),
+                                      ctypes.byref(nf)), "extract_surface")
+    return V, F
+
+
+def marching_cubes_point_cloud(points, iso_mass: float, grid_dx: float, quality: float, min_point, max_point):
+    """The reference GUI's MarchingCubesPointCloud (DiffMPMAnimator3D.cpp:488-514) on
+    the GPU: P2G_Mass (unit point mass) on the grid of spacing grid_dx, G2G_Mass onto
+    a grid refined by `quality`, and the iso_mass level set of the fine masses."""
+    dims = surface_grid_dims(min_point, max_point, grid_dx)
+    coarse = p2g_mass(points, 1.0, dims, grid_dx, min_point)
+    q = np.float32(quality)
+    fdims = tuple(int(np.float32(d) * q) for d in dims)
+    fdx = float(np.float32(grid_dx) / q)
+    fine = g2g_mass(coarse, dims, grid_dx, min_point, fdims, fdx, min_point)
+    return extract_surface(fine, fdims, fdx, min_point, iso_mass)
+
+
+def sphere_union_surface(points, radius: float, grid_dx: float, iso_mass: float, blur_iterations: int, min_point,
+                         max_point):
+    """SphereUnionMarchingCubesSurfaceFromPointCloud (SphereUnionSurfacing.cpp:7-128)
+    on the GPU (grid_dx is the spacing of the field's grid, as there)."""
+    dims = surface_grid_dims(min_point, max_point, grid_dx)
+    f = sphere_field(points, radius, blur_iterations, dims, grid_dx, min_point)
+    return extract_surface(f, dims, grid_dx, min_point, iso_mass)
+
+
+def write_obj(path: str, V, F) -> None:
+    """A mesh as Wavefront OBJ (1-based faces)."""
+    with open(path, "w") as f:
+        for v in np.asarray(V):
+            f.write("v %.9g %.9g %.9g\n" % tuple(v))
+        for t in np.asarray(F):
+            f.write("f %d %d %d\n" % (t[0] + 1, t[1] + 1, t[2] + 1))

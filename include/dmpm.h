@@ -185,6 +185,23 @@ int dmpm_dldf_norm(dmpm_ctx* ctx, int layer, double* norm);
  * Moment buffers live in the context; t is the 1-based step count. */
 int dmpm_adam_step(dmpm_ctx* ctx, int layer, double lr, double beta1, double beta2, double eps, int t,
                    int normalize);
+/* One descent step on the controls, on the device, with one of PointCloud's
+ * rules (same gradient, normalisation and moment buffers as dmpm_adam_step;
+ * the buffers play the roles of MaterialPoint::momentum, vector and vector_max
+ * and are shared by the rules, as in the reference):
+ *   DMPM_DESCEND_ADAM     Descend_Adam            (PointCloud.cpp:83-99)
+ *   DMPM_DESCEND_AMSGRAD  Descend_AMSGrad         (PointCloud.cpp:101-132)
+ *   DMPM_DESCEND_LION     Descend_Lion, beta1 as its beta (PointCloud.cpp:134-162)
+ *   DMPM_DESCEND_GD       Descend_GradientDescent (PointCloud.cpp:164-178)
+ *   DMPM_DESCEND_DLDF     Descend_dLdF: clipped direction, momentum 0.9 (PointCloud.cpp:181-204)
+ * beta2, eps and t are used by ADAM and AMSGRAD only. */
+#define DMPM_DESCEND_ADAM 0
+#define DMPM_DESCEND_AMSGRAD 1
+#define DMPM_DESCEND_LION 2
+#define DMPM_DESCEND_GD 3
+#define DMPM_DESCEND_DLDF 4
+int dmpm_descend(dmpm_ctx* ctx, int layer, int rule, double lr, double beta1, double beta2, double eps, int t,
+                 int normalize);
 /* Fill the state and gradient fields of an array of reference MaterialPoints for one layer. */
 int dmpm_get_points_ref(dmpm_ctx* ctx, int layer, void* points);
 
@@ -320,6 +337,45 @@ int dmpm_mesh_lattice_dims(const float* min_point, const float* max_point, float
 int dmpm_mesh_lattice_points(const float* V, int nv, const int* F, int nf, const float* min_point,
                              const float* max_point, float sampling_dx, float* out, int64_t capacity,
                              int64_t* count);
+
+/* ------------------------------------------------------------------------
+ * Surfaces: headless export of a point cloud as a triangle mesh, the GPU
+ * counterpart of the reference's MarchingCubesPointCloud
+ * (DiffMPMAnimator3D.cpp:488-514) and SphereUnionMarchingCubesSurfaceFromPointCloud
+ * (SphereUnionSurfacing.cpp:7-128).  Host arrays; points are float triples;
+ * grid arrays hold prod(dims) floats in node order (i * dim_y + j) * dim_z + k,
+ * node (i, j, k) at min_point + (i, j, k) * dx.  Each call allocates its device
+ * scratch, runs on the default stream and synchronises.
+ *
+ *   dmpm_surface_grid_dims    ceil((max_x - min_x) / dx) nodes on every axis, as
+ *                             both reference functions size their grids
+ *   dmpm_surface_p2g_mass     SingleThreadMPM::P2G_Mass (ForwardSimulation.cpp:292-327):
+ *                             node masses sum_p w mp_m (float atomics: equal to the
+ *                             reference's point-ordered sums up to rounding)
+ *   dmpm_surface_g2g_mass     SingleThreadMPM::G2G_Mass (ForwardSimulation.cpp:329-367):
+ *                             grid 2's node masses interpolated from grid 1's with
+ *                             grid 1's spacing, bit-identical to the reference
+ *   dmpm_surface_sphere_field the field of SphereUnionMarchingCubesSurfaceFromPointCloud
+ *                             (lines 13-101): max over points of radius - |x - p| inside
+ *                             each sphere, then blur_iterations passes of the 27-node sum
+ *                             divided by 9 on interior nodes; bit-identical
+ *   dmpm_surface_extract      the level set {field = iso} as a triangle mesh (marching
+ *                             tetrahedra, one vertex per crossed grid edge, normals toward
+ *                             decreasing field); the reference calls libigl's marching
+ *                             cubes here, which triangulates the same level set
+ *                             differently.  V: 3 floats per vertex, F: 3 vertex indices
+ *                             per triangle; *nv, *nf: the counts, DMPM_ERR_TOO_LARGE when
+ *                             they exceed the capacities (call with 0 to size).
+ * ------------------------------------------------------------------------ */
+int dmpm_surface_grid_dims(const float* min_point, const float* max_point, float dx, int* dims);
+int dmpm_surface_p2g_mass(const float* points, int64_t n, float mp_m, const int* dims, float dx,
+                          const float* min_point, float* mass);
+int dmpm_surface_g2g_mass(const float* mass1, const int* dims1, float dx1, const float* min1, const int* dims2,
+                          float dx2, const float* min2, float* mass2);
+int dmpm_surface_sphere_field(const float* points, int64_t n, float radius, int blur_iterations, const int* dims,
+                              float dx, const float* min_point, float* field);
+int dmpm_surface_extract(const float* field, const int* dims, float dx, const float* min_point, float iso, float* V,
+                         int64_t v_capacity, int* F, int64_t f_capacity, int64_t* nv, int64_t* nf);
 
 #ifdef __cplusplus
 }

@@ -433,3 +433,66 @@ def test_graph_replay_matches_eager_launches(gpu_ready, exact_case):
         assert relerr(x_g, x_e) < 1e-6
     # the halved dt changed the result (the graph of the old dt was not replayed)
     assert relerr(out[False][4][2], out[False][0][2]) > 1e-6
+
+
+def _descend_reference(rule, d, g, m, v, vmax, lr, b1, b2, eps, t):
+    """PointCloud's descent rules (PointCloud.cpp:83-204) in float32 numpy, on the
+    normalised gradient g; returns the new dFc and moment buffers."""
+    f = np.float32
+    d, g, m, v, vmax = (x.astype(f) for x in (d, g, m, v, vmax))
+    lr, b1, b2, eps = f(lr), f(b1), f(b2), f(eps)
+    if rule in ("adam", "amsgrad"):
+        m = b1 * m + (f(1) - b1) * g
+        v = b2 * v + (f(1) - b2) * g * g
+        c1, c2 = f(1) - b1 ** t, f(1) - b2 ** t
+        if rule == "adam":
+            d = d - lr * ((m / c1) / (np.sqrt(v / c2) + eps))
+        else:
+            vmax = np.maximum(vmax, v / c2)
+            d = d - lr * ((m / c1) / (np.sqrt(vmax) + eps))
+    elif rule == "lion":
+        m = b1 * m + (f(1) - b1) * np.sign(g)
+        d = d - lr * m
+    elif rule == "gd":
+        d = d - lr * g
+    else:  # dldf
+        c = np.clip(g, f(-1), f(1))
+        c = np.where(np.abs(c) < f(1e-3), np.where(c < 0, f(-1e-3), f(1e-3)), c)
+        m = f(0.9) * m + lr * c
+        d = d - m
+    return d, m, v, vmax
+
+
+@pytest.mark.parametrize("rules", [("amsgrad", "amsgrad"), ("lion", "lion"), ("gd", "dldf"), ("adam", "amsgrad")])
+def test_device_descent_rules_match_reference_formulas(gpu_ready, exact_case, rules):
+    """dmpm_descend: Descend_AMSGrad / Descend_Lion / Descend_GradientDescent /
+    Descend_dLdF on the tied control gradient (normalised by its norm), two
+    consecutive steps sharing the moment buffers as MaterialPoint's
+    momentum / vector / vector_max are shared."""
+    sc, o, loss, L = exact_case
+    lr, b1, b2, eps = 1e-2, 0.9, 0.999, 1e-5
+    with make_ctx(sc, "fp32", o.target, adjoint="exact", control="tied") as c:
+        c.setup(L)
+        c.forward(0)
+        c.loss()
+        c.backward(0)
+        g = c.control_grad()
+        d = c.get(0, "dFc")
+        outs = []
+        for t, rule in enumerate(rules, start=1):
+            if rule == "adam":
+                c.adam_step(t=t, lr=lr, beta1=b1, beta2=b2, eps=eps)
+            else:
+                c.descend(rule, lr, t=t, beta1=b1, beta2=b2, eps=eps)
+            outs.append(c.get(0, "dFc"))
+        with pytest.raises(dmpm.DmpmError):
+            c.descend("amsgrad", lr, t=0)
+    gn = (g / np.linalg.norm(g)).astype(np.float32)
+    m = np.zeros_like(gn)
+    v = np.zeros_like(gn)
+    vmax = np.zeros_like(gn)
+    want = d.astype(np.float32)
+    for t, (rule, got) in enumerate(zip(rules, outs), start=1):
+        want, m, v, vmax = _descend_reference(rule, want, gn, m, v, vmax, lr, b1, b2, eps, t)
+        step = want.astype(np.float64) - d
+        assert np.linalg.norm(got - d - step) <= 1e-5 * np.linalg.norm(step), (rule, t)
