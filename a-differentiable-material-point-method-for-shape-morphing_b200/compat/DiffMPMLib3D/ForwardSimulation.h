@@ -20,5 +20,11 @@ void CalculatePointCloudVolumes(PointCloud& curr_point_cloud, Grid& grid);
 // Engine path for the functions above (DMPM_FP32_MIXED by default, or DMPM_FP64).
 void SetEnginePrecision(int precision);
 
+// Mass transfer for headless surfacing (float on the GPU, dmpm_surface_*):
+// node masses of `grid` from points of mass mp_m (ForwardSimulation.cpp:292-327)
+void P2G_Mass(const std::vector<Vec3> points, Grid& grid, float mp_m);
+// grid_2's node masses interpolated from grid_1's (ForwardSimulation.cpp:329-367)
+void G2G_Mass(Grid& grid_1, Grid& grid_2);
+
 }  // namespace SingleThreadMPM
 }  // namespace DiffMPMLib3D

@@ -20,6 +20,7 @@
 #include "DiffMPMLib3D/Elasticity.h"
 #include "DiffMPMLib3D/ForwardSimulation.h"
 #include "DiffMPMLib3D/GeometryLoading.h"
+#include "DiffMPMLib3D/SphereUnionSurfacing.h"
 #include "dmpm.h"
 
 namespace DiffMPMLib3D {
@@ -827,6 +828,71 @@ std::vector<Vec3> GeometryLoading::GeneratePointCloudFromTriangleArrays(const fl
     std::vector<Vec3> pts((size_t)n);
     for (int64_t i = 0; i < n; i++) pts[(size_t)i] = Vec3(buf[3 * i], buf[3 * i + 1], buf[3 * i + 2]);
     return pts;
+}
+
+// ---- headless surfacing (ForwardSimulation.cpp:292-367, SphereUnionSurfacing.cpp:7-128) ----
+
+namespace {
+std::vector<float> grid_masses(const Grid& g) {
+    std::vector<float> m((size_t)g.dim_x * g.dim_y * g.dim_z);
+    size_t q = 0;
+    for (int i = 0; i < g.dim_x; i++)
+        for (int j = 0; j < g.dim_y; j++)
+            for (int k = 0; k < g.dim_z; k++) m[q++] = g.nodes[i][j][k].m;
+    return m;
+}
+void set_grid_masses(Grid& g, const std::vector<float>& m) {
+    size_t q = 0;
+    for (int i = 0; i < g.dim_x; i++)
+        for (int j = 0; j < g.dim_y; j++)
+            for (int k = 0; k < g.dim_z; k++) g.nodes[i][j][k].m = m[q++];
+}
+}  // namespace
+
+void SingleThreadMPM::P2G_Mass(const std::vector<Vec3> points, Grid& grid, float mp_m) {
+    std::vector<float> flat(points.size() * 3);
+    for (size_t i = 0; i < points.size(); i++)
+        for (int c = 0; c < 3; c++) flat[3 * i + c] = points[i][c];
+    const int dims[3] = {grid.dim_x, grid.dim_y, grid.dim_z};
+    std::vector<float> m((size_t)grid.dim_x * grid.dim_y * grid.dim_z);
+    check(nullptr, dmpm_surface_p2g_mass(flat.data(), (int64_t)points.size(), mp_m, dims, grid.dx,
+                                         grid.min_point.data(), m.data()),
+          "dmpm_surface_p2g_mass");
+    set_grid_masses(grid, m);
+}
+
+void SingleThreadMPM::G2G_Mass(Grid& grid_1, Grid& grid_2) {
+    const std::vector<float> m1 = grid_masses(grid_1);
+    const int d1[3] = {grid_1.dim_x, grid_1.dim_y, grid_1.dim_z}, d2[3] = {grid_2.dim_x, grid_2.dim_y, grid_2.dim_z};
+    std::vector<float> m2((size_t)grid_2.dim_x * grid_2.dim_y * grid_2.dim_z);
+    check(nullptr, dmpm_surface_g2g_mass(m1.data(), d1, grid_1.dx, grid_1.min_point.data(), d2, grid_2.dx,
+                                         grid_2.min_point.data(), m2.data()),
+          "dmpm_surface_g2g_mass");
+    set_grid_masses(grid_2, m2);
+}
+
+void SphereUnionSurfaceArrays(const std::vector<Vec3>& points, float radius, float grid_dx, float iso_mass,
+                              int blur_iterations, Vec3 grid_min_point, Vec3 grid_max_point, std::vector<float>& V,
+                              std::vector<int>& F) {
+    int dims[3];
+    check(nullptr, dmpm_surface_grid_dims(grid_min_point.data(), grid_max_point.data(), grid_dx, dims),
+          "dmpm_surface_grid_dims");
+    std::vector<float> flat(points.size() * 3);
+    for (size_t i = 0; i < points.size(); i++)
+        for (int c = 0; c < 3; c++) flat[3 * i + c] = points[i][c];
+    std::vector<float> field((size_t)dims[0] * dims[1] * dims[2]);
+    check(nullptr, dmpm_surface_sphere_field(flat.data(), (int64_t)points.size(), radius, blur_iterations, dims,
+                                             grid_dx, grid_min_point.data(), field.data()),
+          "dmpm_surface_sphere_field");
+    int64_t nv = 0, nf = 0;
+    const int st = dmpm_surface_extract(field.data(), dims, grid_dx, grid_min_point.data(), iso_mass, nullptr, 0,
+                                        nullptr, 0, &nv, &nf);
+    if (st != DMPM_OK && st != DMPM_ERR_TOO_LARGE) check(nullptr, st, "dmpm_surface_extract");
+    V.assign((size_t)nv * 3, 0.f);
+    F.assign((size_t)nf * 3, 0);
+    check(nullptr, dmpm_surface_extract(field.data(), dims, grid_dx, grid_min_point.data(), iso_mass, V.data(), nv,
+                                        F.data(), nf, &nv, &nf),
+          "dmpm_surface_extract");
 }
 
 }  // namespace DiffMPMLib3D

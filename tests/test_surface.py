@@ -138,3 +138,32 @@ def test_gpu_extract_small_cases(gpu_ready):
         assert len(V0) == 0 and len(F0) == 0
     with pytest.raises(dmpm.DmpmError):
         dmpm.extract_surface(f, (n, n, n), -1.0, mn, 0.0)
+
+
+@pytest.mark.gpu
+def test_compat_cpp_surfacing(gpu_ready, gold, tmp_path):
+    """SingleThreadMPM::P2G_Mass / G2G_Mass and SphereUnionMarchingCubesSurfaceFromPointCloud
+    of the C++ compat API (tests/cpp/surface_check.cpp), called as the reference's GUI calls them."""
+    import subprocess
+
+    import build as pkg_build
+
+    repo = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    pkg = os.path.join(repo, "a-differentiable-material-point-method-for-shape-morphing_b200")
+    pkg_build.build_compat()
+    exe = str(tmp_path / "surface_check")
+    subprocess.check_call(["g++", "-std=c++17", "-O2", "-I", os.path.join(pkg, "compat"), "-I",
+                           os.path.join(repo, "include"), os.path.join(repo, "tests", "cpp", "surface_check.cpp"),
+                           "-L", pkg, "-ldmpm_compat", "-ldmpm", "-Wl,-rpath," + pkg, "-o", exe])
+    pf = tmp_path / "pts.f32"
+    gold["points"].tofile(pf)
+    out = tmp_path / "out.bin"
+    subprocess.check_call([exe, str(pf), repr(float(gold["grid_dx"])), repr(float(gold["quality"])),
+                           repr(float(gold["sphere_radius"])), repr(float(gold["sphere_dx"])),
+                           repr(float(gold["sphere_iso"])), str(int(gold["blur"])), str(out)])
+    fine, V, F = osurf.read_blocks(str(out), "ffi")
+    ref = gold["fine_mass"]
+    assert np.abs(fine - ref).max() <= 2e-6 * ref.max()  # P2G_Mass sums with float atomics
+    Vp, Fp = dmpm.sphere_union_surface(gold["points"], gold["sphere_radius"], gold["sphere_dx"], gold["sphere_iso"],
+                                       int(gold["blur"]), gold["box_min"], gold["box_max"])
+    assert np.array_equal(V.reshape(-1, 3), Vp) and np.array_equal(F.reshape(-1, 3), Fp)
