@@ -538,6 +538,30 @@ def mesh_lattice_points(V, F, point_dx: float, min_point=None, max_point=None) -
     return out[: n.value].copy()
 
 
+def mesh_jittered_points(V, F, cell_dx: float, per_axis: int, seed: int, min_point=None, max_point=None) -> np.ndarray:
+    """Jittered stratified points inside a watertight mesh on the GPU
+    (dmpm_mesh_jittered_points): one point per sub-cell of spacing
+    cell_dx / per_axis, kept where the winding number is >= 1/2."""
+    lib = load_library()
+    lib.dmpm_mesh_jittered_points.argtypes = [_P, ctypes.c_int, _P, ctypes.c_int, _P, _P, ctypes.c_float, ctypes.c_int,
+                                              ctypes.c_uint64, _P, ctypes.c_int64, ctypes.POINTER(ctypes.c_int64)]
+    Vf = np.ascontiguousarray(V, dtype=np.float32)
+    Fi = np.ascontiguousarray(F, dtype=np.int32)
+    mn = np.ascontiguousarray(Vf.min(axis=0) if min_point is None else min_point, dtype=np.float32)
+    mx = np.ascontiguousarray(Vf.max(axis=0) if max_point is None else max_point, dtype=np.float32)
+    n = ctypes.c_int64()
+    args = (Vf.ctypes.data, len(Vf), Fi.ctypes.data, len(Fi), mn.ctypes.data, mx.ctypes.data, float(cell_dx),
+            int(per_axis), int(seed) & 0xFFFFFFFFFFFFFFFF)
+    st = lib.dmpm_mesh_jittered_points(*args, None, 0, ctypes.byref(n))
+    if st not in (OK, ERR_TOO_LARGE):
+        raise DmpmError(st, "mesh_jittered_points")
+    out = np.empty((n.value, 3), dtype=np.float32)
+    st = lib.dmpm_mesh_jittered_points(*args, out.ctypes.data, n.value, ctypes.byref(n))
+    if st != OK:
+        raise DmpmError(st, "mesh_jittered_points")
+    return out
+
+
 def read_obj(path: str):
     """Vertices (float32) and triangles (0-based) of the 'v' and 'f' lines of an
     OBJ file; 'f' entries may be v, v/vt, v//vn or v/vt/vn, negative indices

@@ -337,6 +337,18 @@ int dmpm_mesh_lattice_dims(const float* min_point, const float* max_point, float
 int dmpm_mesh_lattice_points(const float* V, int nv, const int* F, int nf, const float* min_point,
                              const float* max_point, float sampling_dx, float* out, int64_t capacity,
                              int64_t* count);
+/* Jittered stratified sampling of the same kind of mesh: the box [min_point,
+ * max_point] is cut into ceil(extent_a / cell_dx) cells per axis a and each
+ * cell into per_axis^3 sub-cells of spacing sdx = cell_dx / per_axis; sub-cell
+ * (i, j, k) (linear index q = (i * n1 + j) * n2 + k over the sub-cell grid)
+ * gets the point min_point + (index + u) * sdx, u_a = (splitmix64(seed + 3 q + a)
+ * >> 40) / 2^24 (SplitMix64's finaliser, Steele et al. 2014; float arithmetic:
+ * index + u, times sdx, plus min), and points with winding number >= 1/2 are
+ * kept in q order.  Not a reference function: the synthetic scenes'
+ * sampling ("jittered stratified, 8 per cell" for per_axis 2) on the GPU. */
+int dmpm_mesh_jittered_points(const float* V, int nv, const int* F, int nf, const float* min_point,
+                              const float* max_point, float cell_dx, int per_axis, uint64_t seed, float* out,
+                              int64_t capacity, int64_t* count);
 
 /* ------------------------------------------------------------------------
  * Surfaces: headless export of a point cloud as a triangle mesh, the GPU

@@ -70,3 +70,39 @@ def lattice_points(V, F, point_dx):
     P = np.stack([X.ravel(), Y.ravel(), Z.ravel()], axis=1)
     keep = winding_numbers(P, V, F) >= 0.5
     return P[keep]
+
+
+_M64 = 0xFFFFFFFFFFFFFFFF
+
+
+def splitmix64(z):
+    """SplitMix64's finaliser (Steele, Lea and Flood 2014) on uint64 arrays."""
+    z = np.asarray(z, dtype=np.uint64)
+    with np.errstate(over="ignore"):
+        z = z + np.uint64(0x9E3779B97F4A7C15)
+        z = (z ^ (z >> np.uint64(30))) * np.uint64(0xBF58476D1CE4E5B9)
+        z = (z ^ (z >> np.uint64(27))) * np.uint64(0x94D049BB133111EB)
+    return z ^ (z >> np.uint64(31))
+
+
+def jittered_points(V, F, cell_dx, per_axis, seed, min_point=None, max_point=None):
+    """dmpm_mesh_jittered_points restated: one point per sub-cell at
+    min + (index + u) * sdx (float32), u from splitmix64(seed + 3 q + axis),
+    kept where the winding number is >= 1/2, in sub-cell order."""
+    V = np.asarray(V, dtype=np.float32)
+    mn = np.asarray(V.min(axis=0) if min_point is None else min_point, dtype=np.float32)
+    mx = np.asarray(V.max(axis=0) if max_point is None else max_point, dtype=np.float32)
+    cdx = np.float32(cell_dx)
+    dims = [int(np.ceil(np.float32(mx[a] - mn[a]) / cdx)) * per_axis for a in range(3)]
+    sdx = np.float32(cdx / np.float32(per_axis))
+    I, J, K = np.meshgrid(*(np.arange(d, dtype=np.int64) for d in dims), indexing="ij")
+    idx = np.stack([I.ravel(), J.ravel(), K.ravel()], axis=1)
+    q = ((idx[:, 0] * dims[1] + idx[:, 1]) * dims[2] + idx[:, 2]).astype(np.uint64)
+    P = np.empty((len(q), 3), dtype=np.float32)
+    with np.errstate(over="ignore"):
+        base = np.uint64(int(seed) & _M64) + np.uint64(3) * q
+        for a in range(3):
+            u = (splitmix64(base + np.uint64(a)) >> np.uint64(40)).astype(np.float32) * np.float32(1.0 / 16777216.0)
+            P[:, a] = mn[a] + (idx[:, a].astype(np.float32) + u) * sdx
+    keep = winding_numbers(P, V, F) >= 0.5
+    return P[keep], dims

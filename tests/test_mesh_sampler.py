@@ -116,3 +116,30 @@ def test_input_file_and_mesh_drive_a_gradient(gpu_ready, tmp_path):
         g = c.control_grad(0)
     assert np.isfinite(loss) and loss > 0
     assert g.shape == (len(pc["x"]), 3, 3) and np.all(np.isfinite(g)) and np.abs(g).max() > 0
+
+
+def test_oracle_jittered_points_stratified():
+    """The restated jittered sampler: every kept point lies in its own sub-cell
+    (one per sub-cell) and the count matches the sphere's volume."""
+    obj, _, _ = _golden("sphere")
+    V, F = omesh.read_obj(obj)
+    cdx, per = 0.09, 2
+    pts, dims = omesh.jittered_points(V, F, cdx, per, seed=1234)
+    mn = V.min(axis=0).astype(np.float32)
+    sdx = np.float32(cdx / per)
+    cell = np.floor((pts - mn) / sdx).astype(np.int64)
+    q = (cell[:, 0] * dims[1] + cell[:, 1]) * dims[2] + cell[:, 2]
+    assert len(np.unique(q)) == len(q)
+    r = (V.max(axis=0) - V.min(axis=0)).mean() / 2
+    vol = 4 / 3 * np.pi * r ** 3
+    assert abs(len(pts) * sdx ** 3 - vol) < 0.05 * vol
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("name,per,seed", [("sphere", 2, 7), ("torus", 3, 2 ** 63 + 5)])
+def test_gpu_jittered_points_match_oracle(gpu_ready, name, per, seed):
+    obj, _, _ = _golden(name)
+    V, F = dmpm.read_obj(obj)
+    want, _ = omesh.jittered_points(V, F, 0.07, per, seed)
+    got = dmpm.mesh_jittered_points(V, F, 0.07, per, seed)
+    assert got.shape == want.shape and np.array_equal(got, want)
