@@ -56,3 +56,26 @@ def test_null_arguments_are_rejected_without_gpu():
     assert lib.dmpm_create(0, 7, None) == dmpm.ERR_ARG
     assert lib.dmpm_destroy(None) == dmpm.ERR_ARG
     assert lib.dmpm_forward(None, 0) == dmpm.ERR_ARG
+
+
+def test_host_only_size_helpers_without_gpu():
+    """The grid-size helpers of the mesh sampler and of the surfacing functions are
+    host arithmetic: the reference's ceil((max - min) / dx) (+ 1 for the sampler's
+    lattice, GeometryLoading.cpp:21-23; the x extent on every axis for the surfacing
+    grids, SphereUnionSurfacing.cpp:13-16), and bad arguments are rejected."""
+    import ctypes
+
+    import numpy as np
+
+    lib = dmpm.load_library()
+    mn = np.float32([-1.0, -0.5, 0.0])
+    mx = np.float32([1.0, 0.5, 0.3])
+    d = np.zeros(3, np.int32)
+    lib.dmpm_mesh_lattice_dims.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_float, ctypes.c_void_p]
+    assert lib.dmpm_mesh_lattice_dims(mn.ctypes.data, mx.ctypes.data, 0.1, d.ctypes.data) == dmpm.OK
+    want = [int(np.ceil(np.float32(mx[a] - mn[a]) / np.float32(0.1))) + 1 for a in range(3)]
+    assert list(d) == want
+    assert lib.dmpm_mesh_lattice_dims(mn.ctypes.data, mx.ctypes.data, -1.0, d.ctypes.data) == dmpm.ERR_ARG
+    assert dmpm.surface_grid_dims(mn, mx, 0.05) == (40, 40, 40)
+    with pytest.raises(dmpm.DmpmError):
+        dmpm.surface_grid_dims(mn, mx, 0.0)

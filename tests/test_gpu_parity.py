@@ -487,6 +487,8 @@ def test_device_descent_rules_match_reference_formulas(gpu_ready, exact_case, ru
             outs.append(c.get(0, "dFc"))
         with pytest.raises(dmpm.DmpmError):
             c.descend("amsgrad", lr, t=0)
+        # an unknown rule is rejected by the C ABI itself
+        assert c.lib.dmpm_descend(c.h, 0, 9, lr, b1, b2, eps, 1, 1) == dmpm.ERR_ARG
     gn = (g / np.linalg.norm(g)).astype(np.float32)
     m = np.zeros_like(gn)
     v = np.zeros_like(gn)

@@ -138,6 +138,17 @@ def test_gpu_extract_small_cases(gpu_ready):
         assert len(V0) == 0 and len(F0) == 0
     with pytest.raises(dmpm.DmpmError):
         dmpm.extract_surface(f, (n, n, n), -1.0, mn, 0.0)
+    # output buffers too small: DMPM_ERR_TOO_LARGE with the sizes needed
+    import ctypes
+
+    lib = dmpm.load_library()
+    d = np.int32([n, n, n])
+    nv, nf = ctypes.c_int64(), ctypes.c_int64()
+    Vs = np.empty((4, 3), np.float32)
+    Fs = np.empty((4, 3), np.int32)
+    st = lib.dmpm_surface_extract(f.ctypes.data, d.ctypes.data, dx, mn.ctypes.data, 0.0, Vs.ctypes.data, 4,
+                                  Fs.ctypes.data, 4, ctypes.byref(nv), ctypes.byref(nf))
+    assert st == dmpm.ERR_TOO_LARGE and (nv.value, nf.value) == (len(V), len(F))
 
 
 @pytest.mark.gpu
