@@ -263,6 +263,26 @@ template <class T> DMPM_HD void polar3(const m3<T>& F, m3<T>& R, m3<T>& S) {
             S.a[i][j] = V.a[i][0] * s[0] * V.a[j][0] + V.a[i][1] * s[1] * V.a[j][1] + V.a[i][2] * s[2] * V.a[j][2];
 }
 
+// one scaled Newton step X <- (z X + c X^-T) / 2, c = cbrt(det X), z = 1 / c;
+// true when the squared change is at most tol times the squared norm
+template <class T> DMPM_HD bool newton_step(m3<T>& X, T tol) {
+    const m3<T> Xit = inv_transpose3(X);
+    const T c = cbrt(det3(X));
+    const T z = T(1) / c;
+    T diff = T(0), nrm = T(0);
+#pragma unroll
+    for (int i = 0; i < 3; i++)
+#pragma unroll
+        for (int j = 0; j < 3; j++) {
+            const T y = T(0.5) * (z * X.a[i][j] + c * Xit.a[i][j]);
+            diff += (y - X.a[i][j]) * (y - X.a[i][j]);
+            nrm += y * y;
+            X.a[i][j] = y;
+        }
+    return diff <= tol * nrm;
+}
+
+
 // Polar decomposition F = R S of a matrix with det F > 0 by the scaled Newton
 // iteration  X <- (z X + X^{-T} / z) / 2,  z = det(X)^{-1/3}  (Higham 1986,
 // determinant scaling), which converges quadratically to the rotation of the
@@ -275,22 +295,10 @@ template <class T> DMPM_HD bool polar_newton(const m3<T>& F, m3<T>& R, m3<T>& S)
     if (!(det3(F) > T(1e-6))) return false;
     m3<T> X = F;
     bool done = false;
-    for (int it = 0; it < 24 && !done; it++) {
-        const m3<T> Xit = inv_transpose3(X);
-        const T c = cbrt(det3(X));  // z = 1 / c
-        const T z = T(1) / c;
-        T diff = T(0), nrm = T(0);
-#pragma unroll
-        for (int i = 0; i < 3; i++)
-#pragma unroll
-            for (int j = 0; j < 3; j++) {
-                const T y = T(0.5) * (z * X.a[i][j] + c * Xit.a[i][j]);
-                diff += (y - X.a[i][j]) * (y - X.a[i][j]);
-                nrm += y * y;
-                X.a[i][j] = y;
-            }
-        done = diff <= T(1e-30) * nrm;  // relative change below 1e-15: converged to rounding
-    }
+    // Near convergence the iteration is quadratic: a step that changes X by a relative
+    // delta leaves an error of about delta^2, so once a step changes X by less than
+    // 1e-9 (squared: 1e-18) X is within FP64 rounding of R.
+    for (int it = 0; it < 24 && !done; it++) done = newton_step<T>(X, T(1e-18));
     if (!done) return false;
     R = X;
     const m3<T> M = mtm(R, F);  // R^T F, symmetric up to rounding
