@@ -15,6 +15,12 @@ void ForwardTimeStep(PointCloud& next_point_cloud, PointCloud& curr_point_cloud,
 void P_op_1(PointCloud& curr_point_cloud);
 void G_Reset(Grid& grid);
 void P2G(const PointCloud& curr_point_cloud, Grid& grid, float dt, float drag);
+// the remaining stages, each one GPU launch over the caller's grid / clouds (dmpm_stage_*)
+void G_op(Grid& grid, float dt, Vec3 f_ext);
+void G_op(Grid& grid, float dt, Vec3 gravity_point, float gravity_mag);
+void G2P(PointCloud& next_point_cloud, const PointCloud& curr_point_cloud, Grid& grid);
+void P_op_2(PointCloud& next_point_cloud, const PointCloud& curr_point_cloud, float dt);
+void P_op_2(PointCloud& next_point_cloud, const PointCloud& curr_point_cloud, float smoothing_factor, float dt);
 void CalculatePointCloudVolumes(PointCloud& curr_point_cloud, Grid& grid);
 
 // Engine path for the functions above (DMPM_FP32_MIXED by default, or DMPM_FP64).

@@ -20,6 +20,7 @@
 #include "DiffMPMLib3D/Elasticity.h"
 #include "DiffMPMLib3D/ForwardSimulation.h"
 #include "DiffMPMLib3D/GeometryLoading.h"
+#include "DiffMPMLib3D/MultiThreadForwardSimulation.h"
 #include "DiffMPMLib3D/SphereUnionSurfacing.h"
 #include "dmpm.h"
 
@@ -519,10 +520,11 @@ void SetEnginePrecision(int precision) { g_stage_precision = precision; }
 
 // Adds this cloud's P2G mass and momentum to the grid (the reference
 // accumulates without resetting, ForwardSimulation.cpp:174-182).  The stress
-// term uses P of F + dFc, evaluated by the engine.
+// term uses P of F + dFc, evaluated by the engine.  Always on the FP64 path,
+// which keeps the momentum (the FP32 path's grid update overwrites it with v).
 void P2G(const PointCloud& pc, Grid& grid, float dt, float drag) {
     if (pc.points.empty()) return;
-    Ctx c(g_stage_precision);
+    Ctx c(DMPM_FP64);
     set_grid(c.h, grid);
     check(c.h, dmpm_set_points_ref(c.h, pc.points.data(), (int)pc.points.size()), "dmpm_set_points_ref");
     std::vector<double> zeros(num_nodes(grid), 0.0);
@@ -540,6 +542,85 @@ void P2G(const PointCloud& pc, Grid& grid, float dt, float drag) {
     });
 }
 
+namespace {
+void grid_arrays(const Grid& g, std::vector<float>& m, std::vector<float>& p, std::vector<float>& v) {
+    const size_t G = num_nodes(g);
+    m.resize(G);
+    p.resize(3 * G);
+    v.resize(3 * G);
+    for_nodes(g, [&](const GridNode& nd, size_t i) {
+        m[i] = nd.m;
+        for (int k = 0; k < 3; k++) {
+            p[3 * i + k] = nd.p[k];
+            v[3 * i + k] = nd.v[k];
+        }
+    });
+}
+void g_op(Grid& grid, float dt, const float* f, const float* gp, float gmag) {
+    std::vector<float> m, p, v;
+    grid_arrays(grid, m, p, v);
+    check(nullptr, dmpm_stage_g_op(grid.dim_x, grid.dim_y, grid.dim_z, grid.dx, grid.min_point.data(), m.data(),
+                                   p.data(), dt, f, gp, gmag, v.data()),
+          "dmpm_stage_g_op");
+    for_nodes(grid, [&](GridNode& nd, size_t i) {
+        for (int k = 0; k < 3; k++) nd.v[k] = v[3 * i + k];
+    });
+}
+}  // namespace
+
+void G_op(Grid& grid, float dt, Vec3 f_ext) { g_op(grid, dt, f_ext.data(), nullptr, 0.f); }
+
+void G_op(Grid& grid, float dt, Vec3 gravity_point, float gravity_mag) {
+    g_op(grid, dt, nullptr, gravity_point.data(), gravity_mag);
+}
+
+void G2P(PointCloud& next, const PointCloud& curr, Grid& grid) {
+    const size_t n = curr.points.size();
+    if (n == 0) return;
+    if (next.points.size() != n) next.points = curr.points;
+    std::vector<float> x(3 * n), gv(3 * num_nodes(grid)), v(3 * n), C(9 * n);
+    for (size_t p = 0; p < n; p++)
+        for (int k = 0; k < 3; k++) x[3 * p + k] = curr.points[p].x[k];
+    for_nodes(grid, [&](const GridNode& nd, size_t i) {
+        for (int k = 0; k < 3; k++) gv[3 * i + k] = nd.v[k];
+    });
+    check(nullptr, dmpm_stage_g2p((int)n, x.data(), grid.dim_x, grid.dim_y, grid.dim_z, grid.dx,
+                                  grid.min_point.data(), gv.data(), v.data(), C.data()),
+          "dmpm_stage_g2p");
+    for (size_t p = 0; p < n; p++) {
+        for (int k = 0; k < 3; k++) next.points[p].v[k] = v[3 * p + k];
+        for (int k = 0; k < 9; k++) next.points[p].C.d[k] = C[9 * p + k];
+    }
+}
+
+void P_op_2(PointCloud& next, const PointCloud& curr, float dt) { P_op_2(next, curr, 0.f, dt); }
+
+void P_op_2(PointCloud& next, const PointCloud& curr, float s, float dt) {
+    const size_t n = next.points.size();
+    if (n == 0) return;
+    std::vector<float> x(3 * n), F(9 * n), D(9 * n), v(3 * n), C(9 * n), xo(3 * n), Fo(9 * n);
+    for (size_t p = 0; p < n; p++) {
+        const MaterialPoint& c = curr.points[p];
+        const MaterialPoint& q = next.points[p];
+        for (int k = 0; k < 3; k++) {
+            x[3 * p + k] = c.x[k];
+            v[3 * p + k] = q.v[k];
+        }
+        for (int k = 0; k < 9; k++) {
+            F[9 * p + k] = c.F.d[k];
+            D[9 * p + k] = c.dFc.d[k];
+            C[9 * p + k] = q.C.d[k];
+        }
+    }
+    check(nullptr, dmpm_stage_p_op_2((int)n, x.data(), F.data(), D.data(), v.data(), C.data(), dt, s, xo.data(),
+                                     Fo.data()),
+          "dmpm_stage_p_op_2");
+    for (size_t p = 0; p < n; p++) {
+        for (int k = 0; k < 3; k++) next.points[p].x[k] = xo[3 * p + k];
+        for (int k = 0; k < 9; k++) next.points[p].F.d[k] = Fo[9 * p + k];
+    }
+}
+
 void CalculatePointCloudVolumes(PointCloud& pc, Grid& grid) {
     if (pc.points.empty()) return;
     P2G(pc, grid, 0.f, 0.f);
@@ -555,6 +636,13 @@ void CalculatePointCloudVolumes(PointCloud& pc, Grid& grid) {
 }
 
 }  // namespace SingleThreadMPM
+
+void MultiThreadMPM::ForwardTimeStep(PointCloud& next, PointCloud& curr, Grid& main_grid,
+                                     std::vector<std::shared_ptr<Grid>>& proxy_grids, float dt, float drag,
+                                     Vec3 f_ext) {
+    (void)proxy_grids;  // per-thread scratch of the CPU version
+    SingleThreadMPM::ForwardTimeStep(next, curr, main_grid, 0.f, dt, drag, f_ext);
+}
 
 // ====================================================================== Back_Timestep (GPU)
 // The engine recomputes layer n's grid from layer n's cloud, which needs the

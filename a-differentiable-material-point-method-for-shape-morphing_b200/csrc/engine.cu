@@ -64,14 +64,23 @@ __global__ void k_unpack_ref(const float* __restrict__ pts, int n, size_t np, T*
     cst[(size_t)KMU * np + p] = (T)m[36];
     for (int q = 0; q < 9; q++) dfc[(size_t)q * np + p] = (T)m[37 + q];
 }
+// Grid fields of one layer.  The stored node holds (p, m), or, where the
+// FP32 path's grid update has overwritten p in place (stored_v), (v, m): then
+// v is read as stored and p is recovered as (v - dt f) m on nodes with
+// |m| > FLT_EPSILON (0 on the others, whose momentum the update discards).
 template <class T>
-__global__ void k_grid_field(const node4<T>* __restrict__ g, size_t G, int field, double dt, double f0, double f1,
-                             double f2, double* out) {
+__global__ void k_grid_field(const node4<T>* __restrict__ g, size_t G, int field, int stored_v, double dt, double f0,
+                             double f1, double f2, double* out) {
     const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= G) return;
     const node4<T> nd = g[i];
     if (field == DMPM_G_M) {
         out[i] = (double)nd.w;
+    } else if (stored_v) {
+        const double f[3] = {f0, f1, f2}, v[3] = {(double)nd.x, (double)nd.y, (double)nd.z};
+        const bool occupied = fabs((double)nd.w) > kFltEps;
+        for (int c = 0; c < 3; c++)
+            out[3 * i + c] = field == DMPM_G_V ? v[c] : (occupied ? (v[c] - dt * f[c]) * (double)nd.w : 0.0);
     } else if (field == DMPM_G_P) {
         out[3 * i] = nd.x; out[3 * i + 1] = nd.y; out[3 * i + 2] = nd.z;
     } else {
@@ -1370,7 +1379,9 @@ template <class T> class Engine : public EngineBase {
                 }
             }
             double* s = staging(3 * G_);
-            k_grid_field<T><<<ggrid(), 256, 0, ctx_->stream>>>(g, G_, field, P.dt, P.f_ext[0], P.f_ext[1], P.f_ext[2], s);
+            const int stored_v = (kWarp && l < L_ - 1) ? 1 : 0;  // the FP32 grid update wrote v over p
+            k_grid_field<T><<<ggrid(), 256, 0, ctx_->stream>>>(g, G_, field, stored_v, P.dt, P.f_ext[0], P.f_ext[1],
+                                                              P.f_ext[2], s);
             launched();
             const size_t cnt = (field == DMPM_G_M) ? G_ : 3 * G_;
             DMPM_CK(cudaMemcpyAsync(out, s, cnt * sizeof(double), cudaMemcpyDeviceToHost, ctx_->stream));

@@ -102,7 +102,10 @@ typedef struct dmpm_ctx dmpm_ctx;
 #define DMPM_F_DLDC_NEXT 16
 #define DMPM_F_DLDFE 19 /* dL/d dFc of the layer (EXACT: differs from dLdF when smoothing != 0) */
 
-/* grid fields (dmpm_get_grid) */
+/* grid fields (dmpm_get_grid).  On the FP32-mixed path the grid update
+ * overwrites each node's momentum with its velocity in place: DMPM_G_V is then
+ * read as stored and DMPM_G_P is recovered as (v - dt f_ext) m on nodes with
+ * |m| > FLT_EPSILON (0 on the others); the FP64 path keeps both exactly. */
 #define DMPM_G_M 0
 #define DMPM_G_V 1
 #define DMPM_G_P 2
@@ -349,6 +352,31 @@ int dmpm_mesh_lattice_points(const float* V, int nv, const int* F, int nf, const
 int dmpm_mesh_jittered_points(const float* V, int nv, const int* F, int nf, const float* min_point,
                               const float* max_point, float cell_dx, int per_axis, uint64_t seed, float* out,
                               int64_t capacity, int64_t* count);
+
+/* ------------------------------------------------------------------------
+ * Single forward stages on caller-held grids and clouds: the reference's
+ * stage-level API (SingleThreadMPM::G_op x2, G2P, P_op_2 x2;
+ * ForwardSimulation.h:29-35), for callers that compose their own steps.  Host
+ * float arrays, 3x3 matrices column-major (9 floats each), grid arrays in node
+ * order (i * dim_y + j) * dim_z + k with node (i, j, k) at min_point + (i, j, k) dx.
+ * Each call allocates its device scratch and synchronises (dmpm_forward runs
+ * the same stages fused, without these copies).
+ *   dmpm_stage_g_op    SingleNode_op over the grid (ForwardSimulation.cpp:53-58, 184-224):
+ *                      v = p / m + dt f where |m| > FLT_EPSILON, v left unchanged elsewhere;
+ *                      f = f_ext, or (gravity_point non-null) gravity_mag times the unit
+ *                      vector from the node to gravity_point (0 where every component of that
+ *                      vector is within 1e-5, Eigen's isZero()); v in/out
+ *   dmpm_stage_g2p     Grid_to_SingleParticle (ForwardSimulation.cpp:60-106):
+ *                      v' = sum w v_g,  C' = 3/dx^2 sum w v_g (x_g - x_p)^T
+ *   dmpm_stage_p_op_2  SingleParticle_op_2 (ForwardSimulation.cpp:108-124):
+ *                      F' = (1 - s)(I + dt C')(F + dFc) + s F,  x' = x + dt v'
+ * ------------------------------------------------------------------------ */
+int dmpm_stage_g_op(int dim_x, int dim_y, int dim_z, float dx, const float* min_point, const float* m, const float* p,
+                    float dt, const float* f_ext, const float* gravity_point, float gravity_mag, float* v);
+int dmpm_stage_g2p(int n, const float* x, int dim_x, int dim_y, int dim_z, float dx, const float* min_point,
+                   const float* grid_v, float* v_out, float* C_out);
+int dmpm_stage_p_op_2(int n, const float* x, const float* F, const float* dFc, const float* v, const float* C,
+                      float dt, float smoothing, float* x_out, float* F_out);
 
 /* ------------------------------------------------------------------------
  * Surfaces: headless export of a point cloud as a triangle mesh, the GPU

@@ -94,3 +94,19 @@ def test_compgraph_cpp_fp32_mixed_close_to_reference(gpu_ready, exe, tmp_path):
     assert abs(r["loss"] - float(g["loss"])) / abs(float(g["loss"])) < 1e-4
     assert relerr(r["x_last"].reshape(-1, 3), g["x_%d" % (ROLLOUT_LAYERS - 1)]) < 1e-5
     assert normrel(cm(r["dLdF0"]), g["dLdF_0"]) < 1e-2
+
+
+def test_stage_level_api_composes_the_fused_step(gpu_ready, tmp_path):
+    """SingleThreadMPM::P_op_1, G_Reset, P2G, G_op, G2P, P_op_2 called one by one
+    (tests/cpp/stages_check.cpp) give the step SingleThreadMPM::ForwardTimeStep
+    gives; MultiThreadMPM::ForwardTimeStep is the step without smoothing; G_op's
+    point-gravity form follows the reference's formula."""
+    import build as pkg_build
+
+    pkg_build.build_compat()
+    exe = str(tmp_path / "stages_check")
+    subprocess.check_call(["g++", "-std=c++17", "-O2", "-I", os.path.join(PKG, "compat"), "-I",
+                           os.path.join(REPO, "include"), os.path.join(REPO, "tests", "cpp", "stages_check.cpp"),
+                           "-L", PKG, "-ldmpm_compat", "-ldmpm", "-Wl,-rpath," + PKG, "-o", exe])
+    res = subprocess.run([exe], capture_output=True, text=True, timeout=300)
+    assert res.returncode == 0, res.stdout + res.stderr

@@ -62,6 +62,22 @@ def test_volumes_and_target_raster(gpu_ready, g64):
             assert np.all(np.isfinite(c.get_grid(1, "grid_dLdm")))
 
 
+def test_fp32_grid_fields_match_reference(gpu_ready, g64, golden_scene):
+    """dmpm_get_grid on the FP32-mixed path, whose grid update overwrites the
+    momentum with the velocity in place: v as stored, p recovered from v and m,
+    both against the reference's grids of the first layers (FP32 tolerances)."""
+    sc = golden_scene
+    with make_ctx(sc, "fp32", g64["target"]) as c:
+        c.setup(ROLLOUT_LAYERS)
+        assert c.forward(0) == dmpm.OK
+        for lay in range(3):
+            m = c.get_grid(lay, "grid_m")
+            assert relerr(m, g64["grid_m_%d" % lay]) < 1e-5, lay
+            assert normrel(c.get_grid(lay, "grid_v"), g64["grid_v_%d" % lay]) < 1e-4, lay
+            occ = np.abs(m) > 1.1920929e-07
+            assert normrel(c.get_grid(lay, "grid_p")[occ], g64["grid_p_%d" % lay][occ]) < 1e-4, lay
+
+
 def test_fp64_forward_matches_reference(gpu_ready, g64, golden_scene):
     sc = golden_scene
     with make_ctx(sc, "fp64", g64["target"], keep_intermediates=True) as c:
