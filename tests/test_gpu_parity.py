@@ -116,6 +116,29 @@ def test_fp64_refcompat_adjoint_matches_reference(gpu_ready, g64, golden_scene):
         assert abs(c.dldf_norm(0) - np.linalg.norm(g64["dLdF_0"])) / np.linalg.norm(g64["dLdF_0"]) < 1e-9
 
 
+def test_fp32_refcompat_inspection_fields(gpu_ready, g64, golden_scene):
+    """The FP32-mixed path's inspection copies (keep_intermediates / keep_adjoints):
+    every particle and grid adjoint field of the first two adjoint steps against the
+    reference's FP64 values, at FP32 tolerances (norm-relative)."""
+    sc = golden_scene
+    with make_ctx(sc, "fp32", g64["target"], keep_adjoints=True, keep_intermediates=True) as c:
+        c.setup(ROLLOUT_LAYERS)
+        c.forward(0)
+        c.loss()
+        assert c.backward(0) == dmpm.OK
+        def close(got, want, what):
+            if not np.any(want):  # e.g. dLdC_next of the top step: the loss zeroes the last layer's dLdC, dLdF
+                assert not np.any(got), what
+            else:
+                assert normrel(got, want) < 2e-3, what
+
+        for lay in (ROLLOUT_LAYERS - 2, ROLLOUT_LAYERS - 3):
+            for k in ("dLdx", "dLdv", "dLdF", "dLdC", "dLdP", "dLdv_next", "dLdC_next"):
+                close(c.get(lay, k), g64["%s_%d" % (k, lay)], (k, lay))
+            for k in ("grid_dLdv", "grid_dLdp", "grid_dLdm"):
+                close(c.get_grid(lay, k), g64["%s_%d" % (k, lay)], (k, lay))
+
+
 def _oracle(sc, L, mode, prec="f64", target=None, control="per_layer"):
     o = OracleGraph(sc, prec, target_m=target)
     o.setup(L, sc.dt, sc.drag, sc.f_ext, sc.smoothing)
