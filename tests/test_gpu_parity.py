@@ -188,6 +188,41 @@ def test_fp32_mixed_matches_fp64_oracle(gpu_ready, exact_case):
         assert normrel(c.get(0, "dLdx"), o.get(0, "dLdx")) < 1e-3
 
 
+def test_particles_at_and_outside_the_grid_boundary(gpu_ready):
+    """A cloud straddling the grid's low corner, some particles up to 1.3 cells
+    outside it, moving outward: stencil nodes outside the grid are skipped, as the
+    reference does (ForwardSimulation.cpp:27-30; Grid.cpp:66-69), and the FP32
+    path's cell keys clamp such particles into border cells.  Both GPU paths
+    against the FP64 oracle, forward and exact adjoint."""
+    sc = scenes.small_scene(seed=13, res=16, radius=0.2, steps=5, v_std=0.4, drag=0.1, smoothing=0.05,
+                            f_ext=(0.0, -1.0, 0.0), offset=(-0.42, -0.42, 0.0))
+    sc.x = sc.x - np.array([1.3, 0.7, 0.0])
+    sc.v[:, 0] -= 0.5
+    assert np.sum(sc.x[:, 0] < 0) > 20 and np.sum(sc.x[:, 0] < -1.0) > 0
+    o = OracleGraph(sc, "f64")
+    sc.vol = o.calc_volumes()
+    L = 6
+    o, loss = _oracle(sc, L, 1)
+    with make_ctx(sc, "fp64", o.target, adjoint="exact", keep_adjoints=True) as c:
+        c.setup(L)
+        assert c.forward(0) == dmpm.OK
+        assert relerr(c.get(L - 1, "x"), o.get(L - 1, "x")) < 1e-10
+        assert relerr(c.get(L - 1, "F"), o.get(L - 1, "F")) < 1e-10
+        assert abs(c.loss() - loss) / abs(loss) < 1e-10
+        assert c.backward(0) == dmpm.OK
+        assert normrel(c.get(0, "dLdFe"), o.get(0, "dLdFe")) < 1e-8
+        assert normrel(c.get(0, "dLdx"), o.get(0, "dLdx")) < 1e-8
+    with make_ctx(sc, "fp32", o.target, adjoint="exact", keep_adjoints=True) as c:
+        c.setup(L)
+        assert c.forward(0) == dmpm.OK
+        assert relerr(c.get(L - 1, "x"), o.get(L - 1, "x")) < 1e-5
+        assert relerr(c.get(L - 1, "F"), o.get(L - 1, "F")) < 1e-4
+        assert abs(c.loss() - loss) / abs(loss) < 1e-4
+        assert c.backward(0) == dmpm.OK
+        assert normrel(c.get(0, "dLdFe"), o.get(0, "dLdFe")) < 1e-3
+        assert normrel(c.get(0, "dLdx"), o.get(0, "dLdx")) < 1e-3
+
+
 def test_fp32_general_path_matches_same_cell_reduction(gpu_ready, exact_case):
     """warp_general disables the same-cell warp reduce-scatter; both paths agree."""
     sc, o, loss, L = exact_case
