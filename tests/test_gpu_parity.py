@@ -223,6 +223,36 @@ def test_particles_at_and_outside_the_grid_boundary(gpu_ready):
         assert normrel(c.get(0, "dLdx"), o.get(0, "dLdx")) < 1e-3
 
 
+@pytest.mark.parametrize("count", [1, 37])
+def test_few_particles_on_a_non_cubic_grid(gpu_ready, count):
+    """One particle, and a count that fills no warp, on a 16 x 12 x 10 grid (the
+    reference's Grid takes any dims; part of the sphere lies beyond z = 10):
+    both GPU paths against the FP64 oracle, forward and exact adjoint."""
+    sc = scenes.small_scene(seed=17, res=16, radius=0.2, steps=4, v_std=0.3, drag=0.1, f_ext=(0.0, -1.0, 0.0))
+    # a compact cluster around the cloud's centre (sparse particles get large volumes
+    # and explode, in the reference as here)
+    keep = np.argsort(np.linalg.norm(sc.x - sc.x.mean(axis=0), axis=1))[:count]
+    for f in ("x", "v", "F", "C", "dFc", "m", "lam", "mu", "vol"):
+        setattr(sc, f, np.ascontiguousarray(getattr(sc, f)[keep]))
+    sc.dims = (16, 12, 10)
+    if count == 1:  # undeformed, so that the lone particle's large volume makes no explosive stress
+        sc.F = np.eye(3)[None].copy()
+        sc.dFc = np.zeros((1, 3, 3))
+    o = OracleGraph(sc, "f64")
+    sc.vol = o.calc_volumes()
+    L = 5
+    o, loss = _oracle(sc, L, 1)
+    for prec, tx, tl, tg in (("fp64", 1e-10, 1e-10, 1e-8), ("fp32", 1e-5, 1e-4, 1e-3)):
+        with make_ctx(sc, prec, o.target, adjoint="exact", keep_adjoints=True) as c:
+            c.setup(L)
+            assert c.forward(0) == dmpm.OK
+            assert relerr(c.get(L - 1, "x"), o.get(L - 1, "x")) < tx, prec
+            assert abs(c.loss() - loss) / abs(loss) < tl, prec
+            assert c.backward(0) == dmpm.OK
+            assert normrel(c.get(0, "dLdFe"), o.get(0, "dLdFe")) < tg, prec
+            assert normrel(c.get(0, "dLdx"), o.get(0, "dLdx")) < tg, prec
+
+
 def test_fp32_general_path_matches_same_cell_reduction(gpu_ready, exact_case):
     """warp_general disables the same-cell warp reduce-scatter; both paths agree."""
     sc, o, loss, L = exact_case
