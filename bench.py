@@ -16,6 +16,7 @@ Our arm (default) prints one JSON line with
              every particle input, forward, loss, adjoint and the read-back of
              the control gradient inside the timed region
   roofline   the dominant kernel's algorithmic bytes / its CUDA-event duration
+  compute    FP32 and FP64 flop rates: ncu-counted flop per particle-step x value
   fp64       the plain FP64 GPU path on the same workload, speedup and
              gradient relative error of the FP32-mixed path against it
   cpu_baseline the reference's own CPU code (oracle/_ref) on a bounded sample
@@ -229,6 +230,22 @@ PER_PARTICLE_BYTES = {
 PER_TOUCHED_NODE_BYTES = {"p2g": 16, "g2p_p_op2": 16, "adj_g2p_scatter": 16, "adj_p2g_gather": 32,
                           "p2g_mass": 4, "loss_dldx": 4}
 PER_GRID_NODE_BYTES = {"g_op": 32, "adj_g_op": 64}
+
+# Executed flop per particle-step of the six hot kernels (add + mul + 2 fma over the predicated-on
+# thread instructions), counted by ncu on the 64^3, 266,868-particle workload
+# (profiles/flops_atomics_hot_kernels_64cubed_267k.txt); it includes the warp-item layout's redundant
+# weight evaluations.  Nominal vector peaks: 148 SMs x 128 FP32 / 64 FP64 lanes x 2 at 1965 MHz.
+FLOP_PER_PARTICLE_STEP = {"fp32": 11364, "fp64": 1187}
+NOMINAL_VECTOR_TFLOPS = {"fp32": 148 * 128 * 2 * 1.965e-3, "fp64": 148 * 64 * 2 * 1.965e-3}
+
+
+def compute_rates(particle_steps_per_s: float) -> dict:
+    out = {"source": "ncu-counted flop per particle-step x measured particle-steps/s, per GPU"}
+    for p, f in FLOP_PER_PARTICLE_STEP.items():
+        tf = particle_steps_per_s * f / 1e12
+        out[p] = {"flop_per_particle_step": f, "tflops": tf, "nominal_tflops": NOMINAL_VECTOR_TFLOPS[p],
+                  "frac": tf / NOMINAL_VECTOR_TFLOPS[p]}
+    return out
 
 
 def algorithmic_bytes(kernel: str, n: int, touched: int, nodes: int) -> float:
@@ -457,8 +474,8 @@ def run_ours(args):
                 "dtype": "f32 (f64 polar/SVD, stress derivative, loss and gradient sums)", "data": "synthetic",
                 "config": workload_config(sc, dt_sub, ckpt),
                 "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
-                "gpu_launches": launches, "roofline": roof, "cpu_baseline": cb, "clocks": clocks, "fp64": fp64,
-                "kernels": kern, "ms_per_step_profiled": ms_prof / args.steps}
+                "gpu_launches": launches, "roofline": roof, "compute": compute_rates(value / world), "cpu_baseline": cb,
+                "clocks": clocks, "fp64": fp64, "kernels": kern, "ms_per_step_profiled": ms_prof / args.steps}
         print(json.dumps(line), flush=True)
     if world > 1:
         import torch.distributed as dist
