@@ -425,6 +425,16 @@ def test_errors_are_reported(gpu_ready):
     with pytest.raises(dmpm.DmpmError) as e:
         c.backward(0)
     assert e.value.status == dmpm.ERR_STATE
+    # an empty cloud is an argument error (there is nothing to differentiate) and
+    # leaves the uploaded cloud and its layers in place
+    z = np.zeros((0, 3))
+    for call in (lambda: c.set_particles(z, z[:, 0], z[:, 0], z[:, 0]),
+                 lambda: c.set_points_ref(np.zeros((0, 118), np.float32))):
+        with pytest.raises(dmpm.DmpmError) as e:
+            call()
+        assert e.value.status == dmpm.ERR_ARG
+    assert c.forward(0) == dmpm.OK
+    assert np.all(np.isfinite(c.get(2, "x")))
     c.close()
 
 
