@@ -18,6 +18,12 @@ Fixtures:
                             per-layer particle state and grids after
                             ComputeForwardPass, EndLayerMassLoss, and every
                             layer's adjoint after ComputeBackwardPass(0).
+  rollout_long_f64.npz      a second seeded sphere (459 particles, 12^3 grid)
+                            rolled out for 1, 10, 30 and 100 steps by the FP64
+                            build: the last layer's x, v, F, the loss and the
+                            layer-0 adjoint (dLdx, dLdv, dLdF, dLdC) of each.  The
+                            reference's adjoint grows about twofold per step, to
+                            ~1e21 at 100 steps.
 """
 from __future__ import annotations
 
@@ -115,6 +121,34 @@ def make_rollout(prec):
     np.savez_compressed(os.path.join(HERE, "rollout_%s.npz" % prec), **out)
 
 
+LONG_STEPS = (1, 10, 30, 100)
+
+
+def long_scene():
+    return scenes.small_scene(seed=31, res=12, radius=0.2, steps=max(LONG_STEPS), v_std=0.3, drag=0.1,
+                              smoothing=0.05, f_ext=(0.0, -1.0, 0.0))
+
+
+def make_rollout_long():
+    sc = long_scene()
+    r = RefGraph(sc, "f64")
+    vol = r.calc_volumes()
+    target = r.target_mass()
+    sc.vol = vol.astype(np.float64)
+    out = {"vol": vol, "target": target}
+    for S in LONG_STEPS:
+        r = RefGraph(sc, "f64", target_m=target)
+        r.setup(S + 1, sc.dt, sc.drag, sc.f_ext, sc.smoothing)
+        r.forward(0)
+        out["loss_%d" % S] = np.array(r.loss())
+        for k in ("x", "v", "F"):
+            out["%s_%d" % (k, S)] = r.get(S, k)
+        r.backward(0)
+        for k in ("dLdx", "dLdv", "dLdF", "dLdC"):
+            out["%s0_%d" % (k, S)] = r.get(0, k)
+    np.savez_compressed(os.path.join(HERE, "rollout_long_f64.npz"), **out)
+
+
 def mpmbin_scene():
     return scenes.small_scene(seed=77, res=8, radius=0.25, v_std=0.3)
 
@@ -135,5 +169,7 @@ if __name__ == "__main__":
         make_elementary(prec)
         make_rollout(prec)
         print("wrote", prec)
+    make_rollout_long()
+    print("wrote rollout_long_f64")
     make_mpmbin()
     print("wrote cloud_ref.mpmbin")

@@ -9,6 +9,8 @@ Tolerances (relative, max-abs over the field / max-abs of the reference):
   FP32 mixed path vs FP64 oracle:     positions 1e-5, deformation 1e-4,
                                       velocities/grid 1e-3, loss 1e-4,
                                       exact control gradient 1e-3 (norm-relative).
+  Long RefCompat rollouts (1-100 steps):  FP64 1e-10 state, 1e-9 adjoint;
+                                      FP32-mixed adjoint 3e-4 norm-relative.
 """
 import numpy as np
 import pytest
@@ -114,6 +116,38 @@ def test_fp64_refcompat_adjoint_matches_reference(gpu_ready, g64, golden_scene):
             for k in ("grid_dLdv", "grid_dLdp", "grid_dLdm"):
                 assert relerr(c.get_grid(lay, k), g64["%s_%d" % (k, lay)]) < 1e-9, (k, lay)
         assert abs(c.dldf_norm(0) - np.linalg.norm(g64["dLdF_0"])) / np.linalg.norm(g64["dLdF_0"]) < 1e-9
+
+
+@pytest.mark.parametrize("steps", [1, 10, 30, 100])
+@pytest.mark.parametrize("prec", ["fp64", "fp32"])
+def test_long_rollouts_match_reference(gpu_ready, prec, steps):
+    """RefCompat rollouts of 1 to 100 steps against the reference's FP64 build
+    (rollout_long_f64): the last layer's state, the loss and the layer-0 adjoint,
+    which the reference's adjoint grows about twofold per step (to ~1e21).
+    Measured on a B200: FP64 loss 2e-14, state <= 5.1e-12, adjoint <= 1.3e-10;
+    FP32-mixed loss <= 2.1e-8, x <= 1.0e-6, F <= 4.8e-6, v <= 4.7e-5, adjoint
+    <= 4.4e-5 norm-relative (at 100 steps)."""
+    from tests.golden.make_golden import long_scene
+
+    g = load_golden("rollout_long_f64")
+    sc = long_scene()
+    sc.vol = np.asarray(g["vol"], dtype=np.float64)
+    fp64 = prec == "fp64"
+    with make_ctx(sc, prec, g["target"], keep_adjoints=True) as c:
+        c.setup(steps + 1)
+        assert c.forward(0) == dmpm.OK
+        loss = c.loss()
+        assert c.backward(0) == dmpm.OK
+        want = float(g["loss_%d" % steps])
+        assert abs(loss - want) / abs(want) < (1e-12 if fp64 else 1e-6)
+        for k, tol32 in (("x", 1e-5), ("F", 1e-4), ("v", 1e-3)):
+            assert relerr(c.get(steps, k), g["%s_%d" % (k, steps)]) < (1e-10 if fp64 else tol32), k
+        for k in ("dLdx", "dLdv", "dLdF", "dLdC"):
+            got, ref = c.get(0, k), g["%s0_%d" % (k, steps)]
+            if fp64:
+                assert relerr(got, ref) < 1e-9, k
+            else:
+                assert normrel(got, ref) < 3e-4, k
 
 
 def test_fp32_refcompat_inspection_fields(gpu_ready, g64, golden_scene):

@@ -86,6 +86,30 @@ def test_rollout_fp32(golden):
     assert relerr(o.get(0, "dLdx"), g["dLdx_0"]) < 1e-3
 
 
+@pytest.mark.parametrize("steps", [1, 10, 30, 100])
+def test_long_rollouts_fp64(golden, steps):
+    """RefCompat rollouts of 1 to 100 steps against the reference's FP64 build:
+    the last layer's state, the loss and the layer-0 adjoint (which the
+    reference's adjoint grows to ~1e21 over 100 steps).  Measured: loss
+    <= 2.1e-16, x and F <= 7.3e-14, v <= 4.6e-12 (the grid velocity p/m of
+    nearly empty nodes), adjoint <= 1.1e-10 (at 100 steps)."""
+    from tests.golden.make_golden import long_scene
+
+    g = golden("rollout_long_f64")
+    sc = long_scene()
+    sc.vol = np.asarray(g["vol"], dtype=np.float64)
+    o = OracleGraph(sc, "f64", target_m=g["target"])
+    o.setup(steps + 1, sc.dt, sc.drag, sc.f_ext, sc.smoothing)
+    o.forward(0)
+    loss = o.loss()
+    o.backward(0, 0)
+    assert abs(loss - float(g["loss_%d" % steps])) / abs(float(g["loss_%d" % steps])) < 1e-12
+    for k in ("x", "v", "F"):
+        assert relerr(o.get(steps, k), g["%s_%d" % (k, steps)]) < 1e-10, k
+    for k in ("dLdx", "dLdv", "dLdF", "dLdC"):
+        assert relerr(o.get(0, k), g["%s0_%d" % (k, steps)]) < 1e-9, k
+
+
 @pytest.mark.parametrize("mode", ["layer0", "tied"])
 def test_exact_adjoint_matches_central_fd(mode):
     """The oracle's exact adjoint against central differences in FP64."""
