@@ -24,6 +24,9 @@ Fixtures:
                             layer-0 adjoint (dLdx, dLdv, dLdF, dLdC) of each.  The
                             reference's adjoint grows about twofold per step, to
                             ~1e21 at 100 steps.
+  rollout_long_f32.npz      the same rollouts by the shipped FP32 build (same
+                            volumes and target), the float reference's own drift
+                            from the FP64 build.
 """
 from __future__ import annotations
 
@@ -130,23 +133,25 @@ def long_scene():
 
 
 def make_rollout_long():
+    """Both builds on the same inputs: volumes and target from the FP64 build."""
     sc = long_scene()
     r = RefGraph(sc, "f64")
     vol = r.calc_volumes()
     target = r.target_mass()
     sc.vol = vol.astype(np.float64)
-    out = {"vol": vol, "target": target}
-    for S in LONG_STEPS:
-        r = RefGraph(sc, "f64", target_m=target)
-        r.setup(S + 1, sc.dt, sc.drag, sc.f_ext, sc.smoothing)
-        r.forward(0)
-        out["loss_%d" % S] = np.array(r.loss())
-        for k in ("x", "v", "F"):
-            out["%s_%d" % (k, S)] = r.get(S, k)
-        r.backward(0)
-        for k in ("dLdx", "dLdv", "dLdF", "dLdC"):
-            out["%s0_%d" % (k, S)] = r.get(0, k)
-    np.savez_compressed(os.path.join(HERE, "rollout_long_f64.npz"), **out)
+    for prec in ("f64", "f32"):
+        out = {"vol": vol, "target": target} if prec == "f64" else {}
+        for S in LONG_STEPS:
+            r = RefGraph(sc, prec, target_m=target)
+            r.setup(S + 1, sc.dt, sc.drag, sc.f_ext, sc.smoothing)
+            r.forward(0)
+            out["loss_%d" % S] = np.array(r.loss())
+            for k in ("x", "v", "F"):
+                out["%s_%d" % (k, S)] = r.get(S, k)
+            r.backward(0)
+            for k in ("dLdx", "dLdv", "dLdF", "dLdC"):
+                out["%s0_%d" % (k, S)] = r.get(0, k)
+        np.savez_compressed(os.path.join(HERE, "rollout_long_%s.npz" % prec), **out)
 
 
 def mpmbin_scene():
@@ -170,6 +175,6 @@ if __name__ == "__main__":
         make_rollout(prec)
         print("wrote", prec)
     make_rollout_long()
-    print("wrote rollout_long_f64")
+    print("wrote rollout_long_f64, rollout_long_f32")
     make_mpmbin()
     print("wrote cloud_ref.mpmbin")
