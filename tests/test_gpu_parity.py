@@ -396,9 +396,14 @@ def test_tied_controls_gradient_is_sum_over_layers(gpu_ready, exact_case):
 
 
 @pytest.mark.parametrize("k", [2, 3])
-def test_checkpointing_matches_store_all(gpu_ready, exact_case, k):
+@pytest.mark.parametrize("prec", ["fp64", "fp32"])
+def test_checkpointing_matches_store_all(gpu_ready, exact_case, prec, k):
+    """Checkpoints every k layers: the backward pass recomputes each segment, and
+    reading a layer that is not stored (layer 3) recomputes it from the segment's
+    checkpoint.  Against the FP64 oracle's store-all run (FP32-mixed at its own
+    tolerances: recomputation reorders its float atomics)."""
     sc, o, loss, L = exact_case
-    with make_ctx(sc, "fp64", o.target, adjoint="exact", control="tied", checkpoint_every=k) as c:
+    with make_ctx(sc, prec, o.target, adjoint="exact", control="tied", checkpoint_every=k) as c:
         c.setup(L)
         assert c.info()["checkpoint_every"] == k
         c.forward(0)
@@ -406,9 +411,18 @@ def test_checkpointing_matches_store_all(gpu_ready, exact_case, k):
         c.backward(0)
         g = c.control_grad()
         x3 = c.get(3, "x")
-    assert abs(lo - loss) / abs(loss) < 1e-10
-    assert relerr(g, sum(o.get(j, "dLdFe") for j in range(L - 1))) < 1e-9
-    assert relerr(x3, o.get(3, "x")) < 1e-10
+        F3 = c.get(3, "F")
+    want = sum(o.get(j, "dLdFe") for j in range(L - 1))
+    if prec == "fp64":
+        assert abs(lo - loss) / abs(loss) < 1e-10
+        assert relerr(g, want) < 1e-9
+        assert relerr(x3, o.get(3, "x")) < 1e-10
+        assert relerr(F3, o.get(3, "F")) < 1e-10
+    else:
+        assert abs(lo - loss) / abs(loss) < 1e-4
+        assert normrel(g, want) < 1e-3
+        assert relerr(x3, o.get(3, "x")) < 1e-5
+        assert relerr(F3, o.get(3, "F")) < 1e-4
 
 
 def test_fd_gradient_on_gpu_fp64(gpu_ready):
