@@ -41,11 +41,11 @@ constexpr int kDefaultTileCap = 1024;
 // (dmpm_set_profiling / dmpm_kernel_stats).
 enum KernelId {
     K_P_OP1 = 0, K_P2G, K_GOP, K_G2P, K_MASS, K_NODE_LOSS, K_LOSS_DLDX, K_ADJ_SCATTER, K_ADJ_GOP, K_ADJ_GATHER,
-    K_ADJ_FINALIZE, K_COUNT
+    K_ADJ_FINALIZE, K_ADJ_TRANSPORT, K_COUNT
 };
 const char* const kKernelNames[K_COUNT] = {"p_op1", "p2g", "g_op", "g2p_p_op2", "p2g_mass", "node_loss",
                                           "loss_dldx", "adj_g2p_scatter", "adj_g_op", "adj_p2g_gather",
-                                          "adj_finalize"};
+                                          "adj_finalize", "adj_finalize_transport"};
 constexpr int kDefaultSortEvery = 8;
 // per-layer auxiliary planes of the FP32 path: G (9), polar R (9), polar S (6)
 constexpr int kAuxPlanes = 24;
@@ -1097,10 +1097,33 @@ template <class T> class Engine : public EngineBase {
             else k_adj_gather_w<false, ITEMS_PERSISTENT><<<wg, 256, 0, ctx_->stream>>>(a);
             launched();
             pend();
-            pbeg(K_ADJ_FINALIZE);
-            launch_finalize(a, ex, ctx_->stream);
-            launched();
-            pend();
+            if (DMPM_SPLIT_FINALIZE && !prof_) {
+                // fork: the transport part on the side stream after the gather,
+                // join: the main stream continues after both parts
+                side_stream();
+                DMPM_CK(cudaEventRecord(ev_fork_, ctx_->stream));
+                DMPM_CK(cudaStreamWaitEvent(side_, ev_fork_, 0));
+                launch_finalize_split(a, ex, ctx_->stream, side_);
+                launched();
+                launched();
+                DMPM_CK(cudaEventRecord(ev_join_, side_));
+                DMPM_CK(cudaStreamWaitEvent(ctx_->stream, ev_join_, 0));
+            } else if (DMPM_SPLIT_FINALIZE) {
+                // profiled: the two parts one after the other, each timed
+                pbeg(K_ADJ_TRANSPORT);
+                launch_finalize_split(a, ex, nullptr, ctx_->stream, FIN_TRANSPORT);
+                launched();
+                pend();
+                pbeg(K_ADJ_FINALIZE);
+                launch_finalize_split(a, ex, ctx_->stream, nullptr, FIN_STRESS);
+                launched();
+                pend();
+            } else {
+                pbeg(K_ADJ_FINALIZE);
+                launch_finalize(a, ex, ctx_->stream);
+                launched();
+                pend();
+            }
             return;
         }
         AdjArgs<T> a{};
@@ -1452,9 +1475,25 @@ template <class T> class Engine : public EngineBase {
         harvest();
         for (cudaEvent_t e : event_pool_) cudaEventDestroy(e);
         if (host_misc_) cudaFreeHost(host_misc_);
+        if (side_) {
+            cudaStreamSynchronize(side_);
+            cudaStreamDestroy(side_);
+            cudaEventDestroy(ev_fork_);
+            cudaEventDestroy(ev_join_);
+        }
+    }
+
+    // second stream (and its fork/join events) for work that runs beside the main stream
+    void side_stream() {
+        if (side_) return;
+        DMPM_CK(cudaStreamCreateWithFlags(&side_, cudaStreamNonBlocking));
+        DMPM_CK(cudaEventCreateWithFlags(&ev_fork_, cudaEventDisableTiming));
+        DMPM_CK(cudaEventCreateWithFlags(&ev_join_, cudaEventDisableTiming));
     }
 
    private:
+    cudaStream_t side_ = nullptr;
+    cudaEvent_t ev_fork_ = nullptr, ev_join_ = nullptr;
     struct LayerSlots {
         T* G = nullptr;
         T* st = nullptr;

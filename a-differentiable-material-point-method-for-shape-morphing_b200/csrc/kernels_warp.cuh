@@ -878,7 +878,13 @@ struct FinGlobal {
     }
     __device__ __forceinline__ double acc(int i) const { return a->ctrl_acc[(size_t)i * a->np + p]; }
 };
-template <bool EXACT, class In> __device__ __forceinline__ void finalize_particle(const WArgs& a, int p, const In& in) {
+// PART selects what one launch computes: 0 everything; FIN_STRESS the FP64 part
+// (P, dP/dF:dLdP, dLdF, the control gradient); FIN_TRANSPORT the FP32 outputs
+// dLdx, dLdv, dLdC, which need neither the polar factors nor dLdF.
+enum : int { FIN_ALL = 0, FIN_STRESS = 1, FIN_TRANSPORT = 2 };
+template <bool EXACT, class In, int PART = FIN_ALL>
+__device__ __forceinline__ void finalize_particle(const WArgs& a, int p, const In& in) {
+    constexpr bool kStress = PART != FIN_TRANSPORT, kTransport = PART != FIN_STRESS;
     const size_t np = a.np, npl = a.npl;
     auto mat = [&](int slot) {  // 9 column-major planes -> m3
         m3<float> m;
@@ -893,6 +899,37 @@ template <bool EXACT, class In> __device__ __forceinline__ void finalize_particl
     for (int r = 0; r < 3; r++)
 #pragma unroll
         for (int c = 0; c < 3; c++) M.a[r][c] = in(FS_GATH + 3 * r + c);
+    const float dx = (float)a.geo.dx;
+    const float k3 = 3.f / (dx * dx);
+    // dLdx = -X/dx - G^T u - 3/dx^2 dLdC_next^T z + dLdx',  dLdv = m (1 - dt drag) u,  dLdC = m M^T
+    auto transport = [&]() {
+        const float mp = in(FS_CST + KM);
+        const m3<float> G = mat(FS_AUX);
+        const m3<float> Cn = mat(FS_CN);
+        float u[3], z[3], gtu[3], ctz[3];
+#pragma unroll
+        for (int c = 0; c < 3; c++) {
+            u[c] = in(FS_GATH + 12 + c);
+            z[c] = in(FS_GATH + 15 + c);
+        }
+        mtv(G, u, gtu);
+        mtv(Cn, z, ctz);
+        float ax0 = 0.f;
+#pragma unroll
+        for (int c = 0; c < 3; c++) {
+            const float X = in(FS_GATH + 9 + c);
+            const float ax = -X / dx - gtu[c] - k3 * ctz[c] + in(FS_AX + c);
+            if (c == 0) ax0 = ax;
+            a.adj[(size_t)(PX + c) * npl + p] = ax;
+            a.adj[(size_t)(PV + c) * npl + p] = mp * (1.f - a.dt * a.drag) * u[c];
+        }
+        store_m3(a.adj + (size_t)PC * npl, npl, p, mp * transpose(M));
+        return ax0;
+    };
+    if constexpr (!kStress) {
+        if (!isfinite(transport())) atomicOr(a.status, ST_NONFINITE_ADJ);
+        return;
+    }
     const m3<float> Fe = mat(FS_F) + mat(FS_DFC);
     const m3<double> Fed = m3_cast<double>(Fe);
     // polar factors computed in FP64 by k_stress for this layer
@@ -906,32 +943,12 @@ template <bool EXACT, class In> __device__ __forceinline__ void finalize_particl
     Sd.a[2][2] = in(FS_AUX + 23);
     const double lam = (double)in(FS_CST + KLAM), mu = (double)in(FS_CST + KMU);
     const m3<float> P = m3_cast<float>(pk_from_polar(Fed, Rd, lam, mu));
-    const float mp = in(FS_CST + KM), vol = in(FS_CST + KVOL);
-    const float dx = (float)a.geo.dx;
-    const float k3 = 3.f / (dx * dx);
+    const float vol = in(FS_CST + KVOL);
     const float kk = -k3 * a.dt * vol;
     const m3<float> dLdP = kk * mtm(M, Fe);
     const m3<float> dFstress = kk * (M * P);
-    const m3<float> G = mat(FS_AUX);
-    const m3<float> Cn = mat(FS_CN);
-    float u[3], z[3], gtu[3], ctz[3];
-#pragma unroll
-    for (int c = 0; c < 3; c++) {
-        u[c] = in(FS_GATH + 12 + c);
-        z[c] = in(FS_GATH + 15 + c);
-    }
-    mtv(G, u, gtu);
-    mtv(Cn, z, ctz);
     float ax0 = 0.f;
-#pragma unroll
-    for (int c = 0; c < 3; c++) {
-        const float X = in(FS_GATH + 9 + c);
-        const float ax = -X / dx - gtu[c] - k3 * ctz[c] + in(FS_AX + c);
-        if (c == 0) ax0 = ax;
-        a.adj[(size_t)(PX + c) * npl + p] = ax;
-        a.adj[(size_t)(PV + c) * npl + p] = mp * (1.f - a.dt * a.drag) * u[c];
-    }
-    store_m3(a.adj + (size_t)PC * npl, npl, p, mp * transpose(M));
+    if constexpr (kTransport) ax0 = transport();
     const m3<float> Cnext = mat(FS_CNEXT);
     const m3<float> dFn = mat(FS_AF);
     const m3<float> Tr = mtm(m3_eye<float>() + a.dt * Cnext, dFn);
@@ -960,10 +977,15 @@ template <bool EXACT, class In> __device__ __forceinline__ void finalize_particl
 // one thread per particle, inputs read from global memory (the REFCOMPAT
 // variant, with its finite-difference dJFit, keeps the compiler's own
 // register budget)
-template <bool EXACT>
+template <bool EXACT, int PART = FIN_ALL>
 __global__ void __launch_bounds__(128, EXACT ? DMPM_FINALIZE_MIN_BLOCKS : 1) k_adj_finalize(WArgs a) {
     const int p = blockIdx.x * blockDim.x + threadIdx.x;
-    if (p < a.n) finalize_particle<EXACT>(a, p, FinGlobal{&a, p});
+    if (p < a.n) finalize_particle<EXACT, FinGlobal, PART>(a, p, FinGlobal{&a, p});
+}
+// the transport part alone: few registers, many resident warps
+static __global__ void __launch_bounds__(256) k_adj_finalize_transport(WArgs a) {
+    const int p = blockIdx.x * blockDim.x + threadIdx.x;
+    if (p < a.n) finalize_particle<true, FinGlobal, FIN_TRANSPORT>(a, p, FinGlobal{&a, p});
 }
 
 // host side: one thread per particle (a variant that first staged each
@@ -976,6 +998,26 @@ inline void launch_finalize(const WArgs& a, bool exact, cudaStream_t st) {
     const unsigned b = (unsigned)((a.n + 127) / 128);
     if (exact) k_adj_finalize<true><<<b, 128, 0, st>>>(a);
     else k_adj_finalize<false><<<b, 128, 0, st>>>(a);
+}
+// The single-scene engine runs the finalize as the two launches below, the
+// transport part on a second stream beside the FP64 part: the FP64 part keeps
+// 128 registers per thread and 16 warps per SM, and the transport part's warps
+// (60 registers) fill the rest of the SMs meanwhile (60.0 against 60.9 ms per
+// gradient evaluation on the 64^3, 267k-particle workload).  0 runs the
+// single kernel.
+#ifndef DMPM_SPLIT_FINALIZE
+#define DMPM_SPLIT_FINALIZE 1
+#endif
+// the same work as two launches: the FP64 part on st, the transport part on
+// side; `parts` selects one of them (FIN_STRESS, FIN_TRANSPORT) or both (FIN_ALL)
+inline void launch_finalize_split(const WArgs& a, bool exact, cudaStream_t st, cudaStream_t side,
+                                  int parts = FIN_ALL) {
+    if (a.n <= 0) return;
+    const unsigned b = (unsigned)((a.n + 127) / 128);
+    if (parts != FIN_STRESS) k_adj_finalize_transport<<<(unsigned)((a.n + 255) / 256), 256, 0, side>>>(a);
+    if (parts == FIN_TRANSPORT) return;
+    if (exact) k_adj_finalize<true, FIN_STRESS><<<b, 128, 0, st>>>(a);
+    else k_adj_finalize<false, FIN_STRESS><<<b, 128, 0, st>>>(a);
 }
 
 }  // namespace dmpm

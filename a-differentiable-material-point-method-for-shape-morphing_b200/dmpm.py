@@ -31,7 +31,7 @@ FIELDS = {"x": 0, "v": 1, "F": 2, "C": 3, "P": 4, "m": 5, "vol": 6, "lam": 7, "m
 WIDTH = {"x": 3, "v": 3, "F": 9, "C": 9, "P": 9, "m": 1, "vol": 1, "lam": 1, "mu": 1, "dFc": 9, "dLdx": 3,
          "dLdv": 3, "dLdF": 9, "dLdC": 9, "dLdP": 9, "dLdv_next": 3, "dLdC_next": 9, "dLdFe": 9}
 GRID_FIELDS = {"grid_m": 0, "grid_v": 1, "grid_p": 2, "grid_dLdv": 3, "grid_dLdp": 4, "grid_dLdm": 5}
-NUM_KERNEL_IDS = 11
+NUM_KERNEL_IDS = 12
 GRID_WIDTH = {"grid_m": 1, "grid_v": 3, "grid_p": 3, "grid_dLdv": 3, "grid_dLdp": 3, "grid_dLdm": 1}
 
 

@@ -259,7 +259,7 @@ int dmpm_compute_volumes_noalloc(int n, const float* x, const float* m, int dim_
  * the summed milliseconds and the launch count of one kernel since profiling
  * was (re)enabled.  Kernel ids run from 0 to DMPM_NUM_KERNEL_IDS - 1;
  * dmpm_kernel_name gives their names (p2g, g2p_p_op2, adj_p2g_gather, ...). */
-#define DMPM_NUM_KERNEL_IDS 11
+#define DMPM_NUM_KERNEL_IDS 12
 int dmpm_set_profiling(dmpm_ctx* ctx, int on);
 int dmpm_kernel_stats(dmpm_ctx* ctx, int kernel_id, double* total_ms, int64_t* launches);
 const char* dmpm_kernel_name(int kernel_id);
