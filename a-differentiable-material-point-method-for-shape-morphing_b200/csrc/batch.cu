@@ -105,6 +105,10 @@ struct BEpoch {
 struct dmpm_batch {
     int device = 0;
     cudaStream_t stream = nullptr;
+    // second stream for the finalize's transport part, forked from and joined
+    // back into stream by the two events
+    cudaStream_t side = nullptr;
+    cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
     std::string err;
     struct Impl;
     std::unique_ptr<Impl> impl;
@@ -561,8 +565,13 @@ struct dmpm_batch::Impl {
         if (ex) k_adj_gather_w<true, ITEMS_BATCH><<<wb, 256, 0, b->stream>>>(a);
         else k_adj_gather_w<false, ITEMS_BATCH><<<wb, 256, 0, b->stream>>>(a);
         launched();
-        launch_finalize(a, ex, b->stream);
+        DMPM_CK(cudaEventRecord(b->ev_fork, b->stream));
+        DMPM_CK(cudaStreamWaitEvent(b->side, b->ev_fork, 0));
+        launch_finalize_split(a, ex, b->stream, b->side);
         launched();
+        launched();
+        DMPM_CK(cudaEventRecord(b->ev_join, b->side));
+        DMPM_CK(cudaStreamWaitEvent(b->stream, b->ev_join, 0));
     }
 
     // the whole gradient evaluation, enqueued on the stream (capturable: no
@@ -760,6 +769,13 @@ int dmpm_batch_create(int device, int count, const dmpm_instance* instances, dmp
         delete b;
         return DMPM_ERR_CUDA;
     }
+    if (cudaStreamCreateWithFlags(&b->side, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaEventCreateWithFlags(&b->ev_fork, cudaEventDisableTiming) != cudaSuccess ||
+        cudaEventCreateWithFlags(&b->ev_join, cudaEventDisableTiming) != cudaSuccess) {
+        cudaGetLastError();
+        dmpm_batch_destroy(b);
+        return DMPM_ERR_CUDA;
+    }
     b->impl.reset(new dmpm_batch::Impl(b));
     const int st = bguard(b, [&](dmpm_batch::Impl& im) { im.create(instances, count); return DMPM_OK; });
     if (st != DMPM_OK) {
@@ -774,8 +790,12 @@ int dmpm_batch_destroy(dmpm_batch* b) {
     if (!b) return DMPM_ERR_ARG;
     cudaSetDevice(b->device);
     cudaStreamSynchronize(b->stream);
+    if (b->side) cudaStreamSynchronize(b->side);
     b->impl.reset();
     cudaStreamDestroy(b->stream);
+    if (b->side) cudaStreamDestroy(b->side);
+    if (b->ev_fork) cudaEventDestroy(b->ev_fork);
+    if (b->ev_join) cudaEventDestroy(b->ev_join);
     delete b;
     return DMPM_OK;
 }

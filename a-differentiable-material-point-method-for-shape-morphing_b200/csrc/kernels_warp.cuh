@@ -229,8 +229,11 @@ __device__ __forceinline__ void load_x_base(const float* st, size_t np, int p, c
 // Minimum resident blocks per SM (the register cap the compiler works to) for
 // the per-particle FP64 kernels: k_stress at 256 threads per block (2: 128
 // registers, no spills; 1 lets it take 132 and run one block per SM),
-// k_adj_finalize at 128 (4: 128 registers with a 32-byte spill, 11 % faster
-// than the 168-register build on the 64^3, 267k-particle workload).
+// k_adj_finalize at 128 (4: 128 registers with a 40-byte spill, 11 % faster
+// than the 168-register build on the 64^3, 267k-particle workload), and its
+// FP64 part alone (5: 96 registers with a 144-byte spill, 40.6 against 45.2 us
+// at 4 and 44.4 us at 6 on the same workload: the extra warps hide more of the
+// load latency than the spills cost).
 // k_stress takes the FP64 polar factors from the scaled Newton iteration
 // (polar_newton) where det(F + dFc) > 0 and from the SVD (polar3) otherwise;
 // 0 uses the SVD everywhere
@@ -242,6 +245,9 @@ __device__ __forceinline__ void load_x_base(const float* st, size_t np, int p, c
 #endif
 #ifndef DMPM_FINALIZE_MIN_BLOCKS
 #define DMPM_FINALIZE_MIN_BLOCKS 4
+#endif
+#ifndef DMPM_FINALIZE_STRESS_MIN_BLOCKS
+#define DMPM_FINALIZE_STRESS_MIN_BLOCKS 5
 #endif
 // and for the adjoint gather and the two scatters, P2G and the adjoint G2P
 // (256 threads per block)
@@ -978,7 +984,9 @@ __device__ __forceinline__ void finalize_particle(const WArgs& a, int p, const I
 // variant, with its finite-difference dJFit, keeps the compiler's own
 // register budget)
 template <bool EXACT, int PART = FIN_ALL>
-__global__ void __launch_bounds__(128, EXACT ? DMPM_FINALIZE_MIN_BLOCKS : 1) k_adj_finalize(WArgs a) {
+__global__ void __launch_bounds__(128, !EXACT ? 1 : PART == FIN_STRESS ? DMPM_FINALIZE_STRESS_MIN_BLOCKS
+                                                                         : DMPM_FINALIZE_MIN_BLOCKS)
+    k_adj_finalize(WArgs a) {
     const int p = blockIdx.x * blockDim.x + threadIdx.x;
     if (p < a.n) finalize_particle<EXACT, FinGlobal, PART>(a, p, FinGlobal{&a, p});
 }
