@@ -234,11 +234,11 @@ PER_TOUCHED_NODE_BYTES = {"p2g": 16, "g2p_p_op2": 16, "adj_g2p_scatter": 16, "ad
                           "p2g_mass": 4, "loss_dldx": 4}
 PER_GRID_NODE_BYTES = {"g_op": 32, "adj_g_op": 64}
 
-# Executed flop per particle-step of the six hot kernels (add + mul + 2 fma over the predicated-on
+# Executed flop per particle-step of the hot kernels (add + mul + 2 fma over the predicated-on
 # thread instructions), counted by ncu on the 64^3, 266,868-particle workload
 # (profiles/flops_atomics_hot_kernels_64cubed_267k.txt); it includes the warp-item layout's redundant
 # weight evaluations.  Nominal vector peaks: 148 SMs x 128 FP32 / 64 FP64 lanes x 2 at 1965 MHz.
-FLOP_PER_PARTICLE_STEP = {"fp32": 11364, "fp64": 1187}
+FLOP_PER_PARTICLE_STEP = {"fp32": 11375, "fp64": 1192}
 NOMINAL_VECTOR_TFLOPS = {"fp32": 148 * 128 * 2 * 1.965e-3, "fp64": 148 * 64 * 2 * 1.965e-3}
 
 
