@@ -1071,7 +1071,7 @@ template <class T> class Engine : public EngineBase {
             if (!a.st || !a.st_next || !a.grid || !a.G) throw StateError{"internal: layer not materialised"};
             DMPM_CK(cudaMemsetAsync(gadj_, 0, G_ * sizeof(node4<T>), ctx_->stream));
             const bool ex = P.adjoint_mode == DMPM_ADJ_EXACT;
-            const unsigned ws = warp_blocks(DMPM_SCATTER_CTAS), wg = warp_blocks(DMPM_GATHER_CTAS);
+            const unsigned ws = warp_blocks(DMPM_ADJ_SCATTER_CTAS), wg = warp_blocks(DMPM_GATHER_CTAS);
             pbeg(K_ADJ_SCATTER);
             if (P.warp_general) {
                 if (ex) k_adj_scatter_w<true, true, ITEMS_PERSISTENT><<<ws, 256, 0, ctx_->stream>>>(a);

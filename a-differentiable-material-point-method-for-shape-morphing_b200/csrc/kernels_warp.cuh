@@ -264,6 +264,15 @@ __device__ __forceinline__ void load_x_base(const float* st, size_t np, int p, c
 #ifndef DMPM_SCATTER_CTAS
 #define DMPM_SCATTER_CTAS DMPM_SCATTER_MIN_BLOCKS
 #endif
+// the adjoint scatter on its own: 4 (64 registers, 84-byte spill) takes 57.3
+// against 59.4 us at 3 on the 64^3, 267k-particle workload, where P2G is
+// faster at 3 (the gather at 4: 87.0 against 78.9 us)
+#ifndef DMPM_ADJ_SCATTER_MIN_BLOCKS
+#define DMPM_ADJ_SCATTER_MIN_BLOCKS 4
+#endif
+#ifndef DMPM_ADJ_SCATTER_CTAS
+#define DMPM_ADJ_SCATTER_CTAS DMPM_ADJ_SCATTER_MIN_BLOCKS
+#endif
 
 // Grid of one instance of a batch: its geometry, the offset of its first node
 // in the batch's concatenated grids and of its first cell key.
@@ -610,7 +619,7 @@ template <int MODE> __global__ void __launch_bounds__(256, 4) k_g2p_w(WArgs a) {
 // ------------------------------------------------------------------ adjoint
 // dLdv_next = dt dLdx' + dLdv';  dLdC_next = c dt dLdF' Fe^T + dLdC'
 // dLdv_g += w dLdv_next + 3/dx^2 w dLdC_next (x_g - x_p)   (BackPropagation.cpp:14-44)
-template <bool EXACT, bool GENERAL, int MODE> __global__ void __launch_bounds__(256, DMPM_SCATTER_MIN_BLOCKS) k_adj_scatter_w(WArgs a) {
+template <bool EXACT, bool GENERAL, int MODE> __global__ void __launch_bounds__(256, DMPM_ADJ_SCATTER_MIN_BLOCKS) k_adj_scatter_w(WArgs a) {
     const int nit = item_count(a);
     const size_t np = a.np, npl = a.npl, npn = a.npn;
     for (int item = first_warp(); item < nit; item = next_item<MODE>(item, nit)) {
