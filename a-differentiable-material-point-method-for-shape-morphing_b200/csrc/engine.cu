@@ -1111,11 +1111,11 @@ template <class T> class Engine : public EngineBase {
             } else if (DMPM_SPLIT_FINALIZE) {
                 // profiled: the two parts one after the other, each timed
                 pbeg(K_ADJ_TRANSPORT);
-                launch_finalize_split(a, ex, nullptr, ctx_->stream, FIN_TRANSPORT);
+                launch_finalize_part(a, ex, FIN_TRANSPORT, ctx_->stream);
                 launched();
                 pend();
                 pbeg(K_ADJ_FINALIZE);
-                launch_finalize_split(a, ex, ctx_->stream, nullptr, FIN_STRESS);
+                launch_finalize_part(a, ex, FIN_STRESS, ctx_->stream);
                 launched();
                 pend();
             } else {

@@ -1025,16 +1025,21 @@ inline void launch_finalize(const WArgs& a, bool exact, cudaStream_t st) {
 #ifndef DMPM_SPLIT_FINALIZE
 #define DMPM_SPLIT_FINALIZE 1
 #endif
-// the same work as two launches: the FP64 part on st, the transport part on
-// side; `parts` selects one of them (FIN_STRESS, FIN_TRANSPORT) or both (FIN_ALL)
-inline void launch_finalize_split(const WArgs& a, bool exact, cudaStream_t st, cudaStream_t side,
-                                  int parts = FIN_ALL) {
+// one part of the finalize (FIN_STRESS or FIN_TRANSPORT) on st
+inline void launch_finalize_part(const WArgs& a, bool exact, int part, cudaStream_t st) {
     if (a.n <= 0) return;
+    if (part == FIN_TRANSPORT) {
+        k_adj_finalize_transport<<<(unsigned)((a.n + 255) / 256), 256, 0, st>>>(a);
+        return;
+    }
     const unsigned b = (unsigned)((a.n + 127) / 128);
-    if (parts != FIN_STRESS) k_adj_finalize_transport<<<(unsigned)((a.n + 255) / 256), 256, 0, side>>>(a);
-    if (parts == FIN_TRANSPORT) return;
     if (exact) k_adj_finalize<true, FIN_STRESS><<<b, 128, 0, st>>>(a);
     else k_adj_finalize<false, FIN_STRESS><<<b, 128, 0, st>>>(a);
+}
+// the same work as two launches: the FP64 part on st, the transport part on side
+inline void launch_finalize_split(const WArgs& a, bool exact, cudaStream_t st, cudaStream_t side) {
+    launch_finalize_part(a, exact, FIN_TRANSPORT, side);
+    launch_finalize_part(a, exact, FIN_STRESS, st);
 }
 
 }  // namespace dmpm
