@@ -79,3 +79,27 @@ def test_host_only_size_helpers_without_gpu():
     assert dmpm.surface_grid_dims(mn, mx, 0.05) == (40, 40, 40)
     with pytest.raises(dmpm.DmpmError):
         dmpm.surface_grid_dims(mn, mx, 0.0)
+
+
+def test_kernel_ids_names_and_bench_tables_agree():
+    """dmpm_kernel_name (host only) names every id below DMPM_NUM_KERNEL_IDS and no
+    other, the Python mirror has the same count, and every kernel bench.py's
+    algorithmic-byte tables describe is one of those names."""
+    import ctypes
+    import sys
+
+    src = open(os.path.join(REPO, "include", "dmpm.h")).read()
+    n = int(re.search(r"#define DMPM_NUM_KERNEL_IDS (\d+)", src).group(1))
+    assert n == dmpm.NUM_KERNEL_IDS
+    lib = dmpm.load_library()
+    lib.dmpm_kernel_name.restype = ctypes.c_char_p
+    names = [lib.dmpm_kernel_name(k) for k in range(n)]
+    assert all(names) and len(set(names)) == n
+    assert lib.dmpm_kernel_name(n) is None and lib.dmpm_kernel_name(-1) is None
+    names = {b.decode() for b in names}
+    sys.path.insert(0, REPO)
+    import bench
+
+    described = set(bench.PER_PARTICLE_BYTES) | set(bench.PER_TOUCHED_NODE_BYTES) | set(bench.PER_GRID_NODE_BYTES)
+    assert described <= names, sorted(described - names)
+    assert {"adj_finalize", "adj_finalize_transport", "adj_p2g_gather"} <= described
