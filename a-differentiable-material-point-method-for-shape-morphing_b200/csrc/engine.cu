@@ -1195,6 +1195,8 @@ template <class T> class Engine : public EngineBase {
         if (control < 0 || control > top) throw ArgError{"control_layer out of range"};
         if (top < L_ - 1 && !layers_[top].adj) throw StateError{"set keep_adjoints to start the adjoint below the last layer"};
         reset_status();
+        // the finalize's second stream exists before any capture of the adjoint steps
+        if (kWarp && DMPM_SPLIT_FINALIZE) side_stream();
         if (ctrl_acc_) DMPM_CK(cudaMemsetAsync(ctrl_acc_, 0, 9 * np_ * sizeof(double), ctx_->stream));
         if (k_ == 1) {
             auto body = [&]() {
