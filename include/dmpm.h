@@ -255,10 +255,13 @@ int dmpm_compute_volumes_noalloc(int n, const float* x, const float* m, int dim_
                                  const float* min_point, float* vol, void* stream);
 
 /* Per-kernel device time.  With profiling on, every hot-path launch is
- * bracketed by CUDA events on the context's stream; dmpm_kernel_stats returns
- * the summed milliseconds and the launch count of one kernel since profiling
- * was (re)enabled.  Kernel ids run from 0 to DMPM_NUM_KERNEL_IDS - 1;
- * dmpm_kernel_name gives their names (p2g, g2p_p_op2, adj_p2g_gather, ...). */
+ * bracketed by CUDA events on the context's stream (the adjoint finalize's two
+ * parts, which otherwise run side by side on two streams, then run one after
+ * the other); dmpm_kernel_stats returns the summed milliseconds and the launch
+ * count of one kernel since profiling was (re)enabled.  Kernel ids run from 0
+ * to DMPM_NUM_KERNEL_IDS - 1; dmpm_kernel_name gives their names (p2g,
+ * g2p_p_op2, adj_p2g_gather, adj_finalize, adj_finalize_transport, ...) and
+ * NULL for any other id. */
 #define DMPM_NUM_KERNEL_IDS 12
 int dmpm_set_profiling(dmpm_ctx* ctx, int on);
 int dmpm_kernel_stats(dmpm_ctx* ctx, int kernel_id, double* total_ms, int64_t* launches);
