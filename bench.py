@@ -878,6 +878,79 @@ def run_config4(args):
     return 0
 
 
+# ---------------------------------------------------------------- mesh sampling and surfacing
+def run_next_rows(args):
+    """The point-cloud sampler and the two surfacing functions on a 1.08M-point
+    workload: the torus fixture (tests/golden/mesh_torus.obj) sampled at a 0.005
+    lattice spacing, then surfaced over [-1, 1]^3 with the fixture's parameters.
+    GPU: the Python API with host arrays, median of 5 after one warm-up, copies
+    included.  CPU baseline: the reference's own sampler and surfacing compiled
+    here (oracle/_ref/ref_mesh, ref_surface: readOBJ or the point file, the
+    computation and the output file), best of 2, on the same host."""
+    import resource
+
+    import torch
+
+    import dmpm
+
+    dmpm.load_library()
+    ref_dir = os.path.join(REPO, "oracle", "_ref")
+    obj = os.path.join(REPO, "tests", "golden", "mesh_torus.obj")
+    dx = 0.005
+    box_min, box_max = (-1.0, -1.0, -1.0), (1.0, 1.0, 1.0)
+
+    def gpu(fn, n=5):
+        fn()
+        torch.cuda.synchronize()
+        ts = []
+        for _ in range(n):
+            t0 = time.perf_counter()
+            out = fn()
+            torch.cuda.synchronize()
+            ts.append(time.perf_counter() - t0)
+        return float(np.median(ts)), out
+
+    def ref(cmd, n=2):
+        best, threads = 1e9, 0.0
+        for _ in range(n):
+            r0 = resource.getrusage(resource.RUSAGE_CHILDREN)
+            t0 = time.perf_counter()
+            subprocess.check_call(cmd, stdout=subprocess.DEVNULL)
+            w = time.perf_counter() - t0
+            r1 = resource.getrusage(resource.RUSAGE_CHILDREN)
+            if w < best:
+                best = w
+                threads = ((r1.ru_utime - r0.ru_utime) + (r1.ru_stime - r0.ru_stime)) / w
+        return best, threads
+
+    import tempfile
+
+    V, F = dmpm.read_obj(obj)
+    t_s, pts = gpu(lambda: dmpm.mesh_lattice_points(V, F, dx))
+    pts = pts.astype(np.float32)
+    out = {"mode": "mesh sampling and surfacing", "points": int(len(pts)), "host_cores": os.cpu_count()}
+    with tempfile.TemporaryDirectory() as tmp:
+        pf = os.path.join(tmp, "pts.f32")
+        r_s, th_s = ref([os.path.join(ref_dir, "ref_mesh"), obj, repr(dx), pf])
+        rp = np.fromfile(pf, dtype=np.float32).reshape(-1, 3)
+        out["points_identical_to_reference"] = bool(rp.shape == pts.shape and np.array_equal(rp, pts))
+        box = ["-1.0", "-1.0", "-1.0", "1.0", "1.0", "1.0"]
+        t_su, (_, Fs) = gpu(lambda: dmpm.sphere_union_surface(pts, 0.025, 0.025, 0.025, 2, box_min, box_max))
+        r_su, th_su = ref([os.path.join(ref_dir, "ref_surface"), "spheres", pf, "0.025", repr(float(np.float32(0.025))),
+                           "0.025", "2", *box, os.path.join(tmp, "sph.bin")])
+        t_mc, (_, Fm) = gpu(lambda: dmpm.marching_cubes_point_cloud(pts, 0.5, 0.05, 2.0, box_min, box_max))
+        r_mc, th_mc = ref([os.path.join(ref_dir, "ref_surface"), "mass", pf, "1.0", "0.05", "2.0", "0.5", *box,
+                           os.path.join(tmp, "mass.bin")])
+    for key, tg, tr, th, tris in (("mesh_sampler", t_s, r_s, th_s, None),
+                                  ("sphere_union_surface", t_su, r_su, th_su, len(Fs)),
+                                  ("marching_cubes_point_cloud", t_mc, r_mc, th_mc, len(Fm))):
+        out[key] = {"gpu_s": tg, "reference_s": tr, "reference_threads": round(th, 1), "speedup": tr / tg}
+        if tris is not None:
+            out[key]["triangles"] = int(tris)
+    print(json.dumps(out), flush=True)
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser(description=__doc__, formatter_class=argparse.RawDescriptionHelpFormatter)
     ap.add_argument("--gpus", type=int, default=1)
@@ -895,6 +968,8 @@ def main():
     ap.add_argument("--fd", action="store_true", help="config 1: adjoint vs central differences, 16 directions")
     ap.add_argument("--instances", type=int, default=48, help="config 3: number of batched instances")
     ap.add_argument("--fd-h", default="1e-3,1e-4,1e-5,1e-6", help="--fd: central-difference steps")
+    ap.add_argument("--next-rows", action="store_true",
+                    help="time the mesh sampler and the surfacing against the reference's own code")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
@@ -902,6 +977,8 @@ def main():
         return run_reference(args)
     if args.fd:
         return run_fd(args)
+    if args.next_rows:
+        return run_next_rows(args)
     if args.config == 0:
         return run_config0(args)
     if args.config == 2:
