@@ -15,6 +15,13 @@ Tensor3x3x3x3 d2_FCE_psi_dF2_mult_trick(const Mat3& F, float lam, float mu);
 Tensor3x3x3x3 d2_FCE_psi_dF2_FD(const Mat3& F, float lam, float mu);
 void CalculateLameParameters(float young_mod, float poisson, float& lam, float& mu);
 
+// d(J F^-T)/dF as T[a][b](i, j) = d(J F^-T)_ab / dF_ij: by central differences with
+// delta = 1e-6 (d_JFit_dF_FD, Elasticity.cpp:7-72) and in closed form from J and
+// F^-T (d_JFit_dF, declared at Elasticity.h:20; the reference defines no body).  Small
+// host utilities off the hot path, evaluated in FP64 and rounded to float.
+Tensor3x3x3x3 d_JFit_dF_FD(const Mat3& F);
+Tensor3x3x3x3 d_JFit_dF(float J, const Mat3& Fit);
+
 // Batched forms: one GPU launch for many matrices (n = size of the vectors).
 std::vector<Mat3> PK_FixedCorotatedElasticityBatch(const std::vector<Mat3>& F, float lam, float mu);
 std::vector<Mat3> d2_FCE_psi_dF2_mult_by_dF_Batch(const std::vector<Mat3>& F, float lam, float mu,

@@ -473,6 +473,49 @@ Tensor3x3x3x3 d2_FCE_psi_dF2_FD(const Mat3& F, float lam, float mu) {
         }
     return t;
 }
+namespace {
+// J F^-T of a 3x3 matrix in FP64: the cofactor matrix (J F^-T = cof(F))
+void jfit_d(const double F[3][3], double out[3][3]) {
+    for (int a = 0; a < 3; a++)
+        for (int b = 0; b < 3; b++) {
+            const int a1 = (a + 1) % 3, a2 = (a + 2) % 3, b1 = (b + 1) % 3, b2 = (b + 2) % 3;
+            out[a][b] = F[a1][b1] * F[a2][b2] - F[a1][b2] * F[a2][b1];
+        }
+}
+}  // namespace
+
+Tensor3x3x3x3 d_JFit_dF_FD(const Mat3& F) {
+    const double delta = 1e-6;
+    double G[3][3];
+    for (int i = 0; i < 3; i++)
+        for (int j = 0; j < 3; j++) G[i][j] = F(i, j);
+    Tensor3x3x3x3 t;
+    for (int i = 0; i < 3; i++)
+        for (int j = 0; j < 3; j++) {
+            const double orig = G[i][j];
+            double fwd[3][3], bwd[3][3];
+            G[i][j] = orig + delta;
+            jfit_d(G, fwd);
+            G[i][j] = orig - delta;
+            jfit_d(G, bwd);
+            G[i][j] = orig;
+            for (int a = 0; a < 3; a++)
+                for (int b = 0; b < 3; b++) t[a][b](i, j) = (float)((fwd[a][b] - bwd[a][b]) / (2.0 * delta));
+        }
+    return t;
+}
+
+// d(J F^-T)_ab / dF_ij = J (F^-T_ab F^-T_ij - F^-T_aj F^-T_ib)  (dJ/dF = J F^-T, dF^-T = -F^-T dF^T F^-T)
+Tensor3x3x3x3 d_JFit_dF(float J, const Mat3& Fit) {
+    Tensor3x3x3x3 t;
+    for (int a = 0; a < 3; a++)
+        for (int b = 0; b < 3; b++)
+            for (int i = 0; i < 3; i++)
+                for (int j = 0; j < 3; j++)
+                    t[a][b](i, j) = (float)((double)J * ((double)Fit(a, b) * Fit(i, j) - (double)Fit(a, j) * Fit(i, b)));
+    return t;
+}
+
 void CalculateLameParameters(float young_mod, float poisson, float& lam, float& mu) {
     lam = young_mod * poisson / ((1.f + poisson) * (1.f - 2.f * poisson));
     mu = young_mod / (2.f + 2.f * poisson);

@@ -356,6 +356,15 @@ class Elementary:
         f(_ptr(a), _ptr(U), _ptr(s), _ptr(V))
         return self._u(U), s, self._u(V)
 
+    def djfit_fd(self, F):
+        """The reference's d_JFit_dF_FD (Elasticity.cpp:7-72): T[a][b](i, j) =
+        d(J F^-T)_ab / dF_ij by central differences, as an (3, 3, 3, 3) array."""
+        assert self.kind == "ref", "the oracle has no standalone d_JFit_dF_FD"
+        f = self.lib.ref_djfit_fd; f.argtypes = [_P, _P]; f.restype = None
+        a = self._m(F); out = np.zeros(81, self.dt)
+        f(_ptr(a), _ptr(out))
+        return out.reshape(3, 3, 3, 3)
+
     def pk(self, F, lam, mu):
         f = self._f("or_pk", "ref_pk"); f.argtypes = [_P, self.R, self.R, _P]; f.restype = None
         a = self._m(F); P = np.zeros(9, self.dt)

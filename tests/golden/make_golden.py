@@ -9,7 +9,8 @@ next to this script.  Needs the reference sources (run where they exist):
 
 Fixtures:
   elementary_{f32,f64}.npz  polar factors, PK stress, dP/dF:dF (reference
-                            finite-difference variant), B-spline values, on the
+                            finite-difference variant), d(J F^-T)/dF by the
+                            reference's d_JFit_dF_FD, B-spline values, on the
                             CheckGradients fixture F = 0.8 Rx(45 deg),
                             lam = 58333, mu = 38888.9 (DiffMPMAnimator3D.cpp:212-243)
                             and on seeded random F.
@@ -78,16 +79,17 @@ def make_elementary(prec):
     e = Elementary("ref", prec)
     Fs, dFs = elementary_inputs()
     lam, mu = 58333.0, 38888.9
-    R, S, P, D2 = [], [], [], []
+    R, S, P, D2, DJ = [], [], [], [], []
     for F, dF in zip(Fs, dFs):
         r, s = e.polar(F)
         R.append(r)
         S.append(s)
         P.append(e.pk(F, lam, mu))
         D2.append(e.d2(F, lam, mu, dF))
+        DJ.append(e.djfit_fd(F))
     xs = np.linspace(-2.5, 2.5, 101)
     np.savez_compressed(os.path.join(HERE, "elementary_%s.npz" % prec), F=Fs, dF=dFs, lam=lam, mu=mu,
-                        R=np.array(R), S=np.array(S), P=np.array(P), d2=np.array(D2), bx=xs,
+                        R=np.array(R), S=np.array(S), P=np.array(P), d2=np.array(D2), djfit=np.array(DJ), bx=xs,
                         b=np.array([e.bspline(x) for x in xs]), bs=np.array([e.bspline_slope(x) for x in xs]))
 
 

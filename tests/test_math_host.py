@@ -156,3 +156,31 @@ def test_newton_polar_matches_svd_polar(mh):
         R = np.zeros(9)
         S = np.zeros(9)
         assert mh.mh_polar_newton_f64(cm(F).ctypes.data_as(P), R.ctypes.data_as(P), S.ctypes.data_as(P)) == 0
+
+
+def test_compat_djfit_matches_reference_fd():
+    """The compat API's d_JFit_dF_FD (a host utility) against the reference's
+    FP64 build on the elementary fixture's 25 matrices, and its closed-form
+    d_JFit_dF against it.  The shipped float build's own central differences
+    (delta = 1e-6 in float, so one float step of J F^-T near 1 moves an entry by
+    0.06) stray from the FP64 build by 6 % of the largest entry at the median
+    and 12.5 % at worst over these matrices."""
+    import build as pkg_build
+
+    pkg_build.build_compat()
+    pkg = os.path.join(os.path.dirname(HERE), "a-differentiable-material-point-method-for-shape-morphing_b200")
+    exe = os.path.join(HERE, "native", "jfit_check")
+    subprocess.check_call(["g++", "-std=c++17", "-O2", "-I", os.path.join(pkg, "compat"), "-I",
+                           os.path.join(os.path.dirname(HERE), "include"), os.path.join(HERE, "cpp", "jfit_check.cpp"),
+                           "-L", pkg, "-ldmpm_compat", "-ldmpm", "-Wl,-rpath," + pkg, "-o", exe])
+    g64, g32 = load_golden("elementary_f64"), load_golden("elementary_f32")
+    Fs = g64["F"]
+    stdin = "%d\n" % len(Fs) + "\n".join(" ".join("%.17g" % v for v in F.reshape(9)) for F in Fs) + "\n"
+    res = subprocess.run([exe], input=stdin, capture_output=True, text=True, check=True)
+    vals = np.array(res.stdout.split(), dtype=np.float64).reshape(len(Fs), 2, 3, 3, 3, 3)
+    fd, closed = vals[:, 0], vals[:, 1]
+    for k in range(len(Fs)):
+        assert relerr(fd[k], g64["djfit"][k]) < 1e-6, k
+        assert relerr(closed[k], g64["djfit"][k]) < 1e-5, k
+        assert relerr(g32["djfit"][k], g64["djfit"][k]) < 0.15, k
+    os.remove(exe)
