@@ -184,3 +184,20 @@ def test_compat_djfit_matches_reference_fd():
         assert relerr(closed[k], g64["djfit"][k]) < 1e-5, k
         assert relerr(g32["djfit"][k], g64["djfit"][k]) < 0.15, k
     os.remove(exe)
+
+
+def test_compat_bspline_is_the_reference_float_bspline():
+    """The compat API's CubicBSpline / CubicBSplineSlope (header-only) give the
+    shipped float build's values bit for bit on the elementary fixture's sweep."""
+    pkg = os.path.join(os.path.dirname(HERE), "a-differentiable-material-point-method-for-shape-morphing_b200")
+    exe = os.path.join(HERE, "native", "bspline_check")
+    subprocess.check_call(["g++", "-std=c++17", "-O2", "-I", os.path.join(pkg, "compat"),
+                           os.path.join(HERE, "cpp", "bspline_check.cpp"), "-o", exe])
+    g = load_golden("elementary_f32")
+    xs = np.asarray(g["bx"], dtype=np.float32)
+    stdin = "%d\n" % len(xs) + "\n".join("%.9g" % x for x in xs) + "\n"
+    res = subprocess.run([exe], input=stdin, capture_output=True, text=True, check=True)
+    vals = np.array(res.stdout.split(), dtype=np.float32).reshape(len(xs), 2)
+    os.remove(exe)
+    assert np.array_equal(vals[:, 0], np.asarray(g["b"], dtype=np.float32))
+    assert np.array_equal(vals[:, 1], np.asarray(g["bs"], dtype=np.float32))
