@@ -33,23 +33,40 @@ def _stale(target, sources):
 
 COMPAT = os.path.join(PKG_DIR, "compat")
 COMPAT_LIB = os.path.join(PKG_DIR, "libdmpm_compat.so")
+COMPAT_EIGEN_LIB = os.path.join(PKG_DIR, "libdmpm_compat_eigen.so")
 
 
-def build_compat(force: bool = False, verbose: bool = False) -> str:
-    """The DiffMPMLib3D-compatible C++ API over libdmpm.so (libdmpm_compat.so)."""
-    build(force=force, verbose=verbose)
-    srcs = [os.path.join(COMPAT, "dmpm_compat.cpp")] + [os.path.join(COMPAT, "DiffMPMLib3D", f)
-                                                         for f in os.listdir(os.path.join(COMPAT, "DiffMPMLib3D"))]
-    srcs.append(LIB)
-    if force or _stale(COMPAT_LIB, srcs):
-        cmd = ["g++", "-std=c++17", "-O2", "-fPIC", "-shared", "-I", COMPAT, "-I", os.path.join(REPO, "include"),
-               "-o", COMPAT_LIB + ".tmp", os.path.join(COMPAT, "dmpm_compat.cpp"), "-L", PKG_DIR, "-ldmpm",
-               "-Wl,-rpath,$ORIGIN"]
+def _compat_sources():
+    return [os.path.join(COMPAT, "dmpm_compat.cpp")] + [os.path.join(COMPAT, "DiffMPMLib3D", f)
+                                                        for f in os.listdir(os.path.join(COMPAT, "DiffMPMLib3D"))]
+
+
+def _build_compat_lib(target, flags, force, verbose):
+    srcs = _compat_sources() + [LIB]
+    if force or _stale(target, srcs):
+        cmd = ["g++", "-std=c++17", "-O2", "-fPIC", "-shared", *flags, "-I", COMPAT, "-I",
+               os.path.join(REPO, "include"), "-o", target + ".tmp", os.path.join(COMPAT, "dmpm_compat.cpp"), "-L",
+               PKG_DIR, "-ldmpm", "-Wl,-rpath,$ORIGIN"]
         if verbose:
             print(" ".join(cmd), file=sys.stderr)
         subprocess.check_call(cmd)
-        os.replace(COMPAT_LIB + ".tmp", COMPAT_LIB)
-    return COMPAT_LIB
+        os.replace(target + ".tmp", target)
+    return target
+
+
+def build_compat(force: bool = False, verbose: bool = False) -> str:
+    """The DiffMPMLib3D-compatible C++ API over libdmpm.so with its own value
+    types (libdmpm_compat.so), for callers built without Eigen."""
+    build(force=force, verbose=verbose)
+    return _build_compat_lib(COMPAT_LIB, ["-DDMPM_COMPAT_NO_EIGEN"], force, verbose)
+
+
+def build_compat_eigen(eigen_include: str, force: bool = False, verbose: bool = False) -> str:
+    """The same API with Vec3 / Mat3 = Eigen::Vector3f / Matrix3f
+    (libdmpm_compat_eigen.so), for callers that do Eigen arithmetic on the
+    reference's types; eigen_include is the directory holding Eigen/Dense."""
+    build(force=force, verbose=verbose)
+    return _build_compat_lib(COMPAT_EIGEN_LIB, ["-DDMPM_COMPAT_EIGEN", "-I", eigen_include], force, verbose)
 
 
 def build(force: bool = False, verbose: bool = False) -> str:

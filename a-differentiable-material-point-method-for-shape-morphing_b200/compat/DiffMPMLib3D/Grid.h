@@ -21,7 +21,7 @@ struct Grid {
     int dim_y;
     int dim_z;
     float dx;
-    Vec3 min_point;
+    Vec3 min_point = Vec3::Zero();
     std::vector<std::vector<std::vector<GridNode>>> nodes;
 };
 

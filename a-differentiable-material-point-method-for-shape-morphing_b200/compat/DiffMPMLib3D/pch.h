@@ -1,12 +1,43 @@
 // pch.h -- value types of the DiffMPMLib3D-compatible C++ API (compat layer
-// over libdmpm.so).  Vec3 and Mat3 have the storage of the reference's
-// Eigen::Vector3f / Eigen::Matrix3f (pch.h:24-25): 3 and 9 floats, matrices
-// column-major, no padding, so MaterialPoint and GridNode keep the
-// reference's byte layout.  Only the operations the API needs are provided.
+// over libdmpm.so).
+//
+// Where Eigen is on the include path (the reference's callers always have it),
+// Vec3 and Mat3 are the reference's own typedefs, Eigen::Vector3f and
+// Eigen::Matrix3f (pch.h:24-25), so caller code that does Eigen arithmetic on
+// MaterialPoint fields compiles unchanged; such callers link
+// libdmpm_compat_eigen.so.  Without Eigen (or with DMPM_COMPAT_NO_EIGEN
+// defined) Vec3 and Mat3 are small structs with the same storage -- 3 and 9
+// floats, matrices column-major, no padding -- and only the operations the API
+// needs; those callers link libdmpm_compat.so.  Either way MaterialPoint and
+// GridNode keep the reference's byte layout.  DMPM_COMPAT_EIGEN forces the
+// Eigen types.
 #pragma once
 #include <cmath>
 #include <memory>
 #include <vector>
+
+#if !defined(DMPM_COMPAT_EIGEN) && !defined(DMPM_COMPAT_NO_EIGEN) && defined(__has_include)
+#if __has_include(<Eigen/Dense>)
+#define DMPM_COMPAT_EIGEN 1
+#endif
+#endif
+
+#ifdef DMPM_COMPAT_EIGEN
+#include <Eigen/Dense>
+
+namespace DiffMPMLib3D {
+
+typedef Eigen::Vector3f Vec3;
+typedef Eigen::Matrix3f Mat3;
+
+// A:B (pch.h:27-30)
+inline float InnerProduct(const Mat3& A, const Mat3& B) { return (A.array() * B.array()).sum(); }
+
+static_assert(sizeof(Vec3) == 12 && sizeof(Mat3) == 36, "Eigen::Vector3f / Matrix3f storage");
+
+}  // namespace DiffMPMLib3D
+
+#else
 
 namespace DiffMPMLib3D {
 
@@ -67,3 +98,5 @@ inline float InnerProduct(const Mat3& A, const Mat3& B) {
 static_assert(sizeof(Vec3) == 12 && sizeof(Mat3) == 36, "Eigen::Vector3f / Matrix3f storage");
 
 }  // namespace DiffMPMLib3D
+
+#endif  // DMPM_COMPAT_EIGEN

@@ -144,7 +144,7 @@ void get_grid_into(dmpm_ctx* h, int layer, Grid& g, bool values, bool adjoints) 
 std::vector<double> to_cm_doubles(const std::vector<Mat3>& M) {
     std::vector<double> a(M.size() * 9);
     for (size_t p = 0; p < M.size(); p++)
-        for (int q = 0; q < 9; q++) a[9 * p + q] = M[p].d[q];
+        for (int q = 0; q < 9; q++) a[9 * p + q] = M[p].data()[q];
     return a;
 }
 
@@ -220,7 +220,8 @@ void PointCloud::Descend_dLdF(float alpha, float gradient_norm) {
     const float momentum_factor = 0.9f, min_clip = 1e-3f, max_clip = 1.0f;
     for (auto& p : points) {
         Mat3 dir = p.dLdF * (1.f / gradient_norm);
-        for (float& v : dir.d) {
+        for (int q = 0; q < 9; q++) {
+            float& v = dir.data()[q];
             if (v > max_clip) v = max_clip;
             else if (v < -max_clip) v = -max_clip;
             else if (std::fabs(v) < min_clip) v = v < 0 ? -min_clip : min_clip;
@@ -234,11 +235,11 @@ void PointCloud::Descend_Adam(float alpha, float gradient_norm, float beta1, flo
     const float c1 = 1.f - std::pow(beta1, (float)t), c2 = 1.f - std::pow(beta2, (float)t);
     for (auto& p : points) {
         for (int k = 0; k < 9; k++) {
-            const float g = p.dLdF.d[k] / gradient_norm;
-            p.momentum.d[k] = beta1 * p.momentum.d[k] + (1.f - beta1) * g;
-            p.vector.d[k] = beta2 * p.vector.d[k] + (1.f - beta2) * g * g;
-            const float mh = p.momentum.d[k] / c1, vh = p.vector.d[k] / c2;
-            p.dFc.d[k] -= alpha * (mh / (std::sqrt(vh) + epsilon));
+            const float g = p.dLdF.data()[k] / gradient_norm;
+            p.momentum.data()[k] = beta1 * p.momentum.data()[k] + (1.f - beta1) * g;
+            p.vector.data()[k] = beta2 * p.vector.data()[k] + (1.f - beta2) * g * g;
+            const float mh = p.momentum.data()[k] / c1, vh = p.vector.data()[k] / c2;
+            p.dFc.data()[k] -= alpha * (mh / (std::sqrt(vh) + epsilon));
         }
     }
 }
@@ -247,28 +248,28 @@ void PointCloud::Descend_AMSGrad(float alpha, float gradient_norm, float beta1, 
     const float c1 = 1.f - std::pow(beta1, (float)t), c2 = 1.f - std::pow(beta2, (float)t);
     for (auto& p : points) {
         for (int k = 0; k < 9; k++) {
-            const float g = p.dLdF.d[k] / gradient_norm;
-            p.momentum.d[k] = beta1 * p.momentum.d[k] + (1.f - beta1) * g;
-            p.vector.d[k] = beta2 * p.vector.d[k] + (1.f - beta2) * g * g;
-            const float mh = p.momentum.d[k] / c1, vh = p.vector.d[k] / c2;
-            p.vector_max.d[k] = std::max(p.vector_max.d[k], vh);
-            p.dFc.d[k] -= alpha * (mh / (std::sqrt(p.vector_max.d[k]) + epsilon));
+            const float g = p.dLdF.data()[k] / gradient_norm;
+            p.momentum.data()[k] = beta1 * p.momentum.data()[k] + (1.f - beta1) * g;
+            p.vector.data()[k] = beta2 * p.vector.data()[k] + (1.f - beta2) * g * g;
+            const float mh = p.momentum.data()[k] / c1, vh = p.vector.data()[k] / c2;
+            p.vector_max.data()[k] = std::max(p.vector_max.data()[k], vh);
+            p.dFc.data()[k] -= alpha * (mh / (std::sqrt(p.vector_max.data()[k]) + epsilon));
         }
     }
 }
 
 void PointCloud::Descend_GradientDescent(float alpha, float gradient_norm) {
     for (auto& p : points)
-        for (int k = 0; k < 9; k++) p.dFc.d[k] -= alpha * p.dLdF.d[k] / gradient_norm;
+        for (int k = 0; k < 9; k++) p.dFc.data()[k] -= alpha * p.dLdF.data()[k] / gradient_norm;
 }
 
 void PointCloud::Descend_Lion(float alpha, float beta, float gradient_norm) {
     for (auto& p : points) {
         for (int k = 0; k < 9; k++) {
-            const float g = p.dLdF.d[k] / gradient_norm;
+            const float g = p.dLdF.data()[k] / gradient_norm;
             const float sg = g > 0.f ? 1.f : (g < 0.f ? -1.f : 0.f);
-            p.momentum.d[k] = beta * p.momentum.d[k] + (1.f - beta) * sg;
-            p.dFc.d[k] -= alpha * p.momentum.d[k];
+            p.momentum.data()[k] = beta * p.momentum.data()[k] + (1.f - beta) * sg;
+            p.dFc.data()[k] -= alpha * p.momentum.data()[k];
         }
     }
 }
@@ -417,7 +418,7 @@ std::vector<Mat3> elementary_batch(int kind, const std::vector<Mat3>& F, float l
           "dmpm_elementary");
     std::vector<Mat3> r(n);
     for (int p = 0; p < n; p++)
-        for (int q = 0; q < 9; q++) r[p].d[q] = (float)out[9 * (size_t)p + q];
+        for (int q = 0; q < 9; q++) r[p].data()[q] = (float)out[9 * (size_t)p + q];
     return r;
 }
 }  // namespace
@@ -554,7 +555,7 @@ void P_op_1(PointCloud& pc) {
     check(nullptr, dmpm_elementary(DMPM_ELEM_PK, n, a.data(), l.data(), m.data(), nullptr, out.data()),
           "dmpm_elementary");
     for (int p = 0; p < n; p++)
-        for (int q = 0; q < 9; q++) pc.points[p].P.d[q] = (float)out[9 * (size_t)p + q];
+        for (int q = 0; q < 9; q++) pc.points[p].P.data()[q] = (float)out[9 * (size_t)p + q];
 }
 
 void G_Reset(Grid& grid) { grid.ResetValues(); }
@@ -632,7 +633,7 @@ void G2P(PointCloud& next, const PointCloud& curr, Grid& grid) {
           "dmpm_stage_g2p");
     for (size_t p = 0; p < n; p++) {
         for (int k = 0; k < 3; k++) next.points[p].v[k] = v[3 * p + k];
-        for (int k = 0; k < 9; k++) next.points[p].C.d[k] = C[9 * p + k];
+        for (int k = 0; k < 9; k++) next.points[p].C.data()[k] = C[9 * p + k];
     }
 }
 
@@ -650,9 +651,9 @@ void P_op_2(PointCloud& next, const PointCloud& curr, float s, float dt) {
             v[3 * p + k] = q.v[k];
         }
         for (int k = 0; k < 9; k++) {
-            F[9 * p + k] = c.F.d[k];
-            D[9 * p + k] = c.dFc.d[k];
-            C[9 * p + k] = q.C.d[k];
+            F[9 * p + k] = c.F.data()[k];
+            D[9 * p + k] = c.dFc.data()[k];
+            C[9 * p + k] = q.C.data()[k];
         }
     }
     check(nullptr, dmpm_stage_p_op_2((int)n, x.data(), F.data(), D.data(), v.data(), C.data(), dt, s, xo.data(),
@@ -660,7 +661,7 @@ void P_op_2(PointCloud& next, const PointCloud& curr, float s, float dt) {
           "dmpm_stage_p_op_2");
     for (size_t p = 0; p < n; p++) {
         for (int k = 0; k < 3; k++) next.points[p].x[k] = xo[3 * p + k];
-        for (int k = 0; k < 9; k++) next.points[p].F.d[k] = Fo[9 * p + k];
+        for (int k = 0; k < 9; k++) next.points[p].F.data()[k] = Fo[9 * p + k];
     }
 }
 

@@ -205,7 +205,8 @@ struct dmpm_batch::Impl {
             s.koff = (uint32_t)koff;
             poff += (size_t)d.n;
             goff += s.G;
-            koff += (uint64_t)(d.dim_x + 8) * (d.dim_y + 8) * (d.dim_z + 8);
+            const int dims[3] = {d.dim_x, d.dim_y, d.dim_z};
+            koff += key_span(dims);
             user2int[idx[k]] = k;
             inst.push_back(s);
         }

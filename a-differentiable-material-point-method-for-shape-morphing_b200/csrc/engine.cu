@@ -27,6 +27,7 @@
 #include "dmpm.h"
 #include "kernels.cuh"
 #include "kernels_warp.cuh"
+#include "kernels_brick.cuh"
 #include "host_common.cuh"
 
 using namespace dmpm;
@@ -233,6 +234,13 @@ template <class T> class Engine : public EngineBase {
         uint32_t* order = nullptr;
         uint32_t* items = nullptr;
         uint32_t* n_items = nullptr;  // device scalar: the warp kernels read it, the host never does
+        // brick units (kernels_brick.cuh) of the same order, when the sort made them:
+        // unit_shift 3 (2^3-cell octants) or 6 (4^3-cell bricks), -1 when the
+        // warp-item kernels serve this epoch
+        uint32_t* units = nullptr;
+        uint32_t* unit_keys = nullptr;
+        uint32_t* n_units = nullptr;
+        int unit_shift = -1;
         bool valid = false;
     };
 
@@ -242,6 +250,10 @@ template <class T> class Engine : public EngineBase {
     void set_grid(int dx_, int dy_, int dz_, double h, const double* mn) {
         if (dx_ <= 0 || dy_ <= 0 || dz_ <= 0 || !(h > 0)) throw ArgError{"grid dims and dx must be positive"};
         if ((double)dx_ * dy_ * dz_ > 2e9) throw ArgError{"grid has more than 2e9 nodes"};
+        {
+            const int d[3] = {dx_, dy_, dz_};
+            if (key_span(d) > (1ull << 32)) throw ArgError{"grid too large for 32-bit cell keys"};
+        }
         const bool same = grid_set_ && geo_.dim[0] == dx_ && geo_.dim[1] == dy_ && geo_.dim[2] == dz_;
         drop_graphs();  // the grid geometry is a kernel argument of every captured launch
         geo_.dim[0] = dx_; geo_.dim[1] = dy_; geo_.dim[2] = dz_;
@@ -391,6 +403,27 @@ template <class T> class Engine : public EngineBase {
         return (unsigned)std::max<size_t>(1, std::min<size_t>(most, (size_t)sms_ * ctas));
     }
     unsigned ggrid() const { return (unsigned)((G_ + 255) / 256); }
+    // Brick units of an epoch into the kernel arguments; returns the unit shift
+    // (3, 6) or -1 when the epoch has none (warp-item kernels)
+    int set_units(WArgs& a, const Epoch& ep) const {
+        a.unit_start = ep.units;
+        a.unit_key = ep.unit_keys;
+        a.n_units_dev = ep.n_units;
+        return ep.units ? ep.unit_shift : -1;
+    }
+    // persistent grid of a brick kernel: as many CTAs as can be resident at once
+    // (its register and shared-memory budget), looked up once per kernel
+    template <class K> unsigned brick_blocks(K kernel) {
+        if (sms_ == 0) warp_blocks();
+        const void* key = reinterpret_cast<const void*>(kernel);
+        auto it = brick_occ_.find(key);
+        if (it == brick_occ_.end()) {
+            int per_sm = 0;
+            DMPM_CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, DMPM_BRICK_THREADS, 0));
+            it = brick_occ_.emplace(key, std::max(1, per_sm)).first;
+        }
+        return (unsigned)(sms_ * it->second);
+    }
 
     void launched() {
         ctx_->launches++;
@@ -558,6 +591,7 @@ template <class T> class Engine : public EngineBase {
         want.keep_adj = P.keep_adjoints; want.keep_int = P.keep_intermediates; want.np = np_; want.G = G_;
         want.sort_every = P.sort_every;
         want.stride = control_stride();
+        want.brick = P.brick_cells != 0;
         if (want == layout_ && (int)layers_.size() == num_layers) {
             reset_layers();
             return;
@@ -708,6 +742,11 @@ template <class T> class Engine : public EngineBase {
             e.order = (uint32_t*)layer_arena_.alloc((size_t)n_ * sizeof(uint32_t));
             e.items = (uint32_t*)layer_arena_.alloc(((size_t)n_ + 1) * sizeof(uint32_t));
             e.n_items = (uint32_t*)layer_arena_.alloc(16);
+            if (ctx_->prm.brick_cells) {
+                e.units = (uint32_t*)layer_arena_.alloc(((size_t)n_ + 1) * sizeof(uint32_t));
+                e.unit_keys = (uint32_t*)layer_arena_.alloc((size_t)n_ * sizeof(uint32_t));
+                e.n_units = (uint32_t*)layer_arena_.alloc(16);
+            }
         }
         const size_t n = (size_t)n_;
         sk_[0] = (uint32_t*)layer_arena_.alloc(n * 4);
@@ -745,7 +784,7 @@ template <class T> class Engine : public EngineBase {
         ka.vals = sv_[0];
         k_cell_keys<T><<<(n + 255) / 256, 256, 0, ctx_->stream>>>(ka);
         launched();
-        const uint64_t max_key = (uint64_t)(geo_.dim[0] + 8) * (geo_.dim[1] + 8) * (geo_.dim[2] + 8);
+        const uint64_t max_key = key_span(geo_.dim);
         int bits = 1;
         while (bits < 32 && (1ull << bits) < max_key) bits++;
         const int rs_tiles = (n + RS_TILE - 1) / RS_TILE;
@@ -771,6 +810,18 @@ template <class T> class Engine : public EngineBase {
         launched();
         k_item_sentinel<<<1, 1, 0, ctx_->stream>>>(e.items, e.n_items, n);
         launched();
+        e.unit_shift = -1;
+        if (ctx_->prm.brick_cells && e.units) {
+            const int shift = ctx_->prm.brick_cells == 4 ? 6 : 3;
+            k_unit_flags<<<(n + 255) / 256, 256, 0, ctx_->stream>>>(sk_[cur], n, shift, sf_);
+            launched();
+            device_scan<OpSum>(sf_, (size_t)n, e.n_units);
+            k_unit_starts<<<(n + 255) / 256, 256, 0, ctx_->stream>>>(sk_[cur], sf_, n, shift, e.units, e.unit_keys);
+            launched();
+            k_item_sentinel<<<1, 1, 0, ctx_->stream>>>(e.units, e.n_units, n);
+            launched();
+            e.unit_shift = shift;
+        }
         e.valid = true;
     }
 
@@ -847,12 +898,15 @@ template <class T> class Engine : public EngineBase {
             a.P = ctx_->prm.keep_intermediates ? (float*)layers_[l].dbgP : nullptr;
             DMPM_CK(cudaMemsetAsync(g, 0, G_ * sizeof(node4<T>), ctx_->stream));
             const unsigned ws = warp_blocks(DMPM_SCATTER_CTAS);
+            const int ush = set_units(a, ep);
             pbeg(K_P_OP1);
             k_stress<<<pgrid256(), 256, 0, ctx_->stream>>>(a);
             launched();
             pend();
             pbeg(K_P2G);
-            if (ctx_->prm.warp_general) k_p2g_w<true, ITEMS_PERSISTENT><<<ws, 256, 0, ctx_->stream>>>(a);
+            if (ush == 3) k_p2g_b<2><<<brick_blocks(k_p2g_b<2>), DMPM_BRICK_THREADS, 0, ctx_->stream>>>(a);
+            else if (ush == 6) k_p2g_b<4><<<brick_blocks(k_p2g_b<4>), DMPM_BRICK_THREADS, 0, ctx_->stream>>>(a);
+            else if (ctx_->prm.warp_general) k_p2g_w<true, ITEMS_PERSISTENT><<<ws, 256, 0, ctx_->stream>>>(a);
             else k_p2g_w<false, ITEMS_PERSISTENT><<<ws, 256, 0, ctx_->stream>>>(a);
             launched();
             pend();
@@ -861,7 +915,9 @@ template <class T> class Engine : public EngineBase {
             launched();
             pend();
             pbeg(K_G2P);
-            k_g2p_w<ITEMS_PERSISTENT><<<warp_blocks(DMPM_G2P_CTAS), 256, 0, ctx_->stream>>>(a);
+            if (ush == 3) k_g2p_b<2><<<brick_blocks(k_g2p_b<2>), DMPM_BRICK_THREADS, 0, ctx_->stream>>>(a);
+            else if (ush == 6) k_g2p_b<4><<<brick_blocks(k_g2p_b<4>), DMPM_BRICK_THREADS, 0, ctx_->stream>>>(a);
+            else k_g2p_w<ITEMS_PERSISTENT><<<warp_blocks(DMPM_G2P_CTAS), 256, 0, ctx_->stream>>>(a);
             launched();
             pend();
             return;
@@ -1072,8 +1128,15 @@ template <class T> class Engine : public EngineBase {
             DMPM_CK(cudaMemsetAsync(gadj_, 0, G_ * sizeof(node4<T>), ctx_->stream));
             const bool ex = P.adjoint_mode == DMPM_ADJ_EXACT;
             const unsigned ws = warp_blocks(DMPM_ADJ_SCATTER_CTAS), wg = warp_blocks(DMPM_GATHER_CTAS);
+            const int ush = set_units(a, ep);
             pbeg(K_ADJ_SCATTER);
-            if (P.warp_general) {
+            if (ush == 3) {
+                if (ex) k_adj_scatter_b<true, 2><<<brick_blocks(k_adj_scatter_b<true, 2>), DMPM_BRICK_THREADS, 0, ctx_->stream>>>(a);
+                else k_adj_scatter_b<false, 2><<<brick_blocks(k_adj_scatter_b<false, 2>), DMPM_BRICK_THREADS, 0, ctx_->stream>>>(a);
+            } else if (ush == 6) {
+                if (ex) k_adj_scatter_b<true, 4><<<brick_blocks(k_adj_scatter_b<true, 4>), DMPM_BRICK_THREADS, 0, ctx_->stream>>>(a);
+                else k_adj_scatter_b<false, 4><<<brick_blocks(k_adj_scatter_b<false, 4>), DMPM_BRICK_THREADS, 0, ctx_->stream>>>(a);
+            } else if (P.warp_general) {
                 if (ex) k_adj_scatter_w<true, true, ITEMS_PERSISTENT><<<ws, 256, 0, ctx_->stream>>>(a);
                 else k_adj_scatter_w<false, true, ITEMS_PERSISTENT><<<ws, 256, 0, ctx_->stream>>>(a);
             } else {
@@ -1093,8 +1156,17 @@ template <class T> class Engine : public EngineBase {
                                           sizeof(node4<T>), G_, cudaMemcpyDeviceToDevice, ctx_->stream));
             }
             pbeg(K_ADJ_GATHER);
-            if (ex) k_adj_gather_w<true, ITEMS_PERSISTENT><<<wg, 256, 0, ctx_->stream>>>(a);
-            else k_adj_gather_w<false, ITEMS_PERSISTENT><<<wg, 256, 0, ctx_->stream>>>(a);
+            if (ush == 3) {
+                if (ex) k_adj_gather_b<true, 2><<<brick_blocks(k_adj_gather_b<true, 2>), DMPM_BRICK_THREADS, 0, ctx_->stream>>>(a);
+                else k_adj_gather_b<false, 2><<<brick_blocks(k_adj_gather_b<false, 2>), DMPM_BRICK_THREADS, 0, ctx_->stream>>>(a);
+            } else if (ush == 6) {
+                if (ex) k_adj_gather_b<true, 4><<<brick_blocks(k_adj_gather_b<true, 4>), DMPM_BRICK_THREADS, 0, ctx_->stream>>>(a);
+                else k_adj_gather_b<false, 4><<<brick_blocks(k_adj_gather_b<false, 4>), DMPM_BRICK_THREADS, 0, ctx_->stream>>>(a);
+            } else if (ex) {
+                k_adj_gather_w<true, ITEMS_PERSISTENT><<<wg, 256, 0, ctx_->stream>>>(a);
+            } else {
+                k_adj_gather_w<false, ITEMS_PERSISTENT><<<wg, 256, 0, ctx_->stream>>>(a);
+            }
             launched();
             pend();
             if (DMPM_SPLIT_FINALIZE && !prof_) {
@@ -1578,13 +1650,15 @@ template <class T> class Engine : public EngineBase {
     double prof_ms_[K_COUNT] = {};
     int64_t prof_cnt_[K_COUNT] = {};
     // the layout the layer storage was allocated for (setup reuses it when unchanged)
+    std::map<const void*, int> brick_occ_;  // resident CTAs per SM of each brick kernel
     struct Layout {
         int L = -1, k_req = -1, control = -1, keep_adj = -1, keep_int = -1, sort_every = -1, stride = -1;
+        bool brick = false;  // epochs carry brick units
         size_t np = 0, G = 0;
         bool operator==(const Layout& o) const {
             return L == o.L && k_req == o.k_req && control == o.control && keep_adj == o.keep_adj &&
                    keep_int == o.keep_int && sort_every == o.sort_every && stride == o.stride && np == o.np &&
-                   G == o.G;
+                   G == o.G && brick == o.brick;
         }
     } layout_;
 };
@@ -1686,7 +1760,8 @@ int dmpm_set_params(dmpm_ctx* ctx, const dmpm_params* p) {
     if (!(p->dt >= 0) || p->adjoint_mode < 0 || p->adjoint_mode > 1 || p->control_mode < 0 || p->control_mode > 1 ||
         p->loss_kind < 0 || p->loss_kind > 1 || p->checkpoint_every < 0 || p->block_size < 0 || p->block_size > 256 ||
         (p->block_size % 32) != 0 || p->tile_cap < 0 || p->tile_cap > 1536 || p->sort_every < 0 ||
-        p->warp_general < 0 || p->warp_general > 1 || p->control_stride < 0 || p->eager < 0 || p->eager > 1) {
+        p->warp_general < 0 || p->warp_general > 1 || p->control_stride < 0 || p->eager < 0 || p->eager > 1 ||
+        (p->brick_cells != 0 && p->brick_cells != 2 && p->brick_cells != 4)) {
         ctx->err = "invalid dmpm_params";
         return DMPM_ERR_ARG;
     }

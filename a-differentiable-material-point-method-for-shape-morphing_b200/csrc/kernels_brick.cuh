@@ -1,0 +1,595 @@
+// kernels_brick.cuh -- FP32 path stencil kernels over cell bricks.
+//
+// The cell sort orders particles brick-major (sort.cuh), so the particles of a
+// unit -- a brick of 4 x 4 x 4 cells (B = 4) or one 2 x 2 x 2 octant of a
+// brick (B = 2) -- are one contiguous run of the sorted order.  Every stencil
+// of a particle whose cell lies in the unit falls inside the unit's node tile
+// of (B + 3)^3 nodes (stencil bases c - 1 .. c + B - 2 plus 3).  A CTA takes a
+// unit, stages the tile in shared memory once, and its threads each handle one
+// particle of the unit, all 64 stencil nodes of it:
+//   G2P and the adjoint P2G gather read the tile (the particles of a warp share
+//   a cell most of the time, so their reads are broadcasts);
+//   P2G and the adjoint G2P scatter add into the tile with shared-memory
+//   atomics -- each lane visits its stencil in its own order (node offsets
+//   xor-ed with lane bits), so the lanes of one cell touch 32 different nodes
+//   at a time -- and the tile is flushed once per unit with one vector
+//   red.global.add per touched node.
+// A particle that has left the unit since the sort (the sort runs every few
+// steps) is handled by the same code with its nodes read from or added to
+// global memory directly.
+//
+// Math per stage is that of kernels.cuh (which cites the reference) and of the
+// warp-item kernels in kernels_warp.cuh, summed in a different order.
+#pragma once
+#include "kernels_warp.cuh"
+
+namespace dmpm {
+
+#ifndef DMPM_BRICK_THREADS
+#define DMPM_BRICK_THREADS 128
+#endif
+// minimum resident CTAs per SM (the register cap the compiler works to)
+#ifndef DMPM_BRICK_G2P_MINB
+#define DMPM_BRICK_G2P_MINB 4
+#endif
+#ifndef DMPM_BRICK_GATHER_MINB
+#define DMPM_BRICK_GATHER_MINB 3
+#endif
+#ifndef DMPM_BRICK_SCATTER_MINB
+#define DMPM_BRICK_SCATTER_MINB 4
+#endif
+
+template <int B> struct BrickShape {
+    static constexpr int shift = B == 4 ? 6 : 3;  // key >> shift names the unit
+    static constexpr int E = B + 3;               // tile nodes per axis
+    static constexpr int NT = E * E * E;
+};
+
+// Tile origin (stencil base of the unit's first cell, c - 5 in key coordinates)
+__device__ __forceinline__ void unit_origin(uint32_t ukey, int shift, const GridGeom& g, int o[3]) {
+    int c[3];
+    unit_first_cell(ukey, shift, g.dim, c);
+#pragma unroll
+    for (int a = 0; a < 3; a++) o[a] = c[a] - 5;
+}
+
+// Per-axis stencil offsets d = x_g - x, weights N(d / dx) and slopes, for the
+// node offsets t ^ perm (t = 0..3) of the stencil starting at base.
+__device__ __forceinline__ void axis_stencil(float x, float mn, float dx, float idx, int base, int perm, float n[4],
+                                             float d[4], float* s) {
+#pragma unroll
+    for (int t = 0; t < 4; t++) {
+        const float xg = mn + (float)(base + (t ^ perm)) * dx;
+        d[t] = xg - x;
+        const float q = d[t] * idx;
+        n[t] = bsp(q);
+        if (s) s[t] = bsp_slope(q);
+    }
+}
+
+// Offset, weight and slope of stencil node t on one axis -- the slab and row
+// loops are not unrolled, so these come from x instead of per-node arrays.
+struct Axis0 {
+    float x, mn, dx, idx;
+    int base;
+    __device__ __forceinline__ void operator()(int t, float& n, float& d, float* s) const {
+        const float xg = mn + (float)(base + t) * dx;
+        d = xg - x;
+        const float q = d * idx;
+        n = bsp(q);
+        if (s) *s = bsp_slope(q);
+    }
+};
+
+// Node record fetch: from the unit's shared tile, or from global memory (zeros
+// outside the grid).  (i, j, k) are stencil offsets from the particle's base.
+template <int B, int R> struct TileFetch {
+    const node4<float>* tile;  // R records per node, node-major
+    int l0, l1, l2;            // particle base relative to the tile origin
+    __device__ __forceinline__ node4<float> operator()(int i, int j, int k, int r) const {
+        constexpr int E = BrickShape<B>::E;
+        return tile[R * (((l0 + i) * E + (l1 + j)) * E + (l2 + k)) + r];
+    }
+};
+template <int R> struct GlobalFetch {
+    const node4<float>* grid;
+    GridGeom g;
+    int goff;
+    int b0, b1, b2;  // particle base
+    __device__ __forceinline__ node4<float> operator()(int i, int j, int k, int r) const {
+        const int gi = b0 + i, gj = b1 + j, gk = b2 + k;
+        if ((unsigned)gi < (unsigned)g.dim[0] && (unsigned)gj < (unsigned)g.dim[1] && (unsigned)gk < (unsigned)g.dim[2])
+            return grid[(size_t)R * ((size_t)goff + ((size_t)gi * g.dim[1] + gj) * g.dim[2] + gk) + r];
+        return node4<float>{0.f, 0.f, 0.f, 0.f};
+    }
+};
+
+// Stage the unit's tile: R consecutive records per node from src (zeros
+// outside the grid).  Every thread of the block calls it.
+template <int B, int R>
+__device__ __forceinline__ void stage_tile(const node4<float>* __restrict__ src, const GridGeom& g, int goff,
+                                           const int o[3], node4<float>* tile) {
+    constexpr int E = BrickShape<B>::E, NT = BrickShape<B>::NT;
+    for (int q = threadIdx.x; q < NT * R; q += blockDim.x) {
+        const int nd = q / R, r = q - nd * R;
+        const int i = nd / (E * E), j = (nd / E) % E, k = nd % E;
+        const int gi = o[0] + i, gj = o[1] + j, gk = o[2] + k;
+        const bool in = (unsigned)gi < (unsigned)g.dim[0] && (unsigned)gj < (unsigned)g.dim[1] &&
+                        (unsigned)gk < (unsigned)g.dim[2];
+        tile[q] = in ? src[(size_t)R * ((size_t)goff + ((size_t)gi * g.dim[1] + gj) * g.dim[2] + gk) + r]
+                     : node4<float>{0.f, 0.f, 0.f, 0.f};
+    }
+}
+
+// is the particle's stencil inside the unit's tile?
+template <int B> __device__ __forceinline__ bool in_unit(const int base[3], const int o[3], int l[3]) {
+    bool in = true;
+#pragma unroll
+    for (int a = 0; a < 3; a++) {
+        l[a] = base[a] - o[a];
+        in &= (unsigned)l[a] < (unsigned)B;
+    }
+    return in;
+}
+
+// ------------------------------------------------------------------ G2P + P_op_2
+// v' = sum w v_g;  C' = 3/dx^2 sum w v_g d^T;  F' = (1 - s)(I + dt C')(F + dFc) + s F;  x' = x + dt v'
+template <class Fetch>
+__device__ __forceinline__ void g2p_sums(const Fetch& f, const Axis0& ax0, const float n1[4], const float d1[4],
+                                         const float n2[4], const float d2[4], float V[3], float Cm[3][3]) {
+    float nd2[4];
+#pragma unroll
+    for (int k = 0; k < 4; k++) nd2[k] = n2[k] * d2[k];
+#pragma unroll
+    for (int r = 0; r < 3; r++) {
+        V[r] = 0.f;
+        Cm[r][0] = Cm[r][1] = Cm[r][2] = 0.f;
+    }
+#pragma unroll 1
+    for (int i = 0; i < 4; i++) {
+        float n0, d0;
+        ax0(i, n0, d0, nullptr);
+        float Vi[3] = {0.f, 0.f, 0.f}, C1i[3] = {0.f, 0.f, 0.f}, C2i[3] = {0.f, 0.f, 0.f};
+#pragma unroll
+        for (int j = 0; j < 4; j++) {
+            float Vj[3] = {0.f, 0.f, 0.f}, Wj[3] = {0.f, 0.f, 0.f};
+#pragma unroll
+            for (int k = 0; k < 4; k++) {
+                const node4<float> g = f(i, j, k, 0);
+                const float vg[3] = {g.x, g.y, g.z};
+#pragma unroll
+                for (int r = 0; r < 3; r++) {
+                    Vj[r] += n2[k] * vg[r];
+                    Wj[r] += nd2[k] * vg[r];
+                }
+            }
+            const float n1d1 = n1[j] * d1[j];
+#pragma unroll
+            for (int r = 0; r < 3; r++) {
+                Vi[r] += n1[j] * Vj[r];
+                C1i[r] += n1d1 * Vj[r];
+                C2i[r] += n1[j] * Wj[r];
+            }
+        }
+        const float n0d0 = n0 * d0;
+#pragma unroll
+        for (int r = 0; r < 3; r++) {
+            V[r] += n0 * Vi[r];
+            Cm[r][0] += n0d0 * Vi[r];
+            Cm[r][1] += n0 * C1i[r];
+            Cm[r][2] += n0 * C2i[r];
+        }
+    }
+}
+
+template <int B>
+__global__ void __launch_bounds__(DMPM_BRICK_THREADS, DMPM_BRICK_G2P_MINB) k_g2p_b(WArgs a) {
+    using S = BrickShape<B>;
+    __shared__ node4<float> tile[S::NT];
+    const int nun = (int)*a.n_units_dev;
+    const size_t np = a.np, npl = a.npl, npn = a.npn;
+    const GridGeom geo = a.geo;
+    const float dx = (float)geo.dx, idx = 1.f / dx, k3 = 3.f / (dx * dx);
+    for (int u = blockIdx.x; u < nun; u += gridDim.x) {
+        int o[3];
+        unit_origin(a.unit_key[u], S::shift, geo, o);
+        const uint32_t q0 = a.unit_start[u], q1 = a.unit_start[u + 1];
+        __syncthreads();  // the previous unit's readers are done with the tile
+        stage_tile<B, 1>(a.grid, geo, 0, o, tile);
+        __syncthreads();
+        for (uint32_t q = q0 + threadIdx.x; q < q1; q += blockDim.x) {
+            const int p = (int)a.items.order[q];
+            float x[3];
+            int base[3];
+            load_x_base(a.st, npl, p, geo, x, base);
+            float n[3][4], d[3][4];
+#pragma unroll
+            for (int c = 1; c < 3; c++) axis_stencil(x[c], (float)geo.mn[c], dx, idx, base[c], 0, n[c], d[c], nullptr);
+            const Axis0 ax0{x[0], (float)geo.mn[0], dx, idx, base[0]};
+            float V[3], Cm[3][3];
+            int l[3];
+            if (in_unit<B>(base, o, l))
+                g2p_sums(TileFetch<B, 1>{tile, l[0], l[1], l[2]}, ax0, n[1], d[1], n[2], d[2], V, Cm);
+            else
+                g2p_sums(GlobalFetch<1>{a.grid, geo, 0, base[0], base[1], base[2]}, ax0, n[1], d[1], n[2], d[2], V,
+                         Cm);
+            m3<float> Cn;
+#pragma unroll
+            for (int r = 0; r < 3; r++)
+#pragma unroll
+                for (int c = 0; c < 3; c++) Cn.a[r][c] = k3 * Cm[r][c];
+            bool finite = true;
+#pragma unroll
+            for (int c = 0; c < 3; c++) {
+                const float xn = x[c] + a.dt * V[c];
+                a.st_next[(size_t)(PX + c) * npn + p] = xn;
+                a.st_next[(size_t)(PV + c) * npn + p] = V[c];
+                finite &= isfinite(xn);
+            }
+            store_m3(a.st_next + (size_t)PC * npn, npn, p, Cn);
+            const m3<float> F = load_m3(a.st + (size_t)PF * npl, npl, p);
+            const m3<float> Fe = F + load_m3(a.dfc, np, p);
+#pragma unroll
+            for (int c = 0; c < 3; c++)
+#pragma unroll
+                for (int r = 0; r < 3; r++) {
+                    const float t =
+                        Fe.a[r][c] + a.dt * (Cn.a[r][0] * Fe.a[0][c] + Cn.a[r][1] * Fe.a[1][c] + Cn.a[r][2] * Fe.a[2][c]);
+                    const float fn = (1.f - a.s) * t + a.s * F.a[r][c];
+                    a.st_next[(size_t)(PF + r + 3 * c) * npn + p] = fn;
+                    finite &= isfinite(fn);
+                }
+            if (!finite) atomicOr(a.status, ST_NONFINITE_FWD);
+        }
+    }
+}
+
+// ------------------------------------------------------------------ adjoint P2G gather
+// Per particle over its 64 nodes (records (dLdp, dLdm), (v, m)):
+//   M[r][c] = sum w d_r dLdp_c,  X = sum sigma grad(N N N),  u = sum w dLdp,  z = sum w v_g,
+//   sigma = m dLdm + dLdp.(m v c_d + G d) + v_g.(dLdv_next + 3/dx^2 dLdC_next d)
+// (the algebra of kernels.cuh:k_adj_gather), written to gath for the finalize.
+struct GatherIn {
+    float mp;
+    float mvp[3], vn[3];
+    m3<float> G, kC;  // G and 3/dx^2 dLdC_next
+};
+template <class Fetch>
+__device__ __forceinline__ void gather_sums(const Fetch& f, const GatherIn& in, const Axis0& ax0, const Axis0& ax1,
+                                            const float n2[4], const float d2[4], const float s2[4], float acc[18]) {
+    float nd2[4];
+#pragma unroll
+    for (int k = 0; k < 4; k++) nd2[k] = n2[k] * d2[k];
+#pragma unroll
+    for (int t = 0; t < 18; t++) acc[t] = 0.f;
+#pragma unroll 1
+    for (int i = 0; i < 4; i++) {
+        float n0, d0, s0;
+        ax0(i, n0, d0, &s0);
+        float hi[3], ei[3];
+#pragma unroll
+        for (int r = 0; r < 3; r++) {
+            hi[r] = in.mvp[r] + in.G.a[r][0] * d0;
+            ei[r] = in.vn[r] + in.kC.a[r][0] * d0;
+        }
+#pragma unroll 1
+        for (int j = 0; j < 4; j++) {
+            float n1, d1, s1;
+            ax1(j, n1, d1, &s1);
+            float hj[3], ej[3];
+#pragma unroll
+            for (int r = 0; r < 3; r++) {
+                hj[r] = hi[r] + in.G.a[r][1] * d1;
+                ej[r] = ei[r] + in.kC.a[r][1] * d1;
+            }
+            // row sums over k: S = sum n2 sigma, T = sum s2 sigma, U = sum n2 dLdp,
+            // Z = sum n2 v_g, W = sum n2 d2 dLdp
+            float Sj = 0.f, Tj = 0.f;
+            float U[3] = {0.f, 0.f, 0.f}, Z[3] = {0.f, 0.f, 0.f}, Wd[3] = {0.f, 0.f, 0.f};
+#pragma unroll
+            for (int k = 0; k < 4; k++) {
+                const node4<float> o = f(i, j, k, 0);
+                const node4<float> vg = f(i, j, k, 1);
+                float sig = in.mp * o.w;
+                sig += o.x * (hj[0] + in.G.a[0][2] * d2[k]);
+                sig += o.y * (hj[1] + in.G.a[1][2] * d2[k]);
+                sig += o.z * (hj[2] + in.G.a[2][2] * d2[k]);
+                sig += vg.x * (ej[0] + in.kC.a[0][2] * d2[k]);
+                sig += vg.y * (ej[1] + in.kC.a[1][2] * d2[k]);
+                sig += vg.z * (ej[2] + in.kC.a[2][2] * d2[k]);
+                Sj += n2[k] * sig;
+                Tj += s2[k] * sig;
+                U[0] += n2[k] * o.x;
+                U[1] += n2[k] * o.y;
+                U[2] += n2[k] * o.z;
+                Z[0] += n2[k] * vg.x;
+                Z[1] += n2[k] * vg.y;
+                Z[2] += n2[k] * vg.z;
+                Wd[0] += nd2[k] * o.x;
+                Wd[1] += nd2[k] * o.y;
+                Wd[2] += nd2[k] * o.z;
+            }
+            // the row's weights: w = n0 n1 n2, grad = (s0 n1 n2, n0 s1 n2, n0 n1 s2)
+            const float w01 = n0 * n1;
+            const float w01d0 = w01 * d0, w01d1 = w01 * d1;
+            acc[9] += (s0 * n1) * Sj;
+            acc[10] += (n0 * s1) * Sj;
+            acc[11] += w01 * Tj;
+#pragma unroll
+            for (int c = 0; c < 3; c++) {
+                acc[12 + c] += w01 * U[c];
+                acc[15 + c] += w01 * Z[c];
+                acc[c] += w01d0 * U[c];
+                acc[3 + c] += w01d1 * U[c];
+                acc[6 + c] += w01 * Wd[c];
+            }
+        }
+    }
+}
+
+template <bool EXACT, int B>
+__global__ void __launch_bounds__(DMPM_BRICK_THREADS, DMPM_BRICK_GATHER_MINB) k_adj_gather_b(WArgs a) {
+    using S = BrickShape<B>;
+    __shared__ node4<float> tile[2 * S::NT];
+    const int nun = (int)*a.n_units_dev;
+    const size_t np = a.np, npl = a.npl;
+    const GridGeom geo = a.geo;
+    const float dx = (float)geo.dx, idx = 1.f / dx, k3 = 3.f / (dx * dx);
+    const float cd = EXACT ? (1.f - a.dt * a.drag) : 1.f;
+    for (int u = blockIdx.x; u < nun; u += gridDim.x) {
+        int o[3];
+        unit_origin(a.unit_key[u], S::shift, geo, o);
+        const uint32_t q0 = a.unit_start[u], q1 = a.unit_start[u + 1];
+        __syncthreads();
+        stage_tile<B, 2>(a.gadj2, geo, 0, o, tile);
+        __syncthreads();
+        for (uint32_t q = q0 + threadIdx.x; q < q1; q += blockDim.x) {
+            const int p = (int)a.items.order[q];
+            float x[3];
+            int base[3];
+            load_x_base(a.st, npl, p, geo, x, base);
+            float n2[4], d2[4], s2[4];
+            axis_stencil(x[2], (float)geo.mn[2], dx, idx, base[2], 0, n2, d2, s2);
+            const Axis0 ax0{x[0], (float)geo.mn[0], dx, idx, base[0]};
+            const Axis0 ax1{x[1], (float)geo.mn[1], dx, idx, base[1]};
+            GatherIn in;
+            in.mp = a.cst[(size_t)KM * np + p];
+#pragma unroll
+            for (int c = 0; c < 3; c++) {
+                in.mvp[c] = in.mp * a.st[(size_t)(PV + c) * npl + p] * cd;
+                in.vn[c] = a.adjn[(size_t)c * np + p];
+            }
+            in.G = load_m3(a.G, npl, p);
+            in.kC = k3 * load_m3(a.adjn + 3 * np, np, p);
+            float acc[18];
+            int l[3];
+            if (in_unit<B>(base, o, l))
+                gather_sums(TileFetch<B, 2>{tile, l[0], l[1], l[2]}, in, ax0, ax1, n2, d2, s2, acc);
+            else
+                gather_sums(GlobalFetch<2>{a.gadj2, geo, 0, base[0], base[1], base[2]}, in, ax0, ax1, n2, d2, s2, acc);
+#pragma unroll
+            for (int t = 0; t < 18; t++) a.gath[(size_t)t * np + p] = acc[t];
+        }
+    }
+}
+
+// ------------------------------------------------------------------ scatters
+// Shared-memory tile of C float channels per node, channel-major (plane c at
+// c * NT), so lanes adding to different nodes of one channel hit different banks.
+// Lane bits permute each lane's stencil order: node offset (t ^ perm_a) on axis
+// a, perm = (lane & 3, lane >> 2 & 3, lane >> 4 & 1), so the 32 lanes of a warp
+// whose particles share a cell add to 32 different nodes at each step.
+struct LanePerm {
+    int p0, p1, p2;
+};
+__device__ __forceinline__ LanePerm lane_perm() {
+    const int lane = threadIdx.x & 31;
+    return LanePerm{lane & 3, (lane >> 2) & 3, (lane >> 4) & 1};
+}
+
+// Flush a tile of C channels into the grid (w = 0 when C == 3) and clear it.
+template <int B, int C>
+__device__ __forceinline__ void flush_tile(float* tile, node4<float>* grid, const GridGeom& g, const int o[3]) {
+    constexpr int E = BrickShape<B>::E, NT = BrickShape<B>::NT;
+    for (int q = threadIdx.x; q < NT; q += blockDim.x) {
+        const int i = q / (E * E), j = (q / E) % E, k = q % E;
+        const int gi = o[0] + i, gj = o[1] + j, gk = o[2] + k;
+        float v[4] = {0.f, 0.f, 0.f, 0.f};
+#pragma unroll
+        for (int c = 0; c < C; c++) {
+            v[c] = tile[c * NT + q];
+            tile[c * NT + q] = 0.f;
+        }
+        const bool in = (unsigned)gi < (unsigned)g.dim[0] && (unsigned)gj < (unsigned)g.dim[1] &&
+                        (unsigned)gk < (unsigned)g.dim[2];
+        if (in && (v[0] != 0.f || v[1] != 0.f || v[2] != 0.f || v[3] != 0.f))
+            red_add4(grid + (((size_t)gi * g.dim[1] + gj) * g.dim[2] + gk), v[0], v[1], v[2], v[3]);
+    }
+}
+
+// Node sink: shared-tile atomics or global vector reductions.  (i, j, k) are
+// stencil offsets from the particle's base (already permuted by the caller).
+template <int B, int C> struct TileSink {
+    float* tile;
+    int l0, l1, l2;
+    __device__ __forceinline__ void operator()(int i, int j, int k, const float (&v)[4]) const {
+        constexpr int E = BrickShape<B>::E, NT = BrickShape<B>::NT;
+        const int q = ((l0 + i) * E + (l1 + j)) * E + (l2 + k);
+#pragma unroll
+        for (int c = 0; c < C; c++) atomicAdd(tile + c * NT + q, v[c]);
+    }
+};
+struct GlobalSink {
+    node4<float>* grid;
+    GridGeom g;
+    int b0, b1, b2;
+    __device__ __forceinline__ void operator()(int i, int j, int k, const float (&v)[4]) const {
+        const int gi = b0 + i, gj = b1 + j, gk = b2 + k;
+        if ((unsigned)gi < (unsigned)g.dim[0] && (unsigned)gj < (unsigned)g.dim[1] && (unsigned)gk < (unsigned)g.dim[2])
+            red_add4(grid + (((size_t)gi * g.dim[1] + gj) * g.dim[2] + gk), v[0], v[1], v[2], v[3]);
+    }
+};
+
+// P2G of one particle: m_g += w m_p;  p_g += w (m_p v (1 - dt drag) + G (x_g - x_p)),
+// nodes in the lane's permuted order (arrays indexed by t hold offset t ^ perm).
+template <class Sink>
+__device__ __forceinline__ void p2g_particle(const Sink& sink, const LanePerm& P, float mp, const float mvd[3],
+                                             const m3<float>& G, const Axis0& ax0, const float n1[4],
+                                             const float d1[4], const float n2[4], const float d2[4]) {
+#pragma unroll 1
+    for (int i = 0; i < 4; i++) {
+        const int ii = i ^ P.p0;
+        float n0, d0;
+        ax0(ii, n0, d0, nullptr);
+        float g0[3];
+#pragma unroll
+        for (int r = 0; r < 3; r++) g0[r] = mvd[r] + G.a[r][0] * d0;
+#pragma unroll
+        for (int j = 0; j < 4; j++) {
+            float g1[3];
+#pragma unroll
+            for (int r = 0; r < 3; r++) g1[r] = g0[r] + G.a[r][1] * d1[j];
+            const float w01 = n0 * n1[j];
+#pragma unroll
+            for (int k = 0; k < 4; k++) {
+                const float wt = w01 * n2[k];
+                float v[4];
+#pragma unroll
+                for (int r = 0; r < 3; r++) v[r] = wt * (g1[r] + G.a[r][2] * d2[k]);
+                v[3] = wt * mp;
+                sink(ii, j ^ P.p1, k ^ P.p2, v);
+            }
+        }
+    }
+}
+
+template <int B>
+__global__ void __launch_bounds__(DMPM_BRICK_THREADS, DMPM_BRICK_SCATTER_MINB) k_p2g_b(WArgs a) {
+    using S = BrickShape<B>;
+    __shared__ float tile[4 * S::NT];
+    for (int q = threadIdx.x; q < 4 * S::NT; q += blockDim.x) tile[q] = 0.f;
+    const int nun = (int)*a.n_units_dev;
+    const size_t np = a.np, npl = a.npl;
+    const GridGeom geo = a.geo;
+    const float dx = (float)geo.dx, idx = 1.f / dx;
+    const float damp = 1.f - a.dt * a.drag;
+    const LanePerm P = lane_perm();
+    for (int u = blockIdx.x; u < nun; u += gridDim.x) {
+        int o[3];
+        unit_origin(a.unit_key[u], S::shift, geo, o);
+        const uint32_t q0 = a.unit_start[u], q1 = a.unit_start[u + 1];
+        __syncthreads();  // the tile is clear
+        for (uint32_t q = q0 + threadIdx.x; q < q1; q += blockDim.x) {
+            const int p = (int)a.items.order[q];
+            float x[3];
+            int base[3];
+            load_x_base(a.st, npl, p, geo, x, base);
+            float n[3][4], d[3][4];
+            axis_stencil(x[1], (float)geo.mn[1], dx, idx, base[1], P.p1, n[1], d[1], nullptr);
+            axis_stencil(x[2], (float)geo.mn[2], dx, idx, base[2], P.p2, n[2], d[2], nullptr);
+            const Axis0 ax0{x[0], (float)geo.mn[0], dx, idx, base[0]};
+            const float mp = a.cst[(size_t)KM * np + p];
+            float mvd[3];
+#pragma unroll
+            for (int c = 0; c < 3; c++) mvd[c] = mp * a.st[(size_t)(PV + c) * npl + p] * damp;
+            const m3<float> G = load_m3(a.G, npl, p);
+            int l[3];
+            if (in_unit<B>(base, o, l))
+                p2g_particle(TileSink<B, 4>{tile, l[0], l[1], l[2]}, P, mp, mvd, G, ax0, n[1], d[1], n[2], d[2]);
+            else
+                p2g_particle(GlobalSink{a.grid, geo, base[0], base[1], base[2]}, P, mp, mvd, G, ax0, n[1], d[1], n[2],
+                             d[2]);
+        }
+        __syncthreads();
+        flush_tile<B, 4>(tile, a.grid, geo, o);
+    }
+}
+
+// adjoint G2P scatter of one particle: dLdv_g += w dLdv_next + 3/dx^2 w dLdC_next (x_g - x_p)
+template <class Sink>
+__device__ __forceinline__ void adj_scatter_particle(const Sink& sink, const LanePerm& P, const float vn[3],
+                                                     const m3<float>& kC, const Axis0& ax0, const float n1[4],
+                                                     const float d1[4], const float n2[4], const float d2[4]) {
+#pragma unroll 1
+    for (int i = 0; i < 4; i++) {
+        const int ii = i ^ P.p0;
+        float n0, d0;
+        ax0(ii, n0, d0, nullptr);
+        float c0[3];
+#pragma unroll
+        for (int r = 0; r < 3; r++) c0[r] = vn[r] + kC.a[r][0] * d0;
+#pragma unroll
+        for (int j = 0; j < 4; j++) {
+            float c1[3];
+#pragma unroll
+            for (int r = 0; r < 3; r++) c1[r] = c0[r] + kC.a[r][1] * d1[j];
+            const float w01 = n0 * n1[j];
+#pragma unroll
+            for (int k = 0; k < 4; k++) {
+                const float wt = w01 * n2[k];
+                float v[4];
+#pragma unroll
+                for (int r = 0; r < 3; r++) v[r] = wt * (c1[r] + kC.a[r][2] * d2[k]);
+                v[3] = 0.f;
+                sink(ii, j ^ P.p1, k ^ P.p2, v);
+            }
+        }
+    }
+}
+
+// dLdv_next = dt dLdx' + dLdv';  dLdC_next = c dt dLdF' Fe^T + dLdC' (stored to adjn for
+// the gather and the finalize), then the scatter above (BackPropagation.cpp:14-44)
+template <bool EXACT, int B>
+__global__ void __launch_bounds__(DMPM_BRICK_THREADS, DMPM_BRICK_SCATTER_MINB) k_adj_scatter_b(WArgs a) {
+    using S = BrickShape<B>;
+    __shared__ float tile[3 * S::NT];
+    for (int q = threadIdx.x; q < 3 * S::NT; q += blockDim.x) tile[q] = 0.f;
+    const int nun = (int)*a.n_units_dev;
+    const size_t np = a.np, npl = a.npl, npn = a.npn;
+    const GridGeom geo = a.geo;
+    const float dx = (float)geo.dx, idx = 1.f / dx, k3 = 3.f / (dx * dx);
+    const float cf = EXACT ? (1.f - a.s) * a.dt : a.dt;
+    const LanePerm P = lane_perm();
+    for (int u = blockIdx.x; u < nun; u += gridDim.x) {
+        int o[3];
+        unit_origin(a.unit_key[u], S::shift, geo, o);
+        const uint32_t q0 = a.unit_start[u], q1 = a.unit_start[u + 1];
+        __syncthreads();
+        for (uint32_t q = q0 + threadIdx.x; q < q1; q += blockDim.x) {
+            const int p = (int)a.items.order[q];
+            float x[3];
+            int base[3];
+            load_x_base(a.st, npl, p, geo, x, base);
+            float vn[3];
+#pragma unroll
+            for (int c = 0; c < 3; c++)
+                vn[c] = a.dt * a.adj_next[(size_t)(PX + c) * npn + p] + a.adj_next[(size_t)(PV + c) * npn + p];
+            const m3<float> Fe = load_m3(a.st + (size_t)PF * npl, npl, p) + load_m3(a.dfc, np, p);
+            const m3<float> Cn = (cf * load_m3(a.adj_next + (size_t)PF * npn, npn, p)) * transpose(Fe) +
+                                 load_m3(a.adj_next + (size_t)PC * npn, npn, p);
+#pragma unroll
+            for (int c = 0; c < 3; c++) a.adjn[(size_t)c * np + p] = vn[c];
+            store_m3(a.adjn + 3 * np, np, p, Cn);
+            if (a.dbg_vnext) {
+#pragma unroll
+                for (int c = 0; c < 3; c++) a.dbg_vnext[(size_t)c * np + p] = vn[c];
+            }
+            if (a.dbg_Cnext) store_m3(a.dbg_Cnext, np, p, Cn);
+            float n[3][4], d[3][4];
+            axis_stencil(x[1], (float)geo.mn[1], dx, idx, base[1], P.p1, n[1], d[1], nullptr);
+            axis_stencil(x[2], (float)geo.mn[2], dx, idx, base[2], P.p2, n[2], d[2], nullptr);
+            const Axis0 ax0{x[0], (float)geo.mn[0], dx, idx, base[0]};
+            const m3<float> kC = k3 * Cn;
+            int l[3];
+            if (in_unit<B>(base, o, l))
+                adj_scatter_particle(TileSink<B, 3>{tile, l[0], l[1], l[2]}, P, vn, kC, ax0, n[1], d[1], n[2], d[2]);
+            else
+                adj_scatter_particle(GlobalSink{a.gadj, geo, base[0], base[1], base[2]}, P, vn, kC, ax0, n[1], d[1],
+                                     n[2], d[2]);
+        }
+        __syncthreads();
+        flush_tile<B, 3>(tile, a.gadj, geo, o);
+    }
+}
+
+}  // namespace dmpm

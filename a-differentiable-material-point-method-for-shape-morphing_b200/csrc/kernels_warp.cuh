@@ -316,6 +316,12 @@ struct WArgs {
     float* dbg_dLdP;
     float* dbg_vnext;
     float* dbg_Cnext;
+    // brick units of the sorted order (kernels_brick.cuh): unit u holds the
+    // sorted positions [unit_start[u], unit_start[u + 1]), all with key >> shift
+    // equal to unit_key[u]; the unit count stays on the device
+    const uint32_t* unit_start;
+    const uint32_t* unit_key;
+    const uint32_t* n_units_dev;
 };
 
 // How a warp-item launch walks its items:

@@ -17,9 +17,15 @@
 //     is cleared at the start of the call, so nothing carries over, but two
 //     calls whose GPU work overlaps (different streams, or different host
 //     threads) race on the array and give wrong results;
-//   * the first call on each device looks the array's device address up
-//     (cudaGetSymbolAddress, with that device current); make that first call
-//     before any stream capture.
+//   * the first call in each CUDA context looks the array's device address
+//     up (cudaGetSymbolAddress, with that context's device current) and keeps
+//     it for that context; make that first call before any stream capture.
+//     The address is keyed by the context's unique id (cuCtxGetId), so a
+//     caller that runs under its own (non-primary) context, or that reset the
+//     device (cudaDeviceReset, after which the library's module is loaded
+//     again, possibly at another address), gets the array of the context it
+//     is calling from.
+#include <cuda.h>  // CUcontext / CUresult for the two driver entry points below
 #include <cuda_runtime.h>
 
 #include <cstdio>
@@ -39,7 +45,12 @@ static __device__ __align__(256) float g_noalloc_mass[kNoAllocMaxNodes];
 
 constexpr int kMaxDevices = 64;
 std::mutex g_setup_mutex;
-float* g_scratch[kMaxDevices] = {};
+// per device: the context the address was looked up in (its unique id) and the address
+struct ScratchAddr {
+    unsigned long long ctx_id = 0;  // 0: not looked up yet
+    float* ptr = nullptr;
+};
+ScratchAddr g_scratch[kMaxDevices];
 
 struct Geom {
     int dim[3];
@@ -50,8 +61,8 @@ struct Geom {
 // mass-only P2G: m_g += w m_p (ForwardSimulation.cpp:11-51 with dt = drag = 0)
 __global__ void k_na_p2g_mass(int n, const float* __restrict__ x, const float* __restrict__ m, Geom g,
                               float* grid) {
-    const int p = blockIdx.x * blockDim.x + threadIdx.x;
-    if (p >= n) return;
+    const size_t p = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= (size_t)n) return;
     float xp[3];
     int base[3];
     dmpm::axis_w<float> w[3];
@@ -77,8 +88,8 @@ __global__ void k_na_p2g_mass(int n, const float* __restrict__ x, const float* _
 // vol_p = m_p / sum_g w m_g  (CalculatePointCloudVolumes, ForwardSimulation.cpp:262-290)
 __global__ void k_na_volumes(int n, const float* __restrict__ x, const float* __restrict__ m, Geom g,
                              const float* __restrict__ grid, float* vol) {
-    const int p = blockIdx.x * blockDim.x + threadIdx.x;
-    if (p >= n) return;
+    const size_t p = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= (size_t)n) return;
     float xp[3];
     int base[3];
     dmpm::axis_w<float> w[3];
@@ -102,26 +113,66 @@ __global__ void k_na_volumes(int n, const float* __restrict__ x, const float* __
     vol[p] = (fabsf(mg) > (float)dmpm::kFltEps) ? m[p] / mg : 0.f;
 }
 
-// Device address of the scratch array for the current device (looked up once).
-int scratch_for_current_device(float** out) {
+// Unique id of the CUDA context current on the calling thread, 0 when there
+// is none (or the driver cannot say).  The two driver functions come through
+// the runtime's entry-point query, so the library needs no link to libcuda.
+unsigned long long current_context_id() {
+    using GetCurrentFn = CUresult (*)(CUcontext*);
+    using GetIdFn = CUresult (*)(CUcontext, unsigned long long*);
+    static GetCurrentFn get_current = nullptr;
+    static GetIdFn get_id = nullptr;
+    static bool resolved = false;
+    if (!resolved) {  // under g_setup_mutex
+        void* f0 = nullptr;
+        void* f1 = nullptr;
+        cudaDriverEntryPointQueryResult q0{}, q1{};
+        if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &f0, cudaEnableDefault, &q0) == cudaSuccess &&
+            q0 == cudaDriverEntryPointSuccess &&
+            cudaGetDriverEntryPoint("cuCtxGetId", &f1, cudaEnableDefault, &q1) == cudaSuccess &&
+            q1 == cudaDriverEntryPointSuccess) {
+            get_current = reinterpret_cast<GetCurrentFn>(f0);
+            get_id = reinterpret_cast<GetIdFn>(f1);
+        }
+        cudaGetLastError();
+        resolved = true;
+    }
+    if (!get_current || !get_id) return 0;
+    CUcontext ctx = nullptr;
+    unsigned long long id = 0;
+    if (get_current(&ctx) != CUDA_SUCCESS || !ctx || get_id(ctx, &id) != CUDA_SUCCESS) return 0;
+    return id;
+}
+
+// Device address of the scratch array in the calling thread's context: looked
+// up with cudaGetSymbolAddress the first time a context calls, then reused
+// while that context stays current.  Where the context id cannot be read the
+// address is looked up on every call.
+int scratch_for_current_context(float** out) {
     int dev = -1;
     if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDevices) {
         cudaGetLastError();
         return DMPM_ERR_CUDA;
     }
     std::lock_guard<std::mutex> lock(g_setup_mutex);
-    if (!g_scratch[dev]) {
-        void* ptr = nullptr;
-        const cudaError_t e = cudaGetSymbolAddress(&ptr, g_noalloc_mass);
-        if (e != cudaSuccess || !ptr) {
-            std::fprintf(stderr, "dmpm_compute_volumes_noalloc: cudaGetSymbolAddress failed on device %d: %s\n", dev,
-                         cudaGetErrorString(e));
-            cudaGetLastError();
-            return DMPM_ERR_CUDA;
-        }
-        g_scratch[dev] = static_cast<float*>(ptr);
+    const unsigned long long id = current_context_id();
+    ScratchAddr& slot = g_scratch[dev];
+    if (id != 0 && slot.ctx_id == id) {
+        *out = slot.ptr;
+        return DMPM_OK;
     }
-    *out = g_scratch[dev];
+    void* ptr = nullptr;
+    const cudaError_t e = cudaGetSymbolAddress(&ptr, g_noalloc_mass);
+    if (e != cudaSuccess || !ptr) {
+        std::fprintf(stderr, "dmpm_compute_volumes_noalloc: cudaGetSymbolAddress failed on device %d: %s\n", dev,
+                     cudaGetErrorString(e));
+        cudaGetLastError();
+        return DMPM_ERR_CUDA;
+    }
+    // the lookup makes the device's primary context current when none was:
+    // read the id again so the next call from this context reuses the address
+    slot.ctx_id = id != 0 ? id : current_context_id();
+    slot.ptr = static_cast<float*>(ptr);
+    *out = slot.ptr;
     return DMPM_OK;
 }
 
@@ -140,7 +191,7 @@ extern "C" int dmpm_compute_volumes_noalloc(int n, const float* x, const float* 
         return DMPM_ERR_TOO_LARGE;
     }
     float* grid = nullptr;
-    const int st = scratch_for_current_device(&grid);
+    const int st = scratch_for_current_context(&grid);
     if (st != DMPM_OK) return st;
     if (n == 0) return DMPM_OK;
     cudaStream_t s = static_cast<cudaStream_t>(stream);
@@ -150,7 +201,7 @@ extern "C" int dmpm_compute_volumes_noalloc(int n, const float* x, const float* 
         cudaGetLastError();
         return DMPM_ERR_CUDA;
     }
-    const unsigned blocks = (unsigned)((n + 255) / 256);
+    const unsigned blocks = (unsigned)(((size_t)n + 255) / 256);
     k_na_p2g_mass<<<blocks, 256, 0, s>>>(n, x, m, g, grid);
     k_na_volumes<<<blocks, 256, 0, s>>>(n, x, m, g, grid, vol);
     return cudaGetLastError() == cudaSuccess ? DMPM_OK : DMPM_ERR_CUDA;

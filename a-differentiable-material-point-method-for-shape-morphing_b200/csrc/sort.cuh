@@ -1,13 +1,20 @@
 // sort.cuh -- stable LSD radix sort of (cell key, particle index) pairs, the
 // scans it needs, and the grouping of sorted particles into warp items.
 //
-// Cell key of a particle = linear index of the cell holding it, computed with
-// the reference's floor((x - min) / dx) by division (ForwardSimulation.cpp:19),
-// shifted so that clamped out-of-grid cells stay non-negative:
-//   c_a = stencil_base_a + 1 + 4            (in [1, dim_a + 5])
-//   key = (c_0 * (dim_1 + 8) + c_1) * (dim_2 + 8) + c_2
-// Sorting is stable, so equal keys keep their index order and the permutation
-// equals a CPU std::stable_sort / numpy argsort(kind="stable") of the keys.
+// Cell key of a particle: the cell holding it, from the reference's
+// floor((x - min) / dx) by division (ForwardSimulation.cpp:19), shifted so that
+// clamped out-of-grid cells stay non-negative,
+//   c_a = stencil_base_a + 1 + 4            (in [1, dim_a + 5]),
+// ordered brick-major: bricks of 4 x 4 x 4 cells, b_a = c_a >> 2, numbered
+// linearly over nb_a = (dim_a + 5) / 4 + 1 bricks per axis, and the 64 cells of
+// a brick in Morton order of their local coordinates l_a = c_a & 3,
+//   key = ((b_0 nb_1 + b_1) nb_2 + b_2) 64 + morton(l_0, l_1, l_2),
+//   morton = (l_0>>1) 32 + (l_1>>1) 16 + (l_2>>1) 8 + (l_0&1) 4 + (l_1&1) 2 + (l_2&1).
+// So the particles of one cell (a run of equal keys), of one 2 x 2 x 2 octant
+// of a brick (equal key >> 3) and of one brick (equal key >> 6) are contiguous
+// in the sorted order.  Sorting is stable, so equal keys keep their index
+// order and the permutation equals a CPU std::stable_sort / numpy
+// argsort(kind="stable") of the keys.
 //
 // Radix sort: 8-bit digits, per pass three kernels --
 //   upsweep   per-tile digit histograms  -> counts[digit][tile]
@@ -42,9 +49,32 @@ template <class T> struct KeyArgs {
     uint32_t* vals;
 };
 
+DMPM_HD uint32_t bricks_per_axis(int dim) { return (uint32_t)(dim + 5) / 4u + 1u; }
+// number of distinct keys of a grid (keys lie in [0, key_span))
+DMPM_HD uint64_t key_span(const int dim[3]) {
+    return (uint64_t)bricks_per_axis(dim[0]) * bricks_per_axis(dim[1]) * bricks_per_axis(dim[2]) * 64u;
+}
 DMPM_HD uint32_t cell_key(const int base[3], const int dim[3]) {
     const uint32_t c0 = (uint32_t)(base[0] + 5), c1 = (uint32_t)(base[1] + 5), c2 = (uint32_t)(base[2] + 5);
-    return (c0 * (uint32_t)(dim[1] + 8) + c1) * (uint32_t)(dim[2] + 8) + c2;
+    const uint32_t brick = ((c0 >> 2) * bricks_per_axis(dim[1]) + (c1 >> 2)) * bricks_per_axis(dim[2]) + (c2 >> 2);
+    const uint32_t l0 = c0 & 3u, l1 = c1 & 3u, l2 = c2 & 3u;
+    const uint32_t morton = ((l0 >> 1) << 5) | ((l1 >> 1) << 4) | ((l2 >> 1) << 3) | ((l0 & 1u) << 2) |
+                            ((l1 & 1u) << 1) | (l2 & 1u);
+    return brick * 64u + morton;
+}
+// First cell (c_0, c_1, c_2) of the unit of 2^(shift/3) cells per axis whose keys
+// share key >> shift (shift 6: a brick, 3: an octant of a brick, 0: a cell).
+DMPM_HD void unit_first_cell(uint32_t key_hi, int shift, const int dim[3], int c[3]) {
+    const uint32_t key = key_hi << shift;
+    uint32_t brick = key >> 6;
+    const uint32_t nb1 = bricks_per_axis(dim[1]), nb2 = bricks_per_axis(dim[2]);
+    const uint32_t b2 = brick % nb2;
+    brick /= nb2;
+    const uint32_t b1 = brick % nb1, b0 = brick / nb1;
+    const uint32_t m = key & 63u;
+    c[0] = (int)(4u * b0 + (((m >> 5) & 1u) << 1) + ((m >> 2) & 1u));
+    c[1] = (int)(4u * b1 + (((m >> 4) & 1u) << 1) + ((m >> 1) & 1u));
+    c[2] = (int)(4u * b2 + (((m >> 3) & 1u) << 1) + (m & 1u));
 }
 
 template <class T> __global__ void k_cell_keys(KeyArgs<T> a) {
@@ -250,6 +280,26 @@ static __global__ void k_item_starts(const uint32_t* __restrict__ keys, const ui
 }
 static __global__ void k_item_sentinel(uint32_t* item_start, const uint32_t* n_items, int n) {
     item_start[*n_items] = (uint32_t)n;
+}
+
+// ------------------------------------------------------------------ units
+// A unit is a run of sorted particles with equal key >> shift: the particles of
+// one brick (shift 6) or one brick octant (shift 3).  flags[i] = 1 where a unit
+// starts; after an exclusive sum scan of flags into idx, k_unit_starts writes
+// each unit's first sorted position and its key >> shift.
+__device__ __forceinline__ bool unit_head(const uint32_t* keys, int i, int shift) {
+    return i == 0 || (keys[i] >> shift) != (keys[i - 1] >> shift);
+}
+static __global__ void k_unit_flags(const uint32_t* __restrict__ keys, int n, int shift, uint32_t* flags) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) flags[i] = unit_head(keys, i, shift) ? 1u : 0u;
+}
+static __global__ void k_unit_starts(const uint32_t* __restrict__ keys, const uint32_t* __restrict__ idx, int n,
+                                     int shift, uint32_t* unit_start, uint32_t* unit_key) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n || !unit_head(keys, i, shift)) return;
+    unit_start[idx[i]] = (uint32_t)i;
+    unit_key[idx[i]] = keys[i] >> shift;
 }
 
 }  // namespace dmpm

@@ -47,7 +47,7 @@ class Params(ctypes.Structure):
                 ("loss_kind", ctypes.c_int), ("checkpoint_every", ctypes.c_int), ("keep_adjoints", ctypes.c_int),
                 ("keep_intermediates", ctypes.c_int), ("block_size", ctypes.c_int), ("tile_cap", ctypes.c_int),
                 ("sort_every", ctypes.c_int), ("warp_general", ctypes.c_int), ("control_stride", ctypes.c_int),
-                ("eager", ctypes.c_int)]
+                ("eager", ctypes.c_int), ("brick_cells", ctypes.c_int)]
 
 
 class Instance(ctypes.Structure):
@@ -239,7 +239,7 @@ class Context:
                    adjoint: str = "refcompat", control: str = "per_layer", loss: str = "ref",
                    checkpoint_every: int = 0, keep_adjoints: bool = False, keep_intermediates: bool = False,
                    block_size: int = 0, tile_cap: int = 0, sort_every: int = 0, warp_general: bool = False,
-                   control_stride: int = 0, eager: bool = False):
+                   control_stride: int = 0, eager: bool = False, brick_cells: int = 0):
         p = Params()
         self.lib.dmpm_default_params(ctypes.byref(p))
         p.dt, p.drag, p.smoothing = float(dt), float(drag), float(smoothing)
@@ -257,6 +257,7 @@ class Context:
         p.warp_general = int(bool(warp_general))
         p.control_stride = int(control_stride)
         p.eager = int(bool(eager))
+        p.brick_cells = int(brick_cells)
         self._ck(self.lib.dmpm_set_params(self.h, ctypes.byref(p)), "set_params")
         self.params = p
 

@@ -172,13 +172,18 @@ def build_scene(instance: int, ppc_root: int):
     return sc
 
 
+# stencil kernels of the FP32 path: 0 = warp items, 2 or 4 = bricks of that many cells per axis
+BRICK_CELLS = 0
+
+
 def setup_ctx(dmpm, sc, prec, device, vol, target, dt, checkpoint_every, control="tied", control_stride=0):
     c = dmpm.Context(prec, device)
     c.set_grid(sc.dims, sc.dx, sc.min_point)
     c.set_particles(sc.x, sc.m, sc.lam, sc.mu, v=sc.v, F=sc.F, C=sc.C, dFc=sc.dFc, vol=vol)
     c.set_target_mass(target)
     c.set_params(dt=dt, drag=sc.drag, f_ext=sc.f_ext, smoothing=sc.smoothing, adjoint="exact", control=control,
-                 loss="ref", checkpoint_every=checkpoint_every, control_stride=control_stride)
+                 loss="ref", checkpoint_every=checkpoint_every, control_stride=control_stride,
+                 brick_cells=BRICK_CELLS if prec == "fp32" else 0)
     c.setup(sc.steps + 1)
     return c
 
@@ -351,6 +356,7 @@ def workload_config(sc, dt_sub, ckpt):
             "particles": sc.n, "grid": list(sc.dims), "layers": sc.steps + 1, "dt": sc.dt,
             "dt_substituted_from": dt_sub, "checkpoint_every": ckpt, "loss": "reference log-mass + min-mass penalty",
             "l2_policy": "inputs larger than L2 (per-rollout layer state > 5 GB, 126 MB L2)",
+            "stencil_kernels": "bricks of %d^3 cells" % BRICK_CELLS if BRICK_CELLS else "warp items",
             "parallelism": "replicas: one independent instance per GPU"}
 
 
@@ -960,6 +966,8 @@ def main():
     ap.add_argument("--ppc-root", type=int, default=3, help="particles per cell = ppc_root^3 (3 -> ~267k)")
     ap.add_argument("--dt", type=float, default=0.0, help="override dt (default: configured, CFL fallback)")
     ap.add_argument("--checkpoint-every", type=int, default=1)
+    ap.add_argument("--brick", type=int, default=None, choices=[0, 2, 4],
+                    help="FP32 stencil kernels: 0 warp items, 2 or 4 cells per brick axis")
     ap.add_argument("--rollout-steps", type=int, default=0, help="override the 200 time steps (profiling runs)")
     ap.add_argument("--no-fp64", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
@@ -973,6 +981,9 @@ def main():
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
+    global BRICK_CELLS
+    if args.brick is not None:
+        BRICK_CELLS = args.brick
     if args.impl == "reference":
         return run_reference(args)
     if args.fd:

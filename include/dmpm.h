@@ -138,6 +138,10 @@ typedef struct {
     int eager;               /* FP32 path with every layer kept: 0 = capture dmpm_forward / dmpm_backward
                                 once per start (top, control) layer and replay them as CUDA graphs;
                                 1 = launch kernel by kernel (per-kernel profiling also does) */
+    int brick_cells;         /* FP32 path: 0 = warp-item stencil kernels (8 particles of a cell per
+                                warp); 2 or 4 = brick kernels: a CTA stages the node tile of a brick
+                                of brick_cells^3 cells in shared memory and each thread handles one
+                                particle of the brick.  Takes effect at the next cell sort. */
 } dmpm_params;
 
 void dmpm_default_params(dmpm_params* p);
@@ -236,11 +240,12 @@ int64_t dmpm_launch_count(const dmpm_ctx* ctx);
 int dmpm_cell_sort(dmpm_ctx* ctx, int layer, uint32_t* keys, uint32_t* order, uint32_t* item_start, int* n_items);
 
 /* Particle volumes without any device allocation.  No counterpart in the
- * reference: it computes what dmpm_compute_volumes computes
- * (CalculatePointCloudVolumes: vol_p = m_p / sum_g w m_g) for callers that
- * cannot call cudaMalloc -- a frame loop that must not take the device-wide
- * synchronisation of cudaMalloc/cudaFree, or a process whose device memory is
- * already held by another framework's caching allocator.
+ * reference.  It computes vol_p = m_p / sum_g w_gp m_g, where m_g = sum_q
+ * w_gq m_q are the node masses of a mass-only particle-to-grid transfer and
+ * w the cubic B-spline weights (the values dmpm_compute_volumes stores), for
+ * callers that cannot call cudaMalloc -- a frame loop that must not take the
+ * device-wide synchronisation of cudaMalloc/cudaFree, or a process whose
+ * device memory is already held by another framework's caching allocator.
  *   x   device, n * 3 floats (x, y, z per particle, lattice units)
  *   m   device, n floats;  vol: device, n floats (output)
  *   min_point: host, 3 floats;  stream: a cudaStream_t (NULL = default stream)
@@ -248,9 +253,11 @@ int dmpm_cell_sort(dmpm_ctx* ctx, int layer, uint32_t* keys, uint32_t* order, ui
  * that loads the library holds it until exit): grids above 1,048,576 nodes
  * (dim_x * dim_y * dim_z) return DMPM_ERR_TOO_LARGE.  The array is shared by
  * all calls on a device and cleared at the start of each call; calls whose GPU
- * work overlaps race on it.  The first call on a device looks the array up
- * with that device current; make it before any stream capture.  Asynchronous
- * with respect to the host: results are ready when the stream is. */
+ * work overlaps race on it.  The first call in each CUDA context (the primary
+ * context of a device, a caller's own context, or the primary context again
+ * after cudaDeviceReset) looks the array's address up in that context; make
+ * it before any stream capture.  Asynchronous with respect to the host:
+ * results are ready when the stream is. */
 int dmpm_compute_volumes_noalloc(int n, const float* x, const float* m, int dim_x, int dim_y, int dim_z, float dx,
                                  const float* min_point, float* vol, void* stream);
 

@@ -21,6 +21,18 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 ORACLE_SO = os.path.join(HERE, "lib", "liboracle.so")
 REF_DIR = os.path.join(HERE, "_ref")
 
+
+def reference_source_dir() -> str:
+    """Where the reference's source tree lies: $DMPM_REFERENCE_DIR, else a
+    directory named "reference" beside this repository's checkout.  Only the
+    recipes that compile the reference (and the tests that call its tools)
+    read it; nothing on the GPU side does."""
+    env = os.environ.get("DMPM_REFERENCE_DIR")
+    if env:
+        return env
+    repo = os.path.dirname(HERE)
+    return os.path.join(os.path.dirname(repo), "reference")
+
 _P = ctypes.c_void_p
 
 
@@ -292,10 +304,30 @@ class RefGraph:
 
     def set(self, layer, name, value):
         code = _REF_PF[name]
-        arr = np.ascontiguousarray(_cm(value) if name in ("F", "C", "dFc", "P") else value, dtype=self.dt_np)
+        matrix = name not in _VEC3 and name not in _SCAL  # 3x3 fields are stored column-major
+        arr = np.ascontiguousarray(_cm(value) if matrix else value, dtype=self.dt_np)
         self._keep_set = arr
         self.lib.ref_graph_set_particles.argtypes = [_P, ctypes.c_int, ctypes.c_int, _P]
         self.lib.ref_graph_set_particles(self.h, layer, code, _ptr(arr))
+
+    def descend(self, rule: str, layer: int, lr: float, gnorm: float, beta1: float = 0.9, beta2: float = 0.999,
+                eps: float = 1e-5, t: int = 1):
+        """One step of PointCloud::Descend_<rule> on a layer (PointCloud.cpp:83-204):
+        adam, amsgrad, lion (beta1 as its beta), gd, dldf."""
+        R, I = self.R, ctypes.c_int
+        if rule in ("adam", "amsgrad"):
+            fn = getattr(self.lib, "ref_graph_descend_" + rule)
+            fn.argtypes = [_P, I, R, R, R, R, R, I]
+            fn(self.h, layer, lr, gnorm, beta1, beta2, eps, t)
+        elif rule == "lion":
+            self.lib.ref_graph_descend_lion.argtypes = [_P, I, R, R, R]
+            self.lib.ref_graph_descend_lion(self.h, layer, lr, beta1, gnorm)
+        elif rule in ("gd", "dldf"):
+            fn = getattr(self.lib, "ref_graph_descend_" + rule)
+            fn.argtypes = [_P, I, R, R]
+            fn(self.h, layer, lr, gnorm)
+        else:
+            raise ValueError(rule)
 
     def time_forward_multithread(self, steps, threads) -> float:
         self.lib.ref_time_forward_multithread.restype = ctypes.c_double

@@ -253,12 +253,21 @@ void ref_graph_get_grid(void* h, int layer, int field, real* out) {
     copy_out_grid(*static_cast<Scene*>(h)->graph->layers[layer].grid, field, out);
 }
 
-// PointCloud::Descend_Adam / Descend_Lion on one layer (PointCloud.cpp:83-162).
+// PointCloud's descent rules on one layer (PointCloud.cpp:83-204).
 void ref_graph_descend_adam(void* h, int layer, real alpha, real gnorm, real b1, real b2, real eps, int t) {
     static_cast<Scene*>(h)->graph->layers[layer].point_cloud->Descend_Adam(alpha, gnorm, b1, b2, eps, t);
 }
+void ref_graph_descend_amsgrad(void* h, int layer, real alpha, real gnorm, real b1, real b2, real eps, int t) {
+    static_cast<Scene*>(h)->graph->layers[layer].point_cloud->Descend_AMSGrad(alpha, gnorm, b1, b2, eps, t);
+}
 void ref_graph_descend_lion(void* h, int layer, real alpha, real beta, real gnorm) {
     static_cast<Scene*>(h)->graph->layers[layer].point_cloud->Descend_Lion(alpha, beta, gnorm);
+}
+void ref_graph_descend_gd(void* h, int layer, real alpha, real gnorm) {
+    static_cast<Scene*>(h)->graph->layers[layer].point_cloud->Descend_GradientDescent(alpha, gnorm);
+}
+void ref_graph_descend_dldf(void* h, int layer, real alpha, real gnorm) {
+    static_cast<Scene*>(h)->graph->layers[layer].point_cloud->Descend_dLdF(alpha, gnorm);
 }
 
 // Timed forward of layers [0, steps) with MultiThreadMPM::ForwardTimeStep

@@ -28,6 +28,13 @@ Fixtures:
   rollout_long_f32.npz      the same rollouts by the shipped FP32 build (same
                             volumes and target), the float reference's own drift
                             from the FP64 build.
+  config0_f64.npz           the small benchmark configuration at full size (a
+                            jittered sphere of 8,778 particles on 32^3, 100 steps
+                            at half the explicit CFL limit) by the FP64 build with
+                            its own adjoint: volumes, target raster, the final
+                            positions, the loss and the layer-0 dLdF and dLdx.
+
+    python tests/golden/make_golden.py [elementary rollout long mpmbin config0]
 """
 from __future__ import annotations
 
@@ -171,12 +178,44 @@ def make_mpmbin():
     r.lib.ref_scene_write_mpmbin(r.h, os.path.join(HERE, "cloud_ref.mpmbin").encode())
 
 
+def config0_scene():
+    """The small benchmark scene (sphere r = 0.2 on 32^3, 8 per cell, 100 steps),
+    its configured dt replaced by half the explicit CFL limit when above it."""
+    sc = scenes.config_scene(0)
+    lim = sc.cfl_dt()
+    if sc.dt > lim:
+        sc.dt = 0.5 * lim
+    return sc
+
+
+def make_config0():
+    sc = config0_scene()
+    r = RefGraph(sc, "f64")
+    vol = r.calc_volumes()
+    target = r.target_mass()
+    sc.vol = vol.astype(np.float64)
+    L = sc.steps + 1
+    r = RefGraph(sc, "f64", target_m=target)
+    r.setup(L, sc.dt, sc.drag, sc.f_ext, sc.smoothing)
+    r.forward(0)
+    loss = r.loss()
+    r.backward(0)
+    np.savez_compressed(os.path.join(HERE, "config0_f64.npz"), vol=vol, target=target, dt=np.array(sc.dt),
+                        x_last=r.get(L - 1, "x"), loss=np.array(loss), dLdF_0=r.get(0, "dLdF"),
+                        dLdx_0=r.get(0, "dLdx"))
+
+
 if __name__ == "__main__":
+    parts = sys.argv[1:] or ["elementary", "rollout", "long", "mpmbin", "config0"]
     for prec in ("f64", "f32"):
-        make_elementary(prec)
-        make_rollout(prec)
-        print("wrote", prec)
-    make_rollout_long()
-    print("wrote rollout_long_f64, rollout_long_f32")
-    make_mpmbin()
-    print("wrote cloud_ref.mpmbin")
+        if "elementary" in parts:
+            make_elementary(prec)
+        if "rollout" in parts:
+            make_rollout(prec)
+    if "long" in parts:
+        make_rollout_long()
+    if "mpmbin" in parts:
+        make_mpmbin()
+    if "config0" in parts:
+        make_config0()
+    print("wrote", " ".join(parts))

@@ -17,7 +17,7 @@ import pytest
 
 import dmpm
 import scenes
-from oracle.lib import OracleGraph
+from oracle.lib import OracleGraph, RefGraph
 from tests.golden.make_golden import ROLLOUT_LAYERS, rollout_scene
 from tests.helpers import load_golden, normrel, relerr
 
@@ -55,12 +55,14 @@ def test_volumes_and_target_raster(gpu_ready, g64):
             c.set_particles(sc.x, sc.m, sc.lam, sc.mu, v=sc.v, F=sc.F, C=sc.C, dFc=sc.dFc)
             c.compute_volumes()
             c.rasterize_target(sc.target_points, sc.target_mp)
+            # the target grid: the reference's mass-only P2G of the target samples
+            # (LoadCompGraph, MPMPolyscope.cpp:142-160), from its FP64 build
+            assert relerr(c.target_mass(), g64["target"]) < tol
             c.set_params(dt=sc.dt)
             c.setup(2)
             assert relerr(c.get(0, "vol"), g64["vol"]) < tol
             c.forward(0)
             c.loss()
-            # the target raster is observable through dL/dm = f(m, target)
             assert np.all(np.isfinite(c.get_grid(1, "grid_dLdm")))
 
 
@@ -148,6 +150,33 @@ def test_long_rollouts_match_reference(gpu_ready, prec, steps):
                 assert relerr(got, ref) < 1e-9, k
             else:
                 assert normrel(got, ref) < 3e-4, k
+
+
+def test_config0_full_size_fp64_matches_reference(gpu_ready):
+    """The plain FP64 GPU path on the small benchmark configuration at full size
+    (8,778 particles, 32^3, 100 steps, the reference's own adjoint with
+    per-layer controls) against the reference's FP64 build (config0_f64):
+    final positions, loss, layer-0 dLdF and dLdx, at the bars of
+    tests/test_oracle_pin.py (the reference's finite-difference d(J F^-T)/dF
+    makes its adjoint move by ~1e-10 under rounding-level input changes)."""
+    from tests.golden.make_golden import config0_scene
+    from tests.test_oracle_pin import _config0_bars
+
+    g = load_golden("config0_f64")
+    sc = config0_scene()
+    sc.vol = np.asarray(g["vol"], dtype=np.float64)
+    L = sc.steps + 1
+    bar = _config0_bars()
+    with make_ctx(sc, "fp64", g["target"], adjoint="refcompat", control="per_layer") as c:
+        c.setup(L)
+        assert c.forward(0) == dmpm.OK
+        loss = c.loss()
+        assert c.backward(0) == dmpm.OK
+        assert relerr(c.get(L - 1, "x"), g["x_last"]) < bar["x"]
+        assert abs(loss - float(g["loss"])) / abs(float(g["loss"])) < bar["loss"]
+        for k in ("dLdF", "dLdx"):
+            assert relerr(c.get(0, k), g[k + "_0"]) < bar["adj_maxabs"], k
+            assert normrel(c.get(0, k), g[k + "_0"]) < bar["adj_norm"], k
 
 
 @pytest.mark.parametrize("steps", [1, 10, 30, 100])
@@ -350,7 +379,12 @@ def _cpu_cell_keys(x, dims, dx=1.0, mn=(0.0, 0.0, 0.0)):
     q = np.floor((x32 - np.asarray(mn, dtype=np.float32)) / np.float32(dx)).astype(np.int64)
     b = np.clip(np.clip(q, -8, np.asarray(dims) + 8) - 1, -4, np.asarray(dims))
     c = b + 5
-    return ((c[:, 0] * (dims[1] + 8) + c[:, 1]) * (dims[2] + 8) + c[:, 2]).astype(np.uint32)
+    nb = (np.asarray(dims) + 5) // 4 + 1
+    br, lo = c >> 2, c & 3
+    brick = (br[:, 0] * nb[1] + br[:, 1]) * nb[2] + br[:, 2]
+    morton = ((lo[:, 0] >> 1) << 5) | ((lo[:, 1] >> 1) << 4) | ((lo[:, 2] >> 1) << 3) | ((lo[:, 0] & 1) << 2) \
+        | ((lo[:, 1] & 1) << 1) | (lo[:, 2] & 1)
+    return (brick * 64 + morton).astype(np.uint32)
 
 
 @pytest.mark.parametrize("shuffle", [False, True])
@@ -537,9 +571,31 @@ def test_nonfinite_is_flagged_not_faulted(gpu_ready):
             assert np.all(np.isfinite(c.get(3, "x")))
 
 
-def test_device_adam_step_matches_reference_formula(gpu_ready, exact_case):
+def _reference_descent(sc, d, g, steps, lr, b1, b2, eps):
+    """The reference's own PointCloud::Descend_* (its float build, compiled from
+    its sources into oracle/_ref) applied to layer 0 of a CompGraph whose dFc
+    is d and whose dLdF is the gradient g, with the same gradient norm: the dFc
+    after each (rule, t) step of `steps`."""
+    from oracle.lib import ref_available
+
+    if not ref_available("f32"):
+        pytest.skip("the reference's float build (oracle/_ref) has not been compiled")
+    r = RefGraph(sc, "f32", target_m=np.zeros(int(np.prod(sc.dims))), target_from_points=False)
+    r.setup(2, sc.dt, sc.drag, sc.f_ext, sc.smoothing)
+    r.set(0, "dFc", d)
+    r.set(0, "dLdF", g)
+    gnorm = float(np.linalg.norm(g))
+    out = []
+    for rule, t in steps:
+        r.descend(rule, 0, lr, gnorm, b1, b2, eps, t)
+        out.append(r.get(0, "dFc").astype(np.float64))
+    return out
+
+
+def test_device_adam_step_matches_reference_descend_adam(gpu_ready, exact_case):
     """dmpm_adam_step = PointCloud::Descend_Adam on the tied control gradient,
-    with the gradient divided by its norm (PointCloud.cpp:83-99)."""
+    with the gradient divided by its norm (PointCloud.cpp:83-99): two steps
+    (the second reuses the moments) against the reference's compiled Descend_Adam."""
     sc, o, loss, L = exact_case
     with make_ctx(sc, "fp32", o.target, adjoint="exact", control="tied") as c:
         c.setup(L)
@@ -550,16 +606,9 @@ def test_device_adam_step_matches_reference_formula(gpu_ready, exact_case):
         d0 = c.get(0, "dFc")
         c.adam_step(t=1, lr=1e-2, beta1=0.9, beta2=0.999, eps=1e-5)
         d1 = c.get(0, "dFc")
-        # a second step reuses the moments
         c.adam_step(t=2, lr=1e-2, beta1=0.9, beta2=0.999, eps=1e-5)
         d2 = c.get(0, "dFc")
-    gn = g / np.linalg.norm(g)
-    m = 0.1 * gn
-    v = 0.001 * gn * gn
-    want1 = d0 - 1e-2 * (m / (1 - 0.9)) / (np.sqrt(v / (1 - 0.999)) + 1e-5)
-    m2 = 0.9 * m + 0.1 * gn
-    v2 = 0.999 * v + 0.001 * gn * gn
-    want2 = want1 - 1e-2 * (m2 / (1 - 0.81)) / (np.sqrt(v2 / (1 - 0.999 ** 2)) + 1e-5)
+    want1, want2 = _reference_descent(sc, d0, g, [("adam", 1), ("adam", 2)], 1e-2, 0.9, 0.999, 1e-5)
     assert relerr(d1 - d0, want1 - d0) < 1e-4
     assert relerr(d2 - d0, want2 - d0) < 1e-4
 
@@ -626,40 +675,13 @@ def test_graph_replay_matches_eager_launches(gpu_ready, exact_case):
     assert relerr(out[False][4][2], out[False][0][2]) > 1e-6
 
 
-def _descend_reference(rule, d, g, m, v, vmax, lr, b1, b2, eps, t):
-    """PointCloud's descent rules (PointCloud.cpp:83-204) in float32 numpy, on the
-    normalised gradient g; returns the new dFc and moment buffers."""
-    f = np.float32
-    d, g, m, v, vmax = (x.astype(f) for x in (d, g, m, v, vmax))
-    lr, b1, b2, eps = f(lr), f(b1), f(b2), f(eps)
-    if rule in ("adam", "amsgrad"):
-        m = b1 * m + (f(1) - b1) * g
-        v = b2 * v + (f(1) - b2) * g * g
-        c1, c2 = f(1) - b1 ** t, f(1) - b2 ** t
-        if rule == "adam":
-            d = d - lr * ((m / c1) / (np.sqrt(v / c2) + eps))
-        else:
-            vmax = np.maximum(vmax, v / c2)
-            d = d - lr * ((m / c1) / (np.sqrt(vmax) + eps))
-    elif rule == "lion":
-        m = b1 * m + (f(1) - b1) * np.sign(g)
-        d = d - lr * m
-    elif rule == "gd":
-        d = d - lr * g
-    else:  # dldf
-        c = np.clip(g, f(-1), f(1))
-        c = np.where(np.abs(c) < f(1e-3), np.where(c < 0, f(-1e-3), f(1e-3)), c)
-        m = f(0.9) * m + lr * c
-        d = d - m
-    return d, m, v, vmax
-
-
 @pytest.mark.parametrize("rules", [("amsgrad", "amsgrad"), ("lion", "lion"), ("gd", "dldf"), ("adam", "amsgrad")])
-def test_device_descent_rules_match_reference_formulas(gpu_ready, exact_case, rules):
+def test_device_descent_rules_match_reference_descend(gpu_ready, exact_case, rules):
     """dmpm_descend: Descend_AMSGrad / Descend_Lion / Descend_GradientDescent /
     Descend_dLdF on the tied control gradient (normalised by its norm), two
     consecutive steps sharing the moment buffers as MaterialPoint's
-    momentum / vector / vector_max are shared."""
+    momentum / vector / vector_max are shared -- against the same two calls of
+    the reference's compiled PointCloud methods (PointCloud.cpp:83-204)."""
     sc, o, loss, L = exact_case
     lr, b1, b2, eps = 1e-2, 0.9, 0.999, 1e-5
     with make_ctx(sc, "fp32", o.target, adjoint="exact", control="tied") as c:
@@ -680,12 +702,7 @@ def test_device_descent_rules_match_reference_formulas(gpu_ready, exact_case, ru
             c.descend("amsgrad", lr, t=0)
         # an unknown rule is rejected by the C ABI itself
         assert c.lib.dmpm_descend(c.h, 0, 9, lr, b1, b2, eps, 1, 1) == dmpm.ERR_ARG
-    gn = (g / np.linalg.norm(g)).astype(np.float32)
-    m = np.zeros_like(gn)
-    v = np.zeros_like(gn)
-    vmax = np.zeros_like(gn)
-    want = d.astype(np.float32)
-    for t, (rule, got) in enumerate(zip(rules, outs), start=1):
-        want, m, v, vmax = _descend_reference(rule, want, gn, m, v, vmax, lr, b1, b2, eps, t)
-        step = want.astype(np.float64) - d
-        assert np.linalg.norm(got - d - step) <= 1e-5 * np.linalg.norm(step), (rule, t)
+    wants = _reference_descent(sc, d, g, [(r, t) for t, r in enumerate(rules, start=1)], lr, b1, b2, eps)
+    for (rule, got, want) in zip(rules, outs, wants):
+        step = want - d
+        assert np.linalg.norm(got - d - step) <= 1e-5 * np.linalg.norm(step), rule

@@ -11,9 +11,10 @@ import numpy as np
 import pytest
 
 import optinput
+from oracle.lib import reference_source_dir
 from tests.helpers import GOLDEN
 
-REF = "/root/reference"
+REF = reference_source_dir()
 
 
 def f32(x):

@@ -142,3 +142,38 @@ def test_exact_adjoint_matches_central_fd(mode):
             fd = (run(dfc_all=sc.dFc + h * D).loss() - run(dfc_all=sc.dFc - h * D).loss()) / (2 * h)
             an = float(sum(np.sum(g.get(k, "dLdFe") * D) for k in range(L - 1)))
         assert abs(fd - an) <= 1e-5 * abs(fd) + 1e-14, (fd, an)
+
+
+def _config0_bars():
+    """Bars for the full-size config-0 comparison.  The reference's adjoint
+    takes d(J F^-T)/dF by central differences with delta = 1e-6
+    (Elasticity.cpp:7-72), which turns rounding-level input differences into
+    ~1e-10 differences of the adjoint: the FP64 build against itself with every
+    position multiplied by (1 + 2^-52) moves dLdF by 1.3e-10 max-abs relative
+    (7.5e-11 norm-relative).  The bars sit a few times above that floor."""
+    return {"x": 1e-12, "loss": 1e-11, "adj_maxabs": 1e-9, "adj_norm": 5e-10}
+
+
+def test_config0_full_size_fp64(golden):
+    """The oracle against the reference's FP64 build on the small benchmark
+    configuration at full size (8,778 particles, 32^3, 100 steps, the
+    reference's own adjoint): final positions, loss, layer-0 dLdF and dLdx."""
+    from tests.golden.make_golden import config0_scene
+    from tests.helpers import normrel
+
+    g = golden("config0_f64")
+    sc = config0_scene()
+    assert abs(sc.dt - float(g["dt"])) == 0.0
+    sc.vol = np.asarray(g["vol"], dtype=np.float64)
+    o = OracleGraph(sc, "f64", target_m=np.asarray(g["target"], dtype=np.float64))
+    L = sc.steps + 1
+    o.setup(L, sc.dt, sc.drag, sc.f_ext, sc.smoothing)
+    o.forward(0)
+    loss = o.loss()
+    o.backward(0, 0)
+    bar = _config0_bars()
+    assert relerr(o.get(L - 1, "x"), g["x_last"]) < bar["x"]
+    assert abs(loss - float(g["loss"])) / abs(float(g["loss"])) < bar["loss"]
+    for k in ("dLdF", "dLdx"):
+        assert relerr(o.get(0, k), g[k + "_0"]) < bar["adj_maxabs"], k
+        assert normrel(o.get(0, k), g[k + "_0"]) < bar["adj_norm"], k

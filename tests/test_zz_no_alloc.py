@@ -39,12 +39,18 @@ def test_noalloc_volumes_match_context_path_twice(gpu_ready):
     m = torch.tensor(sc.m, dtype=torch.float32, device="cuda")
     mn = (ctypes.c_float * 3)(*[float(v) for v in sc.min_point])
     stream = torch.cuda.current_stream().cuda_stream
+    vols = [torch.full((sc.n,), -1.0, dtype=torch.float32, device="cuda") for _ in range(2)]
+    torch.cuda.synchronize()
     for call in range(2):
-        vol = torch.full((sc.n,), -1.0, dtype=torch.float32, device="cuda")
+        vol = vols[call]
+        # the device's free memory (cudaMemGetInfo) must not move across a call after the first
+        free_before = torch.cuda.mem_get_info()[0]
         st = lib.dmpm_compute_volumes_noalloc(sc.n, x.data_ptr(), m.data_ptr(), sc.dims[0], sc.dims[1], sc.dims[2],
                                              float(sc.dx), mn, vol.data_ptr(), stream)
         assert st == dmpm.OK, call
         torch.cuda.synchronize()
+        if call == 1:
+            assert torch.cuda.mem_get_info()[0] == free_before
         got = vol.cpu().numpy().astype(np.float64)
         assert relerr(got, want) < 1e-5, call
 
