@@ -21,6 +21,15 @@ struct PointCloud {
     void Descend_GradientDescent(float alpha, float gradient_norm);
     void Descend_Lion(float alpha, float beta, float gradient_norm);
 
+    // Minibatch variants (PointCloud.cpp:37-82): a random subset of
+    // minibatch_size distinct indices (shuffled with a clock-seeded mt19937, as
+    // the reference does), the gradient norm over those points, and an Adam
+    // step on them only, whose bias correction uses timestep + 1.
+    std::vector<int> generateMinibatchIndices(int total_size, int minibatch_size);
+    float Compute_dLdF_Norm_Stochastic(const std::vector<int>& minibatch_indices);
+    void Descend_Adam_Stochastic(float alpha, float gradient_norm, float beta1, float beta2, float epsilon,
+                                 int timestep, const std::vector<int>& minibatch_indices);
+
     bool ReadFromOBJ(std::string obj_path, float point_mass);
     void WriteToOBJ(std::string obj_path);
     void WriteEntirePointCloudToBinaryFile(std::string file_path);

@@ -5,6 +5,7 @@
 // Optimiser steps, file IO and gradient norms are host code, as in the
 // reference (PointCloud.cpp).
 #include <algorithm>
+#include <chrono>
 #include <cmath>
 #include <cstdint>
 #include <cstdio>
@@ -12,6 +13,7 @@
 #include <fstream>
 #include <iostream>
 #include <limits>
+#include <random>
 #include <stdexcept>
 #include <string>
 
@@ -179,6 +181,49 @@ Grid::Grid(int _dim_x, int _dim_y, int _dim_z, float _dx, Vec3 _min_point)
                 nodes[i][j][k].x = min_point + Vec3((float)i, (float)j, (float)k) * dx;
 }
 
+namespace {
+template <class G, class Node>
+std::vector<std::reference_wrapper<Node>> query_stencil(G& grid, const Vec3& point,
+                                                        std::vector<std::array<int, 3>>* indices) {
+    std::vector<std::reference_wrapper<Node>> ret;
+    int b[3];
+    for (int a = 0; a < 3; a++) b[a] = (int)std::floor((point[a] - grid.min_point[a]) / grid.dx) - 1;
+    for (int i = 0; i < 4; i++)
+        for (int j = 0; j < 4; j++)
+            for (int k = 0; k < 4; k++) {
+                const int n[3] = {b[0] + i, b[1] + j, b[2] + k};
+                if (n[0] < 0 || n[0] >= grid.dim_x || n[1] < 0 || n[1] >= grid.dim_y || n[2] < 0 || n[2] >= grid.dim_z)
+                    continue;
+                ret.push_back(std::ref(grid.nodes[n[0]][n[1]][n[2]]));
+                if (indices) indices->push_back({n[0], n[1], n[2]});
+            }
+    return ret;
+}
+}  // namespace
+
+std::vector<std::reference_wrapper<GridNode>> Grid::QueryPoint_CubicBSpline(Vec3 point,
+                                                                          std::vector<std::array<int, 3>>* indices) {
+    return query_stencil<Grid, GridNode>(*this, point, indices);
+}
+std::vector<std::reference_wrapper<const GridNode>> Grid::QueryPointConst_CubicBSpline(
+    Vec3 point, std::vector<std::array<int, 3>>* indices) const {
+    return query_stencil<const Grid, const GridNode>(*this, point, indices);
+}
+
+std::vector<GridNode> Grid::flatten() const {
+    std::vector<GridNode> flat;
+    flat.reserve(num_nodes(*this));
+    for_nodes(*this, [&](const GridNode& n, size_t) { flat.push_back(n); });
+    return flat;
+}
+
+void Grid::unflatten(const std::vector<GridNode>& flat) {
+    nodes.assign(dim_x, std::vector<std::vector<GridNode>>(dim_y, std::vector<GridNode>(dim_z)));
+    for_nodes(*this, [&](GridNode& n, size_t i) {
+        if (i < flat.size()) n = flat[i];
+    });
+}
+
 std::vector<Vec3> Grid::GetNodePositions() const {
     std::vector<Vec3> r(num_nodes(*this));
     for_nodes(*this, [&](const GridNode& n, size_t i) { r[i] = n.x; });
@@ -254,6 +299,36 @@ void PointCloud::Descend_AMSGrad(float alpha, float gradient_norm, float beta1, 
             const float mh = p.momentum.data()[k] / c1, vh = p.vector.data()[k] / c2;
             p.vector_max.data()[k] = std::max(p.vector_max.data()[k], vh);
             p.dFc.data()[k] -= alpha * (mh / (std::sqrt(p.vector_max.data()[k]) + epsilon));
+        }
+    }
+}
+
+std::vector<int> PointCloud::generateMinibatchIndices(int total_size, int minibatch_size) {
+    std::vector<int> idx((size_t)std::max(0, total_size));
+    for (int i = 0; i < total_size; i++) idx[(size_t)i] = i;
+    std::mt19937 rng((unsigned)std::chrono::system_clock::now().time_since_epoch().count());
+    std::shuffle(idx.begin(), idx.end(), rng);
+    idx.resize((size_t)std::max(0, std::min(minibatch_size, total_size)));
+    return idx;
+}
+
+float PointCloud::Compute_dLdF_Norm_Stochastic(const std::vector<int>& minibatch_indices) {
+    float norm = 0.f;
+    for (int i : minibatch_indices) norm += points[(size_t)i].dLdF.squaredNorm();
+    return std::sqrt(norm);
+}
+
+void PointCloud::Descend_Adam_Stochastic(float alpha, float gradient_norm, float beta1, float beta2, float epsilon,
+                                         int timestep, const std::vector<int>& minibatch_indices) {
+    const float c1 = 1.f - std::pow(beta1, (float)(timestep + 1)), c2 = 1.f - std::pow(beta2, (float)(timestep + 1));
+    for (int i : minibatch_indices) {
+        MaterialPoint& p = points[(size_t)i];
+        for (int k = 0; k < 9; k++) {
+            const float g = p.dLdF.data()[k] / gradient_norm;
+            p.momentum.data()[k] = beta1 * p.momentum.data()[k] + (1.f - beta1) * g;
+            p.vector.data()[k] = beta2 * p.vector.data()[k] + (1.f - beta2) * g * g;
+            const float mh = p.momentum.data()[k] / c1, vh = p.vector.data()[k] / c2;
+            p.dFc.data()[k] -= alpha * (mh / (std::sqrt(vh) + epsilon));
         }
     }
 }

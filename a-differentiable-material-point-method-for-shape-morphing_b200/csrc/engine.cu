@@ -218,6 +218,7 @@ struct dmpm_ctx {
     dmpm_params prm{};
     int64_t prm_gen = 0;  // bumped by dmpm_set_params (captured graphs hold the parameters)
     int64_t launches = 0;
+    DeviceBudget budget;  // device bytes held by the engine's arenas, optional cap (dmpm_set_device_limit)
     std::unique_ptr<EngineBase> eng;
 };
 
@@ -244,7 +245,10 @@ template <class T> class Engine : public EngineBase {
         bool valid = false;
     };
 
-    explicit Engine(dmpm_ctx* c) : ctx_(c) {}
+    explicit Engine(dmpm_ctx* c) : ctx_(c) {
+        for (Arena* a : {&scene_arena_, &scene_arena_grid_, &layer_arena_, &staging_arena_, &misc_arena_})
+            a->set_budget(&ctx_->budget);
+    }
 
     // ---------------------------------------------------------- configuration
     void set_grid(int dx_, int dy_, int dz_, double h, const double* mn) {
@@ -540,7 +544,7 @@ template <class T> class Engine : public EngineBase {
         DMPM_CK(cudaMemsetAsync(scratch_grid_, 0, G_ * sizeof(node4<T>), ctx_->stream));
         if (n > 0) {
             const size_t npt = round_up((size_t)n, 64);
-            Arena tmp;
+            Arena tmp(&ctx_->budget);
             T* st = (T*)tmp.alloc(3 * npt * sizeof(T));
             T* cst = (T*)tmp.alloc(npt * sizeof(T));
             double* s = staging((size_t)n * 3);
@@ -597,6 +601,26 @@ template <class T> class Engine : public EngineBase {
             return;
         }
         drop_graphs();
+        try {
+            allocate_layers(num_layers);
+        } catch (...) {
+            // out of device memory (or over the context's device byte limit):
+            // drop the partial storage so the context reads as not set up, and
+            // a later dmpm_setup with a smaller request (or a higher limit) works
+            layer_arena_.release();
+            layers_.clear();
+            epochs_.clear();
+            L_ = 0;
+            layout_ = Layout{};
+            forward_done_ = loss_done_ = false;
+            throw;
+        }
+        layout_ = want;
+        reset_layers();
+    }
+
+    void allocate_layers(int num_layers) {
+        const dmpm_params& P = ctx_->prm;
         L_ = num_layers;
         layer_arena_.release();
         layers_.assign(L_, LayerSlots{});
@@ -705,8 +729,6 @@ template <class T> class Engine : public EngineBase {
                 layers_[l].dbggdp = g2 + (size_t)l * G_;
             }
         }
-        layout_ = want;
-        reset_layers();
     }
 
     // SetUpCompGraph semantics on allocated storage: layer 0 = the uploaded
@@ -836,7 +858,7 @@ template <class T> class Engine : public EngineBase {
         if (!kWarp) throw StateError{"the cell sort belongs to the FP32 path"};
         if (l < 0 || l >= L_) throw ArgError{"layer out of range"};
         Epoch e{};
-        Arena tmp;
+        Arena tmp(&ctx_->budget);
         e.order = (uint32_t*)tmp.alloc((size_t)n_ * 4);
         e.items = (uint32_t*)tmp.alloc(((size_t)n_ + 1) * 4);
         e.n_items = (uint32_t*)tmp.alloc(16);
@@ -1313,7 +1335,7 @@ template <class T> class Engine : public EngineBase {
             case DMPM_F_P: {
                 if (layers_[l].dbgP && l < L_ - 1) { download_planes(layers_[l].dbgP, 9, out); break; }
                 // recompute P_op_1 of this layer on demand
-                Arena tmp;
+                Arena tmp(&ctx_->budget);
                 T* P = (T*)tmp.alloc(9 * np_ * sizeof(T));
                 FwdArgs<T> a = fwd_args();
                 a.st = materialize_state(l);
@@ -1748,6 +1770,16 @@ int dmpm_get_info(const dmpm_ctx* ctx, int64_t* info, int count) {
     if (!ctx || !info) return DMPM_ERR_ARG;
     if (ctx->precision == DMPM_FP64) static_cast<Engine<double>*>(ctx->eng.get())->info(info, count);
     else static_cast<Engine<float>*>(ctx->eng.get())->info(info, count);
+    return DMPM_OK;
+}
+
+int dmpm_set_device_limit(dmpm_ctx* ctx, int64_t max_bytes) {
+    if (!ctx) return DMPM_ERR_ARG;
+    if (max_bytes < 0) {
+        ctx->err = "device byte limit must be >= 0";
+        return DMPM_ERR_ARG;
+    }
+    ctx->budget.cap = (size_t)max_bytes;
     return DMPM_OK;
 }
 

@@ -29,30 +29,51 @@ struct StateError {
 
 inline size_t round_up(size_t a, size_t b) { return (a + b - 1) / b * b; }
 
+// Device bytes held by the arenas of one context, and an optional cap on them
+// (0 = none): an allocation that would go above the cap fails the way a failed
+// cudaMalloc does, with cudaErrorMemoryAllocation, before any device call.
+struct DeviceBudget {
+    size_t cap = 0;
+    size_t used = 0;
+};
+
 // Device allocation owner.
 class Arena {
    public:
+    Arena() = default;
+    explicit Arena(DeviceBudget* budget) : budget_(budget) {}
+    void set_budget(DeviceBudget* budget) { budget_ = budget; }  // before the first allocation
+    Arena(const Arena&) = delete;
+    Arena& operator=(const Arena&) = delete;
     ~Arena() { release(); }
     void* alloc(size_t bytes) {
         if (bytes == 0) return nullptr;
+        const size_t want = round_up(bytes, 256);
+        if (budget_ && budget_->cap && budget_->used + want > budget_->cap)
+            throw CudaError{cudaErrorMemoryAllocation, "allocation of " + std::to_string(bytes) +
+                                                           " bytes exceeds the context's device byte limit of " +
+                                                           std::to_string(budget_->cap)};
         void* p = nullptr;
-        cudaError_t e = cudaMalloc(&p, round_up(bytes, 256));
+        cudaError_t e = cudaMalloc(&p, want);
         if (e != cudaSuccess) {
             cudaGetLastError();
             throw CudaError{e, "cudaMalloc(" + std::to_string(bytes) + " bytes): " + cudaGetErrorString(e)};
         }
         ptrs_.push_back(p);
-        bytes_ += round_up(bytes, 256);
+        bytes_ += want;
+        if (budget_) budget_->used += want;
         return p;
     }
     void release() {
         for (void* p : ptrs_) cudaFree(p);
         ptrs_.clear();
+        if (budget_) budget_->used -= bytes_;
         bytes_ = 0;
     }
     size_t bytes() const { return bytes_; }
 
    private:
+    DeviceBudget* budget_ = nullptr;
     std::vector<void*> ptrs_;
     size_t bytes_ = 0;
 };

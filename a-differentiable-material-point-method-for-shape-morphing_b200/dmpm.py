@@ -79,6 +79,7 @@ def load_library(path: str = LIB_PATH) -> ctypes.CDLL:
     L.dmpm_get_info.argtypes = [_P, ctypes.POINTER(ctypes.c_int64), ctypes.c_int]
     L.dmpm_set_grid.argtypes = [_P, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_double, _P]
     L.dmpm_set_params.argtypes = [_P, ctypes.POINTER(Params)]
+    L.dmpm_set_device_limit.argtypes = [_P, ctypes.c_int64]
     L.dmpm_default_params.argtypes = [ctypes.POINTER(Params)]
     L.dmpm_default_params.restype = None
     L.dmpm_set_particles.argtypes = [_P, ctypes.c_int] + [_P] * 9
@@ -229,6 +230,10 @@ class Context:
         self._ck(self.lib.dmpm_synchronize(self.h), "synchronize")
 
     # -------------------------------------------------------------- setup
+    def set_device_limit(self, max_bytes: int):
+        """Cap the device bytes this context may hold (0 = none); over it, calls fail with ERR_OOM."""
+        self._ck(self.lib.dmpm_set_device_limit(self.h, int(max_bytes)), "set_device_limit")
+
     def set_grid(self, dims: Sequence[int], dx: float = 1.0, min_point=(0.0, 0.0, 0.0)):
         mn = np.ascontiguousarray(min_point, dtype=np.float64)
         self._ck(self.lib.dmpm_set_grid(self.h, int(dims[0]), int(dims[1]), int(dims[2]), float(dx), mn.ctypes.data),

@@ -166,6 +166,9 @@ def barrier(world: int):
         dist.barrier()
 
 
+FLT_EPSILON = 1.1920928955078125e-07  # the reference's node-mass threshold (ForwardSimulation.cpp:55)
+
+
 # ---------------------------------------------------------------- workload
 def build_scene(instance: int, ppc_root: int):
     sc = scenes.config_scene(1, instance=instance, ppc_root=ppc_root)
@@ -360,6 +363,42 @@ def workload_config(sc, dt_sub, ckpt):
             "parallelism": "replicas: one independent instance per GPU"}
 
 
+def measure_variant(torch, dmpm, sc, vol, target, device, ckpt, args):
+    """One gradient evaluation of scene sc per step on both paths under one
+    storage policy (checkpoint_every = ckpt): FP32-mixed particle-steps/s, device
+    memory held, and the plain FP64 path on the same policy (its throughput and
+    the FP32 gradient's relative error against it)."""
+    if vol is None:
+        sc.dt, _ = _cfl_dt(sc)
+        vol, target = _scene_inputs(dmpm, sc, device)
+    units = sc.n * sc.steps
+    torch.cuda.synchronize()
+    base = _mem_used_gb(torch, device)
+    c = setup_ctx(dmpm, sc, "fp32", device, vol, target, sc.dt, ckpt)
+    for _ in range(args.warmup):
+        gradient_step(c)
+    hbm = _mem_used_gb(torch, device) - base
+    n = max(1, min(args.steps, 5))
+    ms = timed_steps(torch, c, n, lambda: gradient_step(c)) / n
+    g32 = c.control_grad()
+    info = c.info()
+    c.close()
+    out = {"particles": sc.n, "steps": sc.steps, "checkpoint_every": info["checkpoint_every"],
+           "value": units / (ms / 1000.0), "unit": UNIT, "ms_per_gradient": ms, "hbm_gb": hbm,
+           "engine_bytes_gb": info["device_bytes"] / 1e9}
+    if not args.no_fp64:
+        c64 = setup_ctx(dmpm, sc, "fp64", device, vol, target, sc.dt, ckpt)
+        gradient_step(c64)
+        ms64 = timed_steps(torch, c64, 1, lambda: gradient_step(c64))
+        g64 = c64.control_grad()
+        c64.close()
+        rel = float(np.linalg.norm(g32 - g64) / np.linalg.norm(g64))
+        out["fp64"] = {"value": units / (ms64 / 1000.0), "ms_per_gradient": ms64,
+                       "speedup_fp32_mixed_over_fp64": ms64 / ms, "grad_relerr_vs_fp64": rel,
+                       "meets_bar": rel <= 1e-4}
+    return out
+
+
 def run_ours(args):
     import torch
 
@@ -471,6 +510,18 @@ def run_ours(args):
             if b:
                 kern[k]["hbm_frac"] = b / (kern[k]["avg_us"] * 1e-6) / 1e9 / peak
 
+    # the target's other clauses, measured in the same run on one GPU: the same
+    # workload with checkpoints every 15 layers (recompute in between), and the
+    # configuration's own 8 particles per cell
+    variants = None
+    if world == 1 and not args.no_variants:
+        variants = {"checkpointed": measure_variant(torch, dmpm, sc, vol, target, device, 15, args),
+                    "as_specified_8ppc": measure_variant(torch, dmpm, build_scene(rank, 2), None, None, device,
+                                                         ckpt, args)}
+        variants["checkpointed"]["store_all_ms_per_gradient"] = ms_max / args.steps
+        variants["checkpointed"]["recompute_overhead"] = (
+            variants["checkpointed"]["ms_per_gradient"] / (ms_max / args.steps) - 1.0)
+
     cb = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         cb = cpu_baseline(sc, 1)
@@ -484,7 +535,8 @@ def run_ours(args):
                 "config": workload_config(sc, dt_sub, ckpt),
                 "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
                 "gpu_launches": launches, "roofline": roof, "compute": compute_rates(value / world), "cpu_baseline": cb,
-                "clocks": clocks, "fp64": fp64, "kernels": kern, "ms_per_step_profiled": ms_prof / args.steps}
+                "clocks": clocks, "fp64": fp64, "kernels": kern, "ms_per_step_profiled": ms_prof / args.steps,
+                **(variants or {})}
         print(json.dumps(line), flush=True)
     if world > 1:
         import torch.distributed as dist
@@ -552,19 +604,36 @@ def run_fd(args):
         a64 = [float(np.sum(grads["fp64"] * d)) for d in dirs]
         a32 = [float(np.sum(grads["fp32"] * d)) for d in dirs]
         per_h = {}
-        for h in hs:
-            fds = []
+        for hi, h in enumerate(hs):
+            fds, crossings = [], []
             for d in dirs:
                 lp = []
+                occ = None
                 for sgn in (1.0, -1.0):
                     c64.set_layer(0, "dFc", base + sgn * h * d)
                     c64.forward(0)
                     lp.append(c64.loss())
+                    if hi == 0 and loss == "ref":
+                        # node-mass threshold crossings between the two rollouts: nodes
+                        # (over all layers) occupied, |m| > FLT_EPSILON, in one and not the other
+                        masks = [np.abs(c64.get_grid(lay, "grid_m")) > FLT_EPSILON for lay in range(sc.steps + 1)]
+                        if occ is None:
+                            occ = masks
+                        else:
+                            crossings.append(int(sum(int(np.count_nonzero(a != b)) for a, b in zip(occ, masks))))
                 fds.append((lp[0] - lp[1]) / (2 * h))
             e64 = [abs(a - f) / abs(f) for a, f in zip(a64, fds)]
             e32 = [abs(a - f) / abs(f) for a, f in zip(a32, fds)]
             per_h["%g" % h] = {"relerr_fp64_median": float(np.median(e64)), "relerr_fp64_max": float(np.max(e64)),
                                "relerr_fp32_median": float(np.median(e32)), "relerr_fp32_max": float(np.max(e32))}
+            if crossings:
+                per_h["%g" % h]["per_direction"] = [
+                    {"threshold_crossings": cr, "relerr_fp64": e, "relerr_fp32": e3}
+                    for cr, e, e3 in zip(crossings, e64, e32)]
+                zero = [e for cr, e in zip(crossings, e64) if cr == 0]
+                per_h["%g" % h]["directions_without_crossings"] = len(zero)
+                if zero:
+                    per_h["%g" % h]["relerr_fp64_max_without_crossings"] = float(np.max(zero))
         c64.close()
         out[loss] = {"grad_relerr_fp32_vs_fp64": float(np.linalg.norm(grads["fp32"] - grads["fp64"]) /
                                                        np.linalg.norm(grads["fp64"])), "per_h": per_h}
@@ -828,11 +897,13 @@ def run_config4(args):
         c64.close()
         return float(np.linalg.norm(grad32 - g64) / np.linalg.norm(g64))
 
-    # Adam with the reference optimiser's line search (CompGraph.cpp:388-420): step, re-run the
-    # forward pass, keep the step if the loss fell, else step back (Descend_Adam with -alpha, which
-    # updates the moments again, as the reference does) and halve alpha; a frame whose line search
-    # finds no decrease ends its descent.
-    max_ls = 6
+    # Plain Adam (the configuration: 30 iterations at lr 1e-2), or with --line-search the
+    # reference optimiser's line search (CompGraph.cpp:388-420): step, re-run the forward pass,
+    # keep the step if the loss fell, else step back (Descend_Adam with -alpha, which updates the
+    # moments again, as the reference does) and halve alpha; a frame whose line search finds no
+    # decrease ends its descent.
+    out["optimizer"] = "adam with the reference line search" if args.line_search else "adam, fixed lr"
+    max_ls = 6 if args.line_search else 1
     ls_trials, grad_ms, stopped, last, nonfinite = [], [], None, None, None
 
     def statused_gradient(holder):
@@ -855,6 +926,11 @@ def run_config4(args):
             if it == 1:
                 relerrs[1] = fp64_relerr(last[1], last[2])
         t0 = time.perf_counter()
+        if not args.line_search:
+            c.adam_step(t=it, lr=1e-2, layer=0)
+            c.synchronize()
+            times.append(ms + 1000.0 * (time.perf_counter() - t0))
+            continue
         alpha, found = 1e-2, False
         for ls in range(max_ls):
             c.adam_step(t=it, lr=alpha, layer=0)
@@ -971,8 +1047,12 @@ def main():
     ap.add_argument("--rollout-steps", type=int, default=0, help="override the 200 time steps (profiling runs)")
     ap.add_argument("--no-fp64", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-variants", action="store_true",
+                    help="skip the checkpointed and 8-per-cell measurements of the headline line")
     ap.add_argument("--config", type=int, default=1, help="1 = headline workload; 0, 2, 3, 4 = extra measurements")
     ap.add_argument("--iters", type=int, default=30, help="config 4: Adam iterations")
+    ap.add_argument("--line-search", action="store_true",
+                    help="config 4: wrap each Adam step in the reference optimiser's line search")
     ap.add_argument("--fd", action="store_true", help="config 1: adjoint vs central differences, 16 directions")
     ap.add_argument("--instances", type=int, default=48, help="config 3: number of batched instances")
     ap.add_argument("--fd-h", default="1e-3,1e-4,1e-5,1e-6", help="--fd: central-difference steps")

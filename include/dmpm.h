@@ -152,6 +152,16 @@ const char* dmpm_last_error(const dmpm_ctx* ctx);
 int dmpm_get_info(const dmpm_ctx* ctx, int64_t* info, int count); /* n, dims, layers, precision,
                                                                       checkpoint_every, device bytes, ... */
 
+/* Cap on the device bytes this context may hold (0 = no cap, the default).
+ * An allocation that would exceed it fails as a failed cudaMalloc does:
+ * the call returns DMPM_ERR_OOM.  No reference counterpart (the reference
+ * allocates on the host and never reports running out of memory); it lets a
+ * caller bound one context's share of the GPU, and a failed dmpm_setup leaves
+ * the context without layer storage -- calls that need it return
+ * DMPM_ERR_STATE -- until a dmpm_setup that fits succeeds.  Storage already
+ * held is not released by lowering the cap. */
+int dmpm_set_device_limit(dmpm_ctx* ctx, int64_t max_bytes);
+
 int dmpm_set_grid(dmpm_ctx* ctx, int dim_x, int dim_y, int dim_z, double dx, const double* min_point);
 int dmpm_set_params(dmpm_ctx* ctx, const dmpm_params* params);
 

@@ -329,6 +329,23 @@ class RefGraph:
         else:
             raise ValueError(rule)
 
+    def dldf_norm_stochastic(self, layer: int, idx) -> float:
+        """PointCloud::Compute_dLdF_Norm_Stochastic over the given indices."""
+        a = np.ascontiguousarray(idx, dtype=np.int32)
+        fn = self.lib.ref_graph_dldf_norm_stochastic
+        fn.restype = self.R
+        fn.argtypes = [_P, ctypes.c_int, _P, ctypes.c_int]
+        return float(fn(self.h, layer, _ptr(a), len(a)))
+
+    def descend_adam_stochastic(self, layer: int, lr: float, gnorm: float, beta1: float, beta2: float, eps: float,
+                                t: int, idx):
+        """PointCloud::Descend_Adam_Stochastic on the given indices."""
+        a = np.ascontiguousarray(idx, dtype=np.int32)
+        R, I = self.R, ctypes.c_int
+        fn = self.lib.ref_graph_descend_adam_stochastic
+        fn.argtypes = [_P, I, R, R, R, R, R, I, _P, I]
+        fn(self.h, layer, lr, gnorm, beta1, beta2, eps, t, _ptr(a), len(a))
+
     def time_forward_multithread(self, steps, threads) -> float:
         self.lib.ref_time_forward_multithread.restype = ctypes.c_double
         self.lib.ref_time_forward_multithread.argtypes = [_P, ctypes.c_int, ctypes.c_int]

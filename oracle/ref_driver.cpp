@@ -269,6 +269,16 @@ void ref_graph_descend_gd(void* h, int layer, real alpha, real gnorm) {
 void ref_graph_descend_dldf(void* h, int layer, real alpha, real gnorm) {
     static_cast<Scene*>(h)->graph->layers[layer].point_cloud->Descend_dLdF(alpha, gnorm);
 }
+// The minibatch variants (PointCloud.cpp:51-82) on the given indices.
+real ref_graph_dldf_norm_stochastic(void* h, int layer, const int* idx, int nidx) {
+    const std::vector<int> mb(idx, idx + nidx);
+    return static_cast<Scene*>(h)->graph->layers[layer].point_cloud->Compute_dLdF_Norm_Stochastic(mb);
+}
+void ref_graph_descend_adam_stochastic(void* h, int layer, real alpha, real gnorm, real b1, real b2, real eps, int t,
+                                       const int* idx, int nidx) {
+    const std::vector<int> mb(idx, idx + nidx);
+    static_cast<Scene*>(h)->graph->layers[layer].point_cloud->Descend_Adam_Stochastic(alpha, gnorm, b1, b2, eps, t, mb);
+}
 
 // Timed forward of layers [0, steps) with MultiThreadMPM::ForwardTimeStep
 // (MultiThreadForwardSimulation.cpp:7-154) using `threads` proxy grids.

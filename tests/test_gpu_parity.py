@@ -549,6 +549,40 @@ def test_errors_are_reported(gpu_ready):
     c.close()
 
 
+@pytest.mark.parametrize("prec", ["fp64", "fp32"])
+def test_out_of_memory_in_setup_leaves_a_usable_context(gpu_ready, exact_case, prec):
+    """Allocation failure injected on the host: a device byte limit below what
+    dmpm_setup needs makes it fail with DMPM_ERR_OOM (the status a failed
+    cudaMalloc gives) before any kernel runs.  The context then reads as not set
+    up (forward, loss and layer reads return DMPM_ERR_STATE or DMPM_ERR_ARG, no
+    fault), and once the limit is lifted the same context sets up and returns
+    the gradient of a fresh context."""
+    sc, o, loss, L = exact_case
+
+    def gradient(c):
+        c.setup(L)
+        c.forward(0)
+        lo = c.loss()
+        c.backward(0)
+        return lo, c.control_grad()
+
+    with make_ctx(sc, prec, o.target, adjoint="exact", control="tied") as c:
+        want = gradient(c)
+    with make_ctx(sc, prec, o.target, adjoint="exact", control="tied") as c:
+        c.set_device_limit(c.info()["device_bytes"] + 4096)  # the scene fits, its layers do not
+        with pytest.raises(dmpm.DmpmError) as e:
+            c.setup(L)
+        assert e.value.status == dmpm.ERR_OOM
+        assert c.lib.dmpm_forward(c.h, 0) == dmpm.ERR_STATE
+        assert c.lib.dmpm_loss(c.h, None) in (dmpm.ERR_STATE, dmpm.ERR_ARG)
+        with pytest.raises(dmpm.DmpmError):
+            c.get(0, "x")
+        c.set_device_limit(0)
+        got = gradient(c)
+    assert abs(got[0] - want[0]) <= 1e-6 * abs(want[0])
+    assert relerr(got[1], want[1]) < (1e-12 if prec == "fp64" else 1e-4)
+
+
 def test_nonfinite_is_flagged_not_faulted(gpu_ready):
     """A NaN control on one particle propagates to the grid and the cloud (as in
     the reference); the engine reports DMPM_ERR_NONFINITE from forward and
