@@ -156,6 +156,17 @@ class Scene:
     def num_nodes(self) -> int:
         return int(np.prod(self.dims))
 
+    def float32_inputs(self) -> "Scene":
+        """A copy whose per-particle inputs are float32-representable (each
+        value rounded to the nearest float).  The FP32-mixed path rounds its
+        inputs so on upload; giving the FP64 path this copy too makes the two
+        paths compute from identical inputs."""
+        r = lambda a: np.asarray(a, dtype=np.float32).astype(np.float64)
+        out = dataclasses.replace(self)
+        for k in ("x", "v", "F", "C", "dFc", "m", "lam", "mu", "vol"):
+            setattr(out, k, r(getattr(self, k)))
+        return out
+
     def cfl_dt(self) -> float:
         """Explicit P-wave limit dx / c_p in these (lattice) units."""
         rho = float(self.m.mean()) / (1.0 / self.meta.get("ppc", 8))  # lattice density
