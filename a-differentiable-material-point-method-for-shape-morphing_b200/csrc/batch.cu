@@ -272,18 +272,28 @@ struct dmpm_batch::Impl {
         if (u < 0 || u >= count) throw ArgError{"instance out of range"};
         return inst[user2int[u]];
     }
-    void upload(const double* host, int n, int width, float* dst, size_t np) {
+    // diag: added to the diagonal of 3x3 matrices on the way (F <-> strain H = F - I,
+    // the layer storage of the FP32 kernels)
+    void upload(const double* host, int n, int width, float* dst, size_t np, double diag = 0.0) {
         double* s = stage((size_t)n * width);
         DMPM_CK(cudaMemcpyAsync(s, host, (size_t)n * width * sizeof(double), cudaMemcpyHostToDevice, b->stream));
+        if (diag != 0.0) {
+            k_diag_add<<<(unsigned)(((size_t)n * 3 + 255) / 256), 256, 0, b->stream>>>(s, n, diag);
+            launched();
+        }
         const size_t tot = (size_t)n * width;
         k_unpack<float><<<(unsigned)((tot + 255) / 256), 256, 0, b->stream>>>(s, width, n, dst, np);
         launched();
     }
-    void download(const float* src, size_t np, int n, int width, double* host) {
+    void download(const float* src, size_t np, int n, int width, double* host, double diag = 0.0) {
         double* s = stage((size_t)n * width);
         const size_t tot = (size_t)n * width;
         k_pack<float><<<(unsigned)((tot + 255) / 256), 256, 0, b->stream>>>(src, np, width, n, s);
         launched();
+        if (diag != 0.0) {
+            k_diag_add<<<(unsigned)(((size_t)n * 3 + 255) / 256), 256, 0, b->stream>>>(s, n, diag);
+            launched();
+        }
         DMPM_CK(cudaMemcpyAsync(host, s, tot * sizeof(double), cudaMemcpyDeviceToHost, b->stream));
         DMPM_CK(cudaStreamSynchronize(b->stream));
     }
@@ -303,7 +313,7 @@ struct dmpm_batch::Impl {
             for (int p = 0; p < n; p++) eye[9 * p] = eye[9 * p + 4] = eye[9 * p + 8] = 1.0;
             F = eye.data();
         }
-        upload(F, n, 9, l0 + (size_t)PF * np0, np0);
+        upload(F, n, 9, l0 + (size_t)PF * np0, np0, -1.0);
         if (C) upload(C, n, 9, l0 + (size_t)PC * np0, np0);
         else for (int c = 0; c < 9; c++) DMPM_CK(cudaMemsetAsync(l0 + (size_t)(PC + c) * np0, 0, n * sizeof(float), b->stream));
         if (dFc) upload(dFc, n, 9, dfc + s.poff, np0);
@@ -713,7 +723,7 @@ struct dmpm_batch::Impl {
         switch (field) {
             case DMPM_F_X: download(base + (size_t)PX * np, np, s.n, 3, out); break;
             case DMPM_F_V: download(base + (size_t)PV * np, np, s.n, 3, out); break;
-            case DMPM_F_F: download(base + (size_t)PF * np, np, s.n, 9, out); break;
+            case DMPM_F_F: download(base + (size_t)PF * np, np, s.n, 9, out, 1.0); break;
             case DMPM_F_C: download(base + (size_t)PC * np, np, s.n, 9, out); break;
             default: throw ArgError{"field must be DMPM_F_X, _V, _F or _C"};
         }

@@ -54,11 +54,12 @@ constexpr int kAuxPlanes = 24;
 // Reference MaterialPoint (118 floats): x 0, v 3, F 6, C 15, P 24, m 33, vol 34,
 // lam 35, mu 36, dFc 37 (MaterialPoint.h:18-46).
 template <class T>
-__global__ void k_unpack_ref(const float* __restrict__ pts, int n, size_t np, T* st, T* cst, T* dfc) {
+__global__ void k_unpack_ref(const float* __restrict__ pts, int n, size_t np, T* st, T* cst, T* dfc, T diag) {
     const int p = blockIdx.x * blockDim.x + threadIdx.x;
     if (p >= n) return;
     const float* m = pts + (size_t)p * 118;
     for (int q = 0; q < 24; q++) st[(size_t)q * np + p] = (T)m[q];  // x v F C share the plane order
+    for (int q = 0; q < 3; q++) st[(size_t)(PF + 4 * q) * np + p] += diag;  // strain planes: F - I
     cst[(size_t)KM * np + p] = (T)m[33];
     cst[(size_t)KVOL * np + p] = (T)m[34];
     cst[(size_t)KLAM * np + p] = (T)m[35];
@@ -229,6 +230,8 @@ template <class T> class Engine : public EngineBase {
     // FP32 path: cell-sorted warp items (kernels_warp.cuh); FP64 path: plain kernels (kernels.cuh)
     static constexpr bool kTiled = std::is_same<T, float>::value;
     static constexpr bool kWarp = kTiled;
+    // the FP32 path stores each layer's strain H = F - I in the F planes (kernels_warp.cuh)
+    static constexpr bool kStrain = kWarp;
     // one cell sort: the stable order and warp items used for steps
     // [e * sort_every, (e + 1) * sort_every)
     struct Epoch {
@@ -308,19 +311,29 @@ template <class T> class Engine : public EngineBase {
         return staging_;
     }
 
-    void upload_planes(const double* host, int width, T* dst) {
+    // host doubles (width per particle) -> planes; diag is added to the diagonal of
+    // 3x3 matrices first (F -> strain H = F - I on the FP32 path)
+    void upload_planes(const double* host, int width, T* dst, double diag = 0.0) {
         double* s = staging((size_t)n_ * width);
         DMPM_CK(cudaMemcpyAsync(s, host, (size_t)n_ * width * sizeof(double), cudaMemcpyHostToDevice, ctx_->stream));
+        if (diag != 0.0) {
+            k_diag_add<<<(unsigned)(((size_t)n_ * 3 + 255) / 256), 256, 0, ctx_->stream>>>(s, n_, diag);
+            launched();
+        }
         const size_t tot = (size_t)n_ * width;
         k_unpack<T><<<(unsigned)((tot + 255) / 256), 256, 0, ctx_->stream>>>(s, width, n_, dst, np_);
         launched();
     }
 
-    void download_planes(const T* src, int width, double* host) {
+    void download_planes(const T* src, int width, double* host, double diag = 0.0) {
         double* s = staging((size_t)n_ * width);
         const size_t tot = (size_t)n_ * width;
         k_pack<T><<<(unsigned)((tot + 255) / 256), 256, 0, ctx_->stream>>>(src, np_, width, n_, s);
         launched();
+        if (diag != 0.0) {
+            k_diag_add<<<(unsigned)(((size_t)n_ * 3 + 255) / 256), 256, 0, ctx_->stream>>>(s, n_, diag);
+            launched();
+        }
         DMPM_CK(cudaMemcpyAsync(host, s, tot * sizeof(double), cudaMemcpyDeviceToHost, ctx_->stream));
         DMPM_CK(cudaStreamSynchronize(ctx_->stream));
     }
@@ -332,11 +345,11 @@ template <class T> class Engine : public EngineBase {
         upload_planes(x, 3, st0_ + (size_t)PX * np_);
         if (v) upload_planes(v, 3, st0_ + (size_t)PV * np_);
         if (F) {
-            upload_planes(F, 9, st0_ + (size_t)PF * np_);
+            upload_planes(F, 9, st0_ + (size_t)PF * np_, kStrain ? -1.0 : 0.0);
         } else {
             std::vector<double> eye((size_t)n * 9, 0.0);
             for (int p = 0; p < n; p++) eye[9 * p] = eye[9 * p + 4] = eye[9 * p + 8] = 1.0;
-            upload_planes(eye.data(), 9, st0_ + (size_t)PF * np_);
+            upload_planes(eye.data(), 9, st0_ + (size_t)PF * np_, kStrain ? -1.0 : 0.0);
         }
         if (C) upload_planes(C, 9, st0_ + (size_t)PC * np_);
         if (dFc) upload_planes(dFc, 9, dfc0_);
@@ -352,7 +365,8 @@ template <class T> class Engine : public EngineBase {
         const size_t bytes = (size_t)n * 118 * sizeof(float);
         double* s = staging((bytes + 7) / 8);
         DMPM_CK(cudaMemcpyAsync(s, pts, bytes, cudaMemcpyHostToDevice, ctx_->stream));
-        k_unpack_ref<T><<<(n + 255) / 256, 256, 0, ctx_->stream>>>((const float*)s, n, np_, st0_, cst_, dfc0_);
+        k_unpack_ref<T><<<(n + 255) / 256, 256, 0, ctx_->stream>>>((const float*)s, n, np_, st0_, cst_, dfc0_,
+                                                                   kStrain ? T(-1) : T(0));
         launched();
     }
 
@@ -926,9 +940,7 @@ template <class T> class Engine : public EngineBase {
             launched();
             pend();
             pbeg(K_P2G);
-            if (ush == 3) k_p2g_b<2><<<brick_blocks(k_p2g_b<2>), DMPM_BRICK_THREADS, 0, ctx_->stream>>>(a);
-            else if (ush == 6) k_p2g_b<4><<<brick_blocks(k_p2g_b<4>), DMPM_BRICK_THREADS, 0, ctx_->stream>>>(a);
-            else if (ctx_->prm.warp_general) k_p2g_w<true, ITEMS_PERSISTENT><<<ws, 256, 0, ctx_->stream>>>(a);
+            if (ctx_->prm.warp_general) k_p2g_w<true, ITEMS_PERSISTENT><<<ws, 256, 0, ctx_->stream>>>(a);
             else k_p2g_w<false, ITEMS_PERSISTENT><<<ws, 256, 0, ctx_->stream>>>(a);
             launched();
             pend();
@@ -1152,13 +1164,7 @@ template <class T> class Engine : public EngineBase {
             const unsigned ws = warp_blocks(DMPM_ADJ_SCATTER_CTAS), wg = warp_blocks(DMPM_GATHER_CTAS);
             const int ush = set_units(a, ep);
             pbeg(K_ADJ_SCATTER);
-            if (ush == 3) {
-                if (ex) k_adj_scatter_b<true, 2><<<brick_blocks(k_adj_scatter_b<true, 2>), DMPM_BRICK_THREADS, 0, ctx_->stream>>>(a);
-                else k_adj_scatter_b<false, 2><<<brick_blocks(k_adj_scatter_b<false, 2>), DMPM_BRICK_THREADS, 0, ctx_->stream>>>(a);
-            } else if (ush == 6) {
-                if (ex) k_adj_scatter_b<true, 4><<<brick_blocks(k_adj_scatter_b<true, 4>), DMPM_BRICK_THREADS, 0, ctx_->stream>>>(a);
-                else k_adj_scatter_b<false, 4><<<brick_blocks(k_adj_scatter_b<false, 4>), DMPM_BRICK_THREADS, 0, ctx_->stream>>>(a);
-            } else if (P.warp_general) {
+            if (P.warp_general) {
                 if (ex) k_adj_scatter_w<true, true, ITEMS_PERSISTENT><<<ws, 256, 0, ctx_->stream>>>(a);
                 else k_adj_scatter_w<false, true, ITEMS_PERSISTENT><<<ws, 256, 0, ctx_->stream>>>(a);
             } else {
@@ -1330,7 +1336,7 @@ template <class T> class Engine : public EngineBase {
         switch (field) {
             case DMPM_F_X: download_planes(materialize_state(l) + (size_t)PX * np_, 3, out); break;
             case DMPM_F_V: download_planes(materialize_state(l) + (size_t)PV * np_, 3, out); break;
-            case DMPM_F_F: download_planes(materialize_state(l) + (size_t)PF * np_, 9, out); break;
+            case DMPM_F_F: download_planes(materialize_state(l) + (size_t)PF * np_, 9, out, kStrain ? 1.0 : 0.0); break;
             case DMPM_F_C: download_planes(materialize_state(l) + (size_t)PC * np_, 9, out); break;
             case DMPM_F_P: {
                 if (layers_[l].dbgP && l < L_ - 1) { download_planes(layers_[l].dbgP, 9, out); break; }
@@ -1341,6 +1347,7 @@ template <class T> class Engine : public EngineBase {
                 a.st = materialize_state(l);
                 a.dfc = layers_[l].dfc;
                 a.P = P;
+                a.strain = kStrain ? 1 : 0;
                 k_p_op1<T><<<pgrid(), block(), 0, ctx_->stream>>>(a);
                 launched();
                 download_planes(P, 9, out);
@@ -1378,7 +1385,8 @@ template <class T> class Engine : public EngineBase {
             case DMPM_F_X: case DMPM_F_V: case DMPM_F_F: case DMPM_F_C: {
                 if (!layers_[l].st) throw StateError{"layer state is not stored (checkpointing)"};
                 const int off = field == DMPM_F_X ? PX : field == DMPM_F_V ? PV : field == DMPM_F_F ? PF : PC;
-                upload_planes(in, (field == DMPM_F_X || field == DMPM_F_V) ? 3 : 9, layers_[l].st + (size_t)off * np_);
+                upload_planes(in, (field == DMPM_F_X || field == DMPM_F_V) ? 3 : 9, layers_[l].st + (size_t)off * np_,
+                              (field == DMPM_F_F && kStrain) ? -1.0 : 0.0);
                 break;
             }
             case DMPM_F_DLDX: case DMPM_F_DLDV: case DMPM_F_DLDF: case DMPM_F_DLDC: {

@@ -92,6 +92,13 @@ template <class T> __global__ void k_pack(const T* __restrict__ src, size_t np, 
     const int p = (int)(i / width), q = (int)(i % width);
     dst[i] = (double)src[(size_t)q * np + p];
 }
+// add s to the diagonal (entries 0, 4, 8) of n 3x3 matrices stored as 9
+// consecutive doubles each: F <-> the FP32 path's strain planes H = F - I
+static __global__ void k_diag_add(double* a, int n, double s) {
+    const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= (size_t)n * 3) return;
+    a[9 * (i / 3) + 4 * (i % 3)] += s;
+}
 template <class T> __global__ void k_pack_acc(const double* __restrict__ src, size_t np, int n, double* dst) {
     const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= (size_t)n * 9) return;

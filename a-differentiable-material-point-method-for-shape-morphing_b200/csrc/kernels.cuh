@@ -143,6 +143,7 @@ template <class T> struct FwdArgs {
     T* P;               // [9][np] stress of layer n (plain path, or debug copy)
     int tile_cap;
     unsigned* status;
+    int strain;         // the F planes hold H = F - I (the FP32 path's layer storage)
 };
 
 // ------------------------------------------------------------------ P_op_1
@@ -150,7 +151,8 @@ template <class T> struct FwdArgs {
 template <class T> __global__ void k_p_op1(FwdArgs<T> a) {
     const int p = blockIdx.x * blockDim.x + threadIdx.x;
     if (p >= a.n) return;
-    const m3<double> Fe = m3_cast<double>(load_m3(a.st + (size_t)PF * a.np, a.np, p) + load_m3(a.dfc, a.np, p));
+    m3<double> Fe = m3_cast<double>(load_m3(a.st + (size_t)PF * a.np, a.np, p)) + m3_cast<double>(load_m3(a.dfc, a.np, p));
+    if (a.strain) Fe = Fe + m3_eye<double>();  // the F planes hold H = F - I
     const m3<double> P = pk_stress<double>(Fe, (double)a.cst[(size_t)KLAM * a.np + p], (double)a.cst[(size_t)KMU * a.np + p]);
     store_m3(a.P, a.np, p, m3_cast<T>(P));
 }

@@ -6,17 +6,16 @@
 // of a particle whose cell lies in the unit falls inside the unit's node tile
 // of (B + 3)^3 nodes (stencil bases c - 1 .. c + B - 2 plus 3).  A CTA takes a
 // unit, stages the tile in shared memory once, and its threads each handle one
-// particle of the unit, all 64 stencil nodes of it:
-//   G2P and the adjoint P2G gather read the tile (the particles of a warp share
-//   a cell most of the time, so their reads are broadcasts);
-//   P2G and the adjoint G2P scatter add into the tile with shared-memory
-//   atomics -- each lane visits its stencil in its own order (node offsets
-//   xor-ed with lane bits), so the lanes of one cell touch 32 different nodes
-//   at a time -- and the tile is flushed once per unit with one vector
-//   red.global.add per touched node.
+// particle of the unit, all 64 stencil nodes of it, reading the tile (the
+// particles of a warp share a cell most of the time, so their reads are
+// broadcasts).  These are the two stencil kernels that only read the grid: G2P
+// and the adjoint P2G gather.  The scatters stay warp-item kernels
+// (kernels_warp.cuh): adding into a shared tile with shared-memory atomics,
+// even with each lane visiting its stencil in its own order so the lanes of a
+// cell touch different nodes, measured 3-4x slower than the warp's butterfly
+// reduction followed by one vector red.global.add per node.
 // A particle that has left the unit since the sort (the sort runs every few
-// steps) is handled by the same code with its nodes read from or added to
-// global memory directly.
+// steps) is handled by the same code with its nodes read from global memory.
 //
 // Math per stage is that of kernels.cuh (which cites the reference) and of the
 // warp-item kernels in kernels_warp.cuh, summed in a different order.
@@ -35,9 +34,6 @@ namespace dmpm {
 #ifndef DMPM_BRICK_GATHER_MINB
 #define DMPM_BRICK_GATHER_MINB 3
 #endif
-#ifndef DMPM_BRICK_SCATTER_MINB
-#define DMPM_BRICK_SCATTER_MINB 4
-#endif
 
 template <int B> struct BrickShape {
     static constexpr int shift = B == 4 ? 6 : 3;  // key >> shift names the unit
@@ -53,13 +49,13 @@ __device__ __forceinline__ void unit_origin(uint32_t ukey, int shift, const Grid
     for (int a = 0; a < 3; a++) o[a] = c[a] - 5;
 }
 
-// Per-axis stencil offsets d = x_g - x, weights N(d / dx) and slopes, for the
-// node offsets t ^ perm (t = 0..3) of the stencil starting at base.
-__device__ __forceinline__ void axis_stencil(float x, float mn, float dx, float idx, int base, int perm, float n[4],
-                                             float d[4], float* s) {
+// Per-axis stencil offsets d = x_g - x, weights N(d / dx) and slopes of the
+// four nodes t = 0..3 of the stencil starting at base.
+__device__ __forceinline__ void axis_stencil(float x, float mn, float dx, float idx, int base, float n[4], float d[4],
+                                             float* s) {
 #pragma unroll
     for (int t = 0; t < 4; t++) {
-        const float xg = mn + (float)(base + (t ^ perm)) * dx;
+        const float xg = mn + (float)(base + t) * dx;
         d[t] = xg - x;
         const float q = d[t] * idx;
         n[t] = bsp(q);
@@ -204,7 +200,7 @@ __global__ void __launch_bounds__(DMPM_BRICK_THREADS, DMPM_BRICK_G2P_MINB) k_g2p
             load_x_base(a.st, npl, p, geo, x, base);
             float n[3][4], d[3][4];
 #pragma unroll
-            for (int c = 1; c < 3; c++) axis_stencil(x[c], (float)geo.mn[c], dx, idx, base[c], 0, n[c], d[c], nullptr);
+            for (int c = 1; c < 3; c++) axis_stencil(x[c], (float)geo.mn[c], dx, idx, base[c], n[c], d[c], nullptr);
             const Axis0 ax0{x[0], (float)geo.mn[0], dx, idx, base[0]};
             float V[3], Cm[3][3];
             int l[3];
@@ -227,17 +223,18 @@ __global__ void __launch_bounds__(DMPM_BRICK_THREADS, DMPM_BRICK_G2P_MINB) k_g2p
                 finite &= isfinite(xn);
             }
             store_m3(a.st_next + (size_t)PC * npn, npn, p, Cn);
-            const m3<float> F = load_m3(a.st + (size_t)PF * npl, npl, p);
-            const m3<float> Fe = F + load_m3(a.dfc, np, p);
+            // strain update H' = (1 - s)(D + dt C' (I + D)) + s H,  D = H + dFc
+            const m3<float> H = load_m3(a.st + (size_t)PF * npl, npl, p);
+            const m3<float> D = H + load_m3(a.dfc, np, p);
 #pragma unroll
             for (int c = 0; c < 3; c++)
 #pragma unroll
                 for (int r = 0; r < 3; r++) {
-                    const float t =
-                        Fe.a[r][c] + a.dt * (Cn.a[r][0] * Fe.a[0][c] + Cn.a[r][1] * Fe.a[1][c] + Cn.a[r][2] * Fe.a[2][c]);
-                    const float fn = (1.f - a.s) * t + a.s * F.a[r][c];
-                    a.st_next[(size_t)(PF + r + 3 * c) * npn + p] = fn;
-                    finite &= isfinite(fn);
+                    const float t = D.a[r][c] + a.dt * (Cn.a[r][c] + (Cn.a[r][0] * D.a[0][c] + Cn.a[r][1] * D.a[1][c] +
+                                                                       Cn.a[r][2] * D.a[2][c]));
+                    const float hn = (1.f - a.s) * t + a.s * H.a[r][c];
+                    a.st_next[(size_t)(PF + r + 3 * c) * npn + p] = hn;
+                    finite &= isfinite(hn);
                 }
             if (!finite) atomicOr(a.status, ST_NONFINITE_FWD);
         }
@@ -349,7 +346,7 @@ __global__ void __launch_bounds__(DMPM_BRICK_THREADS, DMPM_BRICK_GATHER_MINB) k_
             int base[3];
             load_x_base(a.st, npl, p, geo, x, base);
             float n2[4], d2[4], s2[4];
-            axis_stencil(x[2], (float)geo.mn[2], dx, idx, base[2], 0, n2, d2, s2);
+            axis_stencil(x[2], (float)geo.mn[2], dx, idx, base[2], n2, d2, s2);
             const Axis0 ax0{x[0], (float)geo.mn[0], dx, idx, base[0]};
             const Axis0 ax1{x[1], (float)geo.mn[1], dx, idx, base[1]};
             GatherIn in;
@@ -370,225 +367,6 @@ __global__ void __launch_bounds__(DMPM_BRICK_THREADS, DMPM_BRICK_GATHER_MINB) k_
 #pragma unroll
             for (int t = 0; t < 18; t++) a.gath[(size_t)t * np + p] = acc[t];
         }
-    }
-}
-
-// ------------------------------------------------------------------ scatters
-// Shared-memory tile of C float channels per node, channel-major (plane c at
-// c * NT), so lanes adding to different nodes of one channel hit different banks.
-// Lane bits permute each lane's stencil order: node offset (t ^ perm_a) on axis
-// a, perm = (lane & 3, lane >> 2 & 3, lane >> 4 & 1), so the 32 lanes of a warp
-// whose particles share a cell add to 32 different nodes at each step.
-struct LanePerm {
-    int p0, p1, p2;
-};
-__device__ __forceinline__ LanePerm lane_perm() {
-    const int lane = threadIdx.x & 31;
-    return LanePerm{lane & 3, (lane >> 2) & 3, (lane >> 4) & 1};
-}
-
-// Flush a tile of C channels into the grid (w = 0 when C == 3) and clear it.
-template <int B, int C>
-__device__ __forceinline__ void flush_tile(float* tile, node4<float>* grid, const GridGeom& g, const int o[3]) {
-    constexpr int E = BrickShape<B>::E, NT = BrickShape<B>::NT;
-    for (int q = threadIdx.x; q < NT; q += blockDim.x) {
-        const int i = q / (E * E), j = (q / E) % E, k = q % E;
-        const int gi = o[0] + i, gj = o[1] + j, gk = o[2] + k;
-        float v[4] = {0.f, 0.f, 0.f, 0.f};
-#pragma unroll
-        for (int c = 0; c < C; c++) {
-            v[c] = tile[c * NT + q];
-            tile[c * NT + q] = 0.f;
-        }
-        const bool in = (unsigned)gi < (unsigned)g.dim[0] && (unsigned)gj < (unsigned)g.dim[1] &&
-                        (unsigned)gk < (unsigned)g.dim[2];
-        if (in && (v[0] != 0.f || v[1] != 0.f || v[2] != 0.f || v[3] != 0.f))
-            red_add4(grid + (((size_t)gi * g.dim[1] + gj) * g.dim[2] + gk), v[0], v[1], v[2], v[3]);
-    }
-}
-
-// Node sink: shared-tile atomics or global vector reductions.  (i, j, k) are
-// stencil offsets from the particle's base (already permuted by the caller).
-template <int B, int C> struct TileSink {
-    float* tile;
-    int l0, l1, l2;
-    __device__ __forceinline__ void operator()(int i, int j, int k, const float (&v)[4]) const {
-        constexpr int E = BrickShape<B>::E, NT = BrickShape<B>::NT;
-        const int q = ((l0 + i) * E + (l1 + j)) * E + (l2 + k);
-#pragma unroll
-        for (int c = 0; c < C; c++) atomicAdd(tile + c * NT + q, v[c]);
-    }
-};
-struct GlobalSink {
-    node4<float>* grid;
-    GridGeom g;
-    int b0, b1, b2;
-    __device__ __forceinline__ void operator()(int i, int j, int k, const float (&v)[4]) const {
-        const int gi = b0 + i, gj = b1 + j, gk = b2 + k;
-        if ((unsigned)gi < (unsigned)g.dim[0] && (unsigned)gj < (unsigned)g.dim[1] && (unsigned)gk < (unsigned)g.dim[2])
-            red_add4(grid + (((size_t)gi * g.dim[1] + gj) * g.dim[2] + gk), v[0], v[1], v[2], v[3]);
-    }
-};
-
-// P2G of one particle: m_g += w m_p;  p_g += w (m_p v (1 - dt drag) + G (x_g - x_p)),
-// nodes in the lane's permuted order (arrays indexed by t hold offset t ^ perm).
-template <class Sink>
-__device__ __forceinline__ void p2g_particle(const Sink& sink, const LanePerm& P, float mp, const float mvd[3],
-                                             const m3<float>& G, const Axis0& ax0, const float n1[4],
-                                             const float d1[4], const float n2[4], const float d2[4]) {
-#pragma unroll 1
-    for (int i = 0; i < 4; i++) {
-        const int ii = i ^ P.p0;
-        float n0, d0;
-        ax0(ii, n0, d0, nullptr);
-        float g0[3];
-#pragma unroll
-        for (int r = 0; r < 3; r++) g0[r] = mvd[r] + G.a[r][0] * d0;
-#pragma unroll
-        for (int j = 0; j < 4; j++) {
-            float g1[3];
-#pragma unroll
-            for (int r = 0; r < 3; r++) g1[r] = g0[r] + G.a[r][1] * d1[j];
-            const float w01 = n0 * n1[j];
-#pragma unroll
-            for (int k = 0; k < 4; k++) {
-                const float wt = w01 * n2[k];
-                float v[4];
-#pragma unroll
-                for (int r = 0; r < 3; r++) v[r] = wt * (g1[r] + G.a[r][2] * d2[k]);
-                v[3] = wt * mp;
-                sink(ii, j ^ P.p1, k ^ P.p2, v);
-            }
-        }
-    }
-}
-
-template <int B>
-__global__ void __launch_bounds__(DMPM_BRICK_THREADS, DMPM_BRICK_SCATTER_MINB) k_p2g_b(WArgs a) {
-    using S = BrickShape<B>;
-    __shared__ float tile[4 * S::NT];
-    for (int q = threadIdx.x; q < 4 * S::NT; q += blockDim.x) tile[q] = 0.f;
-    const int nun = (int)*a.n_units_dev;
-    const size_t np = a.np, npl = a.npl;
-    const GridGeom geo = a.geo;
-    const float dx = (float)geo.dx, idx = 1.f / dx;
-    const float damp = 1.f - a.dt * a.drag;
-    const LanePerm P = lane_perm();
-    for (int u = blockIdx.x; u < nun; u += gridDim.x) {
-        int o[3];
-        unit_origin(a.unit_key[u], S::shift, geo, o);
-        const uint32_t q0 = a.unit_start[u], q1 = a.unit_start[u + 1];
-        __syncthreads();  // the tile is clear
-        for (uint32_t q = q0 + threadIdx.x; q < q1; q += blockDim.x) {
-            const int p = (int)a.items.order[q];
-            float x[3];
-            int base[3];
-            load_x_base(a.st, npl, p, geo, x, base);
-            float n[3][4], d[3][4];
-            axis_stencil(x[1], (float)geo.mn[1], dx, idx, base[1], P.p1, n[1], d[1], nullptr);
-            axis_stencil(x[2], (float)geo.mn[2], dx, idx, base[2], P.p2, n[2], d[2], nullptr);
-            const Axis0 ax0{x[0], (float)geo.mn[0], dx, idx, base[0]};
-            const float mp = a.cst[(size_t)KM * np + p];
-            float mvd[3];
-#pragma unroll
-            for (int c = 0; c < 3; c++) mvd[c] = mp * a.st[(size_t)(PV + c) * npl + p] * damp;
-            const m3<float> G = load_m3(a.G, npl, p);
-            int l[3];
-            if (in_unit<B>(base, o, l))
-                p2g_particle(TileSink<B, 4>{tile, l[0], l[1], l[2]}, P, mp, mvd, G, ax0, n[1], d[1], n[2], d[2]);
-            else
-                p2g_particle(GlobalSink{a.grid, geo, base[0], base[1], base[2]}, P, mp, mvd, G, ax0, n[1], d[1], n[2],
-                             d[2]);
-        }
-        __syncthreads();
-        flush_tile<B, 4>(tile, a.grid, geo, o);
-    }
-}
-
-// adjoint G2P scatter of one particle: dLdv_g += w dLdv_next + 3/dx^2 w dLdC_next (x_g - x_p)
-template <class Sink>
-__device__ __forceinline__ void adj_scatter_particle(const Sink& sink, const LanePerm& P, const float vn[3],
-                                                     const m3<float>& kC, const Axis0& ax0, const float n1[4],
-                                                     const float d1[4], const float n2[4], const float d2[4]) {
-#pragma unroll 1
-    for (int i = 0; i < 4; i++) {
-        const int ii = i ^ P.p0;
-        float n0, d0;
-        ax0(ii, n0, d0, nullptr);
-        float c0[3];
-#pragma unroll
-        for (int r = 0; r < 3; r++) c0[r] = vn[r] + kC.a[r][0] * d0;
-#pragma unroll
-        for (int j = 0; j < 4; j++) {
-            float c1[3];
-#pragma unroll
-            for (int r = 0; r < 3; r++) c1[r] = c0[r] + kC.a[r][1] * d1[j];
-            const float w01 = n0 * n1[j];
-#pragma unroll
-            for (int k = 0; k < 4; k++) {
-                const float wt = w01 * n2[k];
-                float v[4];
-#pragma unroll
-                for (int r = 0; r < 3; r++) v[r] = wt * (c1[r] + kC.a[r][2] * d2[k]);
-                v[3] = 0.f;
-                sink(ii, j ^ P.p1, k ^ P.p2, v);
-            }
-        }
-    }
-}
-
-// dLdv_next = dt dLdx' + dLdv';  dLdC_next = c dt dLdF' Fe^T + dLdC' (stored to adjn for
-// the gather and the finalize), then the scatter above (BackPropagation.cpp:14-44)
-template <bool EXACT, int B>
-__global__ void __launch_bounds__(DMPM_BRICK_THREADS, DMPM_BRICK_SCATTER_MINB) k_adj_scatter_b(WArgs a) {
-    using S = BrickShape<B>;
-    __shared__ float tile[3 * S::NT];
-    for (int q = threadIdx.x; q < 3 * S::NT; q += blockDim.x) tile[q] = 0.f;
-    const int nun = (int)*a.n_units_dev;
-    const size_t np = a.np, npl = a.npl, npn = a.npn;
-    const GridGeom geo = a.geo;
-    const float dx = (float)geo.dx, idx = 1.f / dx, k3 = 3.f / (dx * dx);
-    const float cf = EXACT ? (1.f - a.s) * a.dt : a.dt;
-    const LanePerm P = lane_perm();
-    for (int u = blockIdx.x; u < nun; u += gridDim.x) {
-        int o[3];
-        unit_origin(a.unit_key[u], S::shift, geo, o);
-        const uint32_t q0 = a.unit_start[u], q1 = a.unit_start[u + 1];
-        __syncthreads();
-        for (uint32_t q = q0 + threadIdx.x; q < q1; q += blockDim.x) {
-            const int p = (int)a.items.order[q];
-            float x[3];
-            int base[3];
-            load_x_base(a.st, npl, p, geo, x, base);
-            float vn[3];
-#pragma unroll
-            for (int c = 0; c < 3; c++)
-                vn[c] = a.dt * a.adj_next[(size_t)(PX + c) * npn + p] + a.adj_next[(size_t)(PV + c) * npn + p];
-            const m3<float> Fe = load_m3(a.st + (size_t)PF * npl, npl, p) + load_m3(a.dfc, np, p);
-            const m3<float> Cn = (cf * load_m3(a.adj_next + (size_t)PF * npn, npn, p)) * transpose(Fe) +
-                                 load_m3(a.adj_next + (size_t)PC * npn, npn, p);
-#pragma unroll
-            for (int c = 0; c < 3; c++) a.adjn[(size_t)c * np + p] = vn[c];
-            store_m3(a.adjn + 3 * np, np, p, Cn);
-            if (a.dbg_vnext) {
-#pragma unroll
-                for (int c = 0; c < 3; c++) a.dbg_vnext[(size_t)c * np + p] = vn[c];
-            }
-            if (a.dbg_Cnext) store_m3(a.dbg_Cnext, np, p, Cn);
-            float n[3][4], d[3][4];
-            axis_stencil(x[1], (float)geo.mn[1], dx, idx, base[1], P.p1, n[1], d[1], nullptr);
-            axis_stencil(x[2], (float)geo.mn[2], dx, idx, base[2], P.p2, n[2], d[2], nullptr);
-            const Axis0 ax0{x[0], (float)geo.mn[0], dx, idx, base[0]};
-            const m3<float> kC = k3 * Cn;
-            int l[3];
-            if (in_unit<B>(base, o, l))
-                adj_scatter_particle(TileSink<B, 3>{tile, l[0], l[1], l[2]}, P, vn, kC, ax0, n[1], d[1], n[2], d[2]);
-            else
-                adj_scatter_particle(GlobalSink{a.gadj, geo, base[0], base[1], base[2]}, P, vn, kC, ax0, n[1], d[1],
-                                     n[2], d[2]);
-        }
-        __syncthreads();
-        flush_tile<B, 3>(tile, a.gadj, geo, o);
     }
 }
 

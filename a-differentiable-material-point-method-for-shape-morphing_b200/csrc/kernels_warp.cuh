@@ -17,10 +17,35 @@
 // the node loops keep a small register footprint.
 //
 // Math per stage is that of kernels.cuh (which cites the reference).
+//
+// Strain storage: the FP32 path keeps each layer's deformation gradient as its
+// strain H = F - I in the F planes (PF).  Strains of a few 1e-3 keep float's
+// full relative precision this way, where F itself (about 1) would round them
+// to ~1e-4 relative at every step.  Kernels form F = I + H where they need it
+// -- in FP64 for the polar decomposition -- and update H directly:
+//   H' = (1 - s)(D + dt C' (I + D)) + s H,  D = H + dFc.
+// The host converts at upload and download; the FP64 path stores F.
 #pragma once
 #include "sort.cuh"
 
 namespace dmpm {
+
+// F + dFc = I + H + dFc of layer n, in float and (exactly) in double
+__device__ __forceinline__ m3<float> fe_from_strain(const m3<float>& H, const m3<float>& dfc) {
+    m3<float> r = H + dfc;
+    r.a[0][0] += 1.f;
+    r.a[1][1] += 1.f;
+    r.a[2][2] += 1.f;
+    return r;
+}
+__device__ __forceinline__ m3<double> fe_from_strain_d(const m3<float>& H, const m3<float>& dfc) {
+    m3<double> r;
+#pragma unroll
+    for (int i = 0; i < 3; i++)
+#pragma unroll
+        for (int j = 0; j < 3; j++) r.a[i][j] = (double)H.a[i][j] + (double)dfc.a[i][j] + (i == j ? 1.0 : 0.0);
+    return r;
+}
 
 struct WarpItems {
     const uint32_t* order;       // sorted particle indices
@@ -391,8 +416,9 @@ static __global__ void __launch_bounds__(256, DMPM_STRESS_MIN_BLOCKS) k_stress(W
     const size_t np = a.np, npl = a.npl;
     const int p = blockIdx.x * blockDim.x + threadIdx.x;
     if (p < a.n) {
-        const m3<float> Fe = load_m3(a.st + (size_t)PF * npl, npl, p) + load_m3(a.dfc, np, p);
-        const m3<double> Fed = m3_cast<double>(Fe);
+        const m3<float> H = load_m3(a.st + (size_t)PF * npl, npl, p), dfc = load_m3(a.dfc, np, p);
+        const m3<float> Fe = fe_from_strain(H, dfc);
+        const m3<double> Fed = fe_from_strain_d(H, dfc);
         m3<double> Rd, Sd;
         if (!DMPM_NEWTON_POLAR || !polar_newton(Fed, Rd, Sd)) polar3(Fed, Rd, Sd);
         const m3<double> Pd = pk_from_polar(Fed, Rd, (double)a.cst[(size_t)KLAM * np + p], (double)a.cst[(size_t)KMU * np + p]);
@@ -603,19 +629,20 @@ template <int MODE> __global__ void __launch_bounds__(256, 4) k_g2p_w(WArgs a) {
         if (L.s == 1) {
             store_m3(a.st_next + (size_t)PC * npn, npn, p, Cn);
         } else {
+            // column c of the strain: H' = (1 - s)(D + dt C' (I + D)) + s H,  D = H + dFc
             const int c = L.s == 0 ? 0 : L.s - 1;
-            float Fc[3], Fec[3];
+            float Hc[3], Dc[3];
 #pragma unroll
             for (int r = 0; r < 3; r++) {
-                Fc[r] = a.st[(size_t)(PF + r + 3 * c) * npl + p];
-                Fec[r] = Fc[r] + a.dfc[(size_t)(r + 3 * c) * np + p];
+                Hc[r] = a.st[(size_t)(PF + r + 3 * c) * npl + p];
+                Dc[r] = Hc[r] + a.dfc[(size_t)(r + 3 * c) * np + p];
             }
 #pragma unroll
             for (int r = 0; r < 3; r++) {
-                const float t = Fec[r] + a.dt * (Cn.a[r][0] * Fec[0] + Cn.a[r][1] * Fec[1] + Cn.a[r][2] * Fec[2]);
-                const float fn = (1.f - a.s) * t + a.s * Fc[r];
-                a.st_next[(size_t)(PF + r + 3 * c) * npn + p] = fn;
-                finite &= isfinite(fn);
+                const float t = Dc[r] + a.dt * (Cn.a[r][c] + (Cn.a[r][0] * Dc[0] + Cn.a[r][1] * Dc[1] + Cn.a[r][2] * Dc[2]));
+                const float hn = (1.f - a.s) * t + a.s * Hc[r];
+                a.st_next[(size_t)(PF + r + 3 * c) * npn + p] = hn;
+                finite &= isfinite(hn);
             }
         }
         if (!finite) atomicOr(a.status, ST_NONFINITE_FWD);
@@ -646,7 +673,7 @@ template <bool EXACT, bool GENERAL, int MODE> __global__ void __launch_bounds__(
 #pragma unroll
         for (int c = 0; c < 3; c++)
             vn[c] = a.dt * a.adj_next[(size_t)(PX + c) * npn + p] + a.adj_next[(size_t)(PV + c) * npn + p];
-        const m3<float> Fe = load_m3(a.st + (size_t)PF * npl, npl, p) + load_m3(a.dfc, np, p);
+        const m3<float> Fe = fe_from_strain(load_m3(a.st + (size_t)PF * npl, npl, p), load_m3(a.dfc, np, p));
         const float cf = EXACT ? (1.f - a.s) * a.dt : a.dt;
         const m3<float> Cn = (cf * load_m3(a.adj_next + (size_t)PF * npn, npn, p)) * transpose(Fe) +
                              load_m3(a.adj_next + (size_t)PC * npn, npn, p);
@@ -864,7 +891,7 @@ template <bool EXACT, int MODE> __global__ void __launch_bounds__(256, DMPM_GATH
 // controls, the 9 FP64 planes of the control-gradient accumulator.
 enum : int {
     FS_GATH = 0,    // 18: M (9, row-major), X (3), u (3), z (3)
-    FS_F = 18,      // 9: F of layer n
+    FS_F = 18,      // 9: strain H = F - I of layer n
     FS_DFC = 27,    // 9: dFc
     FS_AUX = 36,    // 24: G (9), polar R (9), polar S (6)
     FS_CST = 60,    // 4: m, vol, lam, mu
@@ -951,8 +978,9 @@ __device__ __forceinline__ void finalize_particle(const WArgs& a, int p, const I
         if (!isfinite(transport())) atomicOr(a.status, ST_NONFINITE_ADJ);
         return;
     }
-    const m3<float> Fe = mat(FS_F) + mat(FS_DFC);
-    const m3<double> Fed = m3_cast<double>(Fe);
+    const m3<float> H = mat(FS_F), dfc = mat(FS_DFC);
+    const m3<float> Fe = fe_from_strain(H, dfc);
+    const m3<double> Fed = fe_from_strain_d(H, dfc);
     // polar factors computed in FP64 by k_stress for this layer
     const m3<double> Rd = m3_cast<double>(mat(FS_AUX + 9));
     m3<double> Sd;
