@@ -4,16 +4,19 @@
 // unit -- a brick of 4 x 4 x 4 cells (B = 4) or one 2 x 2 x 2 octant of a
 // brick (B = 2) -- are one contiguous run of the sorted order.  Every stencil
 // of a particle whose cell lies in the unit falls inside the unit's node tile
-// of (B + 3)^3 nodes (stencil bases c - 1 .. c + B - 2 plus 3).  A CTA takes a
-// unit, stages the tile in shared memory once, and its threads each handle one
-// particle of the unit, all 64 stencil nodes of it, reading the tile (the
-// particles of a warp share a cell most of the time, so their reads are
-// broadcasts).  These are the two stencil kernels that only read the grid: G2P
-// and the adjoint P2G gather.  The scatters stay warp-item kernels
-// (kernels_warp.cuh): adding into a shared tile with shared-memory atomics,
-// even with each lane visiting its stencil in its own order so the lanes of a
-// cell touch different nodes, measured 3-4x slower than the warp's butterfly
-// reduction followed by one vector red.global.add per node.
+// of (B + 3)^3 nodes (stencil bases c - 1 .. c + B - 2 plus 3).  G2P, which
+// only reads the grid, runs over units: a CTA takes a unit, stages its node
+// tile in shared memory once, and each thread handles one particle of the unit,
+// all 64 stencil nodes of it, reading the tile (the particles of a warp share a
+// cell most of the time, so the reads are broadcasts).  On the 64^3,
+// 267k-particle workload this takes 36.7 us per step against 48.1 us for the
+// warp-item G2P; at 8 particles per cell, 21.5 against 22.2 us.  The other
+// stencil kernels stay warp-item kernels (kernels_warp.cuh), which measured
+// faster: the adjoint gather over brick tiles took 95-115 us against 79 us
+// (its 18 sums per particle need 128-170 registers per thread, so few warps
+// reside), and P2G and the adjoint scatter adding into shared tiles with
+// shared-memory atomics took 3-4x longer than the warp's butterfly reduction
+// followed by one vector red.global.add per node.
 // A particle that has left the unit since the sort (the sort runs every few
 // steps) is handled by the same code with its nodes read from global memory.
 //
@@ -30,9 +33,6 @@ namespace dmpm {
 // minimum resident CTAs per SM (the register cap the compiler works to)
 #ifndef DMPM_BRICK_G2P_MINB
 #define DMPM_BRICK_G2P_MINB 4
-#endif
-#ifndef DMPM_BRICK_GATHER_MINB
-#define DMPM_BRICK_GATHER_MINB 3
 #endif
 
 template <int B> struct BrickShape {
@@ -237,135 +237,6 @@ __global__ void __launch_bounds__(DMPM_BRICK_THREADS, DMPM_BRICK_G2P_MINB) k_g2p
                     finite &= isfinite(hn);
                 }
             if (!finite) atomicOr(a.status, ST_NONFINITE_FWD);
-        }
-    }
-}
-
-// ------------------------------------------------------------------ adjoint P2G gather
-// Per particle over its 64 nodes (records (dLdp, dLdm), (v, m)):
-//   M[r][c] = sum w d_r dLdp_c,  X = sum sigma grad(N N N),  u = sum w dLdp,  z = sum w v_g,
-//   sigma = m dLdm + dLdp.(m v c_d + G d) + v_g.(dLdv_next + 3/dx^2 dLdC_next d)
-// (the algebra of kernels.cuh:k_adj_gather), written to gath for the finalize.
-struct GatherIn {
-    float mp;
-    float mvp[3], vn[3];
-    m3<float> G, kC;  // G and 3/dx^2 dLdC_next
-};
-template <class Fetch>
-__device__ __forceinline__ void gather_sums(const Fetch& f, const GatherIn& in, const Axis0& ax0, const Axis0& ax1,
-                                            const float n2[4], const float d2[4], const float s2[4], float acc[18]) {
-    float nd2[4];
-#pragma unroll
-    for (int k = 0; k < 4; k++) nd2[k] = n2[k] * d2[k];
-#pragma unroll
-    for (int t = 0; t < 18; t++) acc[t] = 0.f;
-#pragma unroll 1
-    for (int i = 0; i < 4; i++) {
-        float n0, d0, s0;
-        ax0(i, n0, d0, &s0);
-        float hi[3], ei[3];
-#pragma unroll
-        for (int r = 0; r < 3; r++) {
-            hi[r] = in.mvp[r] + in.G.a[r][0] * d0;
-            ei[r] = in.vn[r] + in.kC.a[r][0] * d0;
-        }
-#pragma unroll 1
-        for (int j = 0; j < 4; j++) {
-            float n1, d1, s1;
-            ax1(j, n1, d1, &s1);
-            float hj[3], ej[3];
-#pragma unroll
-            for (int r = 0; r < 3; r++) {
-                hj[r] = hi[r] + in.G.a[r][1] * d1;
-                ej[r] = ei[r] + in.kC.a[r][1] * d1;
-            }
-            // row sums over k: S = sum n2 sigma, T = sum s2 sigma, U = sum n2 dLdp,
-            // Z = sum n2 v_g, W = sum n2 d2 dLdp
-            float Sj = 0.f, Tj = 0.f;
-            float U[3] = {0.f, 0.f, 0.f}, Z[3] = {0.f, 0.f, 0.f}, Wd[3] = {0.f, 0.f, 0.f};
-#pragma unroll
-            for (int k = 0; k < 4; k++) {
-                const node4<float> o = f(i, j, k, 0);
-                const node4<float> vg = f(i, j, k, 1);
-                float sig = in.mp * o.w;
-                sig += o.x * (hj[0] + in.G.a[0][2] * d2[k]);
-                sig += o.y * (hj[1] + in.G.a[1][2] * d2[k]);
-                sig += o.z * (hj[2] + in.G.a[2][2] * d2[k]);
-                sig += vg.x * (ej[0] + in.kC.a[0][2] * d2[k]);
-                sig += vg.y * (ej[1] + in.kC.a[1][2] * d2[k]);
-                sig += vg.z * (ej[2] + in.kC.a[2][2] * d2[k]);
-                Sj += n2[k] * sig;
-                Tj += s2[k] * sig;
-                U[0] += n2[k] * o.x;
-                U[1] += n2[k] * o.y;
-                U[2] += n2[k] * o.z;
-                Z[0] += n2[k] * vg.x;
-                Z[1] += n2[k] * vg.y;
-                Z[2] += n2[k] * vg.z;
-                Wd[0] += nd2[k] * o.x;
-                Wd[1] += nd2[k] * o.y;
-                Wd[2] += nd2[k] * o.z;
-            }
-            // the row's weights: w = n0 n1 n2, grad = (s0 n1 n2, n0 s1 n2, n0 n1 s2)
-            const float w01 = n0 * n1;
-            const float w01d0 = w01 * d0, w01d1 = w01 * d1;
-            acc[9] += (s0 * n1) * Sj;
-            acc[10] += (n0 * s1) * Sj;
-            acc[11] += w01 * Tj;
-#pragma unroll
-            for (int c = 0; c < 3; c++) {
-                acc[12 + c] += w01 * U[c];
-                acc[15 + c] += w01 * Z[c];
-                acc[c] += w01d0 * U[c];
-                acc[3 + c] += w01d1 * U[c];
-                acc[6 + c] += w01 * Wd[c];
-            }
-        }
-    }
-}
-
-template <bool EXACT, int B>
-__global__ void __launch_bounds__(DMPM_BRICK_THREADS, DMPM_BRICK_GATHER_MINB) k_adj_gather_b(WArgs a) {
-    using S = BrickShape<B>;
-    __shared__ node4<float> tile[2 * S::NT];
-    const int nun = (int)*a.n_units_dev;
-    const size_t np = a.np, npl = a.npl;
-    const GridGeom geo = a.geo;
-    const float dx = (float)geo.dx, idx = 1.f / dx, k3 = 3.f / (dx * dx);
-    const float cd = EXACT ? (1.f - a.dt * a.drag) : 1.f;
-    for (int u = blockIdx.x; u < nun; u += gridDim.x) {
-        int o[3];
-        unit_origin(a.unit_key[u], S::shift, geo, o);
-        const uint32_t q0 = a.unit_start[u], q1 = a.unit_start[u + 1];
-        __syncthreads();
-        stage_tile<B, 2>(a.gadj2, geo, 0, o, tile);
-        __syncthreads();
-        for (uint32_t q = q0 + threadIdx.x; q < q1; q += blockDim.x) {
-            const int p = (int)a.items.order[q];
-            float x[3];
-            int base[3];
-            load_x_base(a.st, npl, p, geo, x, base);
-            float n2[4], d2[4], s2[4];
-            axis_stencil(x[2], (float)geo.mn[2], dx, idx, base[2], n2, d2, s2);
-            const Axis0 ax0{x[0], (float)geo.mn[0], dx, idx, base[0]};
-            const Axis0 ax1{x[1], (float)geo.mn[1], dx, idx, base[1]};
-            GatherIn in;
-            in.mp = a.cst[(size_t)KM * np + p];
-#pragma unroll
-            for (int c = 0; c < 3; c++) {
-                in.mvp[c] = in.mp * a.st[(size_t)(PV + c) * npl + p] * cd;
-                in.vn[c] = a.adjn[(size_t)c * np + p];
-            }
-            in.G = load_m3(a.G, npl, p);
-            in.kC = k3 * load_m3(a.adjn + 3 * np, np, p);
-            float acc[18];
-            int l[3];
-            if (in_unit<B>(base, o, l))
-                gather_sums(TileFetch<B, 2>{tile, l[0], l[1], l[2]}, in, ax0, ax1, n2, d2, s2, acc);
-            else
-                gather_sums(GlobalFetch<2>{a.gadj2, geo, 0, base[0], base[1], base[2]}, in, ax0, ax1, n2, d2, s2, acc);
-#pragma unroll
-            for (int t = 0; t < 18; t++) a.gath[(size_t)t * np + p] = acc[t];
         }
     }
 }

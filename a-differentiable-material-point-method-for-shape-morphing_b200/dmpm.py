@@ -244,7 +244,7 @@ class Context:
                    adjoint: str = "refcompat", control: str = "per_layer", loss: str = "ref",
                    checkpoint_every: int = 0, keep_adjoints: bool = False, keep_intermediates: bool = False,
                    block_size: int = 0, tile_cap: int = 0, sort_every: int = 0, warp_general: bool = False,
-                   control_stride: int = 0, eager: bool = False, brick_cells: int = 0):
+                   control_stride: int = 0, eager: bool = False, brick_cells: Optional[int] = None):
         p = Params()
         self.lib.dmpm_default_params(ctypes.byref(p))
         p.dt, p.drag, p.smoothing = float(dt), float(drag), float(smoothing)
@@ -262,7 +262,8 @@ class Context:
         p.warp_general = int(bool(warp_general))
         p.control_stride = int(control_stride)
         p.eager = int(bool(eager))
-        p.brick_cells = int(brick_cells)
+        if brick_cells is not None:  # else the library default (bricks of 2^3 cells for G2P)
+            p.brick_cells = int(brick_cells)
         self._ck(self.lib.dmpm_set_params(self.h, ctypes.byref(p)), "set_params")
         self.params = p
 

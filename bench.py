@@ -175,8 +175,9 @@ def build_scene(instance: int, ppc_root: int):
     return sc
 
 
-# stencil kernels of the FP32 path: 0 = warp items, 2 or 4 = bricks of that many cells per axis
-BRICK_CELLS = 0
+# G2P kernel of the FP32 path: None = the library default (bricks of 2^3 cells), 0 = warp
+# items, 2 or 4 = bricks of that many cells per axis
+BRICK_CELLS = None
 
 
 def setup_ctx(dmpm, sc, prec, device, vol, target, dt, checkpoint_every, control="tied", control_stride=0,
@@ -196,7 +197,7 @@ def setup_ctx(dmpm, sc, prec, device, vol, target, dt, checkpoint_every, control
     c.set_target_mass(target)
     c.set_params(dt=dt, drag=sc.drag, f_ext=sc.f_ext, smoothing=sc.smoothing, adjoint="exact", control=control,
                  loss="ref", checkpoint_every=checkpoint_every, control_stride=control_stride,
-                 brick_cells=BRICK_CELLS if prec == "fp32" else 0)
+                 brick_cells=BRICK_CELLS if prec == "fp32" else None)
     c.setup(sc.steps + 1)
     return c
 
@@ -369,7 +370,7 @@ def workload_config(sc, dt_sub, ckpt):
             "particles": sc.n, "grid": list(sc.dims), "layers": sc.steps + 1, "dt": sc.dt,
             "dt_substituted_from": dt_sub, "checkpoint_every": ckpt, "loss": "reference log-mass + min-mass penalty",
             "l2_policy": "inputs larger than L2 (per-rollout layer state > 5 GB, 126 MB L2)",
-            "stencil_kernels": "bricks of %d^3 cells" % BRICK_CELLS if BRICK_CELLS else "warp items",
+            "g2p_kernel": "warp items" if BRICK_CELLS == 0 else "bricks of %d^3 cells" % (BRICK_CELLS or 2),
             "parallelism": "replicas: one independent instance per GPU"}
 
 
@@ -1073,7 +1074,7 @@ def main():
     ap.add_argument("--dt", type=float, default=0.0, help="override dt (default: configured, CFL fallback)")
     ap.add_argument("--checkpoint-every", type=int, default=1)
     ap.add_argument("--brick", type=int, default=None, choices=[0, 2, 4],
-                    help="FP32 stencil kernels: 0 warp items, 2 or 4 cells per brick axis")
+                    help="FP32 G2P kernel: 0 warp items, 2 or 4 cells per brick axis (default 2)")
     ap.add_argument("--rollout-steps", type=int, default=0, help="override the 200 time steps (profiling runs)")
     ap.add_argument("--no-fp64", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")

@@ -138,11 +138,10 @@ typedef struct {
     int eager;               /* FP32 path with every layer kept: 0 = capture dmpm_forward / dmpm_backward
                                 once per start (top, control) layer and replay them as CUDA graphs;
                                 1 = launch kernel by kernel (per-kernel profiling also does) */
-    int brick_cells;         /* FP32 path: the read-only stencil kernels (G2P and the adjoint P2G
-                                gather) over cell bricks: 0 = warp items (8 particles of a cell per
-                                warp); 2 or 4 = a CTA stages the node tile of a brick of
-                                brick_cells^3 cells in shared memory and each thread handles one
-                                particle of it.  Takes effect at the next cell sort. */
+    int brick_cells;         /* FP32 path, G2P: 2 (default) or 4 = a CTA stages the node tile of a brick
+                                of brick_cells^3 cells in shared memory and each thread handles one
+                                particle of it; 0 = warp items (8 particles of a cell per warp).
+                                Takes effect at the next cell sort. */
 } dmpm_params;
 
 void dmpm_default_params(dmpm_params* p);

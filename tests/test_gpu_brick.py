@@ -1,11 +1,12 @@
-"""Brick kernels of the FP32-mixed path (brick_cells = 2 or 4): one thread per
-particle over the node tile of a brick of cells staged in shared memory.  They
-compute what the warp-item kernels compute, summed in another order, so they
-are held to the same bars against the FP64 oracle (the CPU restatement of the
-reference's ForwardTimeStep / EndLayerMassLoss / Back_Timestep) and to the
-warp-item kernels' results on the same inputs.  Particles that leave their
-brick between cell sorts take the kernels' global-memory path; the long sort
-interval and fast cloud below make many of them."""
+"""The brick G2P of the FP32-mixed path (brick_cells = 2, the default, or 4):
+one thread per particle over the node tile of a brick of cells staged in shared
+memory.  It computes what the warp-item G2P (brick_cells = 0) computes, summed
+in another order, so it is held to the same bars against the FP64 oracle (the
+CPU restatement of the reference's ForwardTimeStep / EndLayerMassLoss /
+Back_Timestep) and to the warp-item kernel's results on the same inputs.
+Particles that leave their brick between cell sorts take the kernel's
+global-memory path; the long sort interval and fast cloud below make many of
+them."""
 import numpy as np
 import pytest
 
@@ -80,7 +81,7 @@ def test_brick_kernels_match_warp_items(gpu_ready, case, brick):
     """Same inputs, same FP32 arithmetic per term: the two kernel families differ
     only by float summation order."""
     sc, o, loss, L = case
-    w = _run(sc, o.target, L)
+    w = _run(sc, o.target, L, brick_cells=0)
     b = _run(sc, o.target, L, brick_cells=brick)
     assert relerr(b["x"], w["x"]) < 1e-5
     assert relerr(b["F"], w["F"]) < 1e-5
