@@ -259,15 +259,11 @@ __device__ __forceinline__ void load_x_base(const float* st, size_t np, int p, c
 // FP64 part alone (5: 96 registers with a 144-byte spill, 40.6 against 45.2 us
 // at 4 and 44.4 us at 6 on the same workload: the extra warps hide more of the
 // load latency than the spills cost).
-// k_stress takes the FP64 polar factors from the Newton-Schulz iteration
-// (polar_schulz) where F + dFc is near a rotation, from the scaled Newton
-// iteration (polar_newton) where det(F + dFc) > 0 otherwise, and from the SVD
-// (polar3) for the rest; 0 uses the SVD everywhere
+// k_stress takes the FP64 polar factors from the scaled Newton iteration
+// (polar_newton) where det(F + dFc) > 0 and from the SVD (polar3) otherwise;
+// 0 uses the SVD everywhere
 #ifndef DMPM_NEWTON_POLAR
 #define DMPM_NEWTON_POLAR 1
-#endif
-#ifndef DMPM_SCHULZ_POLAR
-#define DMPM_SCHULZ_POLAR 1
 #endif
 #ifndef DMPM_STRESS_MIN_BLOCKS
 #define DMPM_STRESS_MIN_BLOCKS 2
@@ -426,8 +422,7 @@ static __global__ void __launch_bounds__(256, DMPM_STRESS_MIN_BLOCKS) k_stress(W
         const m3<float> Fe = fe_from_strain(H, dfc);
         const m3<double> Fed = fe_from_strain_d(H, dfc);
         m3<double> Rd, Sd;
-        if (!DMPM_NEWTON_POLAR || !((DMPM_SCHULZ_POLAR && polar_schulz(Fed, Rd, Sd)) || polar_newton(Fed, Rd, Sd)))
-            polar3(Fed, Rd, Sd);
+        if (!DMPM_NEWTON_POLAR || !polar_newton(Fed, Rd, Sd)) polar3(Fed, Rd, Sd);
         const m3<double> Pd = pk_from_polar(Fed, Rd, (double)a.cst[(size_t)KLAM * np + p], (double)a.cst[(size_t)KMU * np + p]);
         const m3<float> P = m3_cast<float>(Pd);
         if (a.P) store_m3(a.P, npl, p, P);

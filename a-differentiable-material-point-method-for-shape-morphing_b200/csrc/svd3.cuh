@@ -309,49 +309,4 @@ template <class T> DMPM_HD bool polar_newton(const m3<T>& F, m3<T>& R, m3<T>& S)
     return true;
 }
 
-// Polar decomposition F = R S of a matrix near a rotation by the Newton-Schulz
-// iteration  X <- X (3I - X^T X) / 2  (Higham, Functions of Matrices, 2008,
-// section 8.3), which converges quadratically to the rotation of the polar
-// decomposition when every singular value of F lies in (0, sqrt 3), with
-// matrix products only (no inverse, determinant or cube root, which the
-// scaled Newton iteration needs every step).  Used where |F^T F - I|_F < 1/2
-// (strains up to ~20 %, every particle of the benchmark scenes); from there
-// the error e = |X^T X - I| falls as about 3 e^2 / 4 per step, so 1e-2 takes 3
-// steps to FP64 rounding.  Stops once e^2 <= 1e-18 (the next step leaves
-// ~1e-18, below rounding) and returns false -- the caller then falls back to
-// polar_newton -- for det F <= 0, larger strains, or no convergence in 8 steps.
-template <class T> DMPM_HD bool polar_schulz(const m3<T>& F, m3<T>& R, m3<T>& S) {
-    if (!(det3(F) > T(0))) return false;
-    m3<T> X = F;
-    bool done = false;
-    for (int it = 0; it < 8 && !done; it++) {
-        m3<T> E = mtm(X, X);  // X^T X - I, symmetric
-        T e2 = T(0);
-#pragma unroll
-        for (int i = 0; i < 3; i++) {
-            E.a[i][i] -= T(1);
-#pragma unroll
-            for (int j = 0; j < 3; j++) e2 += E.a[i][j] * E.a[i][j];
-        }
-        if (it == 0 && !(e2 < T(0.25))) return false;
-        done = e2 <= T(1e-18);
-        // X <- X (I - E / 2)
-        m3<T> Y;
-#pragma unroll
-        for (int i = 0; i < 3; i++)
-#pragma unroll
-            for (int j = 0; j < 3; j++)
-                Y.a[i][j] = X.a[i][j] - T(0.5) * (X.a[i][0] * E.a[0][j] + X.a[i][1] * E.a[1][j] + X.a[i][2] * E.a[2][j]);
-        X = Y;
-    }
-    if (!done) return false;
-    R = X;
-    const m3<T> M = mtm(R, F);  // R^T F, symmetric up to rounding
-#pragma unroll
-    for (int i = 0; i < 3; i++)
-#pragma unroll
-        for (int j = 0; j < 3; j++) S.a[i][j] = T(0.5) * (M.a[i][j] + M.a[j][i]);
-    return true;
-}
-
 }  // namespace dmpm

@@ -24,9 +24,6 @@ template <class T> static void st(const m3<T>& m, T* a) {
     extern "C" int mh_polar_newton_##SFX(const T* F, T* R, T* S) {                                    \
         m3<T> Rm, Sm; const bool ok = polar_newton(ld(F), Rm, Sm); if (ok) { st(Rm, R); st(Sm, S); }   \
         return ok ? 1 : 0; }                                                                          \
-    extern "C" int mh_polar_schulz_##SFX(const T* F, T* R, T* S) {                                    \
-        m3<T> Rm, Sm; const bool ok = polar_schulz(ld(F), Rm, Sm); if (ok) { st(Rm, R); st(Sm, S); }   \
-        return ok ? 1 : 0; }                                                                          \
     extern "C" void mh_pk_##SFX(const T* F, T lam, T mu, T* P) { st(pk_stress(ld(F), lam, mu), P); } \
     extern "C" void mh_d2_##SFX(const T* F, T lam, T mu, const T* dF, int exact, T* out) {            \
         st(exact ? d2_mult<true>(ld(F), lam, mu, ld(dF)) : d2_mult<false>(ld(F), lam, mu, ld(dF)), out); }

@@ -158,36 +158,6 @@ def test_newton_polar_matches_svd_polar(mh):
         assert mh.mh_polar_newton_f64(cm(F).ctypes.data_as(P), R.ctypes.data_as(P), S.ctypes.data_as(P)) == 0
 
 
-def test_schulz_polar_matches_svd_polar(mh):
-    """polar_schulz (k_stress's polar factors for F near a rotation) gives
-    polar3's R and S to rounding wherever it accepts F -- every F within 10 %
-    strain of a rotation -- and declines inverted F and large strains."""
-    mh.mh_polar_schulz_f64.restype = ctypes.c_int
-    rng = np.random.default_rng(77)
-    accepted = 0
-    for t in range(400):
-        Q, _ = np.linalg.qr(rng.normal(size=(3, 3)))
-        Q *= np.sign(np.linalg.det(Q))
-        scale = [1e-6, 1e-3, 3e-2, 0.1][t % 4]
-        F = Q @ (np.eye(3) + scale * rng.normal(size=(3, 3)))
-        R = np.zeros(9)
-        S = np.zeros(9)
-        ok = mh.mh_polar_schulz_f64(cm(F).ctypes.data_as(P), R.ctypes.data_as(P), S.ctypes.data_as(P))
-        if scale <= 3e-2:
-            assert ok == 1, scale
-        if not ok:
-            continue
-        accepted += 1
-        R0, S0 = polar(mh, F)
-        assert np.abs(un(R) - R0).max() < 1e-13
-        assert np.abs(un(S) - S0).max() < 1e-13 * max(1.0, np.abs(S0).max())
-    assert accepted >= 300
-    for F in (np.diag([1.0, 1.0, -1.0]), np.diag([2.0, 1.0, 1.0]), 3.0 * np.eye(3)):
-        R = np.zeros(9)
-        S = np.zeros(9)
-        assert mh.mh_polar_schulz_f64(cm(F).ctypes.data_as(P), R.ctypes.data_as(P), S.ctypes.data_as(P)) == 0
-
-
 def test_compat_djfit_matches_reference_fd():
     """The compat API's d_JFit_dF_FD (a host utility) against the reference's
     FP64 build on the elementary fixture's 25 matrices, and its closed-form
