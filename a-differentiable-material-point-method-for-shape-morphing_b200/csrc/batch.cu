@@ -149,7 +149,6 @@ struct dmpm_batch::Impl {
     float* adj[2] = {nullptr, nullptr};
     float *adjn = nullptr, *gath = nullptr;
     node4<float>*gadj = nullptr, *gadj2 = nullptr;
-    double* gmass = nullptr;  // FP64 node masses of the P2G in progress (k_gop_inplace)
     double* ctrl_acc = nullptr;
     std::vector<BEpoch> ep;
     int ep_every = 0;
@@ -415,7 +414,6 @@ struct dmpm_batch::Impl {
         gath = (float*)layers.alloc((size_t)18 * np0 * 4);
         ctrl_acc = (double*)layers.alloc((size_t)9 * np0 * 8);
         gadj = (node4<float>*)layers.alloc(Gtot * sizeof(node4<float>));
-        gmass = (double*)layers.alloc(Gtot * sizeof(double));
         gadj2 = (node4<float>*)layers.alloc(2 * Gtot * sizeof(node4<float>));
         for (int i = 0; i < 2; i++) {
             sk[i] = (uint32_t*)layers.alloc(np0 * 4);
@@ -502,7 +500,6 @@ struct dmpm_batch::Impl {
         a.dfc = dfc;
         a.G = aux[t];
         a.grid = grid[t];
-        a.gmass = gmass;
         a.status = status;
         return a;
     }
@@ -517,12 +514,11 @@ struct dmpm_batch::Impl {
         const int pb = particle_block();
         const unsigned wb = warp_blocks(t);
         DMPM_CK(cudaMemsetAsync(grid[t], 0, Gt * sizeof(node4<float>), b->stream));
-        DMPM_CK(cudaMemsetAsync(gmass, 0, Gt * sizeof(double), b->stream));
         k_stress<<<(unsigned)((a.n + pb - 1) / pb), pb, 0, b->stream>>>(a);
         launched();
         k_p2g_w<false, ITEMS_BATCH><<<wb, 256, 0, b->stream>>>(a);
         launched();
-        k_gop_inplace<<<(unsigned)((Gt + 255) / 256), 256, 0, b->stream>>>(grid[t], gmass, Gt, a.dt, a.fext[0], a.fext[1],
+        k_gop_inplace<<<(unsigned)((Gt + 255) / 256), 256, 0, b->stream>>>(grid[t], Gt, a.dt, a.fext[0], a.fext[1],
                                                                              a.fext[2]);
         launched();
         k_g2p_w<ITEMS_BATCH><<<wb, 256, 0, b->stream>>>(a);

@@ -284,7 +284,6 @@ template <class T> class Engine : public EngineBase {
         DMPM_CK(cudaMemsetAsync(target_, 0, G_ * sizeof(T), ctx_->stream));
         dldm_ = (T*)scene_arena_grid_.alloc(G_ * sizeof(T));
         scratch_grid_ = (node4<T>*)scene_arena_grid_.alloc(G_ * sizeof(node4<T>));
-        if (kWarp) gmass_ = (double*)scene_arena_grid_.alloc(G_ * sizeof(double));
     }
 
     void alloc_particles(int n) {
@@ -944,10 +943,8 @@ template <class T> class Engine : public EngineBase {
             a.dfc = (const float*)layers_[l].dfc;
             a.G = (float*)Gd;
             a.grid = (node4<float>*)g;
-            a.gmass = gmass_;
             a.P = ctx_->prm.keep_intermediates ? (float*)layers_[l].dbgP : nullptr;
             DMPM_CK(cudaMemsetAsync(g, 0, G_ * sizeof(node4<T>), ctx_->stream));
-            DMPM_CK(cudaMemsetAsync(gmass_, 0, G_ * sizeof(double), ctx_->stream));
             const unsigned ws = warp_blocks(DMPM_SCATTER_CTAS);
             const int ush = set_units(a, ep);
             pbeg(K_P_OP1);
@@ -960,8 +957,7 @@ template <class T> class Engine : public EngineBase {
             launched();
             pend();
             pbeg(K_GOP);
-            k_gop_inplace<<<ggrid(), 256, 0, ctx_->stream>>>((node4<float>*)g, gmass_, G_, a.dt, a.fext[0], a.fext[1],
-                                                             a.fext[2]);
+            k_gop_inplace<<<ggrid(), 256, 0, ctx_->stream>>>((node4<float>*)g, G_, a.dt, a.fext[0], a.fext[1], a.fext[2]);
             launched();
             pend();
             pbeg(K_G2P);
@@ -1642,7 +1638,6 @@ template <class T> class Engine : public EngineBase {
     T* target_ = nullptr;
     T* dldm_ = nullptr;
     node4<T>* scratch_grid_ = nullptr;
-    double* gmass_ = nullptr;  // FP32 path: FP64 node masses of the P2G in progress
     double* staging_ = nullptr;
     size_t staging_count_ = 0;
     unsigned* status_ = nullptr;

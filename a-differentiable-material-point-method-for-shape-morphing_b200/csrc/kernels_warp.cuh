@@ -326,8 +326,7 @@ struct WArgs {
     const float* cst;      // constants
     const float* dfc;      // dFc of layer n
     float* G;              // [24][npl] per layer: G (9), polar R (9), polar S (6: s00 s01 s02 s11 s12 s22)
-    node4<float>* grid;    // layer n grid: (p, 0) after P2G, (v, m) after k_gop_inplace
-    double* gmass;         // node masses of the P2G in progress, in FP64 (scratch, one grid)
+    node4<float>* grid;    // layer n grid: (p, m) after P2G, (v, m) after k_gop_inplace
     float* P;              // debug: stress of layer n (or null)
     unsigned* status;
     // adjoint
@@ -493,49 +492,31 @@ template <bool GENERAL, int MODE> __global__ void __launch_bounds__(256, DMPM_SC
             if (uniform) {
                 reduce_scatter8<32>(v);
                 const int j = 2 * half + P.jp, k = P.kp;
-                if (((N.mask >> (4 * j + k)) & 1u) && (v[0] != 0.f || v[1] != 0.f || v[2] != 0.f || v[3] != 0.f)) {
-                    red_add4(a.grid + (N.g00 + j * N.sj + k), v[0], v[1], v[2], 0.f);
-                    atomicAdd(a.gmass + (N.g00 + j * N.sj + k), (double)v[3]);
-                }
+                if (((N.mask >> (4 * j + k)) & 1u) && (v[0] != 0.f || v[1] != 0.f || v[2] != 0.f || v[3] != 0.f))
+                    red_add4(a.grid + (N.g00 + j * N.sj + k), v[0], v[1], v[2], v[3]);
             } else if (L.valid) {
 #pragma unroll
                 for (int nd = 0; nd < 8; nd++) {
                     const int j = 2 * half + ((nd >> 2) ^ P.jp), k = (nd & 3) ^ P.kp;
-                    if ((N.mask >> (4 * j + k)) & 1u) {
-                        red_add4(a.grid + (N.g00 + j * N.sj + k), v[nd * 4], v[nd * 4 + 1], v[nd * 4 + 2], 0.f);
-                        atomicAdd(a.gmass + (N.g00 + j * N.sj + k), (double)v[nd * 4 + 3]);
-                    }
+                    if ((N.mask >> (4 * j + k)) & 1u)
+                        red_add4(a.grid + (N.g00 + j * N.sj + k), v[nd * 4], v[nd * 4 + 1], v[nd * 4 + 2], v[nd * 4 + 3]);
                 }
             }
         }
     }
 }
 
-// G_op in place: (p, 0) -> (v, m), v = p/m + dt f where |m| > FLT_EPSILON, else 0.
-// The node mass comes from gmass, where P2G adds each warp item's partial sum --
-// formed in a fixed order from the item's particles -- in FP64, so the sum does
-// not depend on the order of the atomic additions and neither does the
-// occupancy test (a node whose mass lies within float rounding of the
-// threshold would otherwise flip between runs).  The stored float mass keeps
-// the decision: an occupied node whose mass rounds to FLT_EPSILON or below
-// stores the next float above it, so the adjoint's test on the stored mass
-// (k_adj_gop_w) agrees.
-static __global__ void k_gop_inplace(node4<float>* grid, const double* __restrict__ gmass, size_t G, float dt,
-                                     float f0, float f1, float f2) {
+// G_op in place: (p, m) -> (v, m), v = p/m + dt f where |m| > FLT_EPSILON, else 0
+static __global__ void k_gop_inplace(node4<float>* grid, size_t G, float dt, float f0, float f1, float f2) {
     const size_t g = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (g >= G) return;
     node4<float> nd = grid[g];
-    const double m = gmass[g];
-    float mw = (float)m;
-    if (fabs(m) > kFltEps) {
-        nd.x = (float)((double)nd.x / m) + dt * f0;
-        nd.y = (float)((double)nd.y / m) + dt * f1;
-        nd.z = (float)((double)nd.z / m) + dt * f2;
-        if (!(fabsf(mw) > (float)kFltEps)) mw = copysignf(nextafterf((float)kFltEps, 1.f), mw);
-    } else {
-        nd.x = nd.y = nd.z = 0.f;
-    }
-    nd.w = mw;
+    const float f[3] = {f0, f1, f2};
+    float v[3];
+    node_velocity(nd, dt, f, v);
+    nd.x = v[0];
+    nd.y = v[1];
+    nd.z = v[2];
     grid[g] = nd;
 }
 

@@ -280,32 +280,6 @@ def test_fp32_mixed_matches_fp64_oracle(gpu_ready, exact_case):
         assert normrel(c.get(0, "dLdx"), o.get(0, "dLdx")) < 1e-3
 
 
-def test_fp32_node_masses_do_not_depend_on_summation_order(gpu_ready):
-    """The FP32-mixed path adds node masses in FP64 (each warp item's partial sum
-    in a fixed order), so two runs of the same rollout -- whose float atomics
-    land in different orders -- get the same masses, and the grid update's
-    occupancy test (|m| > FLT_EPSILON, ForwardSimulation.cpp:55) takes the same
-    branch at every node of every layer.  With float mass sums a node within
-    rounding of the threshold can flip between runs."""
-    sc = scenes.small_scene(seed=41, res=24, radius=0.25, steps=24, v_std=30.0, drag=0.1, smoothing=0.05,
-                            f_ext=(0.0, -2.0, 0.0), dt=2e-4)
-    sc.v[:, 0] += 400.0
-    sc.vol = OracleGraph(sc, "f64").calc_volumes()
-    L = 25
-    runs = []
-    for _ in range(2):
-        with make_ctx(sc, "fp32", np.zeros(int(np.prod(sc.dims))), adjoint="exact", eager=True) as c:
-            c.setup(L)
-            c.forward(0)
-            runs.append([c.get_grid(lay, "grid_m").astype(np.float32) for lay in range(L - 1)])
-    eps = np.float32(1.1920929e-07)
-    for lay, (a, b) in enumerate(zip(*runs)):
-        assert np.array_equal(np.abs(a) > eps, np.abs(b) > eps), lay
-        # FP64 sums of the same partials differ at most in their last bits, which
-        # the rounding to float almost always removes
-        assert np.max(np.abs(a - b)) <= 2 * np.finfo(np.float32).eps * np.max(np.abs(a)), lay
-
-
 def test_particles_at_and_outside_the_grid_boundary(gpu_ready):
     """A cloud straddling the grid's low corner, some particles up to 1.3 cells
     outside it, moving outward: stencil nodes outside the grid are skipped, as the
