@@ -35,12 +35,6 @@ using namespace dmpm_host;
 
 namespace {
 
-// the adjoint gather reads the brick units' shared tiles when the cell sort made
-// units (brick_cells != 0); 0 keeps the per-item staged gather everywhere
-#ifndef DMPM_GATHER_UNITS
-#define DMPM_GATHER_UNITS 1
-#endif
-
 constexpr int kDefaultBlock = 256;
 constexpr int kDefaultTileCap = 1024;
 
@@ -249,7 +243,6 @@ template <class T> class Engine : public EngineBase {
         // warp-item kernels serve this epoch
         uint32_t* units = nullptr;
         uint32_t* unit_keys = nullptr;
-        uint32_t* unit_items = nullptr;  // first warp item of each unit (n_units + 1 entries)
         uint32_t* n_units = nullptr;
         int unit_shift = -1;
         bool valid = false;
@@ -433,7 +426,6 @@ template <class T> class Engine : public EngineBase {
     int set_units(WArgs& a, const Epoch& ep) const {
         a.unit_start = ep.units;
         a.unit_key = ep.unit_keys;
-        a.unit_item = ep.unit_items;
         a.n_units_dev = ep.n_units;
         return ep.units ? ep.unit_shift : -1;
     }
@@ -789,7 +781,6 @@ template <class T> class Engine : public EngineBase {
             if (ctx_->prm.brick_cells) {
                 e.units = (uint32_t*)layer_arena_.alloc(((size_t)n_ + 1) * sizeof(uint32_t));
                 e.unit_keys = (uint32_t*)layer_arena_.alloc((size_t)n_ * sizeof(uint32_t));
-                e.unit_items = (uint32_t*)layer_arena_.alloc(((size_t)n_ + 1) * sizeof(uint32_t));
                 e.n_units = (uint32_t*)layer_arena_.alloc(16);
             }
         }
@@ -858,15 +849,12 @@ template <class T> class Engine : public EngineBase {
         e.unit_shift = -1;
         if (ctx_->prm.brick_cells && e.units) {
             const int shift = ctx_->prm.brick_cells == 4 ? 6 : 3;
-            // sf_ still holds each position's item index (the scan above); the unit
-            // flags and their scan go into sh_, free since the item starts were written
-            k_unit_flags<<<(n + 255) / 256, 256, 0, ctx_->stream>>>(sk_[cur], n, shift, sh_);
+            k_unit_flags<<<(n + 255) / 256, 256, 0, ctx_->stream>>>(sk_[cur], n, shift, sf_);
             launched();
-            device_scan<OpSum>(sh_, (size_t)n, e.n_units);
-            k_unit_starts<<<(n + 255) / 256, 256, 0, ctx_->stream>>>(sk_[cur], sh_, sf_, n, shift, e.units,
-                                                                     e.unit_keys, e.unit_items);
+            device_scan<OpSum>(sf_, (size_t)n, e.n_units);
+            k_unit_starts<<<(n + 255) / 256, 256, 0, ctx_->stream>>>(sk_[cur], sf_, n, shift, e.units, e.unit_keys);
             launched();
-            k_unit_sentinel<<<1, 1, 0, ctx_->stream>>>(e.units, e.unit_items, e.n_units, e.n_items, n);
+            k_item_sentinel<<<1, 1, 0, ctx_->stream>>>(e.units, e.n_units, n);
             launched();
             e.unit_shift = shift;
         }
@@ -1196,13 +1184,7 @@ template <class T> class Engine : public EngineBase {
                                           sizeof(node4<T>), G_, cudaMemcpyDeviceToDevice, ctx_->stream));
             }
             pbeg(K_ADJ_GATHER);
-            if (DMPM_GATHER_UNITS && ush == 3) {
-                if (ex) k_adj_gather_u<true, 2><<<wg, 256, 0, ctx_->stream>>>(a);
-                else k_adj_gather_u<false, 2><<<wg, 256, 0, ctx_->stream>>>(a);
-            } else if (DMPM_GATHER_UNITS && ush == 6) {
-                if (ex) k_adj_gather_u<true, 4><<<wg, 256, 0, ctx_->stream>>>(a);
-                else k_adj_gather_u<false, 4><<<wg, 256, 0, ctx_->stream>>>(a);
-            } else if (ex) {
+            if (ex) {
                 k_adj_gather_w<true, ITEMS_PERSISTENT><<<wg, 256, 0, ctx_->stream>>>(a);
             } else {
                 k_adj_gather_w<false, ITEMS_PERSISTENT><<<wg, 256, 0, ctx_->stream>>>(a);

@@ -10,16 +10,13 @@
 // all 64 stencil nodes of it, reading the tile (the particles of a warp share a
 // cell most of the time, so the reads are broadcasts).  On the 64^3,
 // 267k-particle workload this takes 36.7 us per step against 48.1 us for the
-// warp-item G2P; at 8 particles per cell, 21.5 against 22.2 us.
-// The adjoint P2G gather keeps the warp items' arithmetic (8 particles x 4
-// stencil slabs per warp, kernels_warp.cuh) but reads a unit tile: a CTA stages
-// the unit's node pairs once and its warps process the unit's items from it.
-// One thread per particle measured slower for the gather (95-115 against
-// 79 us: its 18 sums per particle need 128-170 registers per thread, so few
-// warps reside), and P2G and the adjoint scatter adding into shared tiles with
+// warp-item G2P; at 8 particles per cell, 21.5 against 22.2 us.  The other
+// stencil kernels stay warp-item kernels (kernels_warp.cuh), which measured
+// faster: the adjoint gather over brick tiles took 95-115 us against 79 us
+// (its 18 sums per particle need 128-170 registers per thread, so few warps
+// reside), and P2G and the adjoint scatter adding into shared tiles with
 // shared-memory atomics took 3-4x longer than the warp's butterfly reduction
-// followed by one vector red.global.add per node, so the scatters stay
-// warp-item kernels.
+// followed by one vector red.global.add per node.
 // A particle that has left the unit since the sort (the sort runs every few
 // steps) is handled by the same code with its nodes read from global memory.
 //
@@ -243,52 +240,5 @@ __global__ void __launch_bounds__(DMPM_BRICK_THREADS, DMPM_BRICK_G2P_MINB) k_g2p
         }
     }
 }
-
-// ------------------------------------------------------------------ adjoint P2G gather over units
-// The unit tile: the CTA's current unit (an octant of 2^3 cells, B = 2, or a
-// brick of 4^3 cells, B = 4) has its (B + 3)^3 node pairs in shared memory; a
-// warp whose lanes share a stencil base inside the unit reads them there.  Four
-// slab lanes read nodes (B + 3)^2 records apart, which fall into different
-// banks for both B.
-template <int B> struct UnitTile {
-    static constexpr int E = B + 3;
-    const node4<float>* tile;  // 2 records per node, node (i, j, k) at (i E + j) E + k
-    const int* o;              // node of tile entry (0, 0, 0), in shared memory
-    int off;                   // the warp's stencil base as a tile node index
-    __device__ __forceinline__ bool prepare(const WArgs&, const GridGeom&, int, const int base[3]) {
-        if (!warp_uniform_base(base)) return false;
-        const int l0 = base[0] - o[0], l1 = base[1] - o[1], l2 = base[2] - o[2];
-        off = (l0 * E + l1) * E + l2;
-        return (unsigned)l0 < (unsigned)B && (unsigned)l1 < (unsigned)B && (unsigned)l2 < (unsigned)B;
-    }
-    __device__ __forceinline__ node4<float> rec(int s, int j, int k, int r) const {
-        return tile[2 * (off + (s * E + j) * E + k) + r];
-    }
-};
-
-// The gather over units: a persistent CTA takes a unit, stages the unit's node
-// pairs once (stage_tile) and its warps take the unit's warp items, so an item
-// of a uniform warp reads shared memory only, where k_adj_gather_w stages 64
-// node pairs per item.
-template <bool EXACT, int B> __global__ void __launch_bounds__(256, DMPM_GATHER_MIN_BLOCKS) k_adj_gather_u(WArgs a) {
-    using S = BrickShape<B>;
-    __shared__ node4<float> tile[2 * S::NT];
-    __shared__ int s_o[3];
-    UnitTile<B> src{tile, s_o, 0};
-    const int nun = (int)*a.n_units_dev;
-    const int warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
-    for (int u = blockIdx.x; u < nun; u += gridDim.x) {
-        int o[3];
-        unit_origin(a.unit_key[u], S::shift, a.geo, o);
-        __syncthreads();  // the previous unit's readers are done with the tile
-        if (threadIdx.x < 3) s_o[threadIdx.x] = o[threadIdx.x];
-        stage_tile<B, 2>(a.gadj2, a.geo, 0, o, tile);
-        __syncthreads();
-        const int i1 = (int)a.unit_item[u + 1];
-        for (int item = (int)a.unit_item[u] + warp; item < i1; item += nwarps)
-            gather_item<EXACT, ITEMS_PERSISTENT>(a, item, src);
-    }
-}
-
 
 }  // namespace dmpm

@@ -346,7 +346,6 @@ struct WArgs {
     // equal to unit_key[u]; the unit count stays on the device
     const uint32_t* unit_start;
     const uint32_t* unit_key;
-    const uint32_t* unit_item;    // first warp item of each unit (n_units + 1 entries)
     const uint32_t* n_units_dev;
 };
 
@@ -761,17 +760,10 @@ __global__ void k_adj_gop_w(const node4<float>* __restrict__ grid, const node4<f
 //   M += w d dLdp^T,  X += sigma (N'NN, NN'N, NNN'),  u += w dLdp,  z += w v_g
 //   sigma = m dLdm + dLdp.(m v c_d + G d) + v_g.(dLdv_next + 3/dx^2 dLdC_next d)
 // (the algebra of kernels.cuh:k_adj_gather); written to gath for k_adj_finalize.
-//
-// The item body reads the 64 stencil node pairs of a warp whose lanes share one
-// stencil base from a shared-memory source Src (the per-warp staged stencil of
-// k_adj_gather_w, or the CTA's unit tile of k_adj_gather_u):
-//   bool Src::prepare(a, geo, goff, base)  -- every lane calls it; true when the
-//        warp's stencil is in shared memory (it may stage it first);
-//   node4 Src::rec(s, j, k, r)             -- record r of stencil node (s, j, k).
-// Other warps read their nodes from global memory lane by lane.
-template <bool EXACT, int MODE, class Src>
-__device__ __forceinline__ void gather_item(const WArgs& a, int item, Src& src) {
-        const size_t np = a.np, npl = a.npl;
+template <bool EXACT, int MODE> __global__ void __launch_bounds__(256, DMPM_GATHER_MIN_BLOCKS) k_adj_gather_w(WArgs a) {
+    const int nit = item_count(a);
+    const size_t np = a.np, npl = a.npl;
+    for (int item = first_warp(); item < nit; item = next_item<MODE>(item, nit)) {
         GridGeom geo;
         int goff;
         item_grid<MODE>(a, item, geo, goff);
@@ -840,13 +832,19 @@ __device__ __forceinline__ void gather_item(const WArgs& a, int item, Src& src) 
             S = 0.f;
             T = 0.f;
         };
-        if (src.prepare(a, geo, goff, base)) {
+        if (DMPM_STAGE_NODES && warp_uniform_base(base)) {
+            __shared__ node4<float> s_rec[8][StageRecords<2>::value];
+            node4<float>* sw = s_rec[threadIdx.x >> 5];
+            stage_stencil<2>(a.gadj2, geo, goff, base, sw);
 #pragma unroll
             for (int j = 0; j < 4; j++) {
                 float d1, n1, s1;
                 row_weights(own1, j, d1, n1, s1);
 #pragma unroll
-                for (int k = 0; k < 4; k++) node(src.rec(L.s, j, k, 0), src.rec(L.s, j, k, 1), d1, n1, k);
+                for (int k = 0; k < 4; k++) {
+                    const int n = 16 * L.s + 4 * j + k;
+                    node(sw[stage_index<2>(n, 0)], sw[stage_index<2>(n, 1)], d1, n1, k);
+                }
                 end_row(n1, s1);
             }
         } else {
@@ -871,7 +869,7 @@ __device__ __forceinline__ void gather_item(const WArgs& a, int item, Src& src) 
 #pragma unroll
         for (int c = 0; c < 3; c++) acc[c] = w.d0 * acc[12 + c];
         reduce_slabs<18>(acc);
-        if (!L.valid) return;
+        if (!L.valid) continue;
         if (L.s == 0) {
 #pragma unroll
             for (int i = 0; i < 9; i++) a.gath[(size_t)i * np + p] = acc[i];
@@ -879,27 +877,7 @@ __device__ __forceinline__ void gather_item(const WArgs& a, int item, Src& src) 
 #pragma unroll
             for (int i = 9; i < 18; i++) a.gath[(size_t)i * np + p] = acc[i];
         }
-}
-
-// Per-warp staging: a warp whose 32 lanes share one stencil base copies its 64
-// node pairs into its own shared-memory slice (stage_stencil).
-struct WarpStage {
-    node4<float>* sw;  // this warp's slice, StageRecords<2>::value records
-    __device__ __forceinline__ bool prepare(const WArgs& a, const GridGeom& geo, int goff, const int base[3]) {
-        if (!DMPM_STAGE_NODES || !warp_uniform_base(base)) return false;
-        stage_stencil<2>(a.gadj2, geo, goff, base, sw);
-        return true;
     }
-    __device__ __forceinline__ node4<float> rec(int s, int j, int k, int r) const {
-        return sw[stage_index<2>(16 * s + 4 * j + k, r)];
-    }
-};
-
-template <bool EXACT, int MODE> __global__ void __launch_bounds__(256, DMPM_GATHER_MIN_BLOCKS) k_adj_gather_w(WArgs a) {
-    __shared__ node4<float> s_rec[8][StageRecords<2>::value];
-    WarpStage src{s_rec[threadIdx.x >> 5]};
-    const int nit = item_count(a);
-    for (int item = first_warp(); item < nit; item = next_item<MODE>(item, nit)) gather_item<EXACT, MODE>(a, item, src);
 }
 
 // ------------------------------------------------------------------ finalize

@@ -286,9 +286,7 @@ static __global__ void k_item_sentinel(uint32_t* item_start, const uint32_t* n_i
 // A unit is a run of sorted particles with equal key >> shift: the particles of
 // one brick (shift 6) or one brick octant (shift 3).  flags[i] = 1 where a unit
 // starts; after an exclusive sum scan of flags into idx, k_unit_starts writes
-// each unit's first sorted position, its key >> shift and its first warp item
-// (a unit starts where a cell does, so its first position starts an item;
-// item_idx is the exclusive scan of the item flags).
+// each unit's first sorted position and its key >> shift.
 __device__ __forceinline__ bool unit_head(const uint32_t* keys, int i, int shift) {
     return i == 0 || (keys[i] >> shift) != (keys[i - 1] >> shift);
 }
@@ -296,20 +294,12 @@ static __global__ void k_unit_flags(const uint32_t* __restrict__ keys, int n, in
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i < n) flags[i] = unit_head(keys, i, shift) ? 1u : 0u;
 }
-static __global__ void k_unit_starts(const uint32_t* __restrict__ keys, const uint32_t* __restrict__ idx,
-                                     const uint32_t* __restrict__ item_idx, int n, int shift, uint32_t* unit_start,
-                                     uint32_t* unit_key, uint32_t* unit_item) {
+static __global__ void k_unit_starts(const uint32_t* __restrict__ keys, const uint32_t* __restrict__ idx, int n,
+                                     int shift, uint32_t* unit_start, uint32_t* unit_key) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n || !unit_head(keys, i, shift)) return;
     unit_start[idx[i]] = (uint32_t)i;
     unit_key[idx[i]] = keys[i] >> shift;
-    unit_item[idx[i]] = item_idx[i];
-}
-// one past the last unit: its first position is n, its first item n_items
-static __global__ void k_unit_sentinel(uint32_t* unit_start, uint32_t* unit_item, const uint32_t* n_units,
-                                       const uint32_t* n_items, int n) {
-    unit_start[*n_units] = (uint32_t)n;
-    unit_item[*n_units] = *n_items;
 }
 
 }  // namespace dmpm
