@@ -14,7 +14,10 @@
 // stencil kernels stay warp-item kernels (kernels_warp.cuh), which measured
 // faster: the adjoint gather over brick tiles took 95-115 us against 79 us
 // (its 18 sums per particle need 128-170 registers per thread, so few warps
-// reside), and P2G and the adjoint scatter adding into shared tiles with
+// reside) -- and so did the warp-item gather reading a per-CTA octant tile
+// instead of staging each item's stencil (101 against 79.5 us: the CTA-wide
+// barriers around each octant's staging idle its warps) -- and P2G and the
+// adjoint scatter adding into shared tiles with
 // shared-memory atomics took 3-4x longer than the warp's butterfly reduction
 // followed by one vector red.global.add per node.
 // A particle that has left the unit since the sort (the sort runs every few

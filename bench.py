@@ -626,7 +626,7 @@ def run_fd(args):
         a64 = [float(np.sum(grads["fp64"] * d)) for d in dirs]
         a32 = [float(np.sum(grads["fp32"] * d)) for d in dirs]
         per_h = {}
-        for hi, h in enumerate(hs):
+        for h in hs:
             fds, crossings = [], []
             for d in dirs:
                 lp = []
@@ -635,14 +635,13 @@ def run_fd(args):
                     c64.set_layer(0, "dFc", base + sgn * h * d)
                     c64.forward(0)
                     lp.append(c64.loss())
-                    if hi == 0 and loss == "ref":
-                        # node-mass threshold crossings between the two rollouts: nodes
-                        # (over all layers) occupied, |m| > FLT_EPSILON, in one and not the other
-                        masks = [np.abs(c64.get_grid(lay, "grid_m")) > FLT_EPSILON for lay in range(sc.steps + 1)]
-                        if occ is None:
-                            occ = masks
-                        else:
-                            crossings.append(int(sum(int(np.count_nonzero(a != b)) for a, b in zip(occ, masks))))
+                    # node-mass threshold crossings between the two rollouts: nodes
+                    # (over all layers) occupied, |m| > FLT_EPSILON, in one and not the other
+                    masks = [np.abs(c64.get_grid(lay, "grid_m")) > FLT_EPSILON for lay in range(sc.steps + 1)]
+                    if occ is None:
+                        occ = masks
+                    else:
+                        crossings.append(int(sum(int(np.count_nonzero(a != b)) for a, b in zip(occ, masks))))
                 fds.append((lp[0] - lp[1]) / (2 * h))
             e64 = [abs(a - f) / abs(f) for a, f in zip(a64, fds)]
             e32 = [abs(a - f) / abs(f) for a, f in zip(a32, fds)]
@@ -1086,7 +1085,7 @@ def main():
                     help="config 4: wrap each Adam step in the reference optimiser's line search")
     ap.add_argument("--fd", action="store_true", help="config 1: adjoint vs central differences, 16 directions")
     ap.add_argument("--instances", type=int, default=48, help="config 3: number of batched instances")
-    ap.add_argument("--fd-h", default="1e-3,1e-4,1e-5,1e-6", help="--fd: central-difference steps")
+    ap.add_argument("--fd-h", default="1e-3,1e-4,1e-5,1e-6,1e-7", help="--fd: central-difference steps")
     ap.add_argument("--next-rows", action="store_true",
                     help="time the mesh sampler and the surfacing against the reference's own code")
     args = ap.parse_args()
