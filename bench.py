@@ -178,6 +178,8 @@ def build_scene(instance: int, ppc_root: int):
 # G2P kernel of the FP32 path: None = the library default (bricks of 2^3 cells), 0 = warp
 # items, 2 or 4 = bricks of that many cells per axis
 BRICK_CELLS = None
+# cell-sort interval of the FP32 path (None = the library default, 8 steps)
+SORT_EVERY = None
 
 
 def setup_ctx(dmpm, sc, prec, device, vol, target, dt, checkpoint_every, control="tied", control_stride=0,
@@ -197,7 +199,7 @@ def setup_ctx(dmpm, sc, prec, device, vol, target, dt, checkpoint_every, control
     c.set_target_mass(target)
     c.set_params(dt=dt, drag=sc.drag, f_ext=sc.f_ext, smoothing=sc.smoothing, adjoint="exact", control=control,
                  loss="ref", checkpoint_every=checkpoint_every, control_stride=control_stride,
-                 brick_cells=BRICK_CELLS if prec == "fp32" else None)
+                 brick_cells=BRICK_CELLS if prec == "fp32" else None, sort_every=SORT_EVERY or 0)
     c.setup(sc.steps + 1)
     return c
 
@@ -1074,6 +1076,7 @@ def main():
     ap.add_argument("--checkpoint-every", type=int, default=1)
     ap.add_argument("--brick", type=int, default=None, choices=[0, 2, 4],
                     help="FP32 G2P kernel: 0 warp items, 2 or 4 cells per brick axis (default 2)")
+    ap.add_argument("--sort-every", type=int, default=None, help="FP32 cell-sort interval in steps (default 8)")
     ap.add_argument("--rollout-steps", type=int, default=0, help="override the 200 time steps (profiling runs)")
     ap.add_argument("--no-fp64", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
@@ -1091,9 +1094,10 @@ def main():
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
-    global BRICK_CELLS
+    global BRICK_CELLS, SORT_EVERY
     if args.brick is not None:
         BRICK_CELLS = args.brick
+    SORT_EVERY = args.sort_every
     if args.impl == "reference":
         return run_reference(args)
     if args.fd:
