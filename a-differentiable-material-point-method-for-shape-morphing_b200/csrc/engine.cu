@@ -427,8 +427,12 @@ template <class T> class Engine : public EngineBase {
         a.unit_start = ep.units;
         a.unit_key = ep.unit_keys;
         a.n_units_dev = ep.n_units;
-        return ep.units ? ep.unit_shift : -1;
+        return unit_shift_of(ep);
     }
+    static int unit_shift_of(const Epoch& ep) { return ep.units ? ep.unit_shift : -1; }
+    // A layer grid of the FP32 path holds (p, m) where its step ran the brick G2P
+    // (which applies G_op to the nodes as it reads them), else (v, m) from k_gop_inplace.
+    static bool grid_keeps_p(int ush) { return ush == 3 || ush == 6; }
     // persistent grid of a brick kernel: as many CTAs as can be resident at once
     // (its register and shared-memory budget), looked up once per kernel
     template <class K> unsigned brick_blocks(K kernel) {
@@ -944,10 +948,13 @@ template <class T> class Engine : public EngineBase {
             else k_p2g_w<false, ITEMS_PERSISTENT><<<ws, 256, 0, ctx_->stream>>>(a);
             launched();
             pend();
-            pbeg(K_GOP);
-            k_gop_inplace<<<ggrid(), 256, 0, ctx_->stream>>>((node4<float>*)g, G_, a.dt, a.fext[0], a.fext[1], a.fext[2]);
-            launched();
-            pend();
+            if (ush != 3 && ush != 6) {  // the brick G2P applies G_op to the nodes it reads
+                pbeg(K_GOP);
+                k_gop_inplace<<<ggrid(), 256, 0, ctx_->stream>>>((node4<float>*)g, G_, a.dt, a.fext[0], a.fext[1],
+                                                                 a.fext[2]);
+                launched();
+                pend();
+            }
             pbeg(K_G2P);
             if (ush == 3) k_g2p_b<2><<<brick_blocks(k_g2p_b<2>), DMPM_BRICK_THREADS, 0, ctx_->stream>>>(a);
             else if (ush == 6) k_g2p_b<4><<<brick_blocks(k_g2p_b<4>), DMPM_BRICK_THREADS, 0, ctx_->stream>>>(a);
@@ -1174,8 +1181,12 @@ template <class T> class Engine : public EngineBase {
             launched();
             pend();
             pbeg(K_ADJ_GOP);
-            if (ex) k_adj_gop_w<true><<<ggrid(), 256, 0, ctx_->stream>>>(a.grid, a.gadj, a.gadj2, G_, a.dt, a.fext[0], a.fext[1], a.fext[2]);
-            else k_adj_gop_w<false><<<ggrid(), 256, 0, ctx_->stream>>>(a.grid, a.gadj, a.gadj2, G_, a.dt, a.fext[0], a.fext[1], a.fext[2]);
+            const bool sp = grid_keeps_p(ush);
+            const float f0 = a.fext[0], f1 = a.fext[1], f2 = a.fext[2];
+            if (ex && sp) k_adj_gop_w<true, true><<<ggrid(), 256, 0, ctx_->stream>>>(a.grid, a.gadj, a.gadj2, G_, a.dt, f0, f1, f2);
+            else if (ex) k_adj_gop_w<true, false><<<ggrid(), 256, 0, ctx_->stream>>>(a.grid, a.gadj, a.gadj2, G_, a.dt, f0, f1, f2);
+            else if (sp) k_adj_gop_w<false, true><<<ggrid(), 256, 0, ctx_->stream>>>(a.grid, a.gadj, a.gadj2, G_, a.dt, f0, f1, f2);
+            else k_adj_gop_w<false, false><<<ggrid(), 256, 0, ctx_->stream>>>(a.grid, a.gadj, a.gadj2, G_, a.dt, f0, f1, f2);
             launched();
             pend();
             if (P.keep_intermediates) {
@@ -1500,7 +1511,13 @@ template <class T> class Engine : public EngineBase {
                 }
             }
             double* s = staging(3 * G_);
-            const int stored_v = (kWarp && l < L_ - 1) ? 1 : 0;  // the FP32 grid update wrote v over p
+            // the FP32 warp-item step's grid update wrote v over p; the brick G2P's did not
+            int stored_v = 0;
+            if constexpr (kWarp) {
+                if (l < L_ - 1)
+                    stored_v = grid_keeps_p(unit_shift_of(epochs_[std::min((int)epochs_.size() - 1, l / sort_every())]))
+                                   ? 0 : 1;
+            }
             k_grid_field<T><<<ggrid(), 256, 0, ctx_->stream>>>(g, G_, field, stored_v, P.dt, P.f_ext[0], P.f_ext[1],
                                                               P.f_ext[2], s);
             launched();

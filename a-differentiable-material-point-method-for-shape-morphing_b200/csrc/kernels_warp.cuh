@@ -326,7 +326,7 @@ struct WArgs {
     const float* cst;      // constants
     const float* dfc;      // dFc of layer n
     float* G;              // [24][npl] per layer: G (9), polar R (9), polar S (6: s00 s01 s02 s11 s12 s22)
-    node4<float>* grid;    // layer n grid: (p, m) after P2G, (v, m) after k_gop_inplace
+    node4<float>* grid;    // layer n grid: (p, m) after P2G, (v, m) after k_gop_inplace (not run before the brick G2P)
     float* P;              // debug: stress of layer n (or null)
     unsigned* status;
     // adjoint
@@ -733,20 +733,37 @@ template <bool EXACT, bool GENERAL, int MODE> __global__ void __launch_bounds__(
     }
 }
 
-// adjoint G_op per node: (dLdp, dLdm) from dLdv and the layer's (v, m)
-// The record pair (dLdp, dLdm), (v, m) of a node is stored contiguously (32 B)
-// so the gather reads one sector per node.
-template <bool EXACT>
+// adjoint G_op per node: (dLdp, dLdm) from dLdv and the layer's grid, which
+// holds (v, m) after k_gop_inplace or, where G2P applied G_op as it read the
+// nodes (STORED_P), still (p, m).  The record pair (dLdp, dLdm), (v, m) of a
+// node is stored contiguously (32 B) so the gather reads one sector per node.
+template <bool EXACT, bool STORED_P>
 __global__ void k_adj_gop_w(const node4<float>* __restrict__ grid, const node4<float>* __restrict__ gadj,
                             node4<float>* gadj2, size_t G, float dt, float f0, float f1, float f2) {
     const size_t g = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (g >= G) return;
-    const node4<float> nd = grid[g];
+    node4<float> nd = grid[g];
     const node4<float> dv = gadj[g];
     node4<float> o{0.f, 0.f, 0.f, 0.f};
+    const float f[3] = {f0, f1, f2};
+    float pm[3];  // p / m: the velocity the loss sees through m (v - dt f for the exact adjoint)
+    if (STORED_P) {
+        const bool occ = fabsf(nd.w) > (float)kFltEps;
+        pm[0] = occ ? nd.x / nd.w : 0.f;
+        pm[1] = occ ? nd.y / nd.w : 0.f;
+        pm[2] = occ ? nd.z / nd.w : 0.f;
+        float v[3];
+        node_velocity(nd, dt, f, v);
+        nd.x = v[0];
+        nd.y = v[1];
+        nd.z = v[2];
+    }
     if (fabsf(nd.w) > (float)kFltEps) {
         float v[3] = {nd.x, nd.y, nd.z};
-        if (EXACT) { v[0] -= dt * f0; v[1] -= dt * f1; v[2] -= dt * f2; }
+        if (EXACT) {
+            if (STORED_P) { v[0] = pm[0]; v[1] = pm[1]; v[2] = pm[2]; }
+            else { v[0] -= dt * f0; v[1] -= dt * f1; v[2] -= dt * f2; }
+        }
         o.x = dv.x / nd.w;
         o.y = dv.y / nd.w;
         o.z = dv.z / nd.w;

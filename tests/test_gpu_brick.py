@@ -90,6 +90,29 @@ def test_brick_kernels_match_warp_items(gpu_ready, case, brick):
         assert normrel(b[k], w[k]) < 1e-3, k
 
 
+@pytest.mark.parametrize("adjoint", ["exact", "refcompat"])
+@pytest.mark.parametrize("brick", BRICKS)
+def test_brick_grid_fields_and_adjoints_match_warp_items(gpu_ready, case, brick, adjoint):
+    """The brick G2P applies G_op to the nodes it reads, so its layer grids keep
+    (p, m) where the warp-item step's hold (v, m): dmpm_get_grid and the adjoint
+    G_op (both adjoint modes) read either form and give the same v, p and grid
+    adjoints."""
+    sc, o, loss, L = case
+    out = {}
+    for b in (0, brick):
+        with make_ctx(sc, "fp32", o.target, adjoint=adjoint, keep_intermediates=True, brick_cells=b) as c:
+            c.setup(L)
+            c.forward(0)
+            c.loss()
+            c.backward(0)
+            out[b] = {(lay, k): c.get_grid(lay, k) for lay in (0, L // 2, L - 2)
+                      for k in ("grid_m", "grid_v", "grid_p", "grid_dLdv", "grid_dLdp", "grid_dLdm")}
+            out[b]["dLdx"] = c.get(0, "dLdx")
+    for key, w in out[0].items():
+        adj = key == "dLdx" or key[1].startswith("grid_dLd")
+        assert normrel(out[brick][key], w) < (1e-3 if adj else 1e-4), key  # float summation orders differ
+
+
 @pytest.mark.parametrize("sort_every", [1, 100])
 @pytest.mark.parametrize("brick", BRICKS)
 def test_brick_kernels_with_particles_leaving_their_bricks(gpu_ready, fast_case, brick, sort_every):
