@@ -912,7 +912,7 @@ def run_config4(args):
     vol, target = _scene_inputs(dmpm, sc, 0)
     iters = args.iters
     out = {"mode": "config4", "particles": sc.n, "grid": list(sc.dims), "steps": sc.steps, "dt": sc.dt,
-           "dt_substituted_from": dt_sub, "checkpoint_every": 20, "iterations": iters, "lr": 1e-2}
+           "dt_substituted_from": dt_sub, "checkpoint_every": 20, "iterations": iters, "lr": args.lr}
     torch.cuda.synchronize()
     base = _mem_used_gb(torch, 0)
     frame = dict(control="per_layer", control_stride=sc.steps)  # layer 0 is the only control frame
@@ -929,7 +929,7 @@ def run_config4(args):
         c64.close()
         return float(np.linalg.norm(grad32 - g64) / np.linalg.norm(g64))
 
-    # Plain Adam (the configuration: 30 iterations at lr 1e-2), or with --line-search the
+    # Plain Adam (the configuration: 30 iterations at lr 1e-2; --lr changes it), or with --line-search the
     # reference optimiser's line search (CompGraph.cpp:388-420): step, re-run the forward pass,
     # keep the step if the loss fell, else step back (Descend_Adam with -alpha, which updates the
     # moments again, as the reference does) and halve alpha; a frame whose line search finds no
@@ -959,11 +959,11 @@ def run_config4(args):
                 relerrs[1] = fp64_relerr(last[1], last[2])
         t0 = time.perf_counter()
         if not args.line_search:
-            c.adam_step(t=it, lr=1e-2, layer=0)
+            c.adam_step(t=it, lr=args.lr, layer=0)
             c.synchronize()
             times.append(ms + 1000.0 * (time.perf_counter() - t0))
             continue
-        alpha, found = 1e-2, False
+        alpha, found = args.lr, False
         for ls in range(max_ls):
             c.adam_step(t=it, lr=alpha, layer=0)
             st = c.forward(0)
@@ -1084,6 +1084,7 @@ def main():
                     help="skip the checkpointed and 8-per-cell measurements of the headline line")
     ap.add_argument("--config", type=int, default=1, help="1 = headline workload; 0, 2, 3, 4 = extra measurements")
     ap.add_argument("--iters", type=int, default=30, help="config 4: Adam iterations")
+    ap.add_argument("--lr", type=float, default=1e-2, help="config 4: Adam learning rate (configured: 1e-2)")
     ap.add_argument("--line-search", action="store_true",
                     help="config 4: wrap each Adam step in the reference optimiser's line search")
     ap.add_argument("--fd", action="store_true", help="config 1: adjoint vs central differences, 16 directions")
