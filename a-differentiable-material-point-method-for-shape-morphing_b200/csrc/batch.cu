@@ -514,7 +514,7 @@ struct dmpm_batch::Impl {
         const int pb = particle_block();
         const unsigned wb = warp_blocks(t);
         DMPM_CK(cudaMemsetAsync(grid[t], 0, Gt * sizeof(node4<float>), b->stream));
-        k_stress<<<(unsigned)((a.n + pb - 1) / pb), pb, 0, b->stream>>>(a);
+        k_stress<false><<<(unsigned)((a.n + pb - 1) / pb), pb, 0, b->stream>>>(a);
         launched();
         k_p2g_w<false, ITEMS_BATCH><<<wb, 256, 0, b->stream>>>(a);
         launched();
@@ -570,8 +570,8 @@ struct dmpm_batch::Impl {
         else k_adj_scatter_w<false, false, ITEMS_BATCH><<<wb, 256, 0, b->stream>>>(a);
         launched();
         const unsigned gb = (unsigned)((Gt + 255) / 256);
-        if (ex) k_adj_gop_w<true, false><<<gb, 256, 0, b->stream>>>(grid[t], gadj, gadj2, Gt, a.dt, a.fext[0], a.fext[1], a.fext[2]);
-        else k_adj_gop_w<false, false><<<gb, 256, 0, b->stream>>>(grid[t], gadj, gadj2, Gt, a.dt, a.fext[0], a.fext[1], a.fext[2]);
+        if (ex) k_adj_gop_w<true><<<gb, 256, 0, b->stream>>>(grid[t], gadj, gadj2, Gt, a.dt, a.fext[0], a.fext[1], a.fext[2]);
+        else k_adj_gop_w<false><<<gb, 256, 0, b->stream>>>(grid[t], gadj, gadj2, Gt, a.dt, a.fext[0], a.fext[1], a.fext[2]);
         launched();
         if (ex) k_adj_gather_w<true, ITEMS_BATCH><<<wb, 256, 0, b->stream>>>(a);
         else k_adj_gather_w<false, ITEMS_BATCH><<<wb, 256, 0, b->stream>>>(a);

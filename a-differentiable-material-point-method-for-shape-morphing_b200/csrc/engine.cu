@@ -111,8 +111,9 @@ template <class T> __global__ void k_copy_node_mass(const node4<T>* __restrict__
     const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (i < G) dst[i] = g[i].w;
 }
-// sum of squares of 9 planes (Compute_dLdF_Norm), FP64
-template <class T> __global__ void k_sqnorm9(const T* __restrict__ a, size_t np, int n, double* out) {
+// sum of squares of 9 planes (Compute_dLdF_Norm), FP64: block partial sums into
+// part (summed in order by k_sum_partials)
+template <class T> __global__ void k_sqnorm9(const T* __restrict__ a, size_t np, int n, double* part) {
     __shared__ double s[32];
     const int p = blockIdx.x * blockDim.x + threadIdx.x;
     double v = 0.0;
@@ -124,7 +125,7 @@ template <class T> __global__ void k_sqnorm9(const T* __restrict__ a, size_t np,
     if (threadIdx.x < 32) {
         v = threadIdx.x < (blockDim.x >> 5) ? s[threadIdx.x] : 0.0;
         for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
-        if (threadIdx.x == 0) atomicAdd(out, v);
+        if (threadIdx.x == 0) part[blockIdx.x] = v;
     }
 }
 
@@ -189,7 +190,8 @@ __global__ void k_descend(int kind, T* dfc, const G* __restrict__ grad, T* mom, 
     }
     dfc[i] = (T)d;
 }
-template <class G> __global__ void k_sumsq(const G* __restrict__ a, size_t np, int n, double* out) {
+// sum of squares of a gradient's 9 planes: block partial sums into part
+template <class G> __global__ void k_sumsq(const G* __restrict__ a, size_t np, int n, double* part) {
     __shared__ double s[32];
     const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
     double v = 0.0;
@@ -200,7 +202,7 @@ template <class G> __global__ void k_sumsq(const G* __restrict__ a, size_t np, i
     if (threadIdx.x < 32) {
         v = threadIdx.x < (blockDim.x >> 5) ? s[threadIdx.x] : 0.0;
         for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
-        if (threadIdx.x == 0) atomicAdd(out, v);
+        if (threadIdx.x == 0) part[blockIdx.x] = v;
     }
 }
 
@@ -249,7 +251,7 @@ template <class T> class Engine : public EngineBase {
     };
 
     explicit Engine(dmpm_ctx* c) : ctx_(c) {
-        for (Arena* a : {&scene_arena_, &scene_arena_grid_, &layer_arena_, &staging_arena_, &misc_arena_})
+        for (Arena* a : {&scene_arena_, &scene_arena_grid_, &layer_arena_, &staging_arena_, &misc_arena_, &fix_arena_})
             a->set_budget(&ctx_->budget);
     }
 
@@ -407,6 +409,28 @@ template <class T> class Engine : public EngineBase {
     int block() const { return ctx_->prm.block_size > 0 ? ctx_->prm.block_size : kDefaultBlock; }
     int tile_cap() const { return ctx_->prm.tile_cap > 0 ? ctx_->prm.tile_cap : kDefaultTileCap; }
     unsigned pgrid() const { return (unsigned)((n_ + block() - 1) / block()); }
+    // deterministic mode of the FP32 path: order-independent node sums (fixpoint.cuh)
+    bool det() const { return kWarp && ctx_->prm.deterministic != 0; }
+    void ensure_fix() {
+        if (!det() || (fix_ && fix_G_ == G_)) return;
+        fix_arena_.release();
+        fix_ = nullptr;
+        fixb_ = nullptr;
+        fix_ = (fix4*)fix_arena_.alloc(G_ * sizeof(fix4));
+        fixb_ = (unsigned*)fix_arena_.alloc(FIXB_SLOTS * sizeof(unsigned));
+        fix_G_ = G_;
+    }
+    void clear_fix(int slot) {  // zero the integer sums and one bound slot (-1: all) before a pass
+        DMPM_CK(cudaMemsetAsync(fix_, 0, G_ * sizeof(fix4), ctx_->stream));
+        if (slot < 0) DMPM_CK(cudaMemsetAsync(fixb_, 0, FIXB_SLOTS * sizeof(unsigned), ctx_->stream));
+        else DMPM_CK(cudaMemsetAsync(fixb_ + slot, 0, sizeof(unsigned), ctx_->stream));
+    }
+    // sum part_[0 .. nb) into *out in block order
+    void sum_partials(unsigned nb, double* out) {
+        if (nb > part_n_) throw StateError{"internal: partial-sum buffer too small"};
+        k_sum_partials<<<1, 256, 0, ctx_->stream>>>(part_, (int)nb, out);
+        launched();
+    }
     unsigned pgrid256() const { return (unsigned)((n_ + 255) / 256); }
     // persistent grid of a warp-item kernel: ctas CTAs of 256 threads per SM (the
     // residency its register budget allows), fewer when the particles could not
@@ -427,12 +451,8 @@ template <class T> class Engine : public EngineBase {
         a.unit_start = ep.units;
         a.unit_key = ep.unit_keys;
         a.n_units_dev = ep.n_units;
-        return unit_shift_of(ep);
+        return ep.units ? ep.unit_shift : -1;
     }
-    static int unit_shift_of(const Epoch& ep) { return ep.units ? ep.unit_shift : -1; }
-    // A layer grid of the FP32 path holds (p, m) where its step ran the brick G2P
-    // (which applies G_op to the nodes as it reads them), else (v, m) from k_gop_inplace.
-    static bool grid_keeps_p(int ush) { return ush == 3 || ush == 6; }
     // persistent grid of a brick kernel: as many CTAs as can be resident at once
     // (its register and shared-memory budget), looked up once per kernel
     template <class K> unsigned brick_blocks(K kernel) {
@@ -528,6 +548,20 @@ template <class T> class Engine : public EngineBase {
     }
 
     void launch_mass(const LossArgs<T>& a) {
+        if constexpr (kWarp) {
+            if (det()) {  // integer sums: the raster does not depend on the order of the adds
+                ensure_fix();
+                clear_fix(FIXB_RASTER);
+                k_fix_mass_bound<<<(a.n + 255) / 256, 256, 0, ctx_->stream>>>(a.cst + (size_t)KM * a.npc, a.n,
+                                                                              fixb_ + FIXB_RASTER);
+                launched();
+                k_p2g_mass_fix<<<(a.n + 255) / 256, 256, 0, ctx_->stream>>>(a, fix_, fixb_);
+                launched();
+                k_fix_to_node4<<<ggrid(), 256, 0, ctx_->stream>>>(fix_, fixb_, a.n, G_, 2, a.grid);
+                launched();
+                return;
+            }
+        }
         if (kTiled)
             k_p2g_mass<T, true><<<pgrid(), block(), tile_cap() * sizeof(T), ctx_->stream>>>(a);
         else
@@ -707,6 +741,10 @@ template <class T> class Engine : public EngineBase {
         }
         gadj_ = (node4<T>*)layer_arena_.alloc(gr_bytes);
         gadj2_ = (node4<T>*)layer_arena_.alloc(2 * gr_bytes);
+        // block partial sums: the loss (G / 256 blocks), dLdF norms (n / 32 at the smallest block size),
+        // gradient norms (9 np / 256)
+        part_n_ = std::max({(G_ + 255) / 256, (np_ + 31) / 32, (9 * np_ + 255) / 256}) + 1;
+        part_ = (double*)layer_arena_.alloc(part_n_ * sizeof(double));
         if (!kWarp) {
             gridv_ = (T*)layer_arena_.alloc(3 * G_ * sizeof(T));
             pscratch_ = (T*)layer_arena_.alloc(9 * np_ * sizeof(T));
@@ -926,6 +964,7 @@ template <class T> class Engine : public EngineBase {
     // one ForwardTimeStep: layer l -> out (state of l+1), grid g, G of layer l into Gd
     void step(int l, const T* st, T* out, node4<T>* g, T* Gd, bool allow_sort) {
         if constexpr (kWarp) {
+            ensure_fix();  // allocated already (a no-op) on every captured path
             Epoch& ep = epoch_for(l, st, allow_sort);
             WArgs a = warp_args();
             a.items = WarpItems{ep.order, ep.items, 0};
@@ -936,25 +975,37 @@ template <class T> class Engine : public EngineBase {
             a.G = (float*)Gd;
             a.grid = (node4<float>*)g;
             a.P = ctx_->prm.keep_intermediates ? (float*)layers_[l].dbgP : nullptr;
-            DMPM_CK(cudaMemsetAsync(g, 0, G_ * sizeof(node4<T>), ctx_->stream));
+            const bool dm = det();
+            if (dm) {  // integer node sums, converted into the layer grid after P2G
+                a.fix = fix_;
+                a.fixb = fixb_;
+                clear_fix(-1);
+            } else {
+                DMPM_CK(cudaMemsetAsync(g, 0, G_ * sizeof(node4<T>), ctx_->stream));
+            }
             const unsigned ws = warp_blocks(DMPM_SCATTER_CTAS);
             const int ush = set_units(a, ep);
             pbeg(K_P_OP1);
-            k_stress<<<pgrid256(), 256, 0, ctx_->stream>>>(a);
+            if (dm) k_stress<true><<<pgrid256(), 256, 0, ctx_->stream>>>(a);
+            else k_stress<false><<<pgrid256(), 256, 0, ctx_->stream>>>(a);
             launched();
             pend();
             pbeg(K_P2G);
-            if (ctx_->prm.warp_general) k_p2g_w<true, ITEMS_PERSISTENT><<<ws, 256, 0, ctx_->stream>>>(a);
+            const bool gen = ctx_->prm.warp_general != 0;
+            if (dm && gen) k_p2g_w<true, ITEMS_PERSISTENT, true><<<ws, 256, 0, ctx_->stream>>>(a);
+            else if (dm) k_p2g_w<false, ITEMS_PERSISTENT, true><<<ws, 256, 0, ctx_->stream>>>(a);
+            else if (gen) k_p2g_w<true, ITEMS_PERSISTENT><<<ws, 256, 0, ctx_->stream>>>(a);
             else k_p2g_w<false, ITEMS_PERSISTENT><<<ws, 256, 0, ctx_->stream>>>(a);
             launched();
-            pend();
-            if (ush != 3 && ush != 6) {  // the brick G2P applies G_op to the nodes it reads
-                pbeg(K_GOP);
-                k_gop_inplace<<<ggrid(), 256, 0, ctx_->stream>>>((node4<float>*)g, G_, a.dt, a.fext[0], a.fext[1],
-                                                                 a.fext[2]);
+            if (dm) {
+                k_fix_to_node4<<<ggrid(), 256, 0, ctx_->stream>>>(fix_, fixb_, n_, G_, 0, (node4<float>*)g);
                 launched();
-                pend();
             }
+            pend();
+            pbeg(K_GOP);
+            k_gop_inplace<<<ggrid(), 256, 0, ctx_->stream>>>((node4<float>*)g, G_, a.dt, a.fext[0], a.fext[1], a.fext[2]);
+            launched();
+            pend();
             pbeg(K_G2P);
             if (ush == 3) k_g2p_b<2><<<brick_blocks(k_g2p_b<2>), DMPM_BRICK_THREADS, 0, ctx_->stream>>>(a);
             else if (ush == 6) k_g2p_b<4><<<brick_blocks(k_g2p_b<4>), DMPM_BRICK_THREADS, 0, ctx_->stream>>>(a);
@@ -1048,6 +1099,7 @@ template <class T> class Engine : public EngineBase {
         if (L_ <= 0) throw StateError{"dmpm_setup has not been called"};
         if (start < 0 || start >= L_) throw ArgError{"start_layer out of range"};
         reset_status();
+        ensure_fix();  // before any capture: a captured launch holds the buffer's address
         if (k_ == 1) {
             auto body = [&]() {
                 for (int l = start; l + 1 < L_; l++)
@@ -1115,14 +1167,15 @@ template <class T> class Engine : public EngineBase {
         a.grid = g;
         a.adj = adj_of(L_ - 1, true);
         a.loss = loss_acc_;
+        a.part = part_;
         DMPM_CK(cudaMemsetAsync(g, 0, G_ * sizeof(node4<T>), ctx_->stream));
-        DMPM_CK(cudaMemsetAsync(loss_acc_, 0, sizeof(double), ctx_->stream));
         pbeg(K_MASS);
         launch_mass(a);
         pend();
         pbeg(K_NODE_LOSS);
         k_node_loss<T><<<ggrid(), 256, 0, ctx_->stream>>>(a, G_);
         launched();
+        sum_partials(ggrid(), loss_acc_);
         pend();
         pbeg(K_LOSS_DLDX);
         k_loss_dldx<T><<<pgrid(), block(), 0, ctx_->stream>>>(a);
@@ -1166,12 +1219,32 @@ template <class T> class Engine : public EngineBase {
             a.dbg_vnext = P.keep_intermediates ? (float*)layers_[i].dbgvn : nullptr;
             a.dbg_Cnext = P.keep_intermediates ? (float*)layers_[i].dbgCn : nullptr;
             if (!a.st || !a.st_next || !a.grid || !a.G) throw StateError{"internal: layer not materialised"};
-            DMPM_CK(cudaMemsetAsync(gadj_, 0, G_ * sizeof(node4<T>), ctx_->stream));
             const bool ex = P.adjoint_mode == DMPM_ADJ_EXACT;
+            const bool dm = det();
+            if (dm) {  // integer node sums of dLdv, converted into gadj_ after the scatter
+                a.fix = fix_;
+                a.fixb = fixb_;
+                clear_fix(FIXB_ADJ);
+            } else {
+                DMPM_CK(cudaMemsetAsync(gadj_, 0, G_ * sizeof(node4<T>), ctx_->stream));
+            }
             const unsigned ws = warp_blocks(DMPM_ADJ_SCATTER_CTAS), wg = warp_blocks(DMPM_GATHER_CTAS);
             const int ush = set_units(a, ep);
             pbeg(K_ADJ_SCATTER);
-            if (P.warp_general) {
+            if (dm) {
+                if (ex) k_adj_sources<true><<<pgrid256(), 256, 0, ctx_->stream>>>(a);
+                else k_adj_sources<false><<<pgrid256(), 256, 0, ctx_->stream>>>(a);
+                launched();
+                if (P.warp_general) {
+                    if (ex) k_adj_scatter_w<true, true, ITEMS_PERSISTENT, true><<<ws, 256, 0, ctx_->stream>>>(a);
+                    else k_adj_scatter_w<false, true, ITEMS_PERSISTENT, true><<<ws, 256, 0, ctx_->stream>>>(a);
+                } else {
+                    if (ex) k_adj_scatter_w<true, false, ITEMS_PERSISTENT, true><<<ws, 256, 0, ctx_->stream>>>(a);
+                    else k_adj_scatter_w<false, false, ITEMS_PERSISTENT, true><<<ws, 256, 0, ctx_->stream>>>(a);
+                }
+                launched();
+                k_fix_to_node4<<<ggrid(), 256, 0, ctx_->stream>>>(fix_, fixb_, n_, G_, 1, (node4<float>*)gadj_);
+            } else if (P.warp_general) {
                 if (ex) k_adj_scatter_w<true, true, ITEMS_PERSISTENT><<<ws, 256, 0, ctx_->stream>>>(a);
                 else k_adj_scatter_w<false, true, ITEMS_PERSISTENT><<<ws, 256, 0, ctx_->stream>>>(a);
             } else {
@@ -1181,12 +1254,8 @@ template <class T> class Engine : public EngineBase {
             launched();
             pend();
             pbeg(K_ADJ_GOP);
-            const bool sp = grid_keeps_p(ush);
-            const float f0 = a.fext[0], f1 = a.fext[1], f2 = a.fext[2];
-            if (ex && sp) k_adj_gop_w<true, true><<<ggrid(), 256, 0, ctx_->stream>>>(a.grid, a.gadj, a.gadj2, G_, a.dt, f0, f1, f2);
-            else if (ex) k_adj_gop_w<true, false><<<ggrid(), 256, 0, ctx_->stream>>>(a.grid, a.gadj, a.gadj2, G_, a.dt, f0, f1, f2);
-            else if (sp) k_adj_gop_w<false, true><<<ggrid(), 256, 0, ctx_->stream>>>(a.grid, a.gadj, a.gadj2, G_, a.dt, f0, f1, f2);
-            else k_adj_gop_w<false, false><<<ggrid(), 256, 0, ctx_->stream>>>(a.grid, a.gadj, a.gadj2, G_, a.dt, f0, f1, f2);
+            if (ex) k_adj_gop_w<true><<<ggrid(), 256, 0, ctx_->stream>>>(a.grid, a.gadj, a.gadj2, G_, a.dt, a.fext[0], a.fext[1], a.fext[2]);
+            else k_adj_gop_w<false><<<ggrid(), 256, 0, ctx_->stream>>>(a.grid, a.gadj, a.gadj2, G_, a.dt, a.fext[0], a.fext[1], a.fext[2]);
             launched();
             pend();
             if (P.keep_intermediates) {
@@ -1296,6 +1365,7 @@ template <class T> class Engine : public EngineBase {
     // layer `top` (written by dmpm_loss, or by the caller for top < L-1).
     void backward_range(int top, int control) {
         if (!forward_done_ && L_ > 1) throw StateError{"dmpm_forward has not been run"};
+        ensure_fix();
         if (top < 0 || top > L_ - 1) throw ArgError{"top layer out of range"};
         if (control < 0 || control > top) throw ArgError{"control_layer out of range"};
         if (top < L_ - 1 && !layers_[top].adj) throw StateError{"set keep_adjoints to start the adjoint below the last layer"};
@@ -1438,11 +1508,11 @@ template <class T> class Engine : public EngineBase {
         T* vec = it->second + 9 * np_;
         T* vmax = it->second + 18 * np_;
         double* norm2 = loss_acc_ + 1;
-        DMPM_CK(cudaMemsetAsync(norm2, 0, sizeof(double), ctx_->stream));
         const unsigned blocks = (unsigned)((9 * np_ + 255) / 256);
-        if (grad_fp64) k_sumsq<double><<<blocks, 256, 0, ctx_->stream>>>((const double*)grad, np_, n_, norm2);
-        else k_sumsq<T><<<blocks, 256, 0, ctx_->stream>>>((const T*)grad, np_, n_, norm2);
+        if (grad_fp64) k_sumsq<double><<<blocks, 256, 0, ctx_->stream>>>((const double*)grad, np_, n_, part_);
+        else k_sumsq<T><<<blocks, 256, 0, ctx_->stream>>>((const T*)grad, np_, n_, part_);
         launched();
+        sum_partials(blocks, norm2);
         const float c1 = 1.f - std::pow((float)b1, (float)t), c2 = 1.f - std::pow((float)b2, (float)t);
         if (kind == DMPM_DESCEND_ADAM) {
             if (grad_fp64)
@@ -1488,9 +1558,9 @@ template <class T> class Engine : public EngineBase {
         if (layers_[l].adj) a = layers_[l].adj;
         else if (l == backward_lo_ || l == L_ - 1) a = adj_of(l, false);
         else throw StateError{"adjoint of this layer is not kept"};
-        DMPM_CK(cudaMemsetAsync(loss_acc_ + 1, 0, sizeof(double), ctx_->stream));
-        k_sqnorm9<T><<<pgrid(), block(), 0, ctx_->stream>>>(a + (size_t)PF * np_, np_, n_, loss_acc_ + 1);
+        k_sqnorm9<T><<<pgrid(), block(), 0, ctx_->stream>>>(a + (size_t)PF * np_, np_, n_, part_);
         launched();
+        sum_partials(pgrid(), loss_acc_ + 1);
         DMPM_CK(cudaMemcpyAsync((char*)host_misc_ + 16, loss_acc_ + 1, sizeof(double), cudaMemcpyDeviceToHost, ctx_->stream));
         DMPM_CK(cudaStreamSynchronize(ctx_->stream));
         return std::sqrt(*(double*)((char*)host_misc_ + 16));
@@ -1511,13 +1581,7 @@ template <class T> class Engine : public EngineBase {
                 }
             }
             double* s = staging(3 * G_);
-            // the FP32 warp-item step's grid update wrote v over p; the brick G2P's did not
-            int stored_v = 0;
-            if constexpr (kWarp) {
-                if (l < L_ - 1)
-                    stored_v = grid_keeps_p(unit_shift_of(epochs_[std::min((int)epochs_.size() - 1, l / sort_every())]))
-                                   ? 0 : 1;
-            }
+            const int stored_v = (kWarp && l < L_ - 1) ? 1 : 0;  // the FP32 grid update wrote v over p
             k_grid_field<T><<<ggrid(), 256, 0, ctx_->stream>>>(g, G_, field, stored_v, P.dt, P.f_ext[0], P.f_ext[1],
                                                               P.f_ext[2], s);
             launched();
@@ -1630,7 +1694,7 @@ template <class T> class Engine : public EngineBase {
     bool grid_set_ = false;
     int n_ = 0;
     size_t np_ = 0;
-    Arena scene_arena_, scene_arena_grid_, layer_arena_, staging_arena_, misc_arena_;
+    Arena scene_arena_, scene_arena_grid_, layer_arena_, staging_arena_, misc_arena_, fix_arena_;
     T* cst_ = nullptr;
     T* st0_ = nullptr;
     T* dfc0_ = nullptr;
@@ -1641,6 +1705,12 @@ template <class T> class Engine : public EngineBase {
     size_t staging_count_ = 0;
     unsigned* status_ = nullptr;
     double* loss_acc_ = nullptr;
+    double* part_ = nullptr;  // per-block partial sums of the FP64 reductions (loss, norms)
+    size_t part_n_ = 0;
+    // deterministic mode: integer node sums (G fix4) and their bound slots
+    fix4* fix_ = nullptr;
+    unsigned* fixb_ = nullptr;
+    size_t fix_G_ = 0;
     void* host_misc_ = nullptr;
     int L_ = 0, k_ = 1;
     std::vector<LayerSlots> layers_;
@@ -1813,7 +1883,8 @@ int dmpm_set_params(dmpm_ctx* ctx, const dmpm_params* p) {
         p->loss_kind < 0 || p->loss_kind > 1 || p->checkpoint_every < 0 || p->block_size < 0 || p->block_size > 256 ||
         (p->block_size % 32) != 0 || p->tile_cap < 0 || p->tile_cap > 1536 || p->sort_every < 0 ||
         p->warp_general < 0 || p->warp_general > 1 || p->control_stride < 0 || p->eager < 0 || p->eager > 1 ||
-        (p->brick_cells != 0 && p->brick_cells != 2 && p->brick_cells != 4)) {
+        (p->brick_cells != 0 && p->brick_cells != 2 && p->brick_cells != 4) || p->deterministic < 0 ||
+        p->deterministic > 1) {
         ctx->err = "invalid dmpm_params";
         return DMPM_ERR_ARG;
     }

@@ -369,6 +369,8 @@ template <class T> struct LossArgs {
     T* dldm;             // [G]
     T* adj;              // last layer adjoint [24][np]
     double* loss;        // accumulator
+    double* part;        // per-block partial sums of the loss (summed in order by k_sum_partials), or null:
+                         // each block adds to *loss
     int kind;            // 0 = reference log-mass + penalty, 1 = L2
     int tile_cap;
     unsigned* status;
@@ -432,8 +434,9 @@ template <class T, bool TILED> __global__ void __launch_bounds__(256) k_p2g_mass
 
 // Per-node loss and dL/dm in FP64 (CompGraph.cpp:143-187):
 //   L = sum 1/2 (log(m + 1 + eps) - log(t + 1 + eps))^2 + sum_{m < 1e-3} 10 (1e-3 - m)^2
-// or, for kind 1, L = sum 1/2 (m - t)^2.  Block partial sums are added to one
-// FP64 accumulator.
+// or, for kind 1, L = sum 1/2 (m - t)^2.  Block partial sums go to a.part
+// (k_sum_partials adds them in block order, so the loss is the same in every
+// run) or are added to one FP64 accumulator.
 template <class T> __global__ void __launch_bounds__(256) k_node_loss(LossArgs<T> a, size_t G) {
     __shared__ double s_part[32];
     const size_t g = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
@@ -468,8 +471,26 @@ template <class T> __global__ void __launch_bounds__(256) k_node_loss(LossArgs<T
         double v = threadIdx.x < (blockDim.x >> 5) ? s_part[threadIdx.x] : 0.0;
 #pragma unroll
         for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
-        if (threadIdx.x == 0) atomicAdd(a.loss, v);
+        if (threadIdx.x == 0) {
+            if (a.part) a.part[blockIdx.x] = v;
+            else atomicAdd(a.loss, v);
+        }
     }
+}
+
+// *out = sum of part[0 .. nb) in a fixed order (one block of 256 threads):
+// strided sums per thread, then a tree over the threads
+static __global__ void __launch_bounds__(256) k_sum_partials(const double* __restrict__ part, int nb, double* out) {
+    __shared__ double s[256];
+    double v = 0.0;
+    for (int i = threadIdx.x; i < nb; i += 256) v += part[i];
+    s[threadIdx.x] = v;
+    __syncthreads();
+    for (int h = 128; h > 0; h >>= 1) {
+        if ((int)threadIdx.x < h) s[threadIdx.x] += s[threadIdx.x + h];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) *out = s[0];
 }
 
 // dLdx = sum_g m_p dLdm_g grad w_gp; dLdv = dLdF = dLdC = 0 (CompGraph.cpp:192-241)

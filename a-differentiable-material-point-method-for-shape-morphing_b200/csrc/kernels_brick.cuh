@@ -8,9 +8,7 @@
 // only reads the grid, runs over units: a CTA takes a unit, stages its node
 // tile in shared memory once, and each thread handles one particle of the unit,
 // all 64 stencil nodes of it, reading the tile (the particles of a warp share a
-// cell most of the time, so the reads are broadcasts).  The grid update G_op
-// (v = p/m + dt f) is applied to each node as it is staged, so no separate pass
-// over the grid runs before this kernel and the layer's grid keeps (p, m).  On the 64^3,
+// cell most of the time, so the reads are broadcasts).  On the 64^3,
 // 267k-particle workload this takes 36.7 us per step against 48.1 us for the
 // warp-item G2P; at 8 particles per cell, 21.5 against 22.2 us.  The other
 // stencil kernels stay warp-item kernels (kernels_warp.cuh), which measured
@@ -105,31 +103,11 @@ template <int R> struct GlobalFetch {
     }
 };
 
-// G_op on a node record as it is read: (p, m) -> (v, m), v = p/m + dt f where
-// |m| > FLT_EPSILON, else 0 -- the arithmetic of k_gop_inplace, so a node's v is
-// the same float whichever kernel forms it.
-struct NodeVelocity {
-    float dt, f[3];
-    __device__ __forceinline__ node4<float> operator()(node4<float> nd) const {
-        float v[3];
-        node_velocity(nd, dt, f, v);
-        return node4<float>{v[0], v[1], v[2], nd.w};
-    }
-};
-// GlobalFetch of (p, m) records returning (v, m)
-struct GlobalVelocityFetch {
-    GlobalFetch<1> raw;
-    NodeVelocity vel;
-    __device__ __forceinline__ node4<float> operator()(int i, int j, int k, int r) const {
-        return vel(raw(i, j, k, r));
-    }
-};
-
-// Stage the unit's tile: R consecutive records per node from src, each passed
-// through xf (zeros outside the grid).  Every thread of the block calls it.
-template <int B, int R, class Xf>
+// Stage the unit's tile: R consecutive records per node from src (zeros
+// outside the grid).  Every thread of the block calls it.
+template <int B, int R>
 __device__ __forceinline__ void stage_tile(const node4<float>* __restrict__ src, const GridGeom& g, int goff,
-                                           const int o[3], node4<float>* tile, const Xf& xf) {
+                                           const int o[3], node4<float>* tile) {
     constexpr int E = BrickShape<B>::E, NT = BrickShape<B>::NT;
     for (int q = threadIdx.x; q < NT * R; q += blockDim.x) {
         const int nd = q / R, r = q - nd * R;
@@ -137,7 +115,7 @@ __device__ __forceinline__ void stage_tile(const node4<float>* __restrict__ src,
         const int gi = o[0] + i, gj = o[1] + j, gk = o[2] + k;
         const bool in = (unsigned)gi < (unsigned)g.dim[0] && (unsigned)gj < (unsigned)g.dim[1] &&
                         (unsigned)gk < (unsigned)g.dim[2];
-        tile[q] = in ? xf(src[(size_t)R * ((size_t)goff + ((size_t)gi * g.dim[1] + gj) * g.dim[2] + gk) + r])
+        tile[q] = in ? src[(size_t)R * ((size_t)goff + ((size_t)gi * g.dim[1] + gj) * g.dim[2] + gk) + r]
                      : node4<float>{0.f, 0.f, 0.f, 0.f};
     }
 }
@@ -153,9 +131,7 @@ template <int B> __device__ __forceinline__ bool in_unit(const int base[3], cons
     return in;
 }
 
-// ------------------------------------------------------------------ G_op + G2P + P_op_2
-// v_g = p_g/m_g + dt f (G_op, applied to each node as the tile is staged; the
-// layer's grid keeps (p, m));
+// ------------------------------------------------------------------ G2P + P_op_2
 // v' = sum w v_g;  C' = 3/dx^2 sum w v_g d^T;  F' = (1 - s)(I + dt C')(F + dFc) + s F;  x' = x + dt v'
 template <class Fetch>
 __device__ __forceinline__ void g2p_sums(const Fetch& f, const Axis0& ax0, const float n1[4], const float d1[4],
@@ -213,13 +189,12 @@ __global__ void __launch_bounds__(DMPM_BRICK_THREADS, DMPM_BRICK_G2P_MINB) k_g2p
     const size_t np = a.np, npl = a.npl, npn = a.npn;
     const GridGeom geo = a.geo;
     const float dx = (float)geo.dx, idx = 1.f / dx, k3 = 3.f / (dx * dx);
-    const NodeVelocity vel{a.dt, {a.fext[0], a.fext[1], a.fext[2]}};
     for (int u = blockIdx.x; u < nun; u += gridDim.x) {
         int o[3];
         unit_origin(a.unit_key[u], S::shift, geo, o);
         const uint32_t q0 = a.unit_start[u], q1 = a.unit_start[u + 1];
         __syncthreads();  // the previous unit's readers are done with the tile
-        stage_tile<B, 1>(a.grid, geo, 0, o, tile, vel);
+        stage_tile<B, 1>(a.grid, geo, 0, o, tile);
         __syncthreads();
         for (uint32_t q = q0 + threadIdx.x; q < q1; q += blockDim.x) {
             const int p = (int)a.items.order[q];
@@ -235,8 +210,8 @@ __global__ void __launch_bounds__(DMPM_BRICK_THREADS, DMPM_BRICK_G2P_MINB) k_g2p
             if (in_unit<B>(base, o, l))
                 g2p_sums(TileFetch<B, 1>{tile, l[0], l[1], l[2]}, ax0, n[1], d[1], n[2], d[2], V, Cm);
             else
-                g2p_sums(GlobalVelocityFetch{{a.grid, geo, 0, base[0], base[1], base[2]}, vel}, ax0, n[1], d[1], n[2],
-                         d[2], V, Cm);
+                g2p_sums(GlobalFetch<1>{a.grid, geo, 0, base[0], base[1], base[2]}, ax0, n[1], d[1], n[2], d[2], V,
+                         Cm);
             m3<float> Cn;
 #pragma unroll
             for (int r = 0; r < 3; r++)

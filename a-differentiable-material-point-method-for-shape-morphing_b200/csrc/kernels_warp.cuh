@@ -26,6 +26,7 @@
 //   H' = (1 - s)(D + dt C' (I + D)) + s H,  D = H + dFc.
 // The host converts at upload and download; the FP64 path stores F.
 #pragma once
+#include "fixpoint.cuh"
 #include "sort.cuh"
 
 namespace dmpm {
@@ -326,7 +327,7 @@ struct WArgs {
     const float* cst;      // constants
     const float* dfc;      // dFc of layer n
     float* G;              // [24][npl] per layer: G (9), polar R (9), polar S (6: s00 s01 s02 s11 s12 s22)
-    node4<float>* grid;    // layer n grid: (p, m) after P2G, (v, m) after k_gop_inplace (not run before the brick G2P)
+    node4<float>* grid;    // layer n grid: (p, m) after P2G, (v, m) after k_gop_inplace
     float* P;              // debug: stress of layer n (or null)
     unsigned* status;
     // adjoint
@@ -341,6 +342,9 @@ struct WArgs {
     float* dbg_dLdP;
     float* dbg_vnext;
     float* dbg_Cnext;
+    // deterministic mode (fixpoint.cuh): integer node sums and their bound slots, or null
+    fix4* fix;
+    unsigned* fixb;
     // brick units of the sorted order (kernels_brick.cuh): unit u holds the
     // sorted positions [unit_start[u], unit_start[u + 1]), all with key >> shift
     // equal to unit_key[u]; the unit count stays on the device
@@ -412,9 +416,11 @@ __device__ __forceinline__ void stage_stencil(const node4<float>* __restrict__ s
 // ------------------------------------------------------------------ forward
 // P = PK(F + dFc) in FP64;  G = -3/dx^2 dt vol P Fe^T + m C  (P_op_1 and the
 // particle-constant part of SingleParticle_to_grid, ForwardSimulation.cpp:6-9, 38)
-static __global__ void __launch_bounds__(256, DMPM_STRESS_MIN_BLOCKS) k_stress(WArgs a) {
+// DET: also raise the deterministic mode's P2G bounds (fixpoint.cuh) in a.fixb.
+template <bool DET = false> __global__ void __launch_bounds__(256, DMPM_STRESS_MIN_BLOCKS) k_stress(WArgs a) {
     const size_t np = a.np, npl = a.npl;
     const int p = blockIdx.x * blockDim.x + threadIdx.x;
+    float cmom = 0.f, cmass = 0.f;
     if (p < a.n) {
         const m3<float> H = load_m3(a.st + (size_t)PF * npl, npl, p), dfc = load_m3(a.dfc, np, p);
         const m3<float> Fe = fe_from_strain(H, dfc);
@@ -436,13 +442,35 @@ static __global__ void __launch_bounds__(256, DMPM_STRESS_MIN_BLOCKS) k_stress(W
         const float k = -3.f / (dx * dx) * a.dt * a.cst[(size_t)KVOL * np + p];
         const m3<float> G = (k * P) * transpose(Fe) + a.cst[(size_t)KM * np + p] * load_m3(a.st + (size_t)PC * npl, npl, p);
         store_m3(a.G, npl, p, G);
+        if constexpr (DET) {
+            // bound on P2G's per-particle values: |m v damp + G d| with |d| < 2 dx, and m
+            const float mp = a.cst[(size_t)KM * np + p], damp = 1.f - a.dt * a.drag;
+#pragma unroll
+            for (int c = 0; c < 3; c++) {
+                const float t = fabsf(mp * a.st[(size_t)(PV + c) * npl + p] * damp) +
+                                2.f * dx * (fabsf(G.a[c][0]) + fabsf(G.a[c][1]) + fabsf(G.a[c][2]));
+                cmom = fmaxf(cmom, t);
+            }
+            cmass = mp;
+        }
+    }
+    if constexpr (DET) {  // every lane of every warp reaches these
+        fix_bound(a.fixb + FIXB_MOMENTUM, cmom * 1.001f);
+        fix_bound(a.fixb + FIXB_MASS, cmass * 1.001f);
     }
 }
 
 // P2G: m_g += w m_p;  p_g += w (m_p v (1 - dt drag) + G (x_g - x_p))
-template <bool GENERAL, int MODE> __global__ void __launch_bounds__(256, DMPM_SCATTER_MIN_BLOCKS) k_p2g_w(WArgs a) {
+// DET: integer node sums into a.fix (fixpoint.cuh) instead of float atomics into a.grid.
+template <bool GENERAL, int MODE, bool DET = false>
+__global__ void __launch_bounds__(256, DMPM_SCATTER_MIN_BLOCKS) k_p2g_w(WArgs a) {
     const int nit = item_count(a);
     const size_t np = a.np, npl = a.npl;
+    FixScale sp{1.f, 1.f}, sm{1.f, 1.f};
+    if (DET) {
+        sp = fix_scale(a.fixb + FIXB_MOMENTUM, a.n);
+        sm = fix_scale(a.fixb + FIXB_MASS, a.n);
+    }
     for (int item = first_warp(); item < nit; item = next_item<MODE>(item, nit)) {
         GridGeom geo;
         int goff;
@@ -491,13 +519,19 @@ template <bool GENERAL, int MODE> __global__ void __launch_bounds__(256, DMPM_SC
             if (uniform) {
                 reduce_scatter8<32>(v);
                 const int j = 2 * half + P.jp, k = P.kp;
-                if (((N.mask >> (4 * j + k)) & 1u) && (v[0] != 0.f || v[1] != 0.f || v[2] != 0.f || v[3] != 0.f))
-                    red_add4(a.grid + (N.g00 + j * N.sj + k), v[0], v[1], v[2], v[3]);
+                if (((N.mask >> (4 * j + k)) & 1u) && (v[0] != 0.f || v[1] != 0.f || v[2] != 0.f || v[3] != 0.f)) {
+                    if (DET) fix_red4(a.fix + (N.g00 + j * N.sj + k), v[0], v[1], v[2], v[3], sp.s, sm.s);
+                    else red_add4(a.grid + (N.g00 + j * N.sj + k), v[0], v[1], v[2], v[3]);
+                }
             } else if (L.valid) {
 #pragma unroll
                 for (int nd = 0; nd < 8; nd++) {
                     const int j = 2 * half + ((nd >> 2) ^ P.jp), k = (nd & 3) ^ P.kp;
-                    if ((N.mask >> (4 * j + k)) & 1u)
+                    if (!((N.mask >> (4 * j + k)) & 1u)) continue;
+                    if (DET)
+                        fix_red4(a.fix + (N.g00 + j * N.sj + k), v[nd * 4], v[nd * 4 + 1], v[nd * 4 + 2], v[nd * 4 + 3],
+                                 sp.s, sm.s);
+                    else
                         red_add4(a.grid + (N.g00 + j * N.sj + k), v[nd * 4], v[nd * 4 + 1], v[nd * 4 + 2], v[nd * 4 + 3]);
                 }
             }
@@ -652,9 +686,55 @@ template <int MODE> __global__ void __launch_bounds__(256, 4) k_g2p_w(WArgs a) {
 // ------------------------------------------------------------------ adjoint
 // dLdv_next = dt dLdx' + dLdv';  dLdC_next = c dt dLdF' Fe^T + dLdC'
 // dLdv_g += w dLdv_next + 3/dx^2 w dLdC_next (x_g - x_p)   (BackPropagation.cpp:14-44)
-template <bool EXACT, bool GENERAL, int MODE> __global__ void __launch_bounds__(256, DMPM_ADJ_SCATTER_MIN_BLOCKS) k_adj_scatter_w(WArgs a) {
-    const int nit = item_count(a);
+// The per-particle sources of the adjoint scatter: vn = dt dLdx' + dLdv' and
+// Cn = cf dLdF' Fe^T + dLdC' (cf = (1 - s) dt exact, dt refcompat), from layer
+// n + 1's adjoint and layer n's F + dFc.
+template <bool EXACT>
+__device__ __forceinline__ void adj_sources(const WArgs& a, int p, float vn[3], m3<float>& Cn) {
     const size_t np = a.np, npl = a.npl, npn = a.npn;
+#pragma unroll
+    for (int c = 0; c < 3; c++) vn[c] = a.dt * a.adj_next[(size_t)(PX + c) * npn + p] + a.adj_next[(size_t)(PV + c) * npn + p];
+    const m3<float> Fe = fe_from_strain(load_m3(a.st + (size_t)PF * npl, npl, p), load_m3(a.dfc, np, p));
+    const float cf = EXACT ? (1.f - a.s) * a.dt : a.dt;
+    Cn = (cf * load_m3(a.adj_next + (size_t)PF * npn, npn, p)) * transpose(Fe) +
+         load_m3(a.adj_next + (size_t)PC * npn, npn, p);
+}
+
+// Deterministic mode: the scatter's sources per particle into adjn (which the
+// gather reads too) and their bound |vn + 3/dx^2 Cn d| with |d| < 2 dx into
+// the adjoint bound slot, before the scatter adds anything.
+template <bool EXACT> __global__ void __launch_bounds__(256) k_adj_sources(WArgs a) {
+    const size_t np = a.np;
+    const int p = blockIdx.x * blockDim.x + threadIdx.x;
+    float c = 0.f;
+    if (p < a.n) {
+        float vn[3];
+        m3<float> Cn;
+        adj_sources<EXACT>(a, p, vn, Cn);
+#pragma unroll
+        for (int r = 0; r < 3; r++) a.adjn[(size_t)r * np + p] = vn[r];
+        store_m3(a.adjn + 3 * np, np, p, Cn);
+        if (a.dbg_vnext) {
+#pragma unroll
+            for (int r = 0; r < 3; r++) a.dbg_vnext[(size_t)r * np + p] = vn[r];
+        }
+        if (a.dbg_Cnext) store_m3(a.dbg_Cnext, np, p, Cn);
+        const float dx = (float)a.geo.dx, k3 = 3.f / (dx * dx);
+#pragma unroll
+        for (int r = 0; r < 3; r++)
+            c = fmaxf(c, fabsf(vn[r]) + k3 * 2.f * dx * (fabsf(Cn.a[r][0]) + fabsf(Cn.a[r][1]) + fabsf(Cn.a[r][2])));
+    }
+    fix_bound(a.fixb + FIXB_ADJ, c * 1.001f);
+}
+
+// DET: the sources come from k_adj_sources (adjn) and the node sums go to
+// a.fix as integers (fixpoint.cuh) instead of float atomics into a.gadj.
+template <bool EXACT, bool GENERAL, int MODE, bool DET = false>
+__global__ void __launch_bounds__(256, DMPM_ADJ_SCATTER_MIN_BLOCKS) k_adj_scatter_w(WArgs a) {
+    const int nit = item_count(a);
+    const size_t np = a.np, npl = a.npl;
+    FixScale sa{1.f, 1.f};
+    if (DET) sa = fix_scale(a.fixb + FIXB_ADJ, a.n);
     for (int item = first_warp(); item < nit; item = next_item<MODE>(item, nit)) {
         GridGeom geo;
         int goff;
@@ -670,14 +750,22 @@ template <bool EXACT, bool GENERAL, int MODE> __global__ void __launch_bounds__(
         float own1[3];
         lane_weights_k(x, geo, base, L.s, w, own1, false, P.kp);
         float vn[3];
+        m3<float> Cn;
+        if constexpr (DET) {
 #pragma unroll
-        for (int c = 0; c < 3; c++)
-            vn[c] = a.dt * a.adj_next[(size_t)(PX + c) * npn + p] + a.adj_next[(size_t)(PV + c) * npn + p];
-        const m3<float> Fe = fe_from_strain(load_m3(a.st + (size_t)PF * npl, npl, p), load_m3(a.dfc, np, p));
-        const float cf = EXACT ? (1.f - a.s) * a.dt : a.dt;
-        const m3<float> Cn = (cf * load_m3(a.adj_next + (size_t)PF * npn, npn, p)) * transpose(Fe) +
-                             load_m3(a.adj_next + (size_t)PC * npn, npn, p);
-        if (L.valid) {
+            for (int c = 0; c < 3; c++) vn[c] = a.adjn[(size_t)c * np + p];
+            Cn = load_m3(a.adjn + 3 * np, np, p);
+        } else {
+            const size_t npn = a.npn;
+#pragma unroll
+            for (int c = 0; c < 3; c++)
+                vn[c] = a.dt * a.adj_next[(size_t)(PX + c) * npn + p] + a.adj_next[(size_t)(PV + c) * npn + p];
+            const m3<float> Fe = fe_from_strain(load_m3(a.st + (size_t)PF * npl, npl, p), load_m3(a.dfc, np, p));
+            const float cf = EXACT ? (1.f - a.s) * a.dt : a.dt;
+            Cn = (cf * load_m3(a.adj_next + (size_t)PF * npn, npn, p)) * transpose(Fe) +
+                 load_m3(a.adj_next + (size_t)PC * npn, npn, p);
+        }
+        if (!DET && L.valid) {
             if (L.s == 0) {
 #pragma unroll
                 for (int c = 0; c < 3; c++) a.adjn[(size_t)c * np + p] = vn[c];
@@ -719,13 +807,19 @@ template <bool EXACT, bool GENERAL, int MODE> __global__ void __launch_bounds__(
             if (uniform) {
                 reduce_scatter8<24>(v);
                 const int j = 2 * half + P.jp, k = P.kp;
-                if (((N.mask >> (4 * j + k)) & 1u) && (v[0] != 0.f || v[1] != 0.f || v[2] != 0.f))
-                    red_add4(a.gadj + (N.g00 + j * N.sj + k), v[0], v[1], v[2], 0.f);
+                if (((N.mask >> (4 * j + k)) & 1u) && (v[0] != 0.f || v[1] != 0.f || v[2] != 0.f)) {
+                    if (DET) fix_red4(a.fix + (N.g00 + j * N.sj + k), v[0], v[1], v[2], 0.f, sa.s, sa.s);
+                    else red_add4(a.gadj + (N.g00 + j * N.sj + k), v[0], v[1], v[2], 0.f);
+                }
             } else if (L.valid) {
 #pragma unroll
                 for (int nd = 0; nd < 8; nd++) {
                     const int j = 2 * half + ((nd >> 2) ^ P.jp), k = (nd & 3) ^ P.kp;
-                    if ((N.mask >> (4 * j + k)) & 1u)
+                    if (!((N.mask >> (4 * j + k)) & 1u)) continue;
+                    if (DET)
+                        fix_red4(a.fix + (N.g00 + j * N.sj + k), v[nd * 3], v[nd * 3 + 1], v[nd * 3 + 2], 0.f, sa.s,
+                                 sa.s);
+                    else
                         red_add4(a.gadj + (N.g00 + j * N.sj + k), v[nd * 3], v[nd * 3 + 1], v[nd * 3 + 2], 0.f);
                 }
             }
@@ -733,37 +827,20 @@ template <bool EXACT, bool GENERAL, int MODE> __global__ void __launch_bounds__(
     }
 }
 
-// adjoint G_op per node: (dLdp, dLdm) from dLdv and the layer's grid, which
-// holds (v, m) after k_gop_inplace or, where G2P applied G_op as it read the
-// nodes (STORED_P), still (p, m).  The record pair (dLdp, dLdm), (v, m) of a
-// node is stored contiguously (32 B) so the gather reads one sector per node.
-template <bool EXACT, bool STORED_P>
+// adjoint G_op per node: (dLdp, dLdm) from dLdv and the layer's (v, m)
+// The record pair (dLdp, dLdm), (v, m) of a node is stored contiguously (32 B)
+// so the gather reads one sector per node.
+template <bool EXACT>
 __global__ void k_adj_gop_w(const node4<float>* __restrict__ grid, const node4<float>* __restrict__ gadj,
                             node4<float>* gadj2, size_t G, float dt, float f0, float f1, float f2) {
     const size_t g = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (g >= G) return;
-    node4<float> nd = grid[g];
+    const node4<float> nd = grid[g];
     const node4<float> dv = gadj[g];
     node4<float> o{0.f, 0.f, 0.f, 0.f};
-    const float f[3] = {f0, f1, f2};
-    float pm[3];  // p / m: the velocity the loss sees through m (v - dt f for the exact adjoint)
-    if (STORED_P) {
-        const bool occ = fabsf(nd.w) > (float)kFltEps;
-        pm[0] = occ ? nd.x / nd.w : 0.f;
-        pm[1] = occ ? nd.y / nd.w : 0.f;
-        pm[2] = occ ? nd.z / nd.w : 0.f;
-        float v[3];
-        node_velocity(nd, dt, f, v);
-        nd.x = v[0];
-        nd.y = v[1];
-        nd.z = v[2];
-    }
     if (fabsf(nd.w) > (float)kFltEps) {
         float v[3] = {nd.x, nd.y, nd.z};
-        if (EXACT) {
-            if (STORED_P) { v[0] = pm[0]; v[1] = pm[1]; v[2] = pm[2]; }
-            else { v[0] -= dt * f0; v[1] -= dt * f1; v[2] -= dt * f2; }
-        }
+        if (EXACT) { v[0] -= dt * f0; v[1] -= dt * f1; v[2] -= dt * f2; }
         o.x = dv.x / nd.w;
         o.y = dv.y / nd.w;
         o.z = dv.z / nd.w;

@@ -180,10 +180,12 @@ def build_scene(instance: int, ppc_root: int):
 BRICK_CELLS = None
 # cell-sort interval of the FP32 path (None = the library default, 8 steps)
 SORT_EVERY = None
+# FP32 path with integer node sums (bit-identical repeats), for every FP32 context
+DETERMINISTIC = False
 
 
 def setup_ctx(dmpm, sc, prec, device, vol, target, dt, checkpoint_every, control="tied", control_stride=0,
-              same_inputs=True):
+              same_inputs=True, deterministic=None):
     """An engine context over scene sc.  same_inputs: upload the scene's
     inputs rounded to float32 on both paths -- the FP32-mixed path rounds them
     so anyway, and the FP64 path then computes from the identical values, so a
@@ -199,7 +201,8 @@ def setup_ctx(dmpm, sc, prec, device, vol, target, dt, checkpoint_every, control
     c.set_target_mass(target)
     c.set_params(dt=dt, drag=sc.drag, f_ext=sc.f_ext, smoothing=sc.smoothing, adjoint="exact", control=control,
                  loss="ref", checkpoint_every=checkpoint_every, control_stride=control_stride,
-                 brick_cells=BRICK_CELLS if prec == "fp32" else None, sort_every=SORT_EVERY or 0)
+                 brick_cells=BRICK_CELLS if prec == "fp32" else None, sort_every=SORT_EVERY or 0,
+                 deterministic=DETERMINISTIC if deterministic is None else deterministic)
     c.setup(sc.steps + 1)
     return c
 
@@ -376,18 +379,20 @@ def workload_config(sc, dt_sub, ckpt):
             "parallelism": "replicas: one independent instance per GPU"}
 
 
-def measure_variant(torch, dmpm, sc, vol, target, device, ckpt, args):
+def measure_variant(torch, dmpm, sc, vol, target, device, ckpt, args, deterministic=None):
     """One gradient evaluation of scene sc per step on both paths under one
     storage policy (checkpoint_every = ckpt): FP32-mixed particle-steps/s, device
     memory held, and the plain FP64 path on the same policy (its throughput and
-    the FP32 gradient's relative error against it)."""
+    the FP32 gradient's relative error against it).  deterministic=True: the
+    FP32 path's integer node sums, and a second evaluation in a fresh context
+    to show that the gradient repeats bit for bit."""
     if vol is None:
         sc.dt, _ = _cfl_dt(sc)
         vol, target = _scene_inputs(dmpm, sc, device)
     units = sc.n * sc.steps
     torch.cuda.synchronize()
     base = _mem_used_gb(torch, device)
-    c = setup_ctx(dmpm, sc, "fp32", device, vol, target, sc.dt, ckpt)
+    c = setup_ctx(dmpm, sc, "fp32", device, vol, target, sc.dt, ckpt, deterministic=deterministic)
     for _ in range(args.warmup):
         gradient_step(c)
     hbm = _mem_used_gb(torch, device) - base
@@ -399,6 +404,13 @@ def measure_variant(torch, dmpm, sc, vol, target, device, ckpt, args):
     out = {"particles": sc.n, "steps": sc.steps, "checkpoint_every": info["checkpoint_every"],
            "value": units / (ms / 1000.0), "unit": UNIT, "ms_per_gradient": ms, "hbm_gb": hbm,
            "engine_bytes_gb": info["device_bytes"] / 1e9}
+    if deterministic:
+        c2 = setup_ctx(dmpm, sc, "fp32", device, vol, target, sc.dt, ckpt, deterministic=True)
+        gradient_step(c2)
+        g2 = c2.control_grad()
+        c2.close()
+        out["repeat_bit_identical"] = bool(np.array_equal(g32, g2))
+        out["repeat_relerr"] = float(np.linalg.norm(g2 - g32) / np.linalg.norm(g32))
     if not args.no_fp64:
         c64 = setup_ctx(dmpm, sc, "fp64", device, vol, target, sc.dt, ckpt)
         gradient_step(c64)
@@ -540,6 +552,8 @@ def run_ours(args):
     variants = None
     if world == 1 and not args.no_variants:
         variants = {"checkpointed": measure_variant(torch, dmpm, sc, vol, target, device, 15, args),
+                    "deterministic": measure_variant(torch, dmpm, sc, vol, target, device, ckpt, args,
+                                                     deterministic=True),
                     "as_specified_8ppc": measure_variant(torch, dmpm, build_scene(rank, 2), None, None, device,
                                                          ckpt, args)}
         variants["checkpointed"]["store_all_ms_per_gradient"] = ms_max / args.steps
@@ -739,7 +753,7 @@ def run_config2(args):
     sc.dt, dt_sub = _cfl_dt(sc)
     vol, target = _scene_inputs(dmpm, sc, 0)
     out = {"mode": "config2", "particles": sc.n, "grid": list(sc.dims), "steps": sc.steps, "dt": sc.dt,
-           "dt_substituted_from": dt_sub}
+           "dt_substituted_from": dt_sub, "deterministic": DETERMINISTIC}
     grads = {}
     for ckpt in (1, 25):
         torch.cuda.synchronize()
@@ -751,7 +765,7 @@ def run_config2(args):
         n = max(1, args.steps // 4)
         ms = timed_steps(torch, c, n, lambda: gradient_step(c)) / n
         grads[ckpt] = c.control_grad()
-        if ckpt == 1:  # same inputs twice: the FP32 run-to-run spread (atomic summation order)
+        if ckpt == 1:  # same inputs twice: the FP32 run-to-run spread (float atomic summation order; 0 when deterministic)
             out["grad_relerr_fp32_repeat"] = float(np.linalg.norm(grads[1] - first) / np.linalg.norm(first))
         out["ckpt%d" % ckpt] = {"ms_per_gradient": ms, "particle_steps_per_s": sc.n * sc.steps / (ms / 1000.0),
                                 "hbm_gb": used, "engine_bytes_gb": c.info()["device_bytes"] / 1e9,
@@ -912,7 +926,8 @@ def run_config4(args):
     vol, target = _scene_inputs(dmpm, sc, 0)
     iters = args.iters
     out = {"mode": "config4", "particles": sc.n, "grid": list(sc.dims), "steps": sc.steps, "dt": sc.dt,
-           "dt_substituted_from": dt_sub, "checkpoint_every": 20, "iterations": iters, "lr": args.lr}
+           "dt_substituted_from": dt_sub, "checkpoint_every": 20, "iterations": iters, "lr": args.lr,
+           "deterministic": DETERMINISTIC}
     torch.cuda.synchronize()
     base = _mem_used_gb(torch, 0)
     frame = dict(control="per_layer", control_stride=sc.steps)  # layer 0 is the only control frame
@@ -1077,6 +1092,8 @@ def main():
     ap.add_argument("--brick", type=int, default=None, choices=[0, 2, 4],
                     help="FP32 G2P kernel: 0 warp items, 2 or 4 cells per brick axis (default 2)")
     ap.add_argument("--sort-every", type=int, default=None, help="FP32 cell-sort interval in steps (default 8)")
+    ap.add_argument("--deterministic", action="store_true",
+                    help="FP32 path with integer node sums: gradients repeat bit for bit")
     ap.add_argument("--rollout-steps", type=int, default=0, help="override the 200 time steps (profiling runs)")
     ap.add_argument("--no-fp64", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
@@ -1095,10 +1112,11 @@ def main():
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
-    global BRICK_CELLS, SORT_EVERY
+    global BRICK_CELLS, SORT_EVERY, DETERMINISTIC
     if args.brick is not None:
         BRICK_CELLS = args.brick
     SORT_EVERY = args.sort_every
+    DETERMINISTIC = args.deterministic
     if args.impl == "reference":
         return run_reference(args)
     if args.fd:

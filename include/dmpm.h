@@ -102,13 +102,10 @@ typedef struct dmpm_ctx dmpm_ctx;
 #define DMPM_F_DLDC_NEXT 16
 #define DMPM_F_DLDFE 19 /* dL/d dFc of the layer (EXACT: differs from dLdF when smoothing != 0) */
 
-/* grid fields (dmpm_get_grid).  On the FP32-mixed path with the warp-item G2P
- * (brick_cells 0) the grid update overwrites each node's momentum with its
- * velocity in place: DMPM_G_V is then read as stored and DMPM_G_P is recovered
- * as (v - dt f_ext) m on nodes with |m| > FLT_EPSILON (0 on the others).  The
- * brick G2P (the default) applies the update to the nodes as it reads them, so
- * the grid keeps (p, m) and DMPM_G_V is formed by the same float arithmetic.
- * The FP64 path keeps both exactly. */
+/* grid fields (dmpm_get_grid).  On the FP32-mixed path the grid update
+ * overwrites each node's momentum with its velocity in place: DMPM_G_V is then
+ * read as stored and DMPM_G_P is recovered as (v - dt f_ext) m on nodes with
+ * |m| > FLT_EPSILON (0 on the others); the FP64 path keeps both exactly. */
 #define DMPM_G_M 0
 #define DMPM_G_V 1
 #define DMPM_G_P 2
@@ -145,6 +142,11 @@ typedef struct {
                                 of brick_cells^3 cells in shared memory and each thread handles one
                                 particle of it; 0 = warp items (8 particles of a cell per warp).
                                 Takes effect at the next cell sort. */
+    int deterministic;       /* FP32 path: 1 = node sums (P2G, the adjoint scatter, the mass rasters) as
+                                64-bit integer multiples of a power of two fixed per pass, added with
+                                integer atomics, so gradients and losses are bit-identical from run to
+                                run; 0 (default) = float atomics, whose summation order varies.  The
+                                FP64 reductions (loss, norms) are summed in a fixed order either way. */
 } dmpm_params;
 
 void dmpm_default_params(dmpm_params* p);

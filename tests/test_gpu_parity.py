@@ -68,12 +68,10 @@ def test_volumes_and_target_raster(gpu_ready, g64):
 
 @pytest.mark.parametrize("brick", [0, 2, 4])
 def test_fp32_grid_fields_match_reference(gpu_ready, g64, golden_scene, brick):
-    """dmpm_get_grid on the FP32-mixed path.  With the warp-item G2P
-    (brick_cells 0) the grid update overwrites the momentum with the velocity in
-    place (v as stored, p recovered from v and m); the brick G2P applies the
-    update to the nodes as it reads them and the grid keeps (p, m) (v formed on
-    read).  Both against the reference's grids of the first layers (FP32
-    tolerances)."""
+    """dmpm_get_grid on the FP32-mixed path, whose grid update overwrites the
+    momentum with the velocity in place: v as stored, p recovered from v and m,
+    both against the reference's grids of the first layers (FP32 tolerances),
+    with either G2P kernel (warp items, or bricks of 2^3 or 4^3 cells)."""
     sc = golden_scene
     with make_ctx(sc, "fp32", g64["target"], brick_cells=brick) as c:
         c.setup(ROLLOUT_LAYERS)
