@@ -245,6 +245,7 @@ template <class T> class Engine : public EngineBase {
         // warp-item kernels serve this epoch
         uint32_t* units = nullptr;
         uint32_t* unit_keys = nullptr;
+        uint32_t* unit_items = nullptr;  // first warp item of each unit
         uint32_t* n_units = nullptr;
         int unit_shift = -1;
         bool valid = false;
@@ -451,6 +452,7 @@ template <class T> class Engine : public EngineBase {
         a.unit_start = ep.units;
         a.unit_key = ep.unit_keys;
         a.n_units_dev = ep.n_units;
+        a.unit_item = ep.unit_items;
         return ep.units ? ep.unit_shift : -1;
     }
     // persistent grid of a brick kernel: as many CTAs as can be resident at once
@@ -465,6 +467,20 @@ template <class T> class Engine : public EngineBase {
             it = brick_occ_.emplace(key, std::max(1, per_sm)).first;
         }
         return (unsigned)(sms_ * it->second);
+    }
+
+    // the deterministic adjoint scatter: through each unit's shared node tile when the epoch has units
+    template <bool EX, bool GEN> void launch_adj_scatter_fix_t(const WArgs& a, int ush, unsigned ws) {
+        const unsigned bt = DMPM_BRICK_THREADS;
+        if (ush == 3) k_adj_scatter_fix_b<2, EX, GEN><<<brick_blocks(k_adj_scatter_fix_b<2, EX, GEN>), bt, 0, ctx_->stream>>>(a);
+        else if (ush == 6) k_adj_scatter_fix_b<4, EX, GEN><<<brick_blocks(k_adj_scatter_fix_b<4, EX, GEN>), bt, 0, ctx_->stream>>>(a);
+        else k_adj_scatter_w<EX, GEN, ITEMS_PERSISTENT, true><<<ws, 256, 0, ctx_->stream>>>(a);
+    }
+    void launch_adj_scatter_fix(const WArgs& a, bool ex, bool gen, int ush, unsigned ws) {
+        if (ex && gen) launch_adj_scatter_fix_t<true, true>(a, ush, ws);
+        else if (ex) launch_adj_scatter_fix_t<true, false>(a, ush, ws);
+        else if (gen) launch_adj_scatter_fix_t<false, true>(a, ush, ws);
+        else launch_adj_scatter_fix_t<false, false>(a, ush, ws);
     }
 
     void launched() {
@@ -823,6 +839,7 @@ template <class T> class Engine : public EngineBase {
             if (ctx_->prm.brick_cells) {
                 e.units = (uint32_t*)layer_arena_.alloc(((size_t)n_ + 1) * sizeof(uint32_t));
                 e.unit_keys = (uint32_t*)layer_arena_.alloc((size_t)n_ * sizeof(uint32_t));
+                e.unit_items = (uint32_t*)layer_arena_.alloc(((size_t)n_ + 1) * sizeof(uint32_t));
                 e.n_units = (uint32_t*)layer_arena_.alloc(16);
             }
         }
@@ -897,6 +914,9 @@ template <class T> class Engine : public EngineBase {
             k_unit_starts<<<(n + 255) / 256, 256, 0, ctx_->stream>>>(sk_[cur], sf_, n, shift, e.units, e.unit_keys);
             launched();
             k_item_sentinel<<<1, 1, 0, ctx_->stream>>>(e.units, e.n_units, n);
+            launched();
+            k_unit_items<<<(n + 256) / 256, 256, 0, ctx_->stream>>>(sk_[cur], e.items, e.n_items, sf_, e.n_units, shift,
+                                                                   e.unit_items);
             launched();
             e.unit_shift = shift;
         }
@@ -992,7 +1012,14 @@ template <class T> class Engine : public EngineBase {
             pend();
             pbeg(K_P2G);
             const bool gen = ctx_->prm.warp_general != 0;
-            if (dm && gen) k_p2g_w<true, ITEMS_PERSISTENT, true><<<ws, 256, 0, ctx_->stream>>>(a);
+            const unsigned bt = DMPM_BRICK_THREADS;
+            if (dm && ush == 3) {  // integer sums through each unit's shared node tile
+                if (gen) k_p2g_fix_b<2, true><<<brick_blocks(k_p2g_fix_b<2, true>), bt, 0, ctx_->stream>>>(a);
+                else k_p2g_fix_b<2, false><<<brick_blocks(k_p2g_fix_b<2, false>), bt, 0, ctx_->stream>>>(a);
+            } else if (dm && ush == 6) {
+                if (gen) k_p2g_fix_b<4, true><<<brick_blocks(k_p2g_fix_b<4, true>), bt, 0, ctx_->stream>>>(a);
+                else k_p2g_fix_b<4, false><<<brick_blocks(k_p2g_fix_b<4, false>), bt, 0, ctx_->stream>>>(a);
+            } else if (dm && gen) k_p2g_w<true, ITEMS_PERSISTENT, true><<<ws, 256, 0, ctx_->stream>>>(a);
             else if (dm) k_p2g_w<false, ITEMS_PERSISTENT, true><<<ws, 256, 0, ctx_->stream>>>(a);
             else if (gen) k_p2g_w<true, ITEMS_PERSISTENT><<<ws, 256, 0, ctx_->stream>>>(a);
             else k_p2g_w<false, ITEMS_PERSISTENT><<<ws, 256, 0, ctx_->stream>>>(a);
@@ -1235,13 +1262,7 @@ template <class T> class Engine : public EngineBase {
                 if (ex) k_adj_sources<true><<<pgrid256(), 256, 0, ctx_->stream>>>(a);
                 else k_adj_sources<false><<<pgrid256(), 256, 0, ctx_->stream>>>(a);
                 launched();
-                if (P.warp_general) {
-                    if (ex) k_adj_scatter_w<true, true, ITEMS_PERSISTENT, true><<<ws, 256, 0, ctx_->stream>>>(a);
-                    else k_adj_scatter_w<false, true, ITEMS_PERSISTENT, true><<<ws, 256, 0, ctx_->stream>>>(a);
-                } else {
-                    if (ex) k_adj_scatter_w<true, false, ITEMS_PERSISTENT, true><<<ws, 256, 0, ctx_->stream>>>(a);
-                    else k_adj_scatter_w<false, false, ITEMS_PERSISTENT, true><<<ws, 256, 0, ctx_->stream>>>(a);
-                }
+                launch_adj_scatter_fix(a, ex, P.warp_general != 0, ush, ws);
                 launched();
                 k_fix_to_node4<<<ggrid(), 256, 0, ctx_->stream>>>(fix_, fixb_, n_, G_, 1, (node4<float>*)gadj_);
             } else if (P.warp_general) {

@@ -45,6 +45,32 @@ __device__ __forceinline__ void fix_red4(fix4* p, float a, float b, float c, flo
     fix_red(&p->w, fix_round(d, sd));
 }
 
+// shared-memory integer sums (a CTA's node tile): the same integers, added in shared memory first
+__device__ __forceinline__ void fix_red_shared(long long* p, long long q) {
+    if (q != 0) atomicAdd(reinterpret_cast<unsigned long long*>(p), (unsigned long long)q);
+}
+__device__ __forceinline__ void fix_red4_shared(fix4* p, float a, float b, float c, float d, float sa, float sd) {
+    fix_red_shared(&p->x, fix_round(a, sa));
+    fix_red_shared(&p->y, fix_round(b, sa));
+    fix_red_shared(&p->z, fix_round(c, sa));
+    fix_red_shared(&p->w, fix_round(d, sd));
+}
+
+// A CTA's shared tile of integer node sums: E^3 nodes from grid node o.
+struct FixTile {
+    fix4* t;
+    int o[3];
+    int E;
+};
+// offset in the tile of a stencil's first node (base), or -1 when its 4^3
+// nodes are not all inside the tile
+__device__ __forceinline__ int fix_tile_offset(const FixTile& ft, const int base[3]) {
+    const int l0 = base[0] - ft.o[0], l1 = base[1] - ft.o[1], l2 = base[2] - ft.o[2];
+    const unsigned lim = (unsigned)(ft.E - 3);
+    if ((unsigned)l0 < lim && (unsigned)l1 < lim && (unsigned)l2 < lim) return (l0 * ft.E + l1) * ft.E + l2;
+    return -1;
+}
+
 // Raise slot to the maximum of |c| over the warp; every lane of the warp calls it.
 __device__ __forceinline__ void fix_bound(unsigned* slot, float c) {
     const unsigned b = __reduce_max_sync(0xffffffffu, __float_as_uint(fabsf(c)));

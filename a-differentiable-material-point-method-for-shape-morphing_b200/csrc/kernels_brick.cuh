@@ -244,4 +244,72 @@ __global__ void __launch_bounds__(DMPM_BRICK_THREADS, DMPM_BRICK_G2P_MINB) k_g2p
     }
 }
 
+// ------------------------------------------------------------------ deterministic P2G / adjoint scatter
+// The deterministic mode's integer node sums (fixpoint.cuh) over units: a CTA
+// takes a unit, its warps take the unit's warp items, and each item whose
+// stencil lies in the unit's node tile adds its (reduce-scattered) node sums to
+// the tile's shared-memory integers; the tile is then added to the global
+// integer sums, one 64-bit atomic per nonzero value.  Integer adds in any order
+// give the same sums, so the result is that of k_p2g_w / k_adj_scatter_w with
+// DET, with about (B + 3)^3 global atomics per unit instead of 64 per item and
+// node value.  Items that are not uniform or have left the unit add to global
+// memory directly.
+template <int B> __device__ __forceinline__ void fix_tile_flush(const FixTile& ft, const GridGeom& g, fix4* dst) {
+    constexpr int E = BrickShape<B>::E, NT = BrickShape<B>::NT;
+    for (int q = threadIdx.x; q < NT; q += blockDim.x) {
+        const fix4 t = ft.t[q];
+        if ((t.x | t.y | t.z | t.w) == 0) continue;
+        const int i = q / (E * E), j = (q / E) % E, k = q % E;
+        const int gi = ft.o[0] + i, gj = ft.o[1] + j, gk = ft.o[2] + k;
+        if (!((unsigned)gi < (unsigned)g.dim[0] && (unsigned)gj < (unsigned)g.dim[1] && (unsigned)gk < (unsigned)g.dim[2]))
+            continue;  // nothing is added there: items skip nodes outside the grid
+        fix4* p = dst + ((size_t)gi * g.dim[1] + gj) * g.dim[2] + gk;
+        fix_red(&p->x, t.x);
+        fix_red(&p->y, t.y);
+        fix_red(&p->z, t.z);
+        fix_red(&p->w, t.w);
+    }
+}
+
+template <int B> __device__ __forceinline__ void fix_tile_begin(FixTile& ft, fix4* tile, uint32_t ukey, const GridGeom& g) {
+    constexpr int NT = BrickShape<B>::NT;
+    unit_origin(ukey, BrickShape<B>::shift, g, ft.o);
+    ft.t = tile;
+    ft.E = BrickShape<B>::E;
+    __syncthreads();  // the previous unit's flush has read the tile
+    for (int q = threadIdx.x; q < NT; q += blockDim.x) tile[q] = fix4{0, 0, 0, 0};
+    __syncthreads();
+}
+
+template <int B, bool GENERAL> __global__ void __launch_bounds__(DMPM_BRICK_THREADS) k_p2g_fix_b(WArgs a) {
+    __shared__ fix4 tile[BrickShape<B>::NT];
+    const int nun = (int)*a.n_units_dev;
+    const FixScale sp = fix_scale(a.fixb + FIXB_MOMENTUM, a.n), sm = fix_scale(a.fixb + FIXB_MASS, a.n);
+    const int warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    for (int u = blockIdx.x; u < nun; u += gridDim.x) {
+        FixTile ft;
+        fix_tile_begin<B>(ft, tile, a.unit_key[u], a.geo);
+        for (uint32_t it = a.unit_item[u] + warp; it < a.unit_item[u + 1]; it += nw)
+            p2g_item<GENERAL, ITEMS_PERSISTENT, true, true>(a, (int)it, sp, sm, ft);
+        __syncthreads();
+        fix_tile_flush<B>(ft, a.geo, a.fix);
+    }
+}
+
+template <int B, bool EXACT, bool GENERAL>
+__global__ void __launch_bounds__(DMPM_BRICK_THREADS) k_adj_scatter_fix_b(WArgs a) {
+    __shared__ fix4 tile[BrickShape<B>::NT];
+    const int nun = (int)*a.n_units_dev;
+    const FixScale sa = fix_scale(a.fixb + FIXB_ADJ, a.n);
+    const int warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    for (int u = blockIdx.x; u < nun; u += gridDim.x) {
+        FixTile ft;
+        fix_tile_begin<B>(ft, tile, a.unit_key[u], a.geo);
+        adj_scatter_items<EXACT, GENERAL, ITEMS_PERSISTENT, true, true>(a, (int)a.unit_item[u] + warp,
+                                                                        (int)a.unit_item[u + 1], nw, sa, ft);
+        __syncthreads();
+        fix_tile_flush<B>(ft, a.geo, a.fix);
+    }
+}
+
 }  // namespace dmpm

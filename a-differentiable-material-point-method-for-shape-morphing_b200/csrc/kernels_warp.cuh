@@ -351,6 +351,7 @@ struct WArgs {
     const uint32_t* unit_start;
     const uint32_t* unit_key;
     const uint32_t* n_units_dev;
+    const uint32_t* unit_item;  // first warp item of each unit (n_units + 1 entries), or null
 };
 
 // How a warp-item launch walks its items:
@@ -461,17 +462,14 @@ template <bool DET = false> __global__ void __launch_bounds__(256, DMPM_STRESS_M
 }
 
 // P2G: m_g += w m_p;  p_g += w (m_p v (1 - dt drag) + G (x_g - x_p))
-// DET: integer node sums into a.fix (fixpoint.cuh) instead of float atomics into a.grid.
-template <bool GENERAL, int MODE, bool DET = false>
-__global__ void __launch_bounds__(256, DMPM_SCATTER_MIN_BLOCKS) k_p2g_w(WArgs a) {
-    const int nit = item_count(a);
+// One warp item of P2G.  DET: integer node sums (fixpoint.cuh) into a.fix
+// instead of float atomics into a.grid; with a tile (ft.t non-null), the sums
+// of an item whose stencil lies in the tile go to its shared-memory integers.
+template <bool GENERAL, int MODE, bool DET, bool TILE>
+__device__ __forceinline__ void p2g_item(const WArgs& a, int item, const FixScale& sp, const FixScale& sm,
+                                         const FixTile& ft) {
     const size_t np = a.np, npl = a.npl;
-    FixScale sp{1.f, 1.f}, sm{1.f, 1.f};
-    if (DET) {
-        sp = fix_scale(a.fixb + FIXB_MOMENTUM, a.n);
-        sm = fix_scale(a.fixb + FIXB_MASS, a.n);
-    }
-    for (int item = first_warp(); item < nit; item = next_item<MODE>(item, nit)) {
+    {
         GridGeom geo;
         int goff;
         item_grid<MODE>(a, item, geo, goff);
@@ -496,6 +494,8 @@ __global__ void __launch_bounds__(256, DMPM_SCATTER_MIN_BLOCKS) k_p2g_w(WArgs a)
         }
         LaneNodes N = lane_nodes(geo, base, L.s);
         N.g00 += goff;
+        // tile offset of node (0, 0, 0) of the item's stencil, or -1 when the stencil is not inside the tile
+        const int tile_l = TILE && uniform ? fix_tile_offset(ft, base) : -1;
 #pragma unroll
         for (int half = 0; half < 2; half++) {
             float v[32];
@@ -520,7 +520,9 @@ __global__ void __launch_bounds__(256, DMPM_SCATTER_MIN_BLOCKS) k_p2g_w(WArgs a)
                 reduce_scatter8<32>(v);
                 const int j = 2 * half + P.jp, k = P.kp;
                 if (((N.mask >> (4 * j + k)) & 1u) && (v[0] != 0.f || v[1] != 0.f || v[2] != 0.f || v[3] != 0.f)) {
-                    if (DET) fix_red4(a.fix + (N.g00 + j * N.sj + k), v[0], v[1], v[2], v[3], sp.s, sm.s);
+                    if (TILE && tile_l >= 0)
+                        fix_red4_shared(ft.t + tile_l + (L.s * ft.E + j) * ft.E + k, v[0], v[1], v[2], v[3], sp.s, sm.s);
+                    else if (DET) fix_red4(a.fix + (N.g00 + j * N.sj + k), v[0], v[1], v[2], v[3], sp.s, sm.s);
                     else red_add4(a.grid + (N.g00 + j * N.sj + k), v[0], v[1], v[2], v[3]);
                 }
             } else if (L.valid) {
@@ -537,6 +539,20 @@ __global__ void __launch_bounds__(256, DMPM_SCATTER_MIN_BLOCKS) k_p2g_w(WArgs a)
             }
         }
     }
+}
+
+// P2G over warp items (one item per warp, persistent grid-stride)
+template <bool GENERAL, int MODE, bool DET = false>
+__global__ void __launch_bounds__(256, DMPM_SCATTER_MIN_BLOCKS) k_p2g_w(WArgs a) {
+    const int nit = item_count(a);
+    FixScale sp{1.f, 1.f}, sm{1.f, 1.f};
+    if (DET) {
+        sp = fix_scale(a.fixb + FIXB_MOMENTUM, a.n);
+        sm = fix_scale(a.fixb + FIXB_MASS, a.n);
+    }
+    const FixTile none{nullptr, {0, 0, 0}, 0};
+    for (int item = first_warp(); item < nit; item = next_item<MODE>(item, nit))
+        p2g_item<GENERAL, MODE, DET, false>(a, item, sp, sm, none);
 }
 
 // G_op in place: (p, m) -> (v, m), v = p/m + dt f where |m| > FLT_EPSILON, else 0
@@ -727,15 +743,16 @@ template <bool EXACT> __global__ void __launch_bounds__(256) k_adj_sources(WArgs
     fix_bound(a.fixb + FIXB_ADJ, c * 1.001f);
 }
 
+// Warp items first, first + stride, ... below end of the adjoint scatter.
 // DET: the sources come from k_adj_sources (adjn) and the node sums go to
-// a.fix as integers (fixpoint.cuh) instead of float atomics into a.gadj.
-template <bool EXACT, bool GENERAL, int MODE, bool DET = false>
-__global__ void __launch_bounds__(256, DMPM_ADJ_SCATTER_MIN_BLOCKS) k_adj_scatter_w(WArgs a) {
-    const int nit = item_count(a);
+// a.fix as integers (fixpoint.cuh) instead of float atomics into a.gadj; with a
+// tile, those of an item whose stencil lies in it go to the tile's
+// shared-memory integers.
+template <bool EXACT, bool GENERAL, int MODE, bool DET, bool TILE>
+__device__ __forceinline__ void adj_scatter_items(const WArgs& a, int first, int end, int stride, const FixScale& sa,
+                                                  const FixTile& ft) {
     const size_t np = a.np, npl = a.npl;
-    FixScale sa{1.f, 1.f};
-    if (DET) sa = fix_scale(a.fixb + FIXB_ADJ, a.n);
-    for (int item = first_warp(); item < nit; item = next_item<MODE>(item, nit)) {
+    for (int item = first; item < end; item += stride) {
         GridGeom geo;
         int goff;
         item_grid<MODE>(a, item, geo, goff);
@@ -785,6 +802,7 @@ __global__ void __launch_bounds__(256, DMPM_ADJ_SCATTER_MIN_BLOCKS) k_adj_scatte
         for (int r = 0; r < 3; r++) c0[r] = k3 * Cn.a[r][0] * w.d0;
         LaneNodes N = lane_nodes(geo, base, L.s);
         N.g00 += goff;
+        const int tile_l = TILE && uniform ? fix_tile_offset(ft, base) : -1;
 #pragma unroll
         for (int half = 0; half < 2; half++) {
             float v[24];  // 8 nodes x dLdv_g (3)
@@ -808,7 +826,9 @@ __global__ void __launch_bounds__(256, DMPM_ADJ_SCATTER_MIN_BLOCKS) k_adj_scatte
                 reduce_scatter8<24>(v);
                 const int j = 2 * half + P.jp, k = P.kp;
                 if (((N.mask >> (4 * j + k)) & 1u) && (v[0] != 0.f || v[1] != 0.f || v[2] != 0.f)) {
-                    if (DET) fix_red4(a.fix + (N.g00 + j * N.sj + k), v[0], v[1], v[2], 0.f, sa.s, sa.s);
+                    if (TILE && tile_l >= 0)
+                        fix_red4_shared(ft.t + tile_l + (L.s * ft.E + j) * ft.E + k, v[0], v[1], v[2], 0.f, sa.s, sa.s);
+                    else if (DET) fix_red4(a.fix + (N.g00 + j * N.sj + k), v[0], v[1], v[2], 0.f, sa.s, sa.s);
                     else red_add4(a.gadj + (N.g00 + j * N.sj + k), v[0], v[1], v[2], 0.f);
                 }
             } else if (L.valid) {
@@ -825,6 +845,17 @@ __global__ void __launch_bounds__(256, DMPM_ADJ_SCATTER_MIN_BLOCKS) k_adj_scatte
             }
         }
     }
+}
+
+// adjoint scatter over warp items (one item per warp, persistent grid-stride)
+template <bool EXACT, bool GENERAL, int MODE, bool DET = false>
+__global__ void __launch_bounds__(256, DMPM_ADJ_SCATTER_MIN_BLOCKS) k_adj_scatter_w(WArgs a) {
+    const int nit = item_count(a);
+    FixScale sa{1.f, 1.f};
+    if (DET) sa = fix_scale(a.fixb + FIXB_ADJ, a.n);
+    const FixTile none{nullptr, {0, 0, 0}, 0};
+    const int stride = MODE != ITEMS_PER_WARP ? (int)((gridDim.x * blockDim.x) >> 5) : nit;  // as next_item
+    adj_scatter_items<EXACT, GENERAL, MODE, DET, false>(a, first_warp(), nit, stride, sa, none);
 }
 
 // adjoint G_op per node: (dLdp, dLdm) from dLdv and the layer's (v, m)

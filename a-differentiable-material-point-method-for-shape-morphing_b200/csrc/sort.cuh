@@ -301,5 +301,18 @@ static __global__ void k_unit_starts(const uint32_t* __restrict__ keys, const ui
     unit_start[idx[i]] = (uint32_t)i;
     unit_key[idx[i]] = keys[i] >> shift;
 }
+// Items never straddle units (an item is part of one cell's run), so unit u's
+// items are [unit_item[u], unit_item[u + 1]): item i starts unit idx[p] where
+// its first sorted position p starts one.  The last entry is the item count.
+static __global__ void k_unit_items(const uint32_t* __restrict__ keys, const uint32_t* __restrict__ item_start,
+                                    const uint32_t* __restrict__ n_items, const uint32_t* __restrict__ idx,
+                                    const uint32_t* __restrict__ n_units, int shift, uint32_t* unit_item) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    const int ni = (int)*n_items;
+    if (i == ni) unit_item[*n_units] = (uint32_t)ni;
+    if (i >= ni) return;
+    const uint32_t p = item_start[i];
+    if (unit_head(keys, (int)p, shift)) unit_item[idx[p]] = (uint32_t)i;
+}
 
 }  // namespace dmpm

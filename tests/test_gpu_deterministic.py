@@ -1,7 +1,9 @@
 """The deterministic mode of the FP32-mixed path (dmpm_params::deterministic):
 P2G, the adjoint scatter and the mass rasters sum each node as 64-bit integer
-multiples of a per-pass power of two (csrc/fixpoint.cuh), so two runs on the
-same inputs give bit-identical states, losses and gradients, and so do the
+multiples of a per-pass power of two (csrc/fixpoint.cuh) -- through each
+brick unit's shared-memory node tile when the epoch has units (brick_cells 2
+or 4), straight into global memory otherwise (0) -- so two runs on the same
+inputs give bit-identical states, losses and gradients, and so do the
 checkpointed, eager and graph-replayed evaluations of one gradient.  The
 mode computes the same quantities, so it is held to the FP32 path's bars
 against the FP64 oracle (the CPU restatement of the reference's
@@ -43,11 +45,12 @@ def _gradient(sc, target, L, **params):
         lo = c.loss()
         assert c.backward(0) == dmpm.OK
         return {"loss": lo, "grad": c.control_grad(), "x": c.get(L - 1, "x"), "F": c.get(L - 1, "F"),
-                "m": c.get_grid(L // 2, "grid_m"), "dLdx": c.get(0, "dLdx")}
+                "m": c.get_grid(L // 2, "grid_m"), "dLdx": c.get(0, "dLdx"), "m0": c.get_grid(0, "grid_m"),
+                "v0": c.get_grid(0, "grid_v")}
 
 
 @pytest.mark.parametrize("general", [False, True])
-@pytest.mark.parametrize("brick", [0, 2])
+@pytest.mark.parametrize("brick", [0, 2, 4])
 def test_deterministic_runs_are_bit_identical(gpu_ready, stirred, brick, general):
     sc, o, loss, L = stirred
     kw = dict(deterministic=True, brick_cells=brick, warp_general=general, sort_every=8)
@@ -56,9 +59,14 @@ def test_deterministic_runs_are_bit_identical(gpu_ready, stirred, brick, general
     assert a["loss"] == b["loss"]
     for k in ("grad", "x", "F", "m", "dLdx"):
         assert np.array_equal(a[k], b[k]), k
+    if brick:
+        # the first P2G (before any G2P, whose kernel brick_cells also picks) through the
+        # unit tiles and straight into global memory: the same integers, added elsewhere first
+        w = _gradient(sc, o.target, L, **dict(kw, brick_cells=0))
+        assert np.array_equal(a["m0"], w["m0"]) and np.array_equal(a["v0"], w["v0"])
 
 
-@pytest.mark.parametrize("brick", [0, 2])
+@pytest.mark.parametrize("brick", [0, 2, 4])
 def test_deterministic_mode_matches_fp64_oracle(gpu_ready, stirred, brick):
     sc, o, loss, L = stirred
     r = _gradient(sc, o.target, L, deterministic=True, brick_cells=brick)
