@@ -112,3 +112,53 @@ def test_deterministic_volumes_and_target_raster(gpu_ready):
     assert np.array_equal(out[0][0], out[1][0]) and np.array_equal(out[0][1], out[1][1])
     assert relerr(out[0][0], out[2][0]) < 1e-5
     assert relerr(out[0][1], out[2][1]) < 1e-5
+
+
+def _edge_scene(case):
+    """The boundary and few-particle scenes of tests/test_gpu_parity.py: a cloud
+    partly outside the grid's low corner (clamped cell keys), and 1 or 37
+    particles on a 16 x 12 x 10 grid."""
+    if case == "boundary":
+        sc = scenes.small_scene(seed=13, res=16, radius=0.2, steps=5, v_std=0.4, drag=0.1, smoothing=0.05,
+                                f_ext=(0.0, -1.0, 0.0), offset=(-0.42, -0.42, 0.0))
+        sc.x = sc.x - np.array([1.3, 0.7, 0.0])
+        sc.v[:, 0] -= 0.5
+        return sc, 6
+    count = 1 if case == "one" else 37
+    sc = scenes.small_scene(seed=17, res=16, radius=0.2, steps=4, v_std=0.3, drag=0.1, f_ext=(0.0, -1.0, 0.0))
+    keep = np.argsort(np.linalg.norm(sc.x - sc.x.mean(axis=0), axis=1))[:count]
+    for f in ("x", "v", "F", "C", "dFc", "m", "lam", "mu", "vol"):
+        setattr(sc, f, np.ascontiguousarray(getattr(sc, f)[keep]))
+    sc.dims = (16, 12, 10)
+    if count == 1:
+        sc.F = np.eye(3)[None].copy()
+        sc.dFc = np.zeros((1, 3, 3))
+    return sc, 5
+
+
+@pytest.mark.parametrize("case", ["boundary", "one", "few37"])
+def test_deterministic_mode_at_the_grid_boundary_and_with_few_particles(gpu_ready, case):
+    sc, L = _edge_scene(case)
+    o = OracleGraph(sc, "f64")
+    sc.vol = o.calc_volumes()
+    o = OracleGraph(sc, "f64")
+    o.setup(L, sc.dt, sc.drag, sc.f_ext, sc.smoothing)
+    o.forward(0)
+    loss = o.loss()
+    o.backward(0, 1)
+    runs = []
+    for _ in range(2):
+        with make_ctx(sc, "fp32", o.target, adjoint="exact", keep_adjoints=True, deterministic=True) as c:
+            c.setup(L)
+            assert c.forward(0) == dmpm.OK
+            lo = c.loss()
+            assert c.backward(0) == dmpm.OK
+            runs.append((c.get(L - 1, "x"), lo, c.get(0, "dLdFe"), c.get(0, "dLdx")))
+    x, lo, dfe, dlx = runs[0]
+    assert relerr(x, o.get(L - 1, "x")) < 1e-5
+    assert abs(lo - loss) / abs(loss) < 1e-4
+    assert normrel(dfe, o.get(0, "dLdFe")) < 1e-3
+    assert normrel(dlx, o.get(0, "dLdx")) < 1e-3
+    assert runs[1][1] == lo
+    for a, b in zip(runs[0], runs[1]):
+        assert np.array_equal(np.asarray(a), np.asarray(b))
