@@ -45,23 +45,28 @@ __device__ __forceinline__ void fix_red4(fix4* p, float a, float b, float c, flo
     fix_red(&p->w, fix_round(d, sd));
 }
 
-// shared-memory integer sums (a CTA's node tile): the same integers, added in shared memory first
-__device__ __forceinline__ void fix_red_shared(long long* p, long long q) {
-    if (q != 0) atomicAdd(reinterpret_cast<unsigned long long*>(p), (unsigned long long)q);
-}
-__device__ __forceinline__ void fix_red4_shared(fix4* p, float a, float b, float c, float d, float sa, float sd) {
-    fix_red_shared(&p->x, fix_round(a, sa));
-    fix_red_shared(&p->y, fix_round(b, sa));
-    fix_red_shared(&p->z, fix_round(c, sa));
-    fix_red_shared(&p->w, fix_round(d, sd));
-}
-
-// A CTA's shared tile of integer node sums: E^3 nodes from grid node o.
+// A CTA's shared tile of integer node sums: E^3 nodes from grid node o, one
+// array of E^3 integers per value (x, y, z, w at t, t + nt, t + 2 nt, t + 3 nt):
+// the lanes of a warp add to neighbouring nodes, which this layout spreads
+// over the shared-memory banks (a 32-byte record per node would put a warp's
+// adds into a quarter of them).
 struct FixTile {
-    fix4* t;
+    long long* t;
+    int nt;
     int o[3];
     int E;
 };
+// the same integers as fix_red4, added to the tile in shared memory first
+__device__ __forceinline__ void fix_red_shared(long long* p, long long q) {
+    if (q != 0) atomicAdd(reinterpret_cast<unsigned long long*>(p), (unsigned long long)q);
+}
+__device__ __forceinline__ void fix_red4_tile(const FixTile& ft, int node, float a, float b, float c, float d, float sa,
+                                              float sd) {
+    fix_red_shared(ft.t + node, fix_round(a, sa));
+    fix_red_shared(ft.t + ft.nt + node, fix_round(b, sa));
+    fix_red_shared(ft.t + 2 * ft.nt + node, fix_round(c, sa));
+    fix_red_shared(ft.t + 3 * ft.nt + node, fix_round(d, sd));
+}
 // offset in the tile of a stencil's first node (base), or -1 when its 4^3
 // nodes are not all inside the tile
 __device__ __forceinline__ int fix_tile_offset(const FixTile& ft, const int base[3]) {

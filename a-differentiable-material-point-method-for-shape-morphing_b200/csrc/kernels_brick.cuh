@@ -257,7 +257,7 @@ __global__ void __launch_bounds__(DMPM_BRICK_THREADS, DMPM_BRICK_G2P_MINB) k_g2p
 template <int B> __device__ __forceinline__ void fix_tile_flush(const FixTile& ft, const GridGeom& g, fix4* dst) {
     constexpr int E = BrickShape<B>::E, NT = BrickShape<B>::NT;
     for (int q = threadIdx.x; q < NT; q += blockDim.x) {
-        const fix4 t = ft.t[q];
+        const fix4 t{ft.t[q], ft.t[NT + q], ft.t[2 * NT + q], ft.t[3 * NT + q]};
         if ((t.x | t.y | t.z | t.w) == 0) continue;
         const int i = q / (E * E), j = (q / E) % E, k = q % E;
         const int gi = ft.o[0] + i, gj = ft.o[1] + j, gk = ft.o[2] + k;
@@ -271,18 +271,20 @@ template <int B> __device__ __forceinline__ void fix_tile_flush(const FixTile& f
     }
 }
 
-template <int B> __device__ __forceinline__ void fix_tile_begin(FixTile& ft, fix4* tile, uint32_t ukey, const GridGeom& g) {
+template <int B>
+__device__ __forceinline__ void fix_tile_begin(FixTile& ft, long long* tile, uint32_t ukey, const GridGeom& g) {
     constexpr int NT = BrickShape<B>::NT;
     unit_origin(ukey, BrickShape<B>::shift, g, ft.o);
     ft.t = tile;
+    ft.nt = NT;
     ft.E = BrickShape<B>::E;
     __syncthreads();  // the previous unit's flush has read the tile
-    for (int q = threadIdx.x; q < NT; q += blockDim.x) tile[q] = fix4{0, 0, 0, 0};
+    for (int q = threadIdx.x; q < 4 * NT; q += blockDim.x) tile[q] = 0;
     __syncthreads();
 }
 
 template <int B, bool GENERAL> __global__ void __launch_bounds__(DMPM_BRICK_THREADS) k_p2g_fix_b(WArgs a) {
-    __shared__ fix4 tile[BrickShape<B>::NT];
+    __shared__ long long tile[4 * BrickShape<B>::NT];
     const int nun = (int)*a.n_units_dev;
     const FixScale sp = fix_scale(a.fixb + FIXB_MOMENTUM, a.n), sm = fix_scale(a.fixb + FIXB_MASS, a.n);
     const int warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
@@ -298,7 +300,7 @@ template <int B, bool GENERAL> __global__ void __launch_bounds__(DMPM_BRICK_THRE
 
 template <int B, bool EXACT, bool GENERAL>
 __global__ void __launch_bounds__(DMPM_BRICK_THREADS) k_adj_scatter_fix_b(WArgs a) {
-    __shared__ fix4 tile[BrickShape<B>::NT];
+    __shared__ long long tile[4 * BrickShape<B>::NT];
     const int nun = (int)*a.n_units_dev;
     const FixScale sa = fix_scale(a.fixb + FIXB_ADJ, a.n);
     const int warp = threadIdx.x >> 5, nw = blockDim.x >> 5;

@@ -521,7 +521,7 @@ __device__ __forceinline__ void p2g_item(const WArgs& a, int item, const FixScal
                 const int j = 2 * half + P.jp, k = P.kp;
                 if (((N.mask >> (4 * j + k)) & 1u) && (v[0] != 0.f || v[1] != 0.f || v[2] != 0.f || v[3] != 0.f)) {
                     if (TILE && tile_l >= 0)
-                        fix_red4_shared(ft.t + tile_l + (L.s * ft.E + j) * ft.E + k, v[0], v[1], v[2], v[3], sp.s, sm.s);
+                        fix_red4_tile(ft, tile_l + (L.s * ft.E + j) * ft.E + k, v[0], v[1], v[2], v[3], sp.s, sm.s);
                     else if (DET) fix_red4(a.fix + (N.g00 + j * N.sj + k), v[0], v[1], v[2], v[3], sp.s, sm.s);
                     else red_add4(a.grid + (N.g00 + j * N.sj + k), v[0], v[1], v[2], v[3]);
                 }
@@ -550,7 +550,7 @@ __global__ void __launch_bounds__(256, DMPM_SCATTER_MIN_BLOCKS) k_p2g_w(WArgs a)
         sp = fix_scale(a.fixb + FIXB_MOMENTUM, a.n);
         sm = fix_scale(a.fixb + FIXB_MASS, a.n);
     }
-    const FixTile none{nullptr, {0, 0, 0}, 0};
+    const FixTile none{nullptr, 0, {0, 0, 0}, 0};
     for (int item = first_warp(); item < nit; item = next_item<MODE>(item, nit))
         p2g_item<GENERAL, MODE, DET, false>(a, item, sp, sm, none);
 }
@@ -827,7 +827,7 @@ __device__ __forceinline__ void adj_scatter_items(const WArgs& a, int first, int
                 const int j = 2 * half + P.jp, k = P.kp;
                 if (((N.mask >> (4 * j + k)) & 1u) && (v[0] != 0.f || v[1] != 0.f || v[2] != 0.f)) {
                     if (TILE && tile_l >= 0)
-                        fix_red4_shared(ft.t + tile_l + (L.s * ft.E + j) * ft.E + k, v[0], v[1], v[2], 0.f, sa.s, sa.s);
+                        fix_red4_tile(ft, tile_l + (L.s * ft.E + j) * ft.E + k, v[0], v[1], v[2], 0.f, sa.s, sa.s);
                     else if (DET) fix_red4(a.fix + (N.g00 + j * N.sj + k), v[0], v[1], v[2], 0.f, sa.s, sa.s);
                     else red_add4(a.gadj + (N.g00 + j * N.sj + k), v[0], v[1], v[2], 0.f);
                 }
@@ -853,7 +853,7 @@ __global__ void __launch_bounds__(256, DMPM_ADJ_SCATTER_MIN_BLOCKS) k_adj_scatte
     const int nit = item_count(a);
     FixScale sa{1.f, 1.f};
     if (DET) sa = fix_scale(a.fixb + FIXB_ADJ, a.n);
-    const FixTile none{nullptr, {0, 0, 0}, 0};
+    const FixTile none{nullptr, 0, {0, 0, 0}, 0};
     const int stride = MODE != ITEMS_PER_WARP ? (int)((gridDim.x * blockDim.x) >> 5) : nit;  // as next_item
     adj_scatter_items<EXACT, GENERAL, MODE, DET, false>(a, first_warp(), nit, stride, sa, none);
 }
