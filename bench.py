@@ -930,10 +930,14 @@ def run_config4(args):
            "deterministic": DETERMINISTIC}
     torch.cuda.synchronize()
     base = _mem_used_gb(torch, 0)
-    frame = dict(control="per_layer", control_stride=sc.steps)  # layer 0 is the only control frame
+    if args.controls == "tied":  # one dFc per particle, applied at every step; gradient summed over the layers
+        frame = dict(control="tied")
+    else:  # layer 0 is the only control frame
+        frame = dict(control="per_layer", control_stride=sc.steps)
     c = setup_ctx(dmpm, sc, "fp32", 0, vol, target, sc.dt, 20, **frame)
     out["hbm_gb_fp32"] = _mem_used_gb(torch, 0) - base
-    out["controls"] = "per-particle dFc of layer 0 (one control frame), exact adjoint"
+    out["controls"] = ("per-particle dFc tied over all layers, exact adjoint" if args.controls == "tied" else
+                       "per-particle dFc of layer 0 (one control frame), exact adjoint")
     losses, times, relerrs = [], [], {}
 
     def fp64_relerr(grad32, dfc):
@@ -1102,6 +1106,8 @@ def main():
     ap.add_argument("--config", type=int, default=1, help="1 = headline workload; 0, 2, 3, 4 = extra measurements")
     ap.add_argument("--iters", type=int, default=30, help="config 4: Adam iterations")
     ap.add_argument("--lr", type=float, default=1e-2, help="config 4: Adam learning rate (configured: 1e-2)")
+    ap.add_argument("--controls", choices=["frame", "tied"], default="frame",
+                    help="config 4: descend layer 0's controls (one control frame) or controls tied over all layers")
     ap.add_argument("--line-search", action="store_true",
                     help="config 4: wrap each Adam step in the reference optimiser's line search")
     ap.add_argument("--fd", action="store_true", help="config 1: adjoint vs central differences, 16 directions")
