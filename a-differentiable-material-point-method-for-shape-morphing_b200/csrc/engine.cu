@@ -981,8 +981,12 @@ template <class T> class Engine : public EngineBase {
         return nullptr;
     }
 
-    // one ForwardTimeStep: layer l -> out (state of l+1), grid g, G of layer l into Gd
-    void step(int l, const T* st, T* out, node4<T>* g, T* Gd, bool allow_sort) {
+    // One ForwardTimeStep: layer l -> out (state of l+1), grid g, G of layer l
+    // in Gd.  FP32 path: g_ready = Gd already holds layer l's G (the previous
+    // step's G2P formed it), so the stress stage is skipped; Gd_next non-null =
+    // the brick G2P also forms layer l+1's G there.  Returns whether it did.
+    bool step(int l, const T* st, T* out, node4<T>* g, T* Gd, bool allow_sort, bool g_ready = false,
+              T* Gd_next = nullptr) {
         if constexpr (kWarp) {
             ensure_fix();  // allocated already (a no-op) on every captured path
             Epoch& ep = epoch_for(l, st, allow_sort);
@@ -1005,11 +1009,13 @@ template <class T> class Engine : public EngineBase {
             }
             const unsigned ws = warp_blocks(DMPM_SCATTER_CTAS);
             const int ush = set_units(a, ep);
-            pbeg(K_P_OP1);
-            if (dm) k_stress<true><<<pgrid256(), 256, 0, ctx_->stream>>>(a);
-            else k_stress<false><<<pgrid256(), 256, 0, ctx_->stream>>>(a);
-            launched();
-            pend();
+            if (dm || !g_ready) {
+                pbeg(K_P_OP1);
+                if (dm) k_stress<true><<<pgrid256(), 256, 0, ctx_->stream>>>(a);
+                else k_stress<false><<<pgrid256(), 256, 0, ctx_->stream>>>(a);
+                launched();
+                pend();
+            }
             pbeg(K_P2G);
             const bool gen = ctx_->prm.warp_general != 0;
             const unsigned bt = DMPM_BRICK_THREADS;
@@ -1033,13 +1039,23 @@ template <class T> class Engine : public EngineBase {
             k_gop_inplace<<<ggrid(), 256, 0, ctx_->stream>>>((node4<float>*)g, G_, a.dt, a.fext[0], a.fext[1], a.fext[2]);
             launched();
             pend();
+            // the deterministic mode keeps the standalone stress stage: it also raises the
+            // next P2G's bounds, which that step clears first
+            const bool fuse = Gd_next && !dm && (ush == 3 || ush == 6);
+            if (fuse) {
+                a.dfc_next = (const float*)layers_[l + 1].dfc;
+                a.G_next = (float*)Gd_next;
+                a.P_next = ctx_->prm.keep_intermediates ? (float*)layers_[l + 1].dbgP : nullptr;
+            }
             pbeg(K_G2P);
-            if (ush == 3) k_g2p_b<2><<<brick_blocks(k_g2p_b<2>), DMPM_BRICK_THREADS, 0, ctx_->stream>>>(a);
-            else if (ush == 6) k_g2p_b<4><<<brick_blocks(k_g2p_b<4>), DMPM_BRICK_THREADS, 0, ctx_->stream>>>(a);
+            if (ush == 3 && fuse) k_g2p_b<2, true><<<brick_blocks(k_g2p_b<2, true>), bt, 0, ctx_->stream>>>(a);
+            else if (ush == 6 && fuse) k_g2p_b<4, true><<<brick_blocks(k_g2p_b<4, true>), bt, 0, ctx_->stream>>>(a);
+            else if (ush == 3) k_g2p_b<2><<<brick_blocks(k_g2p_b<2>), bt, 0, ctx_->stream>>>(a);
+            else if (ush == 6) k_g2p_b<4><<<brick_blocks(k_g2p_b<4>), bt, 0, ctx_->stream>>>(a);
             else k_g2p_w<ITEMS_PERSISTENT><<<warp_blocks(DMPM_G2P_CTAS), 256, 0, ctx_->stream>>>(a);
             launched();
             pend();
-            return;
+            return fuse;
         }
         FwdArgs<T> a = fwd_args();
         a.st = st;
@@ -1071,6 +1087,9 @@ template <class T> class Engine : public EngineBase {
             launched();
             pend();
         }
+        (void)g_ready;
+        (void)Gd_next;
+        return false;
     }
 
     void reset_status() {
@@ -1129,8 +1148,10 @@ template <class T> class Engine : public EngineBase {
         ensure_fix();  // before any capture: a captured launch holds the buffer's address
         if (k_ == 1) {
             auto body = [&]() {
+                bool ready = false;  // layer l's G formed by the previous step
                 for (int l = start; l + 1 < L_; l++)
-                    step(l, layers_[l].st, layers_[l + 1].st, layers_[l].grid, layers_[l].G, true);
+                    ready = step(l, layers_[l].st, layers_[l + 1].st, layers_[l].grid, layers_[l].G, true, ready,
+                                 l + 2 < L_ ? layers_[l + 1].G : nullptr);
             };
             if (graphs_ok()) {
                 run_graph({0, start}, body);
@@ -1143,11 +1164,13 @@ template <class T> class Engine : public EngineBase {
         } else {
             const T* cur = materialize_state(start);
             int r = 0;
+            bool ready = false;
             for (int l = start; l + 1 < L_; l++) {
                 T* out = layers_[l + 1].st ? layers_[l + 1].st : ring_[r];
                 if (!layers_[l + 1].st) r ^= 1;
-                // the current state may live in ring_[r] already (ping-pong)
-                step(l, cur, out, seg_grid_[0], gscratch_, true);
+                // the current state may live in ring_[r] already (ping-pong); layer l's G in
+                // gscratch_ is read by P2G before G2P writes layer l+1's there
+                ready = step(l, cur, out, seg_grid_[0], gscratch_, true, ready, l + 2 < L_ ? gscratch_ : nullptr);
                 cur = out;
             }
             seg_lo_ = seg_hi_ = -1;  // segment scratch no longer matches
@@ -1168,16 +1191,18 @@ template <class T> class Engine : public EngineBase {
     void materialize_segment(int c) {
         const int e = std::min(c + k_, L_ - 1);
         const T* cur = layers_[c].st;
+        bool ready = false;
         for (int l = c; l < e; l++) {
             T* out = (l + 1 == e) ? nullptr : seg_st_[l - c];
             T* Gd = seg_G_.empty() ? nullptr : seg_G_[l - c];
             if (out) {
-                step(l, cur, out, seg_grid_[l - c], Gd, false);
+                ready = step(l, cur, out, seg_grid_[l - c], Gd, false, ready,
+                             seg_G_.empty() ? nullptr : seg_G_[l + 1 - c]);
                 cur = out;
             } else {
                 // last step of the segment: only its grid is needed; the output
                 // (layer e) is a stored layer already, write it to scratch ring
-                step(l, cur, ring_[0], seg_grid_[l - c], Gd, false);
+                step(l, cur, ring_[0], seg_grid_[l - c], Gd, false, ready);
             }
         }
         seg_lo_ = c;

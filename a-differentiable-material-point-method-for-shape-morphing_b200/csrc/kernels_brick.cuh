@@ -181,7 +181,10 @@ __device__ __forceinline__ void g2p_sums(const Fetch& f, const Axis0& ax0, const
     }
 }
 
-template <int B>
+// STRESS: also the next step's stress stage for each particle, from the strain
+// and C just formed (stress_particle, the arithmetic of k_stress), into
+// a.G_next -- one pass over the particles fewer per step.
+template <int B, bool STRESS = false>
 __global__ void __launch_bounds__(DMPM_BRICK_THREADS, DMPM_BRICK_G2P_MINB) k_g2p_b(WArgs a) {
     using S = BrickShape<B>;
     __shared__ node4<float> tile[S::NT];
@@ -229,6 +232,7 @@ __global__ void __launch_bounds__(DMPM_BRICK_THREADS, DMPM_BRICK_G2P_MINB) k_g2p
             // strain update H' = (1 - s)(D + dt C' (I + D)) + s H,  D = H + dFc
             const m3<float> H = load_m3(a.st + (size_t)PF * npl, npl, p);
             const m3<float> D = H + load_m3(a.dfc, np, p);
+            m3<float> Hn;
 #pragma unroll
             for (int c = 0; c < 3; c++)
 #pragma unroll
@@ -237,9 +241,12 @@ __global__ void __launch_bounds__(DMPM_BRICK_THREADS, DMPM_BRICK_G2P_MINB) k_g2p
                                                                        Cn.a[r][2] * D.a[2][c]));
                     const float hn = (1.f - a.s) * t + a.s * H.a[r][c];
                     a.st_next[(size_t)(PF + r + 3 * c) * npn + p] = hn;
+                    Hn.a[r][c] = hn;
                     finite &= isfinite(hn);
                 }
             if (!finite) atomicOr(a.status, ST_NONFINITE_FWD);
+            if constexpr (STRESS)
+                stress_particle(a, p, Hn, load_m3(a.dfc_next, np, p), [&]() { return Cn; }, a.G_next, npn, a.P_next);
         }
     }
 }

@@ -342,6 +342,11 @@ struct WArgs {
     float* dbg_dLdP;
     float* dbg_vnext;
     float* dbg_Cnext;
+    // G2P with the next step's stress stage (kernels_brick.cuh): dFc of layer n + 1,
+    // its G planes and its debug P (or null)
+    const float* dfc_next;
+    float* G_next;
+    float* P_next;
     // deterministic mode (fixpoint.cuh): integer node sums and their bound slots, or null
     fix4* fix;
     unsigned* fixb;
@@ -417,6 +422,37 @@ __device__ __forceinline__ void stage_stencil(const node4<float>* __restrict__ s
 // ------------------------------------------------------------------ forward
 // P = PK(F + dFc) in FP64;  G = -3/dx^2 dt vol P Fe^T + m C  (P_op_1 and the
 // particle-constant part of SingleParticle_to_grid, ForwardSimulation.cpp:6-9, 38)
+// The stress stage of particle p: the FP64 polar decomposition of
+// Fe = I + H + dFc (scaled Newton where det > 0, SVD otherwise), P, and
+// G = -3/dx^2 dt vol P Fe^T + m C.  Writes G and the polar factors R, S (for
+// the adjoint's k_adj_finalize) into the planes at Gp (stride ng) and P into Pp
+// unless it is null; returns G.  cfetch() gives C, fetched after the polar so
+// that it holds no registers through it.
+template <class CFetch>
+__device__ __forceinline__ m3<float> stress_particle(const WArgs& a, int p, const m3<float>& H, const m3<float>& dfc,
+                                                     const CFetch& cfetch, float* Gp, size_t ng, float* Pp) {
+    const size_t np = a.np;
+    const m3<float> Fe = fe_from_strain(H, dfc);
+    const m3<double> Fed = fe_from_strain_d(H, dfc);
+    m3<double> Rd, Sd;
+    if (!DMPM_NEWTON_POLAR || !polar_newton(Fed, Rd, Sd)) polar3(Fed, Rd, Sd);
+    const m3<double> Pd = pk_from_polar(Fed, Rd, (double)a.cst[(size_t)KLAM * np + p], (double)a.cst[(size_t)KMU * np + p]);
+    const m3<float> P = m3_cast<float>(Pd);
+    if (Pp) store_m3(Pp, ng, p, P);
+    store_m3(Gp + 9 * ng, ng, p, m3_cast<float>(Rd));
+    Gp[18 * ng + p] = (float)Sd.a[0][0];
+    Gp[19 * ng + p] = (float)Sd.a[0][1];
+    Gp[20 * ng + p] = (float)Sd.a[0][2];
+    Gp[21 * ng + p] = (float)Sd.a[1][1];
+    Gp[22 * ng + p] = (float)Sd.a[1][2];
+    Gp[23 * ng + p] = (float)Sd.a[2][2];
+    const float dx = (float)a.geo.dx;
+    const float k = -3.f / (dx * dx) * a.dt * a.cst[(size_t)KVOL * np + p];
+    const m3<float> G = (k * P) * transpose(Fe) + a.cst[(size_t)KM * np + p] * cfetch();
+    store_m3(Gp, ng, p, G);
+    return G;
+}
+
 // DET: also raise the deterministic mode's P2G bounds (fixpoint.cuh) in a.fixb.
 template <bool DET = false> __global__ void __launch_bounds__(256, DMPM_STRESS_MIN_BLOCKS) k_stress(WArgs a) {
     const size_t np = a.np, npl = a.npl;
@@ -424,26 +460,10 @@ template <bool DET = false> __global__ void __launch_bounds__(256, DMPM_STRESS_M
     float cmom = 0.f, cmass = 0.f;
     if (p < a.n) {
         const m3<float> H = load_m3(a.st + (size_t)PF * npl, npl, p), dfc = load_m3(a.dfc, np, p);
-        const m3<float> Fe = fe_from_strain(H, dfc);
-        const m3<double> Fed = fe_from_strain_d(H, dfc);
-        m3<double> Rd, Sd;
-        if (!DMPM_NEWTON_POLAR || !polar_newton(Fed, Rd, Sd)) polar3(Fed, Rd, Sd);
-        const m3<double> Pd = pk_from_polar(Fed, Rd, (double)a.cst[(size_t)KLAM * np + p], (double)a.cst[(size_t)KMU * np + p]);
-        const m3<float> P = m3_cast<float>(Pd);
-        if (a.P) store_m3(a.P, npl, p, P);
-        // polar factors for the adjoint (k_adj_finalize)
-        store_m3(a.G + 9 * npl, npl, p, m3_cast<float>(Rd));
-        a.G[18 * npl + p] = (float)Sd.a[0][0];
-        a.G[19 * npl + p] = (float)Sd.a[0][1];
-        a.G[20 * npl + p] = (float)Sd.a[0][2];
-        a.G[21 * npl + p] = (float)Sd.a[1][1];
-        a.G[22 * npl + p] = (float)Sd.a[1][2];
-        a.G[23 * npl + p] = (float)Sd.a[2][2];
-        const float dx = (float)a.geo.dx;
-        const float k = -3.f / (dx * dx) * a.dt * a.cst[(size_t)KVOL * np + p];
-        const m3<float> G = (k * P) * transpose(Fe) + a.cst[(size_t)KM * np + p] * load_m3(a.st + (size_t)PC * npl, npl, p);
-        store_m3(a.G, npl, p, G);
+        const m3<float> G = stress_particle(
+            a, p, H, dfc, [&]() { return load_m3(a.st + (size_t)PC * npl, npl, p); }, a.G, npl, a.P);
         if constexpr (DET) {
+            const float dx = (float)a.geo.dx;
             // bound on P2G's per-particle values: |m v damp + G d| with |d| < 2 dx, and m
             const float mp = a.cst[(size_t)KM * np + p], damp = 1.f - a.dt * a.drag;
 #pragma unroll

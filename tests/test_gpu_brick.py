@@ -10,6 +10,7 @@ them."""
 import numpy as np
 import pytest
 
+import dmpm
 import scenes
 from oracle.lib import OracleGraph
 from tests.helpers import normrel, relerr
@@ -164,3 +165,23 @@ def test_brick_kernels_with_checkpointing_and_graphs(gpu_ready, case, brick):
             ref = g
         else:
             assert normrel(g, ref) < 1e-4, kw  # float atomics: summation order differs run to run
+
+
+@pytest.mark.parametrize("ckpt", [1, 3])
+@pytest.mark.parametrize("brick", [0] + BRICKS)
+def test_stress_stage_formed_by_g2p_matches_oracle(gpu_ready, case, brick, ckpt):
+    """With the brick G2P (brick_cells 2 or 4) each step's G2P also forms the next
+    step's stress stage (P, the polar factors and G), which the next step then
+    does not recompute; with warp items (0) a separate kernel forms it.  The
+    per-layer P (keep_intermediates) of every layer against the FP64 oracle,
+    store-all and checkpointed (segments recomputed during the backward pass)."""
+    sc, o, loss, L = case
+    with make_ctx(sc, "fp32", o.target, adjoint="exact", keep_intermediates=True, brick_cells=brick,
+                  checkpoint_every=ckpt) as c:
+        c.setup(L)
+        assert c.forward(0) == dmpm.OK
+        c.loss()
+        assert c.backward(0) == dmpm.OK
+        for lay in range(L - 1):
+            assert normrel(c.get(lay, "P"), o.get(lay, "P")) < 1e-3, lay
+        assert normrel(c.get(0, "dLdFe"), o.get(0, "dLdFe")) < 1e-3
