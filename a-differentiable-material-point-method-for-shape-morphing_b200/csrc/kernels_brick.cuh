@@ -22,6 +22,10 @@
 // followed by one vector red.global.add per node.
 // A particle that has left the unit since the sort (the sort runs every few
 // steps) is handled by the same code with its nodes read from global memory.
+// The G2P thread also forms the next step's stress stage (the FP64 polar
+// decomposition, P and G of layer n + 1) from the strain and C it has just
+// written, so the forward step after it skips the stress kernel: 62.3 against
+// 36.7 + 30.0 us per step on the 64^3, 267k-particle workload.
 //
 // Math per stage is that of kernels.cuh (which cites the reference) and of the
 // warp-item kernels in kernels_warp.cuh, summed in a different order.
