@@ -294,7 +294,18 @@ __device__ __forceinline__ void fix_tile_begin(FixTile& ft, long long* tile, uin
     __syncthreads();
 }
 
-template <int B, bool GENERAL> __global__ void __launch_bounds__(DMPM_BRICK_THREADS) k_p2g_fix_b(WArgs a) {
+// resident CTAs per SM the compiler budgets registers for (6: 80 registers;
+// measured per step on the 64^3, 267k-particle workload: P2G 105.6 us at 6,
+// 110.0 at 8 (64 registers, spills), 116 at the compiler's own choice of 95
+// registers; the scatter 104.2 / 106.3 / 118)
+#ifndef DMPM_FIX_P2G_MINB
+#define DMPM_FIX_P2G_MINB 6
+#endif
+#ifndef DMPM_FIX_SCATTER_MINB
+#define DMPM_FIX_SCATTER_MINB 6
+#endif
+template <int B, bool GENERAL>
+__global__ void __launch_bounds__(DMPM_BRICK_THREADS, DMPM_FIX_P2G_MINB) k_p2g_fix_b(WArgs a) {
     __shared__ long long tile[4 * BrickShape<B>::NT];
     const int nun = (int)*a.n_units_dev;
     const FixScale sp = fix_scale(a.fixb + FIXB_MOMENTUM, a.n), sm = fix_scale(a.fixb + FIXB_MASS, a.n);
@@ -310,7 +321,7 @@ template <int B, bool GENERAL> __global__ void __launch_bounds__(DMPM_BRICK_THRE
 }
 
 template <int B, bool EXACT, bool GENERAL>
-__global__ void __launch_bounds__(DMPM_BRICK_THREADS) k_adj_scatter_fix_b(WArgs a) {
+__global__ void __launch_bounds__(DMPM_BRICK_THREADS, DMPM_FIX_SCATTER_MINB) k_adj_scatter_fix_b(WArgs a) {
     __shared__ long long tile[4 * BrickShape<B>::NT];
     const int nun = (int)*a.n_units_dev;
     const FixScale sa = fix_scale(a.fixb + FIXB_ADJ, a.n);
