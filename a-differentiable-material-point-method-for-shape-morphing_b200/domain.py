@@ -25,7 +25,8 @@ then runs, per rank:
 
 All traffic is point-to-point between neighbouring ranks with
 torch.distributed isend / irecv (NCCL for device tensors over NVLink, gloo for
-host tensors); no collective, no TMA, no multicast.  Each slab must be at
+host tensors); no collective and no copy that reads another GPU's memory
+from inside a kernel.  Each slab must be at
 least two planes wide.  The grids are tensors of shape (planes, dim_y, dim_z,
 channels) in the node order of the engine (plane-major), so a plane is one
 contiguous block.
