@@ -50,6 +50,8 @@ class CompGraph {
     // engine controls (not in the reference)
     void SetSimulationParameters(float dt, float drag, Vec3 f_ext, float smoothing_factor);
     void SetEngineOptions(int precision, int adjoint_mode, int device = 0);
+    // FP32-mixed path: integer node sums, so passes repeat bit for bit (dmpm_params::deterministic)
+    void SetDeterministic(bool on);
     bool sync_grids = true;  // copy every layer's grid and stress P back after each pass
 
    private:
@@ -71,6 +73,7 @@ class CompGraph {
     int precision_ = 1;  // DMPM_FP32_MIXED
     int adjoint_mode_ = 0;
     int device_ = 0;
+    bool deterministic_ = false;
     dmpm_ctx* ctx_ = nullptr;
     int ctx_layers_ = 0;
 };

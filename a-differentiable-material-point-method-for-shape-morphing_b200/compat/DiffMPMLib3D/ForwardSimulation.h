@@ -25,6 +25,9 @@ void CalculatePointCloudVolumes(PointCloud& curr_point_cloud, Grid& grid);
 
 // Engine path for the functions above (DMPM_FP32_MIXED by default, or DMPM_FP64).
 void SetEnginePrecision(int precision);
+// FP32-mixed path: node sums as integers (dmpm_params::deterministic), so the
+// functions above give the same bits on every call with the same inputs.
+void SetEngineDeterministic(bool on);
 
 // Mass transfer for headless surfacing (float on the GPU, dmpm_surface_*):
 // node masses of `grid` from points of mass mp_m (ForwardSimulation.cpp:292-327)

@@ -63,9 +63,15 @@ void set_grid(dmpm_ctx* h, const Grid& g) {
     check(h, dmpm_set_grid(h, g.dim_x, g.dim_y, g.dim_z, g.dx, mn), "dmpm_set_grid");
 }
 
-void set_params(dmpm_ctx* h, float dt, float drag, Vec3 f, float s, int adjoint, int keep_adj, int keep_int) {
+int g_stage_precision = DMPM_FP32_MIXED;
+int g_stage_deterministic = 0;
+
+// det < 0: the stage functions' setting (SingleThreadMPM::SetEngineDeterministic)
+void set_params(dmpm_ctx* h, float dt, float drag, Vec3 f, float s, int adjoint, int keep_adj, int keep_int,
+                int det = -1) {
     dmpm_params p;
     dmpm_default_params(&p);
+    p.deterministic = det < 0 ? g_stage_deterministic : det;
     p.dt = dt;
     p.drag = drag;
     p.f_ext[0] = f[0]; p.f_ext[1] = f[1]; p.f_ext[2] = f[2];
@@ -149,8 +155,6 @@ std::vector<double> to_cm_doubles(const std::vector<Mat3>& M) {
         for (int q = 0; q < 9; q++) a[9 * p + q] = M[p].data()[q];
     return a;
 }
-
-int g_stage_precision = DMPM_FP32_MIXED;
 
 }  // namespace
 
@@ -636,6 +640,7 @@ void P_op_1(PointCloud& pc) {
 void G_Reset(Grid& grid) { grid.ResetValues(); }
 
 void SetEnginePrecision(int precision) { g_stage_precision = precision; }
+void SetEngineDeterministic(bool on) { g_stage_deterministic = on ? 1 : 0; }
 
 // Adds this cloud's P2G mass and momentum to the grid (the reference
 // accumulates without resetting, ForwardSimulation.cpp:174-182).  The stress
@@ -746,8 +751,8 @@ void CalculatePointCloudVolumes(PointCloud& pc, Grid& grid) {
     Ctx c(g_stage_precision);
     set_grid(c.h, grid);
     check(c.h, dmpm_set_points_ref(c.h, pc.points.data(), (int)pc.points.size()), "dmpm_set_points_ref");
+    set_params(c.h, 0.f, 0.f, Vec3::Zero(), 0.f, DMPM_ADJ_REFCOMPAT, 0, 0);  // before: the raster reads the mode
     check(c.h, dmpm_compute_volumes(c.h), "dmpm_compute_volumes");
-    set_params(c.h, 0.f, 0.f, Vec3::Zero(), 0.f, DMPM_ADJ_REFCOMPAT, 0, 0);
     check(c.h, dmpm_setup(c.h, 1), "dmpm_setup");
     std::vector<double> vol(pc.points.size());
     check(c.h, dmpm_get_particles(c.h, 0, DMPM_F_VOL, vol.data()), "dmpm_get_particles");
@@ -831,6 +836,11 @@ void CompGraph::SetEngineOptions(int precision, int adjoint_mode, int device) {
     ctx_layers_ = 0;
 }
 
+void CompGraph::SetDeterministic(bool on) {
+    deterministic_ = on;
+    ctx_layers_ = 0;  // the next pass sets the graph up again with the mode
+}
+
 void CompGraph::EnsureEngine() {
     if (!ctx_) check(nullptr, dmpm_create(device_, precision_, &ctx_), "dmpm_create");
 }
@@ -851,7 +861,7 @@ void CompGraph::SetUpCompGraph(int num_layers) {
     std::vector<double> tm(num_nodes(*target_grid));
     for_nodes(*target_grid, [&](const GridNode& n, size_t i) { tm[i] = n.m; });
     check(ctx_, dmpm_set_target_mass(ctx_, tm.data()), "dmpm_set_target_mass");
-    set_params(ctx_, dt, drag, f_ext, smoothing_factor, adjoint_mode_, 1, 0);
+    set_params(ctx_, dt, drag, f_ext, smoothing_factor, adjoint_mode_, 1, 0, deterministic_ ? 1 : 0);
     check(ctx_, dmpm_setup(ctx_, num_layers), "dmpm_setup");
     ctx_layers_ = num_layers;
 }

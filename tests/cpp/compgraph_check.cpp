@@ -19,7 +19,8 @@ using namespace DiffMPMLib3D;
 static void put(std::FILE* f, double v) { std::fwrite(&v, sizeof(double), 1, f); }
 
 int main(int argc, char** argv) {
-    if (argc != 13) return 2;
+    if (argc != 13 && argc != 14) return 2;
+    const bool det = argc == 14 && std::atoi(argv[13]) != 0;  // integer node sums (repeatable bits)
     const int precision = std::atoi(argv[4]), dim = std::atoi(argv[5]), L = std::atoi(argv[6]);
     const float dt = std::atof(argv[7]), drag = std::atof(argv[8]), s = std::atof(argv[9]);
     const Vec3 f_ext(std::atof(argv[10]), std::atof(argv[11]), std::atof(argv[12]));
@@ -27,6 +28,7 @@ int main(int argc, char** argv) {
     auto tpc = std::make_shared<PointCloud>();
     if (!pc->ReadEntirePointCloudFromBinaryFile(argv[1]) || !tpc->ReadEntirePointCloudFromBinaryFile(argv[2])) return 3;
     SingleThreadMPM::SetEnginePrecision(precision);
+    SingleThreadMPM::SetEngineDeterministic(det);
     auto grid = std::make_shared<Grid>(dim, dim, dim, 1.0f, Vec3(0, 0, 0));
     SingleThreadMPM::CalculatePointCloudVolumes(*pc, *grid);
     auto target = std::make_shared<Grid>(*grid);
@@ -36,6 +38,7 @@ int main(int argc, char** argv) {
     CompGraph cg(pc, grid, target);
     cg.SetSimulationParameters(dt, drag, f_ext, s);
     cg.SetEngineOptions(precision, DMPM_ADJ_REFCOMPAT);
+    cg.SetDeterministic(det);
     cg.SetUpCompGraph(L);
     cg.ComputeForwardPass(0);
     const float loss = cg.EndLayerMassLoss();

@@ -33,7 +33,7 @@ def exe(tmp_path_factory):
     return str(out)
 
 
-def run(exe, tmp_path, precision):
+def run(exe, tmp_path, precision, deterministic=False, tag=""):
     sc = rollout_scene()
     z33 = np.zeros((sc.n, 3, 3))
     write_mpmbin(tmp_path / "cloud.mpmbin", sc.x, sc.v, sc.F, sc.C, z33, sc.m, np.zeros(sc.n), sc.lam, sc.mu, sc.dFc)
@@ -42,10 +42,10 @@ def run(exe, tmp_path, precision):
     eye = np.broadcast_to(np.eye(3), (nt, 3, 3))
     write_mpmbin(tmp_path / "target.mpmbin", sc.target_points, zt, eye, np.zeros((nt, 3, 3)), np.zeros((nt, 3, 3)),
                  np.full(nt, sc.target_mp), np.zeros(nt), np.zeros(nt), np.zeros(nt), np.zeros((nt, 3, 3)))
-    out = tmp_path / ("out%d.bin" % precision)
+    out = tmp_path / ("out%d%s.bin" % (precision, tag))
     args = [exe, str(tmp_path / "cloud.mpmbin"), str(tmp_path / "target.mpmbin"), str(out), str(precision),
             str(sc.dims[0]), str(ROLLOUT_LAYERS), repr(sc.dt), repr(sc.drag), repr(sc.smoothing),
-            *[repr(float(v)) for v in sc.f_ext]]
+            *[repr(float(v)) for v in sc.f_ext]] + (["1"] if deterministic else [])
     res = subprocess.run(args, capture_output=True, text=True, timeout=300)
     assert res.returncode == 0, res.stdout + res.stderr
     a = np.fromfile(out, dtype=np.float64)
@@ -94,6 +94,23 @@ def test_compgraph_cpp_fp32_mixed_close_to_reference(gpu_ready, exe, tmp_path):
     assert abs(r["loss"] - float(g["loss"])) / abs(float(g["loss"])) < 1e-4
     assert relerr(r["x_last"].reshape(-1, 3), g["x_%d" % (ROLLOUT_LAYERS - 1)]) < 1e-5
     assert normrel(cm(r["dLdF0"]), g["dLdF_0"]) < 1e-2
+
+
+def test_compgraph_cpp_deterministic_repeats_bit_for_bit(gpu_ready, exe, tmp_path):
+    """SingleThreadMPM::SetEngineDeterministic and CompGraph::SetDeterministic:
+    the FP32-mixed path with integer node sums, in two processes on the same
+    inputs -- volumes, loss, states and adjoints the same bits, and at the FP32
+    path's distance from the reference."""
+    g = load_golden("rollout_f64")
+    a, sc = run(exe, tmp_path, dmpm.FP32_MIXED, deterministic=True, tag="a")
+    b, _ = run(exe, tmp_path, dmpm.FP32_MIXED, deterministic=True, tag="b")
+    for k in ("vol", "x_last", "dLdF0", "dLdx0", "x1_standalone", "dLdF0_back_timestep", "P0"):
+        assert np.array_equal(a[k], b[k]), k
+    assert a["loss"] == b["loss"]
+    assert relerr(a["vol"], g["vol"]) < 1e-5
+    assert abs(a["loss"] - float(g["loss"])) / abs(float(g["loss"])) < 1e-4
+    assert relerr(a["x_last"].reshape(-1, 3), g["x_%d" % (ROLLOUT_LAYERS - 1)]) < 1e-5
+    assert normrel(cm(a["dLdF0"]), g["dLdF_0"]) < 1e-2
 
 
 def test_stage_level_api_composes_the_fused_step(gpu_ready, tmp_path):
