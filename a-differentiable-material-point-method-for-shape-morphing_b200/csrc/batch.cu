@@ -46,7 +46,7 @@ constexpr int kDefaultSortEvery = 8;
 constexpr int kDefaultCtasPerSm = 3;
 
 // cell key of each particle of the active prefix: its instance's key offset +
-// the one-scene key of sort.cuh (floor division, clamped base)
+// the one-scene key of sort.cuh (the stencil base the warp-item kernels form)
 __global__ void k_cell_keys_batch(int n, size_t np, const float* __restrict__ st, const uint16_t* __restrict__ pinst,
                                   const InstGeo* __restrict__ ig, uint32_t* keys, uint32_t* vals) {
     const int p = blockIdx.x * blockDim.x + threadIdx.x;
@@ -55,7 +55,7 @@ __global__ void k_cell_keys_batch(int n, size_t np, const float* __restrict__ st
     int base[3];
 #pragma unroll
     for (int c = 0; c < 3; c++)
-        base[c] = stencil_base<float>(st[(size_t)(PX + c) * np + p] - (float)g.g.mn[c], (float)g.g.dx, g.g.dim[c]);
+        (void)stencil_coord<float>(load_xd(st, np, p, c, 1), g.g.mn[c], 1.0 / g.g.dx, g.g.dim[c], base[c]);
     keys[p] = g.koff + cell_key(base, g.g.dim);
     vals[p] = (uint32_t)p;
 }
@@ -233,7 +233,7 @@ struct dmpm_batch::Impl {
         dmpm_default_params(&prm);
         prm.adjoint_mode = DMPM_ADJ_EXACT;
         // scene storage
-        st0 = (float*)scene.alloc((size_t)NSTATE * np0 * sizeof(float));
+        st0 = (float*)scene.alloc((size_t)NSTATE_X * np0 * sizeof(float));
         cst = (float*)scene.alloc((size_t)NCONST * np0 * sizeof(float));
         dfc = (float*)scene.alloc((size_t)9 * np0 * sizeof(float));
         pinst = (uint16_t*)scene.alloc(np0 * sizeof(uint16_t));
@@ -243,7 +243,7 @@ struct dmpm_batch::Impl {
         scratch = (node4<float>*)scene.alloc(Gtot * sizeof(node4<float>));
         loss_acc = (double*)scene.alloc(cnt * sizeof(double));
         status = (unsigned*)scene.alloc(16);
-        DMPM_CK(cudaMemsetAsync(st0, 0, (size_t)NSTATE * np0 * sizeof(float), b->stream));
+        DMPM_CK(cudaMemsetAsync(st0, 0, (size_t)NSTATE_X * np0 * sizeof(float), b->stream));
         DMPM_CK(cudaMemsetAsync(cst, 0, (size_t)NCONST * np0 * sizeof(float), b->stream));
         DMPM_CK(cudaMemsetAsync(dfc, 0, (size_t)9 * np0 * sizeof(float), b->stream));
         DMPM_CK(cudaMemsetAsync(target, 0, Gtot * sizeof(float), b->stream));
@@ -304,7 +304,13 @@ struct dmpm_batch::Impl {
         const Inst& s = user_inst(u);
         const int n = s.n;
         float* l0 = st0 + s.poff;
-        upload(x, n, 3, l0 + (size_t)PX * np0, np0);
+        {  // compensated positions: hi and lo planes
+            double* sx = stage((size_t)n * 3);
+            DMPM_CK(cudaMemcpyAsync(sx, x, (size_t)n * 3 * sizeof(double), cudaMemcpyHostToDevice, b->stream));
+            k_unpack_x2<<<(unsigned)(((size_t)n * 3 + 255) / 256), 256, 0, b->stream>>>(
+                sx, n, l0 + (size_t)PX * np0, l0 + (size_t)PXL * np0, np0);
+            launched();
+        }
         if (v) upload(v, n, 3, l0 + (size_t)PV * np0, np0);
         else for (int c = 0; c < 3; c++) DMPM_CK(cudaMemsetAsync(l0 + (size_t)(PV + c) * np0, 0, n * sizeof(float), b->stream));
         std::vector<double> eye;
@@ -382,7 +388,7 @@ struct dmpm_batch::Impl {
 
     size_t layer_bytes() const {
         size_t tot = 0;
-        for (int t = 1; t <= smax; t++) tot += (size_t)NSTATE * S[t] * 4;                 // states
+        for (int t = 1; t <= smax; t++) tot += (size_t)NSTATE_X * S[t] * 4;               // states
         for (int t = 0; t < smax; t++) tot += (size_t)kAux * S[t] * 4 + node_prefix[A[t + 1]] * 16;  // aux, grids
         tot += 2 * (size_t)NSTATE * np0 * 4 + (12 + 18) * np0 * 4 + 9 * np0 * 8 + 3 * Gtot * 16;
         return tot;
@@ -403,7 +409,7 @@ struct dmpm_batch::Impl {
         aux.assign(smax, nullptr);
         grid.assign(smax, nullptr);
         st[0] = st0;
-        for (int t = 1; t <= smax; t++) st[t] = (float*)layers.alloc((size_t)NSTATE * S[t] * 4);
+        for (int t = 1; t <= smax; t++) st[t] = (float*)layers.alloc((size_t)NSTATE_X * S[t] * 4);
         for (int t = 0; t < smax; t++) {
             aux[t] = (float*)layers.alloc((size_t)kAux * S[t] * 4);
             grid[t] = (node4<float>*)layers.alloc(node_prefix[A[t + 1]] * sizeof(node4<float>));
@@ -496,6 +502,7 @@ struct dmpm_batch::Impl {
         a.item_inst = e.item_inst;
         a.st = st[t];
         a.st_next = st[t + 1];
+        a.xlo = 1;
         a.cst = cst;
         a.dfc = dfc;
         a.G = aux[t];
@@ -543,6 +550,7 @@ struct dmpm_batch::Impl {
         la.loss = loss_acc + k;
         la.kind = prm.loss_kind;
         la.tile_cap = 0;
+        la.xlo = 1;
         la.status = status;
         DMPM_CK(cudaMemsetAsync(la.grid, 0, s.G * sizeof(node4<float>), b->stream));
         k_p2g_mass<float, false><<<(s.n + 255) / 256, 256, 0, b->stream>>>(la);
@@ -721,7 +729,15 @@ struct dmpm_batch::Impl {
         const float* base = (layer == 0 ? st0 : st[layer]) + s.poff;
         const size_t np = S[layer];
         switch (field) {
-            case DMPM_F_X: download(base + (size_t)PX * np, np, s.n, 3, out); break;
+            case DMPM_F_X: {
+                double* sx = stage((size_t)s.n * 3);
+                k_pack_x2<<<(unsigned)(((size_t)s.n * 3 + 255) / 256), 256, 0, b->stream>>>(
+                    base + (size_t)PX * np, base + (size_t)PXL * np, np, s.n, sx);
+                launched();
+                DMPM_CK(cudaMemcpyAsync(out, sx, (size_t)s.n * 3 * sizeof(double), cudaMemcpyDeviceToHost, b->stream));
+                DMPM_CK(cudaStreamSynchronize(b->stream));
+                break;
+            }
             case DMPM_F_V: download(base + (size_t)PV * np, np, s.n, 3, out); break;
             case DMPM_F_F: download(base + (size_t)PF * np, np, s.n, 9, out, 1.0); break;
             case DMPM_F_C: download(base + (size_t)PC * np, np, s.n, 9, out); break;

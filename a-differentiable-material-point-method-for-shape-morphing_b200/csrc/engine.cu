@@ -234,6 +234,9 @@ template <class T> class Engine : public EngineBase {
     static constexpr bool kWarp = kTiled;
     // the FP32 path stores each layer's strain H = F - I in the F planes (kernels_warp.cuh)
     static constexpr bool kStrain = kWarp;
+    // state planes per layer: the FP32 path adds the low parts of its
+    // compensated positions (PXL); adjoint layers keep NSTATE planes
+    static constexpr int kNst = kWarp ? (int)NSTATE_X : (int)NSTATE;
     // one cell sort: the stable order and warp items used for steps
     // [e * sort_every, (e + 1) * sort_every)
     struct Epoch {
@@ -287,7 +290,7 @@ template <class T> class Engine : public EngineBase {
         if (n == n_ && cst_) {
             // same cloud size: overwrite in place and keep the layer storage
             DMPM_CK(cudaMemsetAsync(cst_, 0, NCONST * np_ * sizeof(T), ctx_->stream));
-            DMPM_CK(cudaMemsetAsync(st0_, 0, NSTATE * np_ * sizeof(T), ctx_->stream));
+            DMPM_CK(cudaMemsetAsync(st0_, 0, kNst * np_ * sizeof(T), ctx_->stream));
             DMPM_CK(cudaMemsetAsync(dfc0_, 0, 9 * np_ * sizeof(T), ctx_->stream));
             return;
         }
@@ -298,10 +301,10 @@ template <class T> class Engine : public EngineBase {
         layout_ = Layout{};
         scene_arena_.release();
         cst_ = (T*)scene_arena_.alloc(NCONST * np_ * sizeof(T));
-        st0_ = (T*)scene_arena_.alloc(NSTATE * np_ * sizeof(T));
+        st0_ = (T*)scene_arena_.alloc(kNst * np_ * sizeof(T));
         dfc0_ = (T*)scene_arena_.alloc(9 * np_ * sizeof(T));
         DMPM_CK(cudaMemsetAsync(cst_, 0, NCONST * np_ * sizeof(T), ctx_->stream));
-        DMPM_CK(cudaMemsetAsync(st0_, 0, NSTATE * np_ * sizeof(T), ctx_->stream));
+        DMPM_CK(cudaMemsetAsync(st0_, 0, kNst * np_ * sizeof(T), ctx_->stream));
         DMPM_CK(cudaMemsetAsync(dfc0_, 0, 9 * np_ * sizeof(T), ctx_->stream));
     }
 
@@ -328,6 +331,31 @@ template <class T> class Engine : public EngineBase {
         launched();
     }
 
+    // positions: compensated planes (hi, lo) on the FP32 path, plain planes otherwise
+    void upload_x(const double* host, T* st) {
+        if constexpr (kWarp) {
+            double* s = staging((size_t)n_ * 3);
+            DMPM_CK(cudaMemcpyAsync(s, host, (size_t)n_ * 3 * sizeof(double), cudaMemcpyHostToDevice, ctx_->stream));
+            k_unpack_x2<<<(unsigned)(((size_t)n_ * 3 + 255) / 256), 256, 0, ctx_->stream>>>(
+                s, n_, (float*)st + (size_t)PX * np_, (float*)st + (size_t)PXL * np_, np_);
+            launched();
+        } else {
+            upload_planes(host, 3, st + (size_t)PX * np_);
+        }
+    }
+    void download_x(const T* st, double* host) {
+        if constexpr (kWarp) {
+            double* s = staging((size_t)n_ * 3);
+            k_pack_x2<<<(unsigned)(((size_t)n_ * 3 + 255) / 256), 256, 0, ctx_->stream>>>(
+                (const float*)st + (size_t)PX * np_, (const float*)st + (size_t)PXL * np_, np_, n_, s);
+            launched();
+            DMPM_CK(cudaMemcpyAsync(host, s, (size_t)n_ * 3 * sizeof(double), cudaMemcpyDeviceToHost, ctx_->stream));
+            DMPM_CK(cudaStreamSynchronize(ctx_->stream));
+        } else {
+            download_planes(st + (size_t)PX * np_, 3, host);
+        }
+    }
+
     void download_planes(const T* src, int width, double* host, double diag = 0.0) {
         double* s = staging((size_t)n_ * width);
         const size_t tot = (size_t)n_ * width;
@@ -345,7 +373,7 @@ template <class T> class Engine : public EngineBase {
                        const double* m, const double* vol, const double* lam, const double* mu) {
         if (!x || !m || !lam || !mu) throw ArgError{"x, m, lam and mu are required"};
         alloc_particles(n);
-        upload_planes(x, 3, st0_ + (size_t)PX * np_);
+        upload_x(x, st0_);
         if (v) upload_planes(v, 3, st0_ + (size_t)PV * np_);
         if (F) {
             upload_planes(F, 9, st0_ + (size_t)PF * np_, kStrain ? -1.0 : 0.0);
@@ -403,6 +431,7 @@ template <class T> class Engine : public EngineBase {
         a.dldm = dldm_;
         a.kind = ctx_->prm.loss_kind;
         a.tile_cap = tile_cap();
+        a.xlo = kWarp ? 1 : 0;
         a.status = status_;
         return a;
     }
@@ -628,6 +657,7 @@ template <class T> class Engine : public EngineBase {
             a.n = n;
             a.np = a.npc = npt;
             a.st = st;
+            a.xlo = 0;  // target samples: plain float positions
             a.cst = cst;
             a.grid = scratch_grid_;
             launch_mass(a);
@@ -692,7 +722,8 @@ template <class T> class Engine : public EngineBase {
         L_ = num_layers;
         layer_arena_.release();
         layers_.assign(L_, LayerSlots{});
-        const size_t st_bytes = NSTATE * np_ * sizeof(T);
+        const size_t st_bytes = kNst * np_ * sizeof(T);
+        const size_t adj_bytes = NSTATE * np_ * sizeof(T);
         const size_t gr_bytes = G_ * sizeof(node4<T>);
         const bool per_layer = P.control_mode == DMPM_CTRL_PER_LAYER;
         // choose the checkpoint interval
@@ -702,7 +733,7 @@ template <class T> class Engine : public EngineBase {
             DMPM_CK(cudaMemGetInfo(&free_b, &total_b));
             const double need = (double)L_ * (st_bytes + gr_bytes) +
                                 (per_layer ? 2.0 * num_control_layers() * 9 * np_ * sizeof(T) : 0.0) +
-                                (P.keep_adjoints ? (double)L_ * st_bytes : 0.0);
+                                (P.keep_adjoints ? (double)L_ * adj_bytes : 0.0);
             k = need < 0.8 * (double)free_b ? 1 : std::max(2, (int)std::ceil(std::sqrt((double)L_)));
         }
         k_ = std::min(k, std::max(1, L_ - 1));
@@ -712,7 +743,7 @@ template <class T> class Engine : public EngineBase {
         for (int l = 0; l < L_; l++) nstored += stored(l) ? 1 : 0;
         T* sbase = (T*)layer_arena_.alloc((size_t)nstored * st_bytes);
         for (int l = 0, s = 0; l < L_; l++)
-            if (stored(l)) layers_[l].st = sbase + (size_t)(s++) * NSTATE * np_;
+            if (stored(l)) layers_[l].st = sbase + (size_t)(s++) * kNst * np_;
         if (k_ > 1) {
             ring_[0] = (T*)layer_arena_.alloc(st_bytes);
             ring_[1] = (T*)layer_arena_.alloc(st_bytes);
@@ -748,12 +779,12 @@ template <class T> class Engine : public EngineBase {
         }
         // adjoints
         if (P.keep_adjoints) {
-            T* abase = (T*)layer_arena_.alloc((size_t)L_ * st_bytes);
-            DMPM_CK(cudaMemsetAsync(abase, 0, (size_t)L_ * st_bytes, ctx_->stream));
+            T* abase = (T*)layer_arena_.alloc((size_t)L_ * adj_bytes);
+            DMPM_CK(cudaMemsetAsync(abase, 0, (size_t)L_ * adj_bytes, ctx_->stream));
             for (int l = 0; l < L_; l++) layers_[l].adj = abase + (size_t)l * NSTATE * np_;
         } else {
-            adj_pp_[0] = (T*)layer_arena_.alloc(st_bytes);
-            adj_pp_[1] = (T*)layer_arena_.alloc(st_bytes);
+            adj_pp_[0] = (T*)layer_arena_.alloc(adj_bytes);
+            adj_pp_[1] = (T*)layer_arena_.alloc(adj_bytes);
         }
         gadj_ = (node4<T>*)layer_arena_.alloc(gr_bytes);
         gadj2_ = (node4<T>*)layer_arena_.alloc(2 * gr_bytes);
@@ -808,7 +839,7 @@ template <class T> class Engine : public EngineBase {
     // states other than 0 are not copied: each is written by the forward pass
     // before anything reads it.
     void reset_layers() {
-        const size_t st_bytes = NSTATE * np_ * sizeof(T);
+        const size_t st_bytes = kNst * np_ * sizeof(T);
         DMPM_CK(cudaMemcpyAsync(layers_[0].st, st0_, st_bytes, cudaMemcpyDeviceToDevice, ctx_->stream));
         if (ctx_->prm.control_mode == DMPM_CTRL_PER_LAYER) {
             for (int l = 0; l < L_; l++) {
@@ -875,6 +906,7 @@ template <class T> class Engine : public EngineBase {
         ka.np = np_;
         ka.geo = geo_;
         ka.st = st;
+        ka.xlo = kWarp ? 1 : 0;
         ka.keys = sk_[0];
         ka.vals = sv_[0];
         k_cell_keys<T><<<(n + 255) / 256, 256, 0, ctx_->stream>>>(ka);
@@ -960,6 +992,7 @@ template <class T> class Engine : public EngineBase {
         a.s = (float)P.smoothing;
         for (int c = 0; c < 3; c++) a.fext[c] = (float)P.f_ext[c];
         a.cst = (const float*)cst_;
+        a.xlo = 1;
         a.status = status_;
         return a;
     }
@@ -1455,7 +1488,7 @@ template <class T> class Engine : public EngineBase {
             return p;
         };
         switch (field) {
-            case DMPM_F_X: download_planes(materialize_state(l) + (size_t)PX * np_, 3, out); break;
+            case DMPM_F_X: download_x(materialize_state(l), out); break;
             case DMPM_F_V: download_planes(materialize_state(l) + (size_t)PV * np_, 3, out); break;
             case DMPM_F_F: download_planes(materialize_state(l) + (size_t)PF * np_, 9, out, kStrain ? 1.0 : 0.0); break;
             case DMPM_F_C: download_planes(materialize_state(l) + (size_t)PC * np_, 9, out); break;
@@ -1505,7 +1538,11 @@ template <class T> class Engine : public EngineBase {
                 break;
             case DMPM_F_X: case DMPM_F_V: case DMPM_F_F: case DMPM_F_C: {
                 if (!layers_[l].st) throw StateError{"layer state is not stored (checkpointing)"};
-                const int off = field == DMPM_F_X ? PX : field == DMPM_F_V ? PV : field == DMPM_F_F ? PF : PC;
+                if (field == DMPM_F_X) {
+                    upload_x(in, layers_[l].st);
+                    break;
+                }
+                const int off = field == DMPM_F_V ? PV : field == DMPM_F_F ? PF : PC;
                 upload_planes(in, (field == DMPM_F_X || field == DMPM_F_V) ? 3 : 9, layers_[l].st + (size_t)off * np_,
                               (field == DMPM_F_F && kStrain) ? -1.0 : 0.0);
                 break;

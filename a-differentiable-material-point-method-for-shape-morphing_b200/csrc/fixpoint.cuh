@@ -125,18 +125,11 @@ static __global__ void __launch_bounds__(256) k_p2g_mass_fix(LossArgs<float> a, 
     const int p = blockIdx.x * blockDim.x + threadIdx.x;
     if (p >= a.n) return;
     const FixScale sr = fix_scale(slots + FIXB_RASTER, a.n);
-    const float dx = (float)a.geo.dx;
-    float x[3];
     int base[3];
-#pragma unroll
-    for (int c = 0; c < 3; c++) {
-        x[c] = a.st[(size_t)(PX + c) * a.np + p];
-        base[c] = stencil_base<float>(x[c] - (float)a.geo.mn[c], dx, a.geo.dim[c]);
-    }
-    const float mp = a.cst[(size_t)KM * a.npc + p];
     axis_w<float> w[3];
 #pragma unroll
-    for (int c = 0; c < 3; c++) axis_weights(x[c], (float)a.geo.mn[c], dx, base[c], w[c], false);
+    for (int c = 0; c < 3; c++) particle_axis(a.st, a.np, p, c, a.xlo, a.geo, base[c], w[c], false);
+    const float mp = a.cst[(size_t)KM * a.npc + p];
 #pragma unroll 4
     for (int idx = 0; idx < 64; idx++) {
         const int di = idx >> 4, dj = (idx >> 2) & 3, dk = idx & 3;

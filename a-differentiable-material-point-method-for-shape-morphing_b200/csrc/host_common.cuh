@@ -92,6 +92,25 @@ template <class T> __global__ void k_pack(const T* __restrict__ src, size_t np, 
     const int p = (int)(i / width), q = (int)(i % width);
     dst[i] = (double)src[(size_t)q * np + p];
 }
+// n x 3 doubles to compensated position planes (three hi planes from hi, three
+// lo planes from lo, plane stride np): hi = the float nearest x, lo = the float
+// nearest x - hi; and back, x = hi + lo
+static __global__ void k_unpack_x2(const double* __restrict__ src, int n, float* hi, float* lo, size_t np) {
+    const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= (size_t)n * 3) return;
+    const size_t o = (i % 3) * np + i / 3;
+    const double x = src[i];
+    const float h = (float)x;
+    hi[o] = h;
+    lo[o] = (float)(x - (double)h);
+}
+static __global__ void k_pack_x2(const float* __restrict__ hi, const float* __restrict__ lo, size_t np, int n,
+                                 double* dst) {
+    const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= (size_t)n * 3) return;
+    const size_t o = (i % 3) * np + i / 3;
+    dst[i] = (double)hi[o] + (double)lo[o];
+}
 // add s to the diagonal (entries 0, 4, 8) of n 3x3 matrices stored as 9
 // consecutive doubles each: F <-> the FP32 path's strain planes H = F - I
 static __global__ void k_diag_add(double* a, int n, double s) {

@@ -26,6 +26,9 @@
 namespace dmpm {
 
 enum : int { PX = 0, PV = 3, PF = 6, PC = 15, NSTATE = 24 };
+// State planes of the FP32 engines: the 24 above plus the low parts of the
+// positions (compensated positions, below)
+enum : int { PXL = NSTATE, NSTATE_X = NSTATE + 3 };
 enum : int { KM = 0, KVOL = 1, KLAM = 2, KMU = 3, NCONST = 4 };
 enum : unsigned { ST_NONFINITE_FWD = 1u, ST_NONFINITE_ADJ = 2u, ST_NONFINITE_LOSS = 4u };
 
@@ -36,6 +39,43 @@ struct GridGeom {
     double dx;
     double mn[3];
 };
+
+// Compensated positions.  The FP32 engines (single scene and batch) keep each
+// position coordinate as two floats, x = hi + lo: hi in plane PX + c, lo (the float
+// nearest x - hi) in plane PXL + c, so a position carries about 48 bits instead
+// of float32's 24.  A stencil is formed from the lattice coordinate r =
+// (x - mn) / dx, taken in FP64 once per particle: base = floor(r) - 1 and
+// t = r - base, rounded to float.  For a particle inside the grid t lies in
+// [1, 2), so the node offsets q = s - t (s = 0..3) are exact in float and a
+// particle's weights are set to ~1e-7 of a cell, where the float position
+// (x - mn) / dx of a particle half a unit from the origin of a 64^3 grid is
+// rounded to ~4e-6 of a cell.  With xlo = 0 (the mass rasters of target
+// samples, which are plain float positions) lo is taken as 0.
+template <class T> __device__ __forceinline__ double load_xd(const T* st, size_t np, int p, int c, int xlo) {
+    const double h = (double)st[(size_t)(PX + c) * np + p];
+    return xlo ? h + (double)st[(size_t)(PXL + c) * np + p] : h;
+}
+// stencil base (stencil_base's clamp) and lattice coordinate t of one axis
+template <class T> __device__ __forceinline__ T stencil_coord(double x, double mn, double idx, int dim, int& base) {
+    const double r = (x - mn) * idx;
+    base = stencil_base_lattice<double>(r, dim);
+    return (T)(r - (double)base);
+}
+// one axis of a particle's stencil for the one-thread-per-particle kernels:
+// with xlo, base and weights from the compensated position; without, from the
+// stored position as the reference forms them (the FP64 path)
+template <class T>
+__device__ __forceinline__ void particle_axis(const T* st, size_t np, int p, int c, int xlo, const GridGeom& g,
+                                              int& base, axis_w<T>& w, bool slopes) {
+    if (xlo) {
+        const T t = stencil_coord<T>(load_xd(st, np, p, c, 1), g.mn[c], 1.0 / g.dx, g.dim[c], base);
+        axis_weights_lattice<T>(t, (T)g.dx, w, slopes);
+    } else {
+        const T x = st[(size_t)(PX + c) * np + p];
+        base = stencil_base<T>(x - (T)g.mn[c], (T)g.dx, g.dim[c]);
+        axis_weights<T>(x, (T)g.mn[c], (T)g.dx, base, w, slopes);
+    }
+}
 
 template <class T> DMPM_HD m3<T> load_m3(const T* base, size_t np, int i) {
     m3<T> r;
@@ -373,6 +413,7 @@ template <class T> struct LossArgs {
                          // each block adds to *loss
     int kind;            // 0 = reference log-mass + penalty, 1 = L2
     int tile_cap;
+    int xlo;             // st carries the low parts of compensated positions (planes PXL)
     unsigned* status;
 };
 
@@ -381,21 +422,14 @@ template <class T, bool TILED> __global__ void __launch_bounds__(256) k_p2g_mass
     extern __shared__ __align__(16) unsigned char smem_raw[];
     const int p = blockIdx.x * blockDim.x + threadIdx.x;
     const bool valid = p < a.n;
-    const T dx = (T)a.geo.dx;
-    T x[3] = {0, 0, 0};
     int base[3] = {0, 0, 0};
     T mp = 0;
+    axis_w<T> w[3];
     if (valid) {
 #pragma unroll
-        for (int c = 0; c < 3; c++) {
-            x[c] = a.st[(size_t)(PX + c) * a.np + p];
-            base[c] = stencil_base<T>(x[c] - (T)a.geo.mn[c], dx, a.geo.dim[c]);
-        }
+        for (int c = 0; c < 3; c++) particle_axis(a.st, a.np, p, c, a.xlo, a.geo, base[c], w[c], false);
         mp = a.cst[(size_t)KM * a.npc + p];
     }
-    axis_w<T> w[3];
-#pragma unroll
-    for (int c = 0; c < 3; c++) axis_weights(x[c], (T)a.geo.mn[c], dx, base[c], w[c], false);
     TileBox tb;
     tb.ok = false;
     T* tile = reinterpret_cast<T*>(smem_raw);
@@ -498,16 +532,10 @@ template <class T> __global__ void __launch_bounds__(256) k_loss_dldx(LossArgs<T
     const int p = blockIdx.x * blockDim.x + threadIdx.x;
     if (p >= a.n) return;
     const T dx = (T)a.geo.dx;
-    T x[3];
     int base[3];
-#pragma unroll
-    for (int c = 0; c < 3; c++) {
-        x[c] = a.st[(size_t)(PX + c) * a.np + p];
-        base[c] = stencil_base<T>(x[c] - (T)a.geo.mn[c], dx, a.geo.dim[c]);
-    }
     axis_w<T> w[3];
 #pragma unroll
-    for (int c = 0; c < 3; c++) axis_weights(x[c], (T)a.geo.mn[c], dx, base[c], w[c], true);
+    for (int c = 0; c < 3; c++) particle_axis(a.st, a.np, p, c, a.xlo, a.geo, base[c], w[c], true);
     const T mp = a.cst[(size_t)KM * a.npc + p];
     T acc[3] = {0, 0, 0};
     const T ndx = -T(1) / dx;
@@ -836,17 +864,10 @@ template <class T, bool TILED, bool EXACT> __global__ void __launch_bounds__(256
 template <class T> __global__ void k_volumes(LossArgs<T> a, T* vol_out) {
     const int p = blockIdx.x * blockDim.x + threadIdx.x;
     if (p >= a.n) return;
-    const T dx = (T)a.geo.dx;
-    T x[3];
     int base[3];
-#pragma unroll
-    for (int c = 0; c < 3; c++) {
-        x[c] = a.st[(size_t)(PX + c) * a.np + p];
-        base[c] = stencil_base<T>(x[c] - (T)a.geo.mn[c], dx, a.geo.dim[c]);
-    }
     axis_w<T> w[3];
 #pragma unroll
-    for (int c = 0; c < 3; c++) axis_weights(x[c], (T)a.geo.mn[c], dx, base[c], w[c], false);
+    for (int c = 0; c < 3; c++) particle_axis(a.st, a.np, p, c, a.xlo, a.geo, base[c], w[c], false);
     T mg = 0;
     for (int idx = 0; idx < 64; idx++) {
         const int di = idx >> 4, dj = (idx >> 2) & 3, dk = idx & 3;

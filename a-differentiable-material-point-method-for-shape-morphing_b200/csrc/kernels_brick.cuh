@@ -57,28 +57,25 @@ __device__ __forceinline__ void unit_origin(uint32_t ukey, int shift, const Grid
 }
 
 // Per-axis stencil offsets d = x_g - x, weights N(d / dx) and slopes of the
-// four nodes t = 0..3 of the stencil starting at base.
-__device__ __forceinline__ void axis_stencil(float x, float mn, float dx, float idx, int base, float n[4], float d[4],
-                                             float* s) {
+// four nodes k = 0..3 of the stencil, from the lattice coordinate t of the
+// particle (load_x_base): d = (k - t) dx.
+__device__ __forceinline__ void axis_stencil(float t, float dx, float n[4], float d[4], float* s) {
 #pragma unroll
-    for (int t = 0; t < 4; t++) {
-        const float xg = mn + (float)(base + t) * dx;
-        d[t] = xg - x;
-        const float q = d[t] * idx;
-        n[t] = bsp(q);
-        if (s) s[t] = bsp_slope(q);
+    for (int k = 0; k < 4; k++) {
+        const float q = (float)k - t;
+        d[k] = q * dx;
+        n[k] = bsp(q);
+        if (s) s[k] = bsp_slope(q);
     }
 }
 
-// Offset, weight and slope of stencil node t on one axis -- the slab and row
-// loops are not unrolled, so these come from x instead of per-node arrays.
+// Offset, weight and slope of stencil node k on one axis -- the slab and row
+// loops are not unrolled, so these come from t instead of per-node arrays.
 struct Axis0 {
-    float x, mn, dx, idx;
-    int base;
-    __device__ __forceinline__ void operator()(int t, float& n, float& d, float* s) const {
-        const float xg = mn + (float)(base + t) * dx;
-        d = xg - x;
-        const float q = d * idx;
+    float t, dx;
+    __device__ __forceinline__ void operator()(int k, float& n, float& d, float* s) const {
+        const float q = (float)k - t;
+        d = q * dx;
         n = bsp(q);
         if (s) *s = bsp_slope(q);
     }
@@ -195,7 +192,7 @@ __global__ void __launch_bounds__(DMPM_BRICK_THREADS, DMPM_BRICK_G2P_MINB) k_g2p
     const int nun = (int)*a.n_units_dev;
     const size_t np = a.np, npl = a.npl, npn = a.npn;
     const GridGeom geo = a.geo;
-    const float dx = (float)geo.dx, idx = 1.f / dx, k3 = 3.f / (dx * dx);
+    const float dx = (float)geo.dx, k3 = 3.f / (dx * dx);
     for (int u = blockIdx.x; u < nun; u += gridDim.x) {
         int o[3];
         unit_origin(a.unit_key[u], S::shift, geo, o);
@@ -205,13 +202,14 @@ __global__ void __launch_bounds__(DMPM_BRICK_THREADS, DMPM_BRICK_G2P_MINB) k_g2p
         __syncthreads();
         for (uint32_t q = q0 + threadIdx.x; q < q1; q += blockDim.x) {
             const int p = (int)a.items.order[q];
-            float x[3];
+            float t[3];
             int base[3];
-            load_x_base(a.st, npl, p, geo, x, base);
+            double xd[3];
+            load_x_base(a.st, npl, p, geo, t, base, a.xlo, xd);
             float n[3][4], d[3][4];
 #pragma unroll
-            for (int c = 1; c < 3; c++) axis_stencil(x[c], (float)geo.mn[c], dx, idx, base[c], n[c], d[c], nullptr);
-            const Axis0 ax0{x[0], (float)geo.mn[0], dx, idx, base[0]};
+            for (int c = 1; c < 3; c++) axis_stencil(t[c], dx, n[c], d[c], nullptr);
+            const Axis0 ax0{t[0], dx};
             float V[3], Cm[3][3];
             int l[3];
             if (in_unit<B>(base, o, l))
@@ -227,8 +225,7 @@ __global__ void __launch_bounds__(DMPM_BRICK_THREADS, DMPM_BRICK_G2P_MINB) k_g2p
             bool finite = true;
 #pragma unroll
             for (int c = 0; c < 3; c++) {
-                const float xn = x[c] + a.dt * V[c];
-                a.st_next[(size_t)(PX + c) * npn + p] = xn;
+                const float xn = store_x(a.st_next, npn, p, c, xd[c], a.dt, V[c], a.xlo);
                 a.st_next[(size_t)(PV + c) * npn + p] = V[c];
                 finite &= isfinite(xn);
             }

@@ -171,15 +171,13 @@ __device__ __forceinline__ float bsp_slope(float q) {
 // stencil node s on all three axes; axis-1 and axis-2 values of the other
 // nodes come from the sibling lanes by shuffles.  Every lane of the warp must
 // call this (full-mask shuffles).
-__device__ __forceinline__ void lane_weights(const float x[3], const GridGeom& g, const int base[3], int s, LaneW& w,
-                                             bool slopes) {
-    const float dx = (float)g.dx, idx = 1.f / dx;
+__device__ __forceinline__ void lane_weights(const float t[3], const GridGeom& g, int s, LaneW& w, bool slopes) {
+    const float dx = (float)g.dx;
     float d[3], n[3], sl[3];
 #pragma unroll
     for (int c = 0; c < 3; c++) {
-        const float xg = (float)g.mn[c] + (float)(base[c] + s) * dx;
-        d[c] = xg - x[c];
-        const float q = d[c] * idx;
+        const float q = (float)s - t[c];  // node offset in cells (exact for t in [1, 2))
+        d[c] = q * dx;
         n[c] = bsp(q);
         sl[c] = slopes ? bsp_slope(q) : 0.f;
     }
@@ -208,15 +206,14 @@ __device__ __forceinline__ void lane_weights(const float x[3], const GridGeom& g
 // row_weights (three shuffles) when it reaches that row, so only one row's
 // values are live at a time.  Fills d0, n0, s0 and the axis-2 arrays of w,
 // the latter in the order of node k ^ kperm (reduce_scatter8's permutation).
-__device__ __forceinline__ void lane_weights_k(const float x[3], const GridGeom& g, const int base[3], int s,
-                                               LaneW& w, float own1[3], bool slopes, int kperm = 0) {
-    const float dx = (float)g.dx, idx = 1.f / dx;
+__device__ __forceinline__ void lane_weights_k(const float t[3], const GridGeom& g, int s, LaneW& w, float own1[3],
+                                               bool slopes, int kperm = 0) {
+    const float dx = (float)g.dx;
     float d[3], n[3], sl[3];
 #pragma unroll
     for (int c = 0; c < 3; c++) {
-        const float xg = (float)g.mn[c] + (float)(base[c] + s) * dx;
-        d[c] = xg - x[c];
-        const float q = d[c] * idx;
+        const float q = (float)s - t[c];
+        d[c] = q * dx;
         n[c] = bsp(q);
         sl[c] = slopes ? bsp_slope(q) : 0.f;
     }
@@ -242,13 +239,42 @@ __device__ __forceinline__ void row_weights(const float own1[3], int j, float& d
     s1 = __shfl_sync(0xffffffffu, own1[2], src);
 }
 
-__device__ __forceinline__ void load_x_base(const float* st, size_t np, int p, const GridGeom& g, float x[3],
-                                            int base[3]) {
+// stencil base and lattice coordinates t = (x - mn) / dx - base of particle p
+// (compensated positions when xlo: load_xd, stencil_coord); xd, if given,
+// receives the positions
+__device__ __forceinline__ void load_x_base(const float* st, size_t np, int p, const GridGeom& g, float t[3],
+                                            int base[3], int xlo, double* xd = nullptr) {
+    const double idx = 1.0 / g.dx;
 #pragma unroll
     for (int c = 0; c < 3; c++) {
-        x[c] = st[(size_t)(PX + c) * np + p];
-        base[c] = stencil_base<float>(x[c] - (float)g.mn[c], (float)g.dx, g.dim[c]);
+        const double x = load_xd(st, np, p, c, xlo);
+        if (xd) xd[c] = x;
+        t[c] = stencil_coord<float>(x, g.mn[c], idx, g.dim[c], base[c]);
     }
+}
+// x' = x + dt v of axis c from the position x read by load_x_base, into the
+// next layer's planes (hi and, when xlo, lo); returns the stored hi.  The
+// brick G2P keeps x in registers from its first load (64.6 us per step on the
+// 64^3, 267k-particle workload, against 67.4 us re-reading it before the
+// store); the warp-item G2P re-reads it (advance_x), as holding it there
+// costs 52 bytes of spill at its 64-register budget.
+__device__ __forceinline__ float store_x(float* st_next, size_t npn, int p, int c, double x, float dt, float v,
+                                         int xlo) {
+    if (!xlo) {
+        const float xn = (float)x + dt * v;
+        st_next[(size_t)(PX + c) * npn + p] = xn;
+        return xn;
+    }
+    const double xn = x + (double)(dt * v);
+    const float hi = (float)xn;
+    st_next[(size_t)(PX + c) * npn + p] = hi;
+    st_next[(size_t)(PXL + c) * npn + p] = (float)(xn - (double)hi);
+    return hi;
+}
+// the same, re-reading x from layer n's planes
+__device__ __forceinline__ float advance_x(const float* st, float* st_next, size_t npl, size_t npn, int p, int c,
+                                           float dt, float v, int xlo) {
+    return store_x(st_next, npn, p, c, load_xd(st, npl, p, c, xlo), dt, v, xlo);
 }
 
 // ------------------------------------------------------------------ args
@@ -324,6 +350,7 @@ struct WArgs {
     const uint16_t* item_inst;
     const float* st;       // layer n state
     float* st_next;        // layer n+1 state
+    int xlo;               // st and st_next carry the low parts of compensated positions (planes PXL)
     const float* cst;      // constants
     const float* dfc;      // dFc of layer n
     float* G;              // [24][npl] per layer: G (9), polar R (9), polar S (6: s00 s01 s02 s11 s12 s22)
@@ -494,15 +521,15 @@ __device__ __forceinline__ void p2g_item(const WArgs& a, int item, const FixScal
         int goff;
         item_grid<MODE>(a, item, geo, goff);
         const ItemLane L = item_lane(a.items, item);
-        float x[3];
+        float t[3];
         int base[3];
-        load_x_base(a.st, npl, L.p, geo, x, base);
+        load_x_base(a.st, npl, L.p, geo, t, base, a.xlo);
         const bool uniform = !GENERAL && warp_uniform_base(base);
         // slot (jj, kk) of each half holds node (2 half + (jj ^ P.jp), kk ^ P.kp)
         const ScatterPerm P = scatter_perm();
         LaneW w;
         float own1[3];
-        lane_weights_k(x, geo, base, L.s, w, own1, false, P.kp);
+        lane_weights_k(t, geo, L.s, w, own1, false, P.kp);
         const float mp = L.valid ? a.cst[(size_t)KM * np + L.p] : 0.f;
         const float damp = 1.f - a.dt * a.drag;
         float mvd[3], g0[3];
@@ -603,12 +630,12 @@ template <int MODE> __global__ void __launch_bounds__(256, 4) k_g2p_w(WArgs a) {
         int goff;
         item_grid<MODE>(a, item, geo, goff);
         const ItemLane L = item_lane(a.items, item);
-        float x[3];
+        float t[3];
         int base[3];
-        load_x_base(a.st, npl, L.p, geo, x, base);
+        load_x_base(a.st, npl, L.p, geo, t, base, a.xlo);
         LaneW w;
         float own1[3];
-        lane_weights_k(x, geo, base, L.s, w, own1, false);
+        lane_weights_k(t, geo, L.s, w, own1, false);
         // v = sum w v_g and C = sum w v_g d^T (scaled by 3/dx^2 at the end), with the
         // weight w = n0 n1[j] n2[k] and d = (d0, d1[j], d2[k]) factored per stencil row:
         // the node loop accumulates only the k-dependent sums, the row applies n0 n1[j]
@@ -690,8 +717,7 @@ template <int MODE> __global__ void __launch_bounds__(256, 4) k_g2p_w(WArgs a) {
         if (L.s == 0) {
 #pragma unroll
             for (int c = 0; c < 3; c++) {
-                const float xn = x[c] + a.dt * acc[c];
-                a.st_next[(size_t)(PX + c) * npn + p] = xn;
+                const float xn = advance_x(a.st, a.st_next, npl, npn, p, c, a.dt, acc[c], a.xlo);
                 a.st_next[(size_t)(PV + c) * npn + p] = acc[c];
                 finite &= isfinite(xn);
             }
@@ -778,14 +804,14 @@ __device__ __forceinline__ void adj_scatter_items(const WArgs& a, int first, int
         item_grid<MODE>(a, item, geo, goff);
         const ItemLane L = item_lane(a.items, item);
         const int p = L.p;
-        float x[3];
+        float t[3];
         int base[3];
-        load_x_base(a.st, npl, p, geo, x, base);
+        load_x_base(a.st, npl, p, geo, t, base, a.xlo);
         const bool uniform = !GENERAL && warp_uniform_base(base);
         const ScatterPerm P = scatter_perm();  // as in k_p2g_w
         LaneW w;
         float own1[3];
-        lane_weights_k(x, geo, base, L.s, w, own1, false, P.kp);
+        lane_weights_k(t, geo, L.s, w, own1, false, P.kp);
         float vn[3];
         m3<float> Cn;
         if constexpr (DET) {
@@ -914,12 +940,12 @@ template <bool EXACT, int MODE> __global__ void __launch_bounds__(256, DMPM_GATH
         item_grid<MODE>(a, item, geo, goff);
         const ItemLane L = item_lane(a.items, item);
         const int p = L.p;
-        float x[3];
+        float t[3];
         int base[3];
-        load_x_base(a.st, npl, p, geo, x, base);
+        load_x_base(a.st, npl, p, geo, t, base, a.xlo);
         LaneW w;
         float own1[3];
-        lane_weights_k(x, geo, base, L.s, w, own1, true);
+        lane_weights_k(t, geo, L.s, w, own1, true);
         const float mp = a.cst[(size_t)KM * np + p];
         const float cd = EXACT ? (1.f - a.dt * a.drag) : 1.f;
         const float dx = (float)geo.dx;

@@ -166,13 +166,14 @@ template <class T> struct axis_w {
     T d[4], n[4], s[4];
 };
 
-// floor(x_rel / dx) - 1 by division, as the reference computes it.  The
+// floor(x_rel / dx) - 1 by division, as the reference computes it
+// (stencil_base_lattice: floor(r) - 1 of a lattice coordinate r).  The
 // result is clamped to [-4, dim]: a stencil starting outside that range has
 // no node inside the grid either way, and the clamp keeps all later index
 // arithmetic (tile extents, node indices) bounded for any input, including
 // non-finite positions.
-template <class T> DMPM_HD int stencil_base(T xrel, T dx, int dim) {
-    const T q = floor(xrel / dx);
+template <class T> DMPM_HD int stencil_base_lattice(T r, int dim) {
+    const T q = floor(r);
     int b;
     if (!(q > T(-8))) b = -8;                    // also catches NaN
     else if (q > T(dim + 8)) b = dim + 8;
@@ -180,6 +181,7 @@ template <class T> DMPM_HD int stencil_base(T xrel, T dx, int dim) {
     b -= 1;
     return b < -4 ? -4 : (b > dim ? dim : b);
 }
+template <class T> DMPM_HD int stencil_base(T xrel, T dx, int dim) { return stencil_base_lattice<T>(xrel / dx, dim); }
 
 template <class T> DMPM_HD void axis_weights(T x, T mn, T dx, int base, axis_w<T>& w, bool slopes) {
 #pragma unroll
@@ -188,6 +190,16 @@ template <class T> DMPM_HD void axis_weights(T x, T mn, T dx, int base, axis_w<T
         const T d = xg - x;
         const T q = d / dx;
         w.d[k] = d;
+        w.n[k] = bspline(q);
+        w.s[k] = slopes ? bspline_slope(q) : T(0);
+    }
+}
+// the same from the lattice coordinate t = (x - mn) / dx - base: d_k = (k - t) dx
+template <class T> DMPM_HD void axis_weights_lattice(T t, T dx, axis_w<T>& w, bool slopes) {
+#pragma unroll
+    for (int k = 0; k < 4; k++) {
+        const T q = (T)k - t;
+        w.d[k] = q * dx;
         w.n[k] = bspline(q);
         w.s[k] = slopes ? bspline_slope(q) : T(0);
     }

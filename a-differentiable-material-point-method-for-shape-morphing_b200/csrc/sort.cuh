@@ -45,6 +45,7 @@ template <class T> struct KeyArgs {
     size_t np;
     GridGeom geo;
     const T* st;  // layer state (x planes)
+    int xlo;      // st carries the low parts of compensated positions (planes PXL)
     uint32_t* keys;
     uint32_t* vals;
 };
@@ -82,8 +83,12 @@ template <class T> __global__ void k_cell_keys(KeyArgs<T> a) {
     if (p >= a.n) return;
     int base[3];
 #pragma unroll
-    for (int c = 0; c < 3; c++)
-        base[c] = stencil_base<T>(a.st[(size_t)(PX + c) * a.np + p] - (T)a.geo.mn[c], (T)a.geo.dx, a.geo.dim[c]);
+    for (int c = 0; c < 3; c++) {
+        if (a.xlo)  // the base the FP32 stencil kernels form (load_xd, stencil_coord)
+            (void)stencil_coord<float>(load_xd(a.st, a.np, p, c, 1), a.geo.mn[c], 1.0 / a.geo.dx, a.geo.dim[c], base[c]);
+        else
+            base[c] = stencil_base<T>(a.st[(size_t)(PX + c) * a.np + p] - (T)a.geo.mn[c], (T)a.geo.dx, a.geo.dim[c]);
+    }
     a.keys[p] = cell_key(base, a.geo.dim);
     a.vals[p] = (uint32_t)p;
 }

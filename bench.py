@@ -242,17 +242,18 @@ def timed_steps(torch, c, steps, fn):
 # accumulator 8 B), the sorted-order index of the warp-item kernels (4 B per
 # particle), and its grid records: per touched node for the particle-parallel
 # kernels, per grid node for the node-parallel ones.
+# (positions are compensated float pairs, hi + lo: 6 floats per particle)
 PER_PARTICLE_BYTES = {
     "p_op1": (9 + 9 + 4 + 9) * 4 + 24 * 4,                  # F, dFc, m/vol/lam/mu, C -> G, R, S
-    "p2g": (3 + 1 + 3 + 9 + 1) * 4,                         # x, m, v, G, order
-    "g2p_p_op2": (3 + 9 + 9 + 1) * 4 + 24 * 4,              # x, F, dFc, order -> x, v, C, F
-    "adj_g2p_scatter": (3 + 24 + 9 + 9 + 1) * 4 + 12 * 4,   # x, adjoint', F, dFc, order -> dLdv', dLdC'
-    "adj_p2g_gather": (3 + 1 + 3 + 12 + 9 + 1) * 4 + 18 * 4,  # x, m, v, dLdv'/dLdC', G, order -> M, X, u, z
+    "p2g": (6 + 1 + 3 + 9 + 1) * 4,                         # x, m, v, G, order
+    "g2p_p_op2": (6 + 9 + 9 + 1) * 4 + 27 * 4,              # x, F, dFc, order -> x, v, C, F
+    "adj_g2p_scatter": (6 + 24 + 9 + 9 + 1) * 4 + 12 * 4,   # x, adjoint', F, dFc, order -> dLdv', dLdC'
+    "adj_p2g_gather": (6 + 1 + 3 + 12 + 9 + 1) * 4 + 18 * 4,  # x, m, v, dLdv'/dLdC', G, order -> M, X, u, z
     # the finalize runs as two launches (both read M): the FP64 part and the FP32 transport part
     "adj_finalize": (9 + 9 + 9 + 9 + 6 + 3 + 9 + 9) * 4 + 9 * 4 + 9 * 8 * 2,  # M, F, dFc, R, S, vol/lam/mu,
                                                                                  # C', dLdF' -> dLdF, FP64 acc
     "adj_finalize_transport": (18 + 9 + 9 + 3 + 1) * 4 + 15 * 4,  # M/X/u/z, G, dLdC', dLdx', m -> dLdx, dLdv, dLdC
-    "p2g_mass": 4 * 4, "loss_dldx": 4 * 4 + 24 * 4,
+    "p2g_mass": 7 * 4, "loss_dldx": 7 * 4 + 24 * 4,
 }
 PER_TOUCHED_NODE_BYTES = {"p2g": 16, "g2p_p_op2": 16, "adj_g2p_scatter": 16, "adj_p2g_gather": 32,
                           "p2g_mass": 4, "loss_dldx": 4}

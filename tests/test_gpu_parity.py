@@ -376,9 +376,11 @@ def test_fp32_sort_interval_does_not_change_results(gpu_ready, exact_case, sort_
 
 
 def _cpu_cell_keys(x, dims, dx=1.0, mn=(0.0, 0.0, 0.0)):
-    """Cell keys exactly as the engine defines them, in float32 on the CPU."""
-    x32 = np.asarray(x, dtype=np.float32)
-    q = np.floor((x32 - np.asarray(mn, dtype=np.float32)) / np.float32(dx)).astype(np.int64)
+    """Cell keys exactly as the engine defines them, on the CPU: the stencil
+    base floor((x - mn) / dx) - 1 of each position in FP64 (the FP32 engine
+    keeps positions as float pairs hi + lo, which c.get returns summed)."""
+    x64 = np.asarray(x, dtype=np.float64)
+    q = np.floor((x64 - np.asarray(mn, dtype=np.float64)) * (1.0 / dx)).astype(np.int64)
     b = np.clip(np.clip(q, -8, np.asarray(dims) + 8) - 1, -4, np.asarray(dims))
     c = b + 5
     nb = (np.asarray(dims) + 5) // 4 + 1
