@@ -170,7 +170,10 @@ int dmpm_set_device_limit(dmpm_ctx* ctx, int64_t max_bytes);
 int dmpm_set_grid(dmpm_ctx* ctx, int dim_x, int dim_y, int dim_z, double dx, const double* min_point);
 int dmpm_set_params(dmpm_ctx* ctx, const dmpm_params* params);
 
-/* Initial point cloud (layer 0).  dFc, vol may be NULL (zeros). */
+/* Initial point cloud (layer 0).  dFc, vol may be NULL (zeros).  The FP32
+ * context keeps each position coordinate as a pair of floats (hi + lo, about
+ * 48 bits), so x comes back from dmpm_get_particles as given to ~2^-48 of its
+ * size; the other fields are stored as floats. */
 int dmpm_set_particles(dmpm_ctx* ctx, int n, const double* x, const double* v, const double* F,
                        const double* C, const double* dFc, const double* m, const double* vol,
                        const double* lam, const double* mu);
