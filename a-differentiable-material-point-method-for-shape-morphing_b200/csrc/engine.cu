@@ -287,6 +287,7 @@ template <class T> class Engine : public EngineBase {
 
     void alloc_particles(int n) {
         if (n <= 0) throw ArgError{"particle count must be positive"};
+        permuted_ = false;  // a new cloud arrives in the caller's order
         if (n == n_ && cst_) {
             // same cloud size: overwrite in place and keep the layer storage
             DMPM_CK(cudaMemsetAsync(cst_, 0, NCONST * np_ * sizeof(T), ctx_->stream));
@@ -300,12 +301,44 @@ template <class T> class Engine : public EngineBase {
         layers_.clear();
         layout_ = Layout{};
         scene_arena_.release();
+        perm_ = nullptr;
         cst_ = (T*)scene_arena_.alloc(NCONST * np_ * sizeof(T));
         st0_ = (T*)scene_arena_.alloc(kNst * np_ * sizeof(T));
         dfc0_ = (T*)scene_arena_.alloc(9 * np_ * sizeof(T));
         DMPM_CK(cudaMemsetAsync(cst_, 0, NCONST * np_ * sizeof(T), ctx_->stream));
         DMPM_CK(cudaMemsetAsync(st0_, 0, kNst * np_ * sizeof(T), ctx_->stream));
         DMPM_CK(cudaMemsetAsync(dfc0_, 0, 9 * np_ * sizeof(T), ctx_->stream));
+    }
+
+    const uint32_t* perm() const { return permuted_ ? perm_ : nullptr; }
+
+    // Store the cloud in the order of its cell keys (the stable cell sort of
+    // layer 0): particles that share stencil nodes then sit together in every
+    // plane, as they do when the caller's order is spatial.  Transfers map
+    // indices through perm_ from here on, so callers see their own order.
+    void reorder_scene() {
+        if constexpr (kWarp) {
+            // scratch: the first epoch's order and items (recomputed by the next forward
+            // pass) and layer 0's state planes (overwritten from st0_ right after)
+            Epoch& e = epochs_[0];
+            cell_sort(st0_, e);  // e.order[i] = index of the i-th particle in cell order
+            if (!perm_) perm_ = (uint32_t*)scene_arena_.alloc((size_t)n_ * 4);
+            DMPM_CK(cudaMemcpyAsync(perm_, e.order, (size_t)n_ * 4, cudaMemcpyDeviceToDevice, ctx_->stream));
+            T* buf = layers_[0].st;
+            auto permute = [&](T* a, int planes) {
+                const size_t tot = (size_t)n_ * planes;
+                k_gather_planes<T><<<(unsigned)((tot + 255) / 256), 256, 0, ctx_->stream>>>(a, planes, np_, n_, perm_,
+                                                                                            buf);
+                launched();
+                DMPM_CK(cudaMemcpyAsync(a, buf, (size_t)planes * np_ * sizeof(T), cudaMemcpyDeviceToDevice,
+                                        ctx_->stream));
+            };
+            permute(st0_, kNst);
+            permute(cst_, NCONST);
+            permute(dfc0_, 9);
+            permuted_ = true;
+            for (Epoch& ep : epochs_) ep.valid = false;
+        }
     }
 
     double* staging(size_t count) {
@@ -327,7 +360,7 @@ template <class T> class Engine : public EngineBase {
             launched();
         }
         const size_t tot = (size_t)n_ * width;
-        k_unpack<T><<<(unsigned)((tot + 255) / 256), 256, 0, ctx_->stream>>>(s, width, n_, dst, np_);
+        k_unpack<T><<<(unsigned)((tot + 255) / 256), 256, 0, ctx_->stream>>>(s, width, n_, dst, np_, perm());
         launched();
     }
 
@@ -337,7 +370,7 @@ template <class T> class Engine : public EngineBase {
             double* s = staging((size_t)n_ * 3);
             DMPM_CK(cudaMemcpyAsync(s, host, (size_t)n_ * 3 * sizeof(double), cudaMemcpyHostToDevice, ctx_->stream));
             k_unpack_x2<<<(unsigned)(((size_t)n_ * 3 + 255) / 256), 256, 0, ctx_->stream>>>(
-                s, n_, (float*)st + (size_t)PX * np_, (float*)st + (size_t)PXL * np_, np_);
+                s, n_, (float*)st + (size_t)PX * np_, (float*)st + (size_t)PXL * np_, np_, perm());
             launched();
         } else {
             upload_planes(host, 3, st + (size_t)PX * np_);
@@ -347,7 +380,7 @@ template <class T> class Engine : public EngineBase {
         if constexpr (kWarp) {
             double* s = staging((size_t)n_ * 3);
             k_pack_x2<<<(unsigned)(((size_t)n_ * 3 + 255) / 256), 256, 0, ctx_->stream>>>(
-                (const float*)st + (size_t)PX * np_, (const float*)st + (size_t)PXL * np_, np_, n_, s);
+                (const float*)st + (size_t)PX * np_, (const float*)st + (size_t)PXL * np_, np_, n_, s, perm());
             launched();
             DMPM_CK(cudaMemcpyAsync(host, s, (size_t)n_ * 3 * sizeof(double), cudaMemcpyDeviceToHost, ctx_->stream));
             DMPM_CK(cudaStreamSynchronize(ctx_->stream));
@@ -359,7 +392,7 @@ template <class T> class Engine : public EngineBase {
     void download_planes(const T* src, int width, double* host, double diag = 0.0) {
         double* s = staging((size_t)n_ * width);
         const size_t tot = (size_t)n_ * width;
-        k_pack<T><<<(unsigned)((tot + 255) / 256), 256, 0, ctx_->stream>>>(src, np_, width, n_, s);
+        k_pack<T><<<(unsigned)((tot + 255) / 256), 256, 0, ctx_->stream>>>(src, np_, width, n_, s, perm());
         launched();
         if (diag != 0.0) {
             k_diag_add<<<(unsigned)(((size_t)n_ * 3 + 255) / 256), 256, 0, ctx_->stream>>>(s, n_, diag);
@@ -839,6 +872,7 @@ template <class T> class Engine : public EngineBase {
     // states other than 0 are not copied: each is written by the forward pass
     // before anything reads it.
     void reset_layers() {
+        if (ctx_->prm.reorder_particles && !permuted_) reorder_scene();
         const size_t st_bytes = kNst * np_ * sizeof(T);
         DMPM_CK(cudaMemcpyAsync(layers_[0].st, st0_, st_bytes, cudaMemcpyDeviceToDevice, ctx_->stream));
         if (ctx_->prm.control_mode == DMPM_CTRL_PER_LAYER) {
@@ -977,7 +1011,13 @@ template <class T> class Engine : public EngineBase {
         if (keys) DMPM_CK(cudaMemcpyAsync(keys, sk_[sorted_], (size_t)n_ * 4, cudaMemcpyDeviceToHost, ctx_->stream));
         if (order) DMPM_CK(cudaMemcpyAsync(order, e.order, (size_t)n_ * 4, cudaMemcpyDeviceToHost, ctx_->stream));
         if (items) DMPM_CK(cudaMemcpyAsync(items, e.items, ((size_t)ni + 1) * 4, cudaMemcpyDeviceToHost, ctx_->stream));
+        std::vector<uint32_t> perm;
+        if (order && permuted_) {  // positions in the caller's indices
+            perm.resize((size_t)n_);
+            DMPM_CK(cudaMemcpyAsync(perm.data(), perm_, (size_t)n_ * 4, cudaMemcpyDeviceToHost, ctx_->stream));
+        }
         DMPM_CK(cudaStreamSynchronize(ctx_->stream));
+        for (size_t i = 0; i < perm.size(); i++) order[i] = perm[order[i]];
         if (n_items) *n_items = (int)ni;
     }
 
@@ -1624,7 +1664,8 @@ template <class T> class Engine : public EngineBase {
         if (!out) throw ArgError{"out is NULL"};
         if (ctrl_acc_) {
             double* s = staging((size_t)n_ * 9);
-            k_pack_acc<T><<<(unsigned)(((size_t)n_ * 9 + 255) / 256), 256, 0, ctx_->stream>>>(ctrl_acc_, np_, n_, s);
+            k_pack_acc<T><<<(unsigned)(((size_t)n_ * 9 + 255) / 256), 256, 0, ctx_->stream>>>(ctrl_acc_, np_, n_, s,
+                                                                                            perm());
             launched();
             DMPM_CK(cudaMemcpyAsync(out, s, (size_t)n_ * 9 * sizeof(double), cudaMemcpyDeviceToHost, ctx_->stream));
             DMPM_CK(cudaStreamSynchronize(ctx_->stream));
@@ -1781,6 +1822,10 @@ template <class T> class Engine : public EngineBase {
     T* cst_ = nullptr;
     T* st0_ = nullptr;
     T* dfc0_ = nullptr;
+    // cloud stored in cell order (dmpm_params::reorder_particles): perm_[i] =
+    // the caller's index of device particle i, applied to every transfer
+    uint32_t* perm_ = nullptr;
+    bool permuted_ = false;
     T* target_ = nullptr;
     T* dldm_ = nullptr;
     node4<T>* scratch_grid_ = nullptr;
@@ -1967,7 +2012,7 @@ int dmpm_set_params(dmpm_ctx* ctx, const dmpm_params* p) {
         (p->block_size % 32) != 0 || p->tile_cap < 0 || p->tile_cap > 1536 || p->sort_every < 0 ||
         p->warp_general < 0 || p->warp_general > 1 || p->control_stride < 0 || p->eager < 0 || p->eager > 1 ||
         (p->brick_cells != 0 && p->brick_cells != 2 && p->brick_cells != 4) || p->deterministic < 0 ||
-        p->deterministic > 1) {
+        p->deterministic > 1 || p->reorder_particles < 0 || p->reorder_particles > 1) {
         ctx->err = "invalid dmpm_params";
         return DMPM_ERR_ARG;
     }

@@ -4,6 +4,7 @@
 #pragma once
 #include <cuda_runtime.h>
 
+#include <cstdint>
 #include <string>
 #include <vector>
 
@@ -80,36 +81,56 @@ class Arena {
 
 
 // ---------------------------------------------------------------- layout kernels
-template <class T> __global__ void k_unpack(const double* __restrict__ src, int width, int n, T* dst, size_t np) {
-    const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= (size_t)n * width) return;
-    const int p = (int)(i / width), q = (int)(i % width);
-    dst[(size_t)q * np + p] = (T)src[i];
+// Host arrays hold width values per particle in the caller's order; device
+// planes hold particle i at plane offset i.  perm (or null: the identity) maps
+// a device index to the caller's index, for a cloud stored in cell order.
+__device__ __forceinline__ size_t caller_index(const uint32_t* perm, int i) { return perm ? perm[i] : (size_t)i; }
+template <class T>
+__global__ void k_unpack(const double* __restrict__ src, int width, int n, T* dst, size_t np,
+                         const uint32_t* __restrict__ perm = nullptr) {
+    const size_t t = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= (size_t)n * width) return;
+    const int i = (int)(t / width), q = (int)(t % width);
+    dst[(size_t)q * np + i] = (T)src[caller_index(perm, i) * width + q];
 }
-template <class T> __global__ void k_pack(const T* __restrict__ src, size_t np, int width, int n, double* dst) {
-    const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= (size_t)n * width) return;
-    const int p = (int)(i / width), q = (int)(i % width);
-    dst[i] = (double)src[(size_t)q * np + p];
+template <class T>
+__global__ void k_pack(const T* __restrict__ src, size_t np, int width, int n, double* dst,
+                       const uint32_t* __restrict__ perm = nullptr) {
+    const size_t t = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= (size_t)n * width) return;
+    const int i = (int)(t / width), q = (int)(t % width);
+    dst[caller_index(perm, i) * width + q] = (double)src[(size_t)q * np + i];
+}
+// dst plane q, entry i = src plane q, entry perm[i] (planes planes of stride np)
+template <class T>
+__global__ void k_gather_planes(const T* __restrict__ src, int planes, size_t np, int n,
+                                const uint32_t* __restrict__ perm, T* dst) {
+    const size_t t = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= (size_t)n * planes) return;
+    const int q = (int)(t / n), i = (int)(t % n);
+    dst[(size_t)q * np + i] = src[(size_t)q * np + perm[i]];
 }
 // n x 3 doubles to compensated position planes (three hi planes from hi, three
 // lo planes from lo, plane stride np): hi = the float nearest x, lo = the float
 // nearest x - hi; and back, x = hi + lo
-static __global__ void k_unpack_x2(const double* __restrict__ src, int n, float* hi, float* lo, size_t np) {
-    const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= (size_t)n * 3) return;
-    const size_t o = (i % 3) * np + i / 3;
-    const double x = src[i];
+static __global__ void k_unpack_x2(const double* __restrict__ src, int n, float* hi, float* lo, size_t np,
+                                   const uint32_t* __restrict__ perm = nullptr) {
+    const size_t t = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= (size_t)n * 3) return;
+    const int i = (int)(t / 3), c = (int)(t % 3);
+    const size_t o = (size_t)c * np + i;
+    const double x = src[caller_index(perm, i) * 3 + c];
     const float h = (float)x;
     hi[o] = h;
     lo[o] = (float)(x - (double)h);
 }
 static __global__ void k_pack_x2(const float* __restrict__ hi, const float* __restrict__ lo, size_t np, int n,
-                                 double* dst) {
-    const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= (size_t)n * 3) return;
-    const size_t o = (i % 3) * np + i / 3;
-    dst[i] = (double)hi[o] + (double)lo[o];
+                                 double* dst, const uint32_t* __restrict__ perm = nullptr) {
+    const size_t t = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= (size_t)n * 3) return;
+    const int i = (int)(t / 3), c = (int)(t % 3);
+    const size_t o = (size_t)c * np + i;
+    dst[caller_index(perm, i) * 3 + c] = (double)hi[o] + (double)lo[o];
 }
 // add s to the diagonal (entries 0, 4, 8) of n 3x3 matrices stored as 9
 // consecutive doubles each: F <-> the FP32 path's strain planes H = F - I
@@ -118,10 +139,12 @@ static __global__ void k_diag_add(double* a, int n, double s) {
     if (i >= (size_t)n * 3) return;
     a[9 * (i / 3) + 4 * (i % 3)] += s;
 }
-template <class T> __global__ void k_pack_acc(const double* __restrict__ src, size_t np, int n, double* dst) {
-    const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= (size_t)n * 9) return;
-    const int p = (int)(i / 9), q = (int)(i % 9);
-    dst[i] = src[(size_t)q * np + p];
+template <class T>
+__global__ void k_pack_acc(const double* __restrict__ src, size_t np, int n, double* dst,
+                           const uint32_t* __restrict__ perm = nullptr) {
+    const size_t t = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= (size_t)n * 9) return;
+    const int i = (int)(t / 9), q = (int)(t % 9);
+    dst[caller_index(perm, i) * 9 + q] = src[(size_t)q * np + i];
 }
 }  // namespace dmpm_host

@@ -47,7 +47,8 @@ class Params(ctypes.Structure):
                 ("loss_kind", ctypes.c_int), ("checkpoint_every", ctypes.c_int), ("keep_adjoints", ctypes.c_int),
                 ("keep_intermediates", ctypes.c_int), ("block_size", ctypes.c_int), ("tile_cap", ctypes.c_int),
                 ("sort_every", ctypes.c_int), ("warp_general", ctypes.c_int), ("control_stride", ctypes.c_int),
-                ("eager", ctypes.c_int), ("brick_cells", ctypes.c_int), ("deterministic", ctypes.c_int)]
+                ("eager", ctypes.c_int), ("brick_cells", ctypes.c_int), ("deterministic", ctypes.c_int),
+                ("reorder_particles", ctypes.c_int)]
 
 
 class Instance(ctypes.Structure):
@@ -245,7 +246,7 @@ class Context:
                    checkpoint_every: int = 0, keep_adjoints: bool = False, keep_intermediates: bool = False,
                    block_size: int = 0, tile_cap: int = 0, sort_every: int = 0, warp_general: bool = False,
                    control_stride: int = 0, eager: bool = False, brick_cells: Optional[int] = None,
-                   deterministic: bool = False):
+                   deterministic: bool = False, reorder_particles: bool = False):
         p = Params()
         self.lib.dmpm_default_params(ctypes.byref(p))
         p.dt, p.drag, p.smoothing = float(dt), float(drag), float(smoothing)
@@ -266,6 +267,7 @@ class Context:
         if brick_cells is not None:  # else the library default (bricks of 2^3 cells for G2P)
             p.brick_cells = int(brick_cells)
         p.deterministic = int(bool(deterministic))
+        p.reorder_particles = int(bool(reorder_particles))
         self._ck(self.lib.dmpm_set_params(self.h, ctypes.byref(p)), "set_params")
         self.params = p
 

@@ -172,6 +172,10 @@ FLT_EPSILON = 1.1920928955078125e-07  # the reference's node-mass threshold (For
 # ---------------------------------------------------------------- workload
 def build_scene(instance: int, ppc_root: int):
     sc = scenes.config_scene(1, instance=instance, ppc_root=ppc_root)
+    if SHUFFLE:  # the same cloud handed over in a seeded random order
+        perm = np.random.default_rng(2024 + instance).permutation(sc.n)
+        for f in ("x", "v", "F", "C", "dFc", "m", "lam", "mu", "vol"):
+            setattr(sc, f, np.ascontiguousarray(getattr(sc, f)[perm]))
     return sc
 
 
@@ -182,6 +186,10 @@ BRICK_CELLS = None
 SORT_EVERY = None
 # FP32 path with integer node sums (bit-identical repeats), for every FP32 context
 DETERMINISTIC = False
+# the caller's particle order: False = the scene's lattice order, True = a seeded random permutation
+SHUFFLE = False
+# FP32 path: the engine stores the cloud in cell order at setup (dmpm_params::reorder_particles)
+REORDER = False
 
 
 def setup_ctx(dmpm, sc, prec, device, vol, target, dt, checkpoint_every, control="tied", control_stride=0,
@@ -202,7 +210,8 @@ def setup_ctx(dmpm, sc, prec, device, vol, target, dt, checkpoint_every, control
     c.set_params(dt=dt, drag=sc.drag, f_ext=sc.f_ext, smoothing=sc.smoothing, adjoint="exact", control=control,
                  loss="ref", checkpoint_every=checkpoint_every, control_stride=control_stride,
                  brick_cells=BRICK_CELLS if prec == "fp32" else None, sort_every=SORT_EVERY or 0,
-                 deterministic=DETERMINISTIC if deterministic is None else deterministic)
+                 deterministic=DETERMINISTIC if deterministic is None else deterministic,
+                 reorder_particles=REORDER and prec == "fp32")
     c.setup(sc.steps + 1)
     return c
 
@@ -377,6 +386,8 @@ def workload_config(sc, dt_sub, ckpt):
             "dt_substituted_from": dt_sub, "checkpoint_every": ckpt, "loss": "reference log-mass + min-mass penalty",
             "l2_policy": "inputs larger than L2 (per-rollout layer state > 5 GB, 126 MB L2)",
             "g2p_kernel": "warp items" if BRICK_CELLS == 0 else "bricks of %d^3 cells" % (BRICK_CELLS or 2),
+            "particle_order": "seeded random permutation" if SHUFFLE else "lattice",
+            "reorder_particles": REORDER,
             "parallelism": "replicas: one independent instance per GPU"}
 
 
@@ -1099,6 +1110,9 @@ def main():
     ap.add_argument("--sort-every", type=int, default=None, help="FP32 cell-sort interval in steps (default 8)")
     ap.add_argument("--deterministic", action="store_true",
                     help="FP32 path with integer node sums: gradients repeat bit for bit")
+    ap.add_argument("--shuffle", action="store_true", help="hand the cloud over in a seeded random order")
+    ap.add_argument("--reorder", action="store_true",
+                    help="FP32 path: store the cloud in cell order at setup (reorder_particles)")
     ap.add_argument("--rollout-steps", type=int, default=0, help="override the 200 time steps (profiling runs)")
     ap.add_argument("--no-fp64", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
@@ -1119,11 +1133,13 @@ def main():
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
-    global BRICK_CELLS, SORT_EVERY, DETERMINISTIC
+    global BRICK_CELLS, SORT_EVERY, DETERMINISTIC, SHUFFLE, REORDER
     if args.brick is not None:
         BRICK_CELLS = args.brick
     SORT_EVERY = args.sort_every
     DETERMINISTIC = args.deterministic
+    SHUFFLE = args.shuffle
+    REORDER = args.reorder
     if args.impl == "reference":
         return run_reference(args)
     if args.fd:

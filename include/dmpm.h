@@ -147,6 +147,13 @@ typedef struct {
                                 integer atomics, so gradients and losses are bit-identical from run to
                                 run; 0 (default) = float atomics, whose summation order varies.  The
                                 FP64 reductions (loss, norms) are summed in a fixed order either way. */
+    int reorder_particles;   /* FP32 path: 1 = dmpm_setup stores the cloud in the order of its cell keys
+                                (the stable cell sort of layer 0), so particles that share stencil
+                                nodes sit together in memory whatever order the caller gave them in;
+                                every particle array passed through this ABI stays in the caller's
+                                order (the engine maps indices), dmpm_cell_sort included.  The order
+                                is fixed until the next dmpm_set_particles / dmpm_set_points_ref.
+                                0 (default) = the caller's order. */
 } dmpm_params;
 
 void dmpm_default_params(dmpm_params* p);
