@@ -52,6 +52,9 @@ class CompGraph {
     void SetEngineOptions(int precision, int adjoint_mode, int device = 0);
     // FP32-mixed path: integer node sums, so passes repeat bit for bit (dmpm_params::deterministic)
     void SetDeterministic(bool on);
+    // FP32-mixed path: store the cloud in cell order on the device (dmpm_params::reorder_particles);
+    // every layer's points keep their order here
+    void SetReorderParticles(bool on);
     bool sync_grids = true;  // copy every layer's grid and stress P back after each pass
 
    private:
@@ -74,6 +77,7 @@ class CompGraph {
     int adjoint_mode_ = 0;
     int device_ = 0;
     bool deterministic_ = false;
+    bool reorder_ = false;
     dmpm_ctx* ctx_ = nullptr;
     int ctx_layers_ = 0;
 };

@@ -68,10 +68,11 @@ int g_stage_deterministic = 0;
 
 // det < 0: the stage functions' setting (SingleThreadMPM::SetEngineDeterministic)
 void set_params(dmpm_ctx* h, float dt, float drag, Vec3 f, float s, int adjoint, int keep_adj, int keep_int,
-                int det = -1) {
+                int det = -1, int reorder = 0) {
     dmpm_params p;
     dmpm_default_params(&p);
     p.deterministic = det < 0 ? g_stage_deterministic : det;
+    p.reorder_particles = reorder;
     p.dt = dt;
     p.drag = drag;
     p.f_ext[0] = f[0]; p.f_ext[1] = f[1]; p.f_ext[2] = f[2];
@@ -841,6 +842,11 @@ void CompGraph::SetDeterministic(bool on) {
     ctx_layers_ = 0;  // the next pass sets the graph up again with the mode
 }
 
+void CompGraph::SetReorderParticles(bool on) {
+    reorder_ = on;
+    ctx_layers_ = 0;
+}
+
 void CompGraph::EnsureEngine() {
     if (!ctx_) check(nullptr, dmpm_create(device_, precision_, &ctx_), "dmpm_create");
 }
@@ -861,7 +867,8 @@ void CompGraph::SetUpCompGraph(int num_layers) {
     std::vector<double> tm(num_nodes(*target_grid));
     for_nodes(*target_grid, [&](const GridNode& n, size_t i) { tm[i] = n.m; });
     check(ctx_, dmpm_set_target_mass(ctx_, tm.data()), "dmpm_set_target_mass");
-    set_params(ctx_, dt, drag, f_ext, smoothing_factor, adjoint_mode_, 1, 0, deterministic_ ? 1 : 0);
+    set_params(ctx_, dt, drag, f_ext, smoothing_factor, adjoint_mode_, 1, 0, deterministic_ ? 1 : 0,
+               reorder_ && precision_ == DMPM_FP32_MIXED ? 1 : 0);
     check(ctx_, dmpm_setup(ctx_, num_layers), "dmpm_setup");
     ctx_layers_ = num_layers;
 }

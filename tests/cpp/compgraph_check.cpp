@@ -19,8 +19,9 @@ using namespace DiffMPMLib3D;
 static void put(std::FILE* f, double v) { std::fwrite(&v, sizeof(double), 1, f); }
 
 int main(int argc, char** argv) {
-    if (argc != 13 && argc != 14) return 2;
-    const bool det = argc == 14 && std::atoi(argv[13]) != 0;  // integer node sums (repeatable bits)
+    if (argc < 13 || argc > 15) return 2;
+    const bool det = argc >= 14 && std::atoi(argv[13]) != 0;      // integer node sums (repeatable bits)
+    const bool reorder = argc == 15 && std::atoi(argv[14]) != 0;  // cloud stored in cell order on the device
     const int precision = std::atoi(argv[4]), dim = std::atoi(argv[5]), L = std::atoi(argv[6]);
     const float dt = std::atof(argv[7]), drag = std::atof(argv[8]), s = std::atof(argv[9]);
     const Vec3 f_ext(std::atof(argv[10]), std::atof(argv[11]), std::atof(argv[12]));
@@ -39,6 +40,7 @@ int main(int argc, char** argv) {
     cg.SetSimulationParameters(dt, drag, f_ext, s);
     cg.SetEngineOptions(precision, DMPM_ADJ_REFCOMPAT);
     cg.SetDeterministic(det);
+    cg.SetReorderParticles(reorder);
     cg.SetUpCompGraph(L);
     cg.ComputeForwardPass(0);
     const float loss = cg.EndLayerMassLoss();

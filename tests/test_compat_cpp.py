@@ -33,7 +33,7 @@ def exe(tmp_path_factory):
     return str(out)
 
 
-def run(exe, tmp_path, precision, deterministic=False, tag=""):
+def run(exe, tmp_path, precision, deterministic=False, tag="", reorder=False):
     sc = rollout_scene()
     z33 = np.zeros((sc.n, 3, 3))
     write_mpmbin(tmp_path / "cloud.mpmbin", sc.x, sc.v, sc.F, sc.C, z33, sc.m, np.zeros(sc.n), sc.lam, sc.mu, sc.dFc)
@@ -45,7 +45,7 @@ def run(exe, tmp_path, precision, deterministic=False, tag=""):
     out = tmp_path / ("out%d%s.bin" % (precision, tag))
     args = [exe, str(tmp_path / "cloud.mpmbin"), str(tmp_path / "target.mpmbin"), str(out), str(precision),
             str(sc.dims[0]), str(ROLLOUT_LAYERS), repr(sc.dt), repr(sc.drag), repr(sc.smoothing),
-            *[repr(float(v)) for v in sc.f_ext]] + (["1"] if deterministic else [])
+            *[repr(float(v)) for v in sc.f_ext]] + (["1" if deterministic else "0", "1" if reorder else "0"])
     res = subprocess.run(args, capture_output=True, text=True, timeout=300)
     assert res.returncode == 0, res.stdout + res.stderr
     a = np.fromfile(out, dtype=np.float64)
@@ -111,6 +111,20 @@ def test_compgraph_cpp_deterministic_repeats_bit_for_bit(gpu_ready, exe, tmp_pat
     assert abs(a["loss"] - float(g["loss"])) / abs(float(g["loss"])) < 1e-4
     assert relerr(a["x_last"].reshape(-1, 3), g["x_%d" % (ROLLOUT_LAYERS - 1)]) < 1e-5
     assert normrel(cm(a["dLdF0"]), g["dLdF_0"]) < 1e-2
+
+
+def test_compgraph_cpp_reorder_keeps_the_callers_order(gpu_ready, exe, tmp_path):
+    """CompGraph::SetReorderParticles: the engine stores the cloud in cell
+    order, and every layer's points, states and adjoints come back in the
+    caller's order -- the same values as without reordering, to the FP32
+    path's summation-order noise."""
+    a, _ = run(exe, tmp_path, dmpm.FP32_MIXED, deterministic=True, tag="plain")
+    b, _ = run(exe, tmp_path, dmpm.FP32_MIXED, deterministic=True, tag="reorder", reorder=True)
+    assert np.array_equal(a["vol"], b["vol"])  # the stage functions' volumes: no reordering there
+    assert abs(a["loss"] - b["loss"]) <= 1e-6 * abs(a["loss"])
+    assert relerr(b["x_last"], a["x_last"]) < 1e-6
+    assert normrel(b["dLdF0"], a["dLdF0"]) < 1e-4
+    assert normrel(b["dLdx0"], a["dLdx0"]) < 1e-4
 
 
 def test_stage_level_api_composes_the_fused_step(gpu_ready, tmp_path):
