@@ -931,123 +931,136 @@ __global__ void k_adj_gop_w(const node4<float>* __restrict__ grid, const node4<f
 //   M += w d dLdp^T,  X += sigma (N'NN, NN'N, NNN'),  u += w dLdp,  z += w v_g
 //   sigma = m dLdm + dLdp.(m v c_d + G d) + v_g.(dLdv_next + 3/dx^2 dLdC_next d)
 // (the algebra of kernels.cuh:k_adj_gather); written to gath for k_adj_finalize.
+// One warp item of the adjoint gather: the item's particles (lane L, stencil
+// coordinates t, base) read their 64 stencil node pairs from sw, the item's
+// staged copy, or from global memory when sw is null.
+template <bool EXACT>
+__device__ __forceinline__ void gather_item(const WArgs& a, const GridGeom& geo, int goff, const ItemLane& L,
+                                            const float t[3], const int base[3], const node4<float>* sw) {
+    const size_t np = a.np, npl = a.npl;
+    const int p = L.p;
+    LaneW w;
+    float own1[3];
+    lane_weights_k(t, geo, L.s, w, own1, true);
+    const float mp = a.cst[(size_t)KM * np + p];
+    const float cd = EXACT ? (1.f - a.dt * a.drag) : 1.f;
+    const float dx = (float)geo.dx;
+    const float k3 = 3.f / (dx * dx);
+    float mvp[3], vn[3];
+#pragma unroll
+    for (int c = 0; c < 3; c++) {
+        mvp[c] = mp * a.st[(size_t)(PV + c) * npl + p] * cd;
+        vn[c] = a.adjn[(size_t)c * np + p];
+    }
+    const m3<float> G = load_m3(a.G, npl, p);
+    const m3<float> Cn = load_m3(a.adjn + 3 * np, np, p);
+    // sigma's node-dependent pieces: h_g = mvp + G d,  e_g = vn + k3 Cn d
+    float h0[3], e0[3];
+#pragma unroll
+    for (int r = 0; r < 3; r++) {
+        h0[r] = mvp[r] + G.a[r][0] * w.d0;
+        e0[r] = vn[r] + k3 * Cn.a[r][0] * w.d0;
+    }
+    float acc[18];  // M (9, row-major: M[r][c] = sum w d_r dLdp_c), X (3), u (3), z (3)
+#pragma unroll
+    for (int i = 0; i < 18; i++) acc[i] = 0.f;
+    // Factored sums: on this lane d0, n0 and s0 are constant and on a row d1, n1, s1, so
+    //   M[0][c] = d0 u_c (formed after the loop),
+    //   X0 = s0 sum_j n1 S_j,  X1 = n0 sum_j s1 S_j,  X2 = n0 sum_j n1 T_j,
+    // with the row sums S_j = sum_k n2_k sigma, T_j = sum_k s2_k sigma.
+    float S = 0.f, T = 0.f;
+    // one node (j, k) of the lane's slab, with row j's axis-1 values d1, n1
+    auto node = [&](const node4<float>& o, const node4<float>& vg, float d1, float n1, int k) {
+        float h[3], e[3];
+#pragma unroll
+        for (int r = 0; r < 3; r++) {
+            h[r] = h0[r] + G.a[r][1] * d1 + G.a[r][2] * w.d2[k];
+            e[r] = e0[r] + k3 * Cn.a[r][1] * d1 + k3 * Cn.a[r][2] * w.d2[k];
+        }
+        const float wt = (w.n0 * n1) * w.n2[k];
+        const float sig = mp * o.w + o.x * h[0] + o.y * h[1] + o.z * h[2] + vg.x * e[0] + vg.y * e[1] + vg.z * e[2];
+        S += w.n2[k] * sig;
+        T += w.s2[k] * sig;
+        const float wo[3] = {wt * o.x, wt * o.y, wt * o.z};
+        acc[15] += wt * vg.x;
+        acc[16] += wt * vg.y;
+        acc[17] += wt * vg.z;
+#pragma unroll
+        for (int c = 0; c < 3; c++) {
+            acc[12 + c] += wo[c];
+            acc[3 + c] += d1 * wo[c];
+            acc[6 + c] += w.d2[k] * wo[c];
+        }
+    };
+    auto end_row = [&](float n1, float s1) {
+        acc[9] += n1 * S;
+        acc[10] += s1 * S;
+        acc[11] += n1 * T;
+        S = 0.f;
+        T = 0.f;
+    };
+    if (sw) {
+#pragma unroll
+        for (int j = 0; j < 4; j++) {
+            float d1, n1, s1;
+            row_weights(own1, j, d1, n1, s1);
+#pragma unroll
+            for (int k = 0; k < 4; k++) {
+                const int n = 16 * L.s + 4 * j + k;
+                node(sw[stage_index<2>(n, 0)], sw[stage_index<2>(n, 1)], d1, n1, k);
+            }
+            end_row(n1, s1);
+        }
+    } else {
+        LaneNodes N = lane_nodes(geo, base, L.s);
+        N.g00 += goff;
+#pragma unroll
+        for (int j = 0; j < 4; j++) {
+            float d1, n1, s1;
+            row_weights(own1, j, d1, n1, s1);
+#pragma unroll
+            for (int k = 0; k < 4; k++) {
+                if (!((N.mask >> (4 * j + k)) & 1u)) continue;
+                const int g = N.g00 + j * N.sj + k;
+                node(a.gadj2[2 * g], a.gadj2[2 * g + 1], d1, n1, k);
+            }
+            end_row(n1, s1);
+        }
+    }
+    acc[9] *= w.s0;
+    acc[10] *= w.n0;
+    acc[11] *= w.n0;
+#pragma unroll
+    for (int c = 0; c < 3; c++) acc[c] = w.d0 * acc[12 + c];
+    reduce_slabs<18>(acc);
+    if (!L.valid) return;
+    if (L.s == 0) {
+#pragma unroll
+        for (int i = 0; i < 9; i++) a.gath[(size_t)i * np + p] = acc[i];
+    } else if (L.s == 1) {
+#pragma unroll
+        for (int i = 9; i < 18; i++) a.gath[(size_t)i * np + p] = acc[i];
+    }
+}
+
 template <bool EXACT, int MODE> __global__ void __launch_bounds__(256, DMPM_GATHER_MIN_BLOCKS) k_adj_gather_w(WArgs a) {
     const int nit = item_count(a);
-    const size_t np = a.np, npl = a.npl;
+    const size_t npl = a.npl;
+    __shared__ node4<float> s_rec[8][StageRecords<2>::value];
     for (int item = first_warp(); item < nit; item = next_item<MODE>(item, nit)) {
         GridGeom geo;
         int goff;
         item_grid<MODE>(a, item, geo, goff);
         const ItemLane L = item_lane(a.items, item);
-        const int p = L.p;
         float t[3];
         int base[3];
-        load_x_base(a.st, npl, p, geo, t, base, a.xlo);
-        LaneW w;
-        float own1[3];
-        lane_weights_k(t, geo, L.s, w, own1, true);
-        const float mp = a.cst[(size_t)KM * np + p];
-        const float cd = EXACT ? (1.f - a.dt * a.drag) : 1.f;
-        const float dx = (float)geo.dx;
-        const float k3 = 3.f / (dx * dx);
-        float mvp[3], vn[3];
-#pragma unroll
-        for (int c = 0; c < 3; c++) {
-            mvp[c] = mp * a.st[(size_t)(PV + c) * npl + p] * cd;
-            vn[c] = a.adjn[(size_t)c * np + p];
-        }
-        const m3<float> G = load_m3(a.G, npl, p);
-        const m3<float> Cn = load_m3(a.adjn + 3 * np, np, p);
-        // sigma's node-dependent pieces: h_g = mvp + G d,  e_g = vn + k3 Cn d
-        float h0[3], e0[3];
-#pragma unroll
-        for (int r = 0; r < 3; r++) {
-            h0[r] = mvp[r] + G.a[r][0] * w.d0;
-            e0[r] = vn[r] + k3 * Cn.a[r][0] * w.d0;
-        }
-        float acc[18];  // M (9, row-major: M[r][c] = sum w d_r dLdp_c), X (3), u (3), z (3)
-#pragma unroll
-        for (int i = 0; i < 18; i++) acc[i] = 0.f;
-        // Factored sums: on this lane d0, n0 and s0 are constant and on a row d1, n1, s1, so
-        //   M[0][c] = d0 u_c (formed after the loop),
-        //   X0 = s0 sum_j n1 S_j,  X1 = n0 sum_j s1 S_j,  X2 = n0 sum_j n1 T_j,
-        // with the row sums S_j = sum_k n2_k sigma, T_j = sum_k s2_k sigma.
-        float S = 0.f, T = 0.f;
-        // one node (j, k) of the lane's slab, with row j's axis-1 values d1, n1
-        auto node = [&](const node4<float>& o, const node4<float>& vg, float d1, float n1, int k) {
-            float h[3], e[3];
-#pragma unroll
-            for (int r = 0; r < 3; r++) {
-                h[r] = h0[r] + G.a[r][1] * d1 + G.a[r][2] * w.d2[k];
-                e[r] = e0[r] + k3 * Cn.a[r][1] * d1 + k3 * Cn.a[r][2] * w.d2[k];
-            }
-            const float wt = (w.n0 * n1) * w.n2[k];
-            const float sig = mp * o.w + o.x * h[0] + o.y * h[1] + o.z * h[2] + vg.x * e[0] + vg.y * e[1] + vg.z * e[2];
-            S += w.n2[k] * sig;
-            T += w.s2[k] * sig;
-            const float wo[3] = {wt * o.x, wt * o.y, wt * o.z};
-            acc[15] += wt * vg.x;
-            acc[16] += wt * vg.y;
-            acc[17] += wt * vg.z;
-#pragma unroll
-            for (int c = 0; c < 3; c++) {
-                acc[12 + c] += wo[c];
-                acc[3 + c] += d1 * wo[c];
-                acc[6 + c] += w.d2[k] * wo[c];
-            }
-        };
-        auto end_row = [&](float n1, float s1) {
-            acc[9] += n1 * S;
-            acc[10] += s1 * S;
-            acc[11] += n1 * T;
-            S = 0.f;
-            T = 0.f;
-        };
+        load_x_base(a.st, npl, L.p, geo, t, base, a.xlo);
+        node4<float>* sw = nullptr;
         if (DMPM_STAGE_NODES && warp_uniform_base(base)) {
-            __shared__ node4<float> s_rec[8][StageRecords<2>::value];
-            node4<float>* sw = s_rec[threadIdx.x >> 5];
+            sw = s_rec[threadIdx.x >> 5];
             stage_stencil<2>(a.gadj2, geo, goff, base, sw);
-#pragma unroll
-            for (int j = 0; j < 4; j++) {
-                float d1, n1, s1;
-                row_weights(own1, j, d1, n1, s1);
-#pragma unroll
-                for (int k = 0; k < 4; k++) {
-                    const int n = 16 * L.s + 4 * j + k;
-                    node(sw[stage_index<2>(n, 0)], sw[stage_index<2>(n, 1)], d1, n1, k);
-                }
-                end_row(n1, s1);
-            }
-        } else {
-            LaneNodes N = lane_nodes(geo, base, L.s);
-            N.g00 += goff;
-#pragma unroll
-            for (int j = 0; j < 4; j++) {
-                float d1, n1, s1;
-                row_weights(own1, j, d1, n1, s1);
-#pragma unroll
-                for (int k = 0; k < 4; k++) {
-                    if (!((N.mask >> (4 * j + k)) & 1u)) continue;
-                    const int g = N.g00 + j * N.sj + k;
-                    node(a.gadj2[2 * g], a.gadj2[2 * g + 1], d1, n1, k);
-                }
-                end_row(n1, s1);
-            }
         }
-        acc[9] *= w.s0;
-        acc[10] *= w.n0;
-        acc[11] *= w.n0;
-#pragma unroll
-        for (int c = 0; c < 3; c++) acc[c] = w.d0 * acc[12 + c];
-        reduce_slabs<18>(acc);
-        if (!L.valid) continue;
-        if (L.s == 0) {
-#pragma unroll
-            for (int i = 0; i < 9; i++) a.gath[(size_t)i * np + p] = acc[i];
-        } else if (L.s == 1) {
-#pragma unroll
-            for (int i = 9; i < 18; i++) a.gath[(size_t)i * np + p] = acc[i];
-        }
+        gather_item<EXACT>(a, geo, goff, L, t, base, sw);
     }
 }
 
