@@ -514,6 +514,11 @@ struct dmpm_batch::Impl {
         const size_t most = (P[t + 1] * 32 + 255) / 256;  // one item per particle at most
         return (unsigned)std::max<size_t>(1, std::min<size_t>(most, (size_t)sms * ctas_per_sm()));
     }
+    // the adjoint scatter's persistent grid: its own blocks per SM (kernels_warp.cuh), not the tuned setting
+    unsigned scatter_blocks(int t) const {
+        const size_t most = (P[t + 1] * 32 + DMPM_ADJ_SCATTER_THREADS - 1) / DMPM_ADJ_SCATTER_THREADS;
+        return (unsigned)std::max<size_t>(1, std::min<size_t>(most, (size_t)sms * DMPM_ADJ_SCATTER_CTAS));
+    }
 
     void step(int t) {
         WArgs a = args(t);
@@ -523,7 +528,7 @@ struct dmpm_batch::Impl {
         DMPM_CK(cudaMemsetAsync(grid[t], 0, Gt * sizeof(node4<float>), b->stream));
         k_stress<false><<<(unsigned)((a.n + pb - 1) / pb), pb, 0, b->stream>>>(a);
         launched();
-        k_p2g_w<false, ITEMS_BATCH><<<wb, 256, 0, b->stream>>>(a);
+        k_p2g_w<false, ITEMS_BATCH><<<wb, DMPM_P2G_THREADS, 0, b->stream>>>(a);
         launched();
         k_gop_inplace<<<(unsigned)((Gt + 255) / 256), 256, 0, b->stream>>>(grid[t], Gt, a.dt, a.fext[0], a.fext[1],
                                                                              a.fext[2]);
@@ -574,15 +579,16 @@ struct dmpm_batch::Impl {
         const unsigned wb = warp_blocks(t);
         const bool ex = prm.adjoint_mode == DMPM_ADJ_EXACT;
         DMPM_CK(cudaMemsetAsync(gadj, 0, Gt * sizeof(node4<float>), b->stream));
-        if (ex) k_adj_scatter_w<true, false, ITEMS_BATCH><<<wb, 256, 0, b->stream>>>(a);
-        else k_adj_scatter_w<false, false, ITEMS_BATCH><<<wb, 256, 0, b->stream>>>(a);
+        const unsigned ws = scatter_blocks(t);
+        if (ex) k_adj_scatter_w<true, false, ITEMS_BATCH><<<ws, DMPM_ADJ_SCATTER_THREADS, 0, b->stream>>>(a);
+        else k_adj_scatter_w<false, false, ITEMS_BATCH><<<ws, DMPM_ADJ_SCATTER_THREADS, 0, b->stream>>>(a);
         launched();
         const unsigned gb = (unsigned)((Gt + 255) / 256);
         if (ex) k_adj_gop_w<true><<<gb, 256, 0, b->stream>>>(grid[t], gadj, gadj2, Gt, a.dt, a.fext[0], a.fext[1], a.fext[2]);
         else k_adj_gop_w<false><<<gb, 256, 0, b->stream>>>(grid[t], gadj, gadj2, Gt, a.dt, a.fext[0], a.fext[1], a.fext[2]);
         launched();
-        if (ex) k_adj_gather_w<true, ITEMS_BATCH><<<wb, 256, 0, b->stream>>>(a);
-        else k_adj_gather_w<false, ITEMS_BATCH><<<wb, 256, 0, b->stream>>>(a);
+        if (ex) k_adj_gather_w<true, ITEMS_BATCH><<<wb, DMPM_GATHER_THREADS, 0, b->stream>>>(a);
+        else k_adj_gather_w<false, ITEMS_BATCH><<<wb, DMPM_GATHER_THREADS, 0, b->stream>>>(a);
         launched();
         DMPM_CK(cudaEventRecord(b->ev_fork, b->stream));
         DMPM_CK(cudaStreamWaitEvent(b->side, b->ev_fork, 0));

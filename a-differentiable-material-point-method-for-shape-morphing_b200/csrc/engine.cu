@@ -498,13 +498,15 @@ template <class T> class Engine : public EngineBase {
     // persistent grid of a warp-item kernel: ctas CTAs of 256 threads per SM (the
     // residency its register budget allows), fewer when the particles could not
     // fill them (at most one item per particle)
-    unsigned warp_blocks(int ctas = 3) {
+    // persistent grid of a warp-item kernel: ctas blocks of `threads` per SM, or
+    // one warp per particle when that is fewer
+    unsigned warp_blocks(int ctas = 3, int threads = 256) {
         if (sms_ == 0) {
             int dev = 0;
             DMPM_CK(cudaGetDevice(&dev));
             DMPM_CK(cudaDeviceGetAttribute(&sms_, cudaDevAttrMultiProcessorCount, dev));
         }
-        const size_t most = ((size_t)n_ * 32 + 255) / 256;
+        const size_t most = ((size_t)n_ * 32 + threads - 1) / threads;
         return (unsigned)std::max<size_t>(1, std::min<size_t>(most, (size_t)sms_ * ctas));
     }
     unsigned ggrid() const { return (unsigned)((G_ + 255) / 256); }
@@ -536,7 +538,7 @@ template <class T> class Engine : public EngineBase {
         const unsigned bt = DMPM_BRICK_THREADS;
         if (ush == 3) k_adj_scatter_fix_b<2, EX, GEN><<<brick_blocks(k_adj_scatter_fix_b<2, EX, GEN>), bt, 0, ctx_->stream>>>(a);
         else if (ush == 6) k_adj_scatter_fix_b<4, EX, GEN><<<brick_blocks(k_adj_scatter_fix_b<4, EX, GEN>), bt, 0, ctx_->stream>>>(a);
-        else k_adj_scatter_w<EX, GEN, ITEMS_PERSISTENT, true><<<ws, 256, 0, ctx_->stream>>>(a);
+        else k_adj_scatter_w<EX, GEN, ITEMS_PERSISTENT, true><<<ws, DMPM_ADJ_SCATTER_THREADS, 0, ctx_->stream>>>(a);
     }
     void launch_adj_scatter_fix(const WArgs& a, bool ex, bool gen, int ush, unsigned ws) {
         if (ex && gen) launch_adj_scatter_fix_t<true, true>(a, ush, ws);
@@ -1080,7 +1082,7 @@ template <class T> class Engine : public EngineBase {
             } else {
                 DMPM_CK(cudaMemsetAsync(g, 0, G_ * sizeof(node4<T>), ctx_->stream));
             }
-            const unsigned ws = warp_blocks(DMPM_SCATTER_CTAS);
+            const unsigned ws = warp_blocks(DMPM_SCATTER_CTAS, DMPM_P2G_THREADS);
             const int ush = set_units(a, ep);
             if (dm || !g_ready) {
                 pbeg(K_P_OP1);
@@ -1098,10 +1100,10 @@ template <class T> class Engine : public EngineBase {
             } else if (dm && ush == 6) {
                 if (gen) k_p2g_fix_b<4, true><<<brick_blocks(k_p2g_fix_b<4, true>), bt, 0, ctx_->stream>>>(a);
                 else k_p2g_fix_b<4, false><<<brick_blocks(k_p2g_fix_b<4, false>), bt, 0, ctx_->stream>>>(a);
-            } else if (dm && gen) k_p2g_w<true, ITEMS_PERSISTENT, true><<<ws, 256, 0, ctx_->stream>>>(a);
-            else if (dm) k_p2g_w<false, ITEMS_PERSISTENT, true><<<ws, 256, 0, ctx_->stream>>>(a);
-            else if (gen) k_p2g_w<true, ITEMS_PERSISTENT><<<ws, 256, 0, ctx_->stream>>>(a);
-            else k_p2g_w<false, ITEMS_PERSISTENT><<<ws, 256, 0, ctx_->stream>>>(a);
+            } else if (dm && gen) k_p2g_w<true, ITEMS_PERSISTENT, true><<<ws, DMPM_P2G_THREADS, 0, ctx_->stream>>>(a);
+            else if (dm) k_p2g_w<false, ITEMS_PERSISTENT, true><<<ws, DMPM_P2G_THREADS, 0, ctx_->stream>>>(a);
+            else if (gen) k_p2g_w<true, ITEMS_PERSISTENT><<<ws, DMPM_P2G_THREADS, 0, ctx_->stream>>>(a);
+            else k_p2g_w<false, ITEMS_PERSISTENT><<<ws, DMPM_P2G_THREADS, 0, ctx_->stream>>>(a);
             launched();
             if (dm) {
                 k_fix_to_node4<<<ggrid(), 256, 0, ctx_->stream>>>(fix_, fixb_, n_, G_, 0, (node4<float>*)g);
@@ -1353,7 +1355,8 @@ template <class T> class Engine : public EngineBase {
             } else {
                 DMPM_CK(cudaMemsetAsync(gadj_, 0, G_ * sizeof(node4<T>), ctx_->stream));
             }
-            const unsigned ws = warp_blocks(DMPM_ADJ_SCATTER_CTAS), wg = warp_blocks(DMPM_GATHER_CTAS);
+            const unsigned ws = warp_blocks(DMPM_ADJ_SCATTER_CTAS, DMPM_ADJ_SCATTER_THREADS),
+                           wg = warp_blocks(DMPM_GATHER_CTAS, DMPM_GATHER_THREADS);
             const int ush = set_units(a, ep);
             pbeg(K_ADJ_SCATTER);
             if (dm) {
@@ -1364,11 +1367,11 @@ template <class T> class Engine : public EngineBase {
                 launched();
                 k_fix_to_node4<<<ggrid(), 256, 0, ctx_->stream>>>(fix_, fixb_, n_, G_, 1, (node4<float>*)gadj_);
             } else if (P.warp_general) {
-                if (ex) k_adj_scatter_w<true, true, ITEMS_PERSISTENT><<<ws, 256, 0, ctx_->stream>>>(a);
-                else k_adj_scatter_w<false, true, ITEMS_PERSISTENT><<<ws, 256, 0, ctx_->stream>>>(a);
+                if (ex) k_adj_scatter_w<true, true, ITEMS_PERSISTENT><<<ws, DMPM_ADJ_SCATTER_THREADS, 0, ctx_->stream>>>(a);
+                else k_adj_scatter_w<false, true, ITEMS_PERSISTENT><<<ws, DMPM_ADJ_SCATTER_THREADS, 0, ctx_->stream>>>(a);
             } else {
-                if (ex) k_adj_scatter_w<true, false, ITEMS_PERSISTENT><<<ws, 256, 0, ctx_->stream>>>(a);
-                else k_adj_scatter_w<false, false, ITEMS_PERSISTENT><<<ws, 256, 0, ctx_->stream>>>(a);
+                if (ex) k_adj_scatter_w<true, false, ITEMS_PERSISTENT><<<ws, DMPM_ADJ_SCATTER_THREADS, 0, ctx_->stream>>>(a);
+                else k_adj_scatter_w<false, false, ITEMS_PERSISTENT><<<ws, DMPM_ADJ_SCATTER_THREADS, 0, ctx_->stream>>>(a);
             }
             launched();
             pend();
@@ -1384,9 +1387,9 @@ template <class T> class Engine : public EngineBase {
             }
             pbeg(K_ADJ_GATHER);
             if (ex) {
-                k_adj_gather_w<true, ITEMS_PERSISTENT><<<wg, 256, 0, ctx_->stream>>>(a);
+                k_adj_gather_w<true, ITEMS_PERSISTENT><<<wg, DMPM_GATHER_THREADS, 0, ctx_->stream>>>(a);
             } else {
-                k_adj_gather_w<false, ITEMS_PERSISTENT><<<wg, 256, 0, ctx_->stream>>>(a);
+                k_adj_gather_w<false, ITEMS_PERSISTENT><<<wg, DMPM_GATHER_THREADS, 0, ctx_->stream>>>(a);
             }
             launched();
             pend();

@@ -306,8 +306,14 @@ __device__ __forceinline__ float advance_x(const float* st, float* st_next, size
 #ifndef DMPM_GATHER_MIN_BLOCKS
 #define DMPM_GATHER_MIN_BLOCKS 3
 #endif
+#ifndef DMPM_GATHER_THREADS
+#define DMPM_GATHER_THREADS 256
+#endif
 #ifndef DMPM_SCATTER_MIN_BLOCKS
 #define DMPM_SCATTER_MIN_BLOCKS 3
+#endif
+#ifndef DMPM_P2G_THREADS
+#define DMPM_P2G_THREADS 256
 #endif
 // CTAs per SM of the persistent grids (no more than the register budget above lets reside)
 #ifndef DMPM_GATHER_CTAS
@@ -316,11 +322,16 @@ __device__ __forceinline__ float advance_x(const float* st, float* st_next, size
 #ifndef DMPM_SCATTER_CTAS
 #define DMPM_SCATTER_CTAS DMPM_SCATTER_MIN_BLOCKS
 #endif
-// the adjoint scatter on its own: 4 (64 registers, 84-byte spill) takes 57.3
-// against 59.4 us at 3 on the 64^3, 267k-particle workload, where P2G is
-// faster at 3 (the gather at 4: 87.0 against 78.9 us)
+// the adjoint scatter on its own, in blocks of 128 threads: 7 per SM (72
+// registers, 28-byte spill, 28 warps) take 53.3 us on the 64^3, 267k-particle
+// workload, against 55.4 us for 4 blocks of 256 (64 registers, 68-byte
+// spill), 59.4 us for 3 of 256 and 55.7 us for 5 of 128 (95 registers, no
+// spill); P2G is faster at 3 blocks of 256 (the gather at 4: 87.0 against 78.9 us)
 #ifndef DMPM_ADJ_SCATTER_MIN_BLOCKS
-#define DMPM_ADJ_SCATTER_MIN_BLOCKS 4
+#define DMPM_ADJ_SCATTER_MIN_BLOCKS 7
+#endif
+#ifndef DMPM_ADJ_SCATTER_THREADS
+#define DMPM_ADJ_SCATTER_THREADS 128
 #endif
 #ifndef DMPM_ADJ_SCATTER_CTAS
 #define DMPM_ADJ_SCATTER_CTAS DMPM_ADJ_SCATTER_MIN_BLOCKS
@@ -590,7 +601,7 @@ __device__ __forceinline__ void p2g_item(const WArgs& a, int item, const FixScal
 
 // P2G over warp items (one item per warp, persistent grid-stride)
 template <bool GENERAL, int MODE, bool DET = false>
-__global__ void __launch_bounds__(256, DMPM_SCATTER_MIN_BLOCKS) k_p2g_w(WArgs a) {
+__global__ void __launch_bounds__(DMPM_P2G_THREADS, DMPM_SCATTER_MIN_BLOCKS) k_p2g_w(WArgs a) {
     const int nit = item_count(a);
     FixScale sp{1.f, 1.f}, sm{1.f, 1.f};
     if (DET) {
@@ -895,7 +906,7 @@ __device__ __forceinline__ void adj_scatter_items(const WArgs& a, int first, int
 
 // adjoint scatter over warp items (one item per warp, persistent grid-stride)
 template <bool EXACT, bool GENERAL, int MODE, bool DET = false>
-__global__ void __launch_bounds__(256, DMPM_ADJ_SCATTER_MIN_BLOCKS) k_adj_scatter_w(WArgs a) {
+__global__ void __launch_bounds__(DMPM_ADJ_SCATTER_THREADS, DMPM_ADJ_SCATTER_MIN_BLOCKS) k_adj_scatter_w(WArgs a) {
     const int nit = item_count(a);
     FixScale sa{1.f, 1.f};
     if (DET) sa = fix_scale(a.fixb + FIXB_ADJ, a.n);
@@ -1043,7 +1054,8 @@ __device__ __forceinline__ void gather_item(const WArgs& a, const GridGeom& geo,
     }
 }
 
-template <bool EXACT, int MODE> __global__ void __launch_bounds__(256, DMPM_GATHER_MIN_BLOCKS) k_adj_gather_w(WArgs a) {
+template <bool EXACT, int MODE>
+__global__ void __launch_bounds__(DMPM_GATHER_THREADS, DMPM_GATHER_MIN_BLOCKS) k_adj_gather_w(WArgs a) {
     const int nit = item_count(a);
     const size_t npl = a.npl;
     __shared__ node4<float> s_rec[8][StageRecords<2>::value];
