@@ -301,8 +301,9 @@ __device__ __forceinline__ float advance_x(const float* st, float* st_next, size
 #ifndef DMPM_FINALIZE_STRESS_MIN_BLOCKS
 #define DMPM_FINALIZE_STRESS_MIN_BLOCKS 5
 #endif
-// and for the adjoint gather and the two scatters, P2G and the adjoint G2P
-// (256 threads per block)
+// and for the warp-item kernels: the adjoint gather and P2G in blocks of
+// DMPM_GATHER_THREADS / DMPM_P2G_THREADS (256), the adjoint scatter below in
+// blocks of DMPM_ADJ_SCATTER_THREADS (128)
 #ifndef DMPM_GATHER_MIN_BLOCKS
 #define DMPM_GATHER_MIN_BLOCKS 3
 #endif
